@@ -1,0 +1,284 @@
+#!/usr/bin/env python
+"""Benchmark of the Monte Carlo hot path on B200.
+
+Workload (one "step"): the Heston European strike strip - kappa=2, theta=0.04,
+xi=0.5, rho=-0.7, v0=0.04, S0=100, r=0.03, q=0, T=1; 41 call strikes 80..120
+priced from one shared set of 2^20 paths x 256 Euler steps (the reference's
+Heston Euler step, variance floored after each step), FP32 Philox4x32-10
+paths, compensated FP32 -> FP64 sums, seed 7 (+ rank for replicas).
+
+value  = path-steps/s of the device kernels (inputs resident, CUDA events on
+         the engine's stream, L2 flushed between timed iterations), summed over
+         ranks / max rank time.
+e2e    = the same metric through the public API (openferric_b200.price_strike_strip),
+         host wall clock, including the strike upload and the result readback.
+cpu_baseline / --impl reference = the CPU restatement of the reference's
+         Monte Carlo (xoshiro256++ + Acklam, FP64, OpenMP over all host
+         cores) on a bounded sample of the same workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "path-steps/s & priced+Greeks options/s at SE≤1e-4: FP32+adjoint vs FP64 plain"
+UNIT = "path-steps/s"
+HESTON = dict(mu=0.03, kappa=2.0, theta=0.04, xi=0.5, rho=-0.7, v0=0.04)
+S0, RATE, T = 100.0, 0.03, 1.0
+STRIKES = [80.0 + k for k in range(41)]
+PATHS, STEPS, SEED = 1 << 20, 256, 7
+PATH_STEPS = float(PATHS) * STEPS
+# Declared algorithmic work of one Heston Euler path-step in the FP32 kernel:
+# two inverse-normal draws (x, (1+x)(1-x), w - c, 8-term Horner, x*P: 24 flops
+# each) and the step (correlation 3, log-spot 6, variance 6, floors 2): 65 FP32
+# flops (FMA = 2) plus 3 SFU operations (2 lg2, 1 sqrt).
+FLOPS_PER_STEP = 65.0
+SFU_PER_STEP = 3.0
+CONFIG = {"workload": "heston_euler_strike_strip", "paths": PATHS, "steps": STEPS, "strikes": 41,
+          "strike_range": [80, 120], "kappa": 2.0, "theta": 0.04, "xi": 0.5, "rho": -0.7, "v0": 0.04, "s0": S0,
+          "r": RATE, "q": 0.0, "T": T, "seed": SEED, "rng": "philox4x32-10", "path_dtype": "fp32",
+          "sum_dtype": "kahan-fp32->fp64",
+          "l2": "flushed between timed iterations (256 MiB write); the kernel reads no HBM input"}
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + ",".join(self.FIELDS),
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1])]
+        mx = [num(r[2]) for r in rows if num(r[2])]
+        pw = [num(r[3]) for r in rows if num(r[3])]
+        load = [s for s, w in zip(sm, pw) if w and w > 250.0] or sm
+        reasons = set()
+        for r in rows:
+            for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows), "power_w_max": max(pw) if pw else None}
+
+
+def cpu_sample(threads, target_s, max_paths=PATHS):
+    """Times the oracle strip (CPU restatement of the reference MC) on a
+    sample sized to about target_s seconds; returns (path-steps/s, sample)."""
+    from oracle import oracle as orc
+    from openferric_b200 import _abi as A
+    from openferric_b200.engines import Heston, HestonPathGenerator
+    gen = HestonPathGenerator(Heston(**HESTON), S0, T, STEPS).to_abi()
+    df = math.exp(-RATE * T)
+
+    def run(paths):
+        cfg = A.OfMcConfig(num_paths=paths, seed=SEED, discount_factor=df)
+        t0 = time.perf_counter()
+        orc.mc_strip(gen, A.OF_CALL, STRIKES, cfg, threads=threads)
+        return time.perf_counter() - t0
+
+    probe = 1 << 12
+    dt = run(probe)
+    paths = int(min(max_paths, max(probe, probe * target_s / max(dt, 1e-6))))
+    dt = run(paths)
+    return paths * STEPS / dt, {"paths": paths, "steps": STEPS, "strikes": 41, "seconds": round(dt, 3)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    per_step = max(2.0, min(10.0, 150.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_sample(threads, per_step / 4)
+    vals, sample = [], None
+    for _ in range(args.steps):
+        v, sample = cpu_sample(threads, per_step)
+        vals.append(v)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * PATH_STEPS / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": CONFIG,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{sample['paths']} paths x {STEPS} steps x 41 strikes per step (bounded)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "oracle/of_oracle.c: C restatement of openferric's MonteCarloEngine::run with the Heston "
+                    "Euler generator (no Rust toolchain to build the reference); OpenMP over all host cores"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local_rank = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import openferric_b200 as of
+    from openferric_b200.engines import StripPlan
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    ctx = of.context(local_rank)
+    gen = of.HestonPathGenerator(of.Heston(**HESTON), S0, T, STEPS)
+    df = math.exp(-RATE * T)
+    seed = SEED + rank
+    plan = StripPlan(gen, of.OptionType.Call, STRIKES, PATHS, seed, df)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", local_rank))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
+
+    for _ in range(max(3, args.warmup)):
+        plan.launch()
+    prices = plan.results()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                flush.zero_()
+                starts[i].record(stream)
+                plan.launch()
+                ends[i].record(stream)
+        stream.synchronize()
+        torch.cuda.synchronize()
+    kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(kernel_ms)
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{local_rank}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    prices = plan.results()
+    clk = clocks.summary()
+
+    # End to end through the public API (host wall clock, sync inside each call).
+    for _ in range(2):
+        of.price_strike_strip(gen, of.OptionType.Call, STRIKES, PATHS, seed, df)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_prices = of.price_strike_strip(gen, of.OptionType.Call, STRIKES, PATHS, seed, df)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=f"cuda:{local_rank}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    ms_per_step = total_ms / args.steps
+    value = world * PATH_STEPS * args.steps / (total_ms / 1e3)
+    per_gpu = PATH_STEPS / (ms_per_step / 1e3)
+    sm_max = clk.get("sm_max_mhz") or 1965.0
+    peak_fp32 = 148 * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s, derived from the SM clock
+    achieved = per_gpu * FLOPS_PER_STEP / 1e12
+    sfu_peak = 148 * 16 * sm_max * 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": dict(CONFIG, parallelism=f"replicas{world}"),
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
+                     "frac": achieved / peak_fp32, "traffic": None,
+                     "peak_source": f"derived: 148 SM x 128 FP32 lanes x 2 x {sm_max:.0f} MHz (no FP32 figure in "
+                                    f"MEASURED_PEAKS.json)",
+                     "sfu_frac": per_gpu * SFU_PER_STEP / sfu_peak},
+        "e2e": {"value": world * PATH_STEPS * args.steps / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": 41 * 4, "d2h_bytes_per_step": 41 * 2 * 8},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk,
+        "kernel_ms": {"min": min(kernel_ms), "median": statistics.median(kernel_ms), "max": max(kernel_ms)},
+        "check": {"price_K100": prices[20][0], "stderr_K100": prices[20][1],
+                  "e2e_price_K100": e2e_prices[20][0]},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, sample = cpu_sample(os.cpu_count() or 1, 10.0)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": f"{sample['paths']} paths x {STEPS} Heston Euler steps x 41 strikes, "
+                                          f"FP64 xoshiro256++/Acklam oracle, {sample['seconds']} s"}
+    plan.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,216 @@
+/*
+ * of_gpu.h - C ABI of the B200 Monte Carlo pricing engine (libofgpu.so).
+ *
+ * Plain C, no CUDA or torch types: every argument is a POD struct, a plain
+ * pointer to caller-owned host memory, or a size.  Device memory is owned by
+ * the library inside an of_ctx (pooled, grown on demand, released by
+ * of_ctx_destroy).  All calls are synchronous to the caller unless stated.
+ *
+ * Each entry point names the openferric interface it replaces (path:line in
+ * the rosssaunders/openferric source tree).  The Rust-side extern block that a
+ * maintainer adds to bind these is shown in INTEGRATION.md.
+ *
+ * Error behaviour follows openferric's `PricingError` (src/core/engine.rs:293-302):
+ * OF_ERR_INVALID_INPUT  -> PricingError::InvalidInput
+ * OF_ERR_NUMERICAL      -> PricingError::NumericalError
+ * OF_ERR_CONVERGENCE    -> PricingError::ConvergenceFailure
+ * the remaining codes are device-side failures with no reference counterpart.
+ * The message of the last failure on a context is returned by of_ctx_last_error.
+ */
+#ifndef OF_GPU_H
+#define OF_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OF_GPU_ABI_VERSION 1
+
+typedef enum of_status {
+  OF_OK = 0,
+  OF_ERR_INVALID_INPUT = 1,
+  OF_ERR_NUMERICAL = 2,
+  OF_ERR_CUDA = 3,
+  OF_ERR_TIMEOUT = 4,
+  OF_ERR_UNSUPPORTED = 5,
+  OF_ERR_ALLOC = 6,
+  OF_ERR_CONVERGENCE = 7
+} of_status;
+
+/* openferric core::OptionType (src/core/types.rs:13-19) */
+enum { OF_CALL = 0, OF_PUT = 1 };
+
+/* Path dynamics.  GBM = mc::GbmPathGenerator (src/mc/simulation.rs:40-77);
+ * HESTON_EULER = mc::HestonPathGenerator full-truncation Euler
+ * (src/mc/simulation.rs:80-117, src/models/stochastic.rs:56-71);
+ * HESTON_QE = Andersen (2008) quadratic-exponential scheme (no reference
+ * counterpart; FP32 Philox mode only). */
+enum { OF_MODEL_GBM = 0, OF_MODEL_HESTON_EULER = 1, OF_MODEL_HESTON_QE = 2 };
+
+/* MonteCarloInstrument payoffs (src/engines/monte_carlo/mc_engine.rs:441-584). */
+enum { OF_PAYOFF_VANILLA = 0, OF_PAYOFF_BARRIER = 1, OF_PAYOFF_ASIAN = 2 };
+enum { OF_BARRIER_UP = 0, OF_BARRIER_DOWN = 1 };
+enum { OF_BARRIER_IN = 0, OF_BARRIER_OUT = 1 };
+enum { OF_AVG_ARITHMETIC = 0, OF_AVG_GEOMETRIC = 1 };
+enum { OF_STRIKE_FIXED = 0, OF_STRIKE_FLOATING = 1 };
+
+/* Control-variate evaluators (ControlVariate, src/mc/simulation.rs:120-124):
+ * VANILLA_TERMINAL = vanilla payoff of the terminal spot (mc_engine.rs:458-485),
+ * GEOMETRIC_ASIAN  = geometric-average fixed-strike payoff (mc_engine.rs:546-583),
+ * TERMINAL_SPOT    = the terminal spot itself (simulation.rs:441-444). */
+enum {
+  OF_CV_NONE = 0,
+  OF_CV_VANILLA_TERMINAL = 1,
+  OF_CV_GEOMETRIC_ASIAN = 2,
+  OF_CV_TERMINAL_SPOT = 3
+};
+
+/* Arithmetic mode of a Monte Carlo run.
+ * FP64_REFERENCE: openferric's own draws - one xoshiro256++ stream per sample
+ *   seeded with seed + i*7919 (src/math/fast_rng.rs:30-81,181-214), Acklam
+ *   inverse CDF (src/math/fast_norm.rs:54-139), FP64 path arithmetic.
+ * FP32_PHILOX: counter-based Philox4x32-10 normals, FP32 path state,
+ *   compensated FP32 per-thread sums, FP64 cross-thread reduction. */
+enum { OF_PREC_FP64_REFERENCE = 0, OF_PREC_FP32_PHILOX = 1 };
+
+typedef struct of_model {
+  int32_t kind; /* OF_MODEL_* */
+  int32_t reserved0;
+  double s0;
+  double mu; /* risk-neutral drift r - q */
+  double sigma; /* GBM volatility */
+  double maturity; /* simulation horizon in years */
+  int64_t steps;
+  double kappa, theta, xi, rho, v0; /* Heston parameters */
+} of_model;
+
+typedef struct of_payoff {
+  int32_t kind; /* OF_PAYOFF_* */
+  int32_t option_type; /* OF_CALL / OF_PUT */
+  double strike;
+  int32_t barrier_direction; /* OF_BARRIER_UP / DOWN */
+  int32_t barrier_style; /* OF_BARRIER_IN / OUT */
+  double barrier_level;
+  double rebate;
+  int32_t averaging; /* OF_AVG_* */
+  int32_t strike_type; /* OF_STRIKE_* */
+  const double* observation_times; /* host array, n_observations entries */
+  int64_t n_observations;
+  double expiry; /* instrument expiry used to map observation times to steps */
+} of_payoff;
+
+typedef struct of_mc_config {
+  int64_t num_paths;
+  uint64_t seed;
+  int32_t antithetic; /* 0/1 */
+  int32_t precision; /* OF_PREC_* */
+  int32_t control_variate; /* OF_CV_* */
+  int32_t reserved0;
+  double cv_expected; /* E[Y] of the control variate, undiscounted */
+  double discount_factor;
+  /* Test hook (the injection point PathGenerator::generate_from_normals,
+   * src/mc/simulation.rs:22): host array of normals laid out
+   * [sample][step][stream], streams = 1 for GBM and 2 for Heston.  NULL draws
+   * the normals on the device.  FP64_REFERENCE mode only. */
+  const double* injected_normals;
+  int64_t n_injected;
+} of_mc_config;
+
+typedef struct of_mc_result {
+  double price;
+  double stderr_;
+  int64_t samples; /* antithetic pairs count as one sample, as in the reference */
+  double sum_x, sum_x2, sum_y, sum_xy, sum_y2; /* the five running sums */
+  double kernel_ms; /* device time of the simulation kernels (CUDA events) */
+} of_mc_result;
+
+typedef struct of_ctx of_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+of_status of_ctx_create(int device, of_ctx** out);
+void of_ctx_destroy(of_ctx* ctx);
+const char* of_status_str(of_status status);
+const char* of_ctx_last_error(const of_ctx* ctx);
+/* Runs subsequent work on a caller-owned cudaStream_t (NULL restores the
+ * context's own stream).  Lets torch or another runtime order its work with
+ * the engine's. */
+of_status of_ctx_set_stream(of_ctx* ctx, void* cuda_stream);
+of_status of_ctx_get_stream(of_ctx* ctx, void** cuda_stream);
+int of_abi_version(void);
+int of_device_sm_count(of_ctx* ctx);
+
+/* ---- generic Monte Carlo run -------------------------------------------- */
+/* Replaces mc::MonteCarloEngine::run (src/mc/simulation.rs:182-348) with a
+ * built-in payoff in place of the Rust closure; the caller (the Rust
+ * PricingEngine impl) has already validated the instrument, resolved the vol
+ * and computed cv_expected, as MonteCarloPricingEngine::price does
+ * (src/engines/monte_carlo/mc_engine.rs:875-975). */
+of_status of_mc_run(of_ctx* ctx, const of_model* model, const of_payoff* payoff,
+                    const of_mc_config* cfg, of_mc_result* out);
+
+/* European payoffs on many strikes from ONE shared path set: result[k] is the
+ * (price, stderr) of strike k.  The multi-strike form of MonteCarloEngine::run
+ * (src/mc/simulation.rs:182-348) for the Heston strike strip; FP32_PHILOX mode
+ * (precision field ignored), antithetic supported, no control variate. */
+of_status of_mc_strip(of_ctx* ctx, const of_model* model, int32_t option_type,
+                      const double* strikes, int64_t n_strikes, const of_mc_config* cfg,
+                      of_mc_result* results);
+
+/* Plan form of of_mc_strip: device buffers and a captured CUDA graph are
+ * built once; launch enqueues one replay on the context stream without a host
+ * sync; results waits for the last replay and reads it back. */
+typedef struct of_strip_plan of_strip_plan;
+of_status of_strip_plan_create(of_ctx* ctx, const of_model* model, int32_t option_type,
+                               const double* strikes, int64_t n_strikes, const of_mc_config* cfg,
+                               of_strip_plan** out);
+of_status of_strip_plan_launch(of_strip_plan* plan);
+of_status of_strip_plan_results(of_strip_plan* plan, of_mc_result* results);
+void of_strip_plan_destroy(of_strip_plan* plan);
+
+/* ---- batched book (one persistent launch) ------------------------------- */
+/* One option of a book: the model, payoff and variance-reduction settings
+ * MonteCarloPricingEngine::price derives per instrument
+ * (src/engines/monte_carlo/mc_engine.rs:875-975).  FP32_PHILOX mode. */
+typedef struct of_book_entry {
+  of_model model;
+  of_payoff payoff;
+  int64_t num_paths;
+  int32_t antithetic;
+  int32_t control_variate; /* OF_CV_* */
+  double cv_expected;
+  double discount_factor;
+} of_book_entry;
+
+typedef struct of_book_config {
+  uint64_t seed;
+  int32_t block;            /* threads per block, 0 = autotuned */
+  int32_t paths_per_thread; /* samples per thread per tile, 0 = autotuned */
+  int32_t use_graph;        /* capture the launch in a CUDA graph */
+  int32_t reserved0;
+} of_book_config;
+
+/* Prices every entry of a book in one persistent kernel launch: the work is
+ * cut into (option, path-block) tiles, longest first, and CTAs pull tiles
+ * from a device counter.  Replaces a loop of MonteCarloPricingEngine::price
+ * calls (src/engines/monte_carlo/mc_engine.rs:875-975), one per instrument. */
+of_status of_mc_price_book(of_ctx* ctx, const of_book_entry* entries, int64_t n,
+                           const of_book_config* cfg, of_mc_result* results);
+
+typedef struct of_book_plan of_book_plan;
+of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* entries, int64_t n,
+                              const of_book_config* cfg, of_book_plan** out);
+of_status of_book_plan_launch(of_book_plan* plan);
+of_status of_book_plan_results(of_book_plan* plan, of_mc_result* results);
+/* Tile shape the plan uses (after autotuning) and its total path-steps. */
+of_status of_book_plan_info(of_book_plan* plan, int32_t* block, int32_t* paths_per_thread,
+                            int64_t* n_tiles, double* path_steps);
+void of_book_plan_destroy(of_book_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OF_GPU_H */

@@ -1,0 +1,110 @@
+"""ctypes mirror of include/of_gpu.h (declarations only; nothing is loaded here).
+
+Field order and widths must match the header exactly; tests/test_abi.py checks
+the sizes against the compiled library's own view of them.
+"""
+import ctypes as C
+
+OF_OK = 0
+OF_ERR_INVALID_INPUT = 1
+OF_ERR_NUMERICAL = 2
+OF_ERR_CUDA = 3
+OF_ERR_TIMEOUT = 4
+OF_ERR_UNSUPPORTED = 5
+OF_ERR_ALLOC = 6
+OF_ERR_CONVERGENCE = 7
+
+OF_CALL, OF_PUT = 0, 1
+OF_MODEL_GBM, OF_MODEL_HESTON_EULER, OF_MODEL_HESTON_QE = 0, 1, 2
+OF_PAYOFF_VANILLA, OF_PAYOFF_BARRIER, OF_PAYOFF_ASIAN = 0, 1, 2
+OF_BARRIER_UP, OF_BARRIER_DOWN = 0, 1
+OF_BARRIER_IN, OF_BARRIER_OUT = 0, 1
+OF_AVG_ARITHMETIC, OF_AVG_GEOMETRIC = 0, 1
+OF_STRIKE_FIXED, OF_STRIKE_FLOATING = 0, 1
+OF_CV_NONE, OF_CV_VANILLA_TERMINAL, OF_CV_GEOMETRIC_ASIAN, OF_CV_TERMINAL_SPOT = 0, 1, 2, 3
+OF_PREC_FP64_REFERENCE, OF_PREC_FP32_PHILOX = 0, 1
+
+
+class OfModel(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("s0", C.c_double),
+        ("mu", C.c_double),
+        ("sigma", C.c_double),
+        ("maturity", C.c_double),
+        ("steps", C.c_int64),
+        ("kappa", C.c_double),
+        ("theta", C.c_double),
+        ("xi", C.c_double),
+        ("rho", C.c_double),
+        ("v0", C.c_double),
+    ]
+
+
+class OfPayoff(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("option_type", C.c_int32),
+        ("strike", C.c_double),
+        ("barrier_direction", C.c_int32),
+        ("barrier_style", C.c_int32),
+        ("barrier_level", C.c_double),
+        ("rebate", C.c_double),
+        ("averaging", C.c_int32),
+        ("strike_type", C.c_int32),
+        ("observation_times", C.POINTER(C.c_double)),
+        ("n_observations", C.c_int64),
+        ("expiry", C.c_double),
+    ]
+
+
+class OfMcConfig(C.Structure):
+    _fields_ = [
+        ("num_paths", C.c_int64),
+        ("seed", C.c_uint64),
+        ("antithetic", C.c_int32),
+        ("precision", C.c_int32),
+        ("control_variate", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("cv_expected", C.c_double),
+        ("discount_factor", C.c_double),
+        ("injected_normals", C.POINTER(C.c_double)),
+        ("n_injected", C.c_int64),
+    ]
+
+
+class OfBookEntry(C.Structure):
+    _fields_ = [
+        ("model", OfModel),
+        ("payoff", OfPayoff),
+        ("num_paths", C.c_int64),
+        ("antithetic", C.c_int32),
+        ("control_variate", C.c_int32),
+        ("cv_expected", C.c_double),
+        ("discount_factor", C.c_double),
+    ]
+
+
+class OfBookConfig(C.Structure):
+    _fields_ = [
+        ("seed", C.c_uint64),
+        ("block", C.c_int32),
+        ("paths_per_thread", C.c_int32),
+        ("use_graph", C.c_int32),
+        ("reserved0", C.c_int32),
+    ]
+
+
+class OfMcResult(C.Structure):
+    _fields_ = [
+        ("price", C.c_double),
+        ("stderr_", C.c_double),
+        ("samples", C.c_int64),
+        ("sum_x", C.c_double),
+        ("sum_x2", C.c_double),
+        ("sum_y", C.c_double),
+        ("sum_xy", C.c_double),
+        ("sum_y2", C.c_double),
+        ("kernel_ms", C.c_double),
+    ]

@@ -1,0 +1,165 @@
+"""Loader of libofgpu.so and the per-device engine context.
+
+The product path has no CPU fallback: if the library or a GPU is missing,
+every pricing call raises `GpuUnavailable`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+from . import _abi as A
+from .core import PricingError
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libofgpu.so")
+
+# Every symbol include/of_gpu.h declares.
+EXPORTED = [
+    "of_abi_version", "of_ctx_create", "of_ctx_destroy", "of_status_str", "of_ctx_last_error", "of_ctx_set_stream",
+    "of_ctx_get_stream", "of_device_sm_count", "of_mc_run", "of_mc_strip", "of_strip_plan_create",
+    "of_strip_plan_launch", "of_strip_plan_results", "of_strip_plan_destroy", "of_mc_price_book",
+    "of_book_plan_create", "of_book_plan_launch", "of_book_plan_results", "of_book_plan_info",
+    "of_book_plan_destroy",
+]
+
+
+class GpuUnavailable(RuntimeError):
+    """The CUDA library or a GPU is missing; the engine has no CPU path."""
+
+
+class OfGpuError(RuntimeError):
+    """A device-side failure (CUDA error, allocation failure, timeout)."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(message)
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def _declare(L):
+    P = C.POINTER
+    vp = C.c_void_p
+    L.of_abi_version.restype = C.c_int
+    L.of_ctx_create.argtypes = [C.c_int, P(vp)]
+    L.of_ctx_destroy.argtypes = [vp]
+    L.of_ctx_destroy.restype = None
+    L.of_status_str.restype = C.c_char_p
+    L.of_status_str.argtypes = [C.c_int]
+    L.of_ctx_last_error.restype = C.c_char_p
+    L.of_ctx_last_error.argtypes = [vp]
+    L.of_ctx_set_stream.argtypes = [vp, vp]
+    L.of_ctx_get_stream.argtypes = [vp, P(vp)]
+    L.of_device_sm_count.argtypes = [vp]
+    L.of_mc_run.argtypes = [vp, P(A.OfModel), P(A.OfPayoff), P(A.OfMcConfig), P(A.OfMcResult)]
+    L.of_mc_strip.argtypes = [vp, P(A.OfModel), C.c_int32, P(C.c_double), C.c_int64, P(A.OfMcConfig),
+                              P(A.OfMcResult)]
+    L.of_strip_plan_create.argtypes = [vp, P(A.OfModel), C.c_int32, P(C.c_double), C.c_int64, P(A.OfMcConfig),
+                                       P(vp)]
+    L.of_strip_plan_launch.argtypes = [vp]
+    L.of_strip_plan_results.argtypes = [vp, P(A.OfMcResult)]
+    L.of_strip_plan_destroy.argtypes = [vp]
+    L.of_strip_plan_destroy.restype = None
+    L.of_mc_price_book.argtypes = [vp, P(A.OfBookEntry), C.c_int64, P(A.OfBookConfig), P(A.OfMcResult)]
+    L.of_book_plan_create.argtypes = [vp, P(A.OfBookEntry), C.c_int64, P(A.OfBookConfig), P(vp)]
+    L.of_book_plan_launch.argtypes = [vp]
+    L.of_book_plan_results.argtypes = [vp, P(A.OfMcResult)]
+    L.of_book_plan_info.argtypes = [vp, P(C.c_int32), P(C.c_int32), P(C.c_int64), P(C.c_double)]
+    L.of_book_plan_destroy.argtypes = [vp]
+    L.of_book_plan_destroy.restype = None
+    for name in ["of_ctx_create", "of_ctx_set_stream", "of_ctx_get_stream", "of_mc_run", "of_mc_strip",
+                 "of_strip_plan_create", "of_strip_plan_launch", "of_strip_plan_results", "of_mc_price_book",
+                 "of_book_plan_create", "of_book_plan_launch", "of_book_plan_results", "of_book_plan_info"]:
+        getattr(L, name).restype = C.c_int
+
+
+def load():
+    """Loads libofgpu.so (building it first when nvcc is available)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                try:
+                    from .build import build
+                    build()
+                except Exception as e:  # pragma: no cover - depends on toolchain
+                    raise GpuUnavailable(f"libofgpu.so is missing and could not be built: {e}") from e
+            L = C.CDLL(LIB_PATH)
+            _declare(L)
+            if L.of_abi_version() != 1:
+                raise GpuUnavailable("libofgpu.so ABI version mismatch")
+            _lib = L
+    return _lib
+
+
+def raise_for(status: int, ctx_handle=None):
+    if status == A.OF_OK:
+        return
+    L = load()
+    msg = L.of_ctx_last_error(ctx_handle).decode() if ctx_handle else L.of_status_str(status).decode()
+    if status in (A.OF_ERR_INVALID_INPUT, A.OF_ERR_UNSUPPORTED):
+        raise PricingError.InvalidInput(msg)
+    if status == A.OF_ERR_NUMERICAL:
+        raise PricingError.NumericalError(msg)
+    if status == A.OF_ERR_CONVERGENCE:
+        raise PricingError.ConvergenceFailure(msg)
+    raise OfGpuError(status, f"{L.of_status_str(status).decode()}: {msg}")
+
+
+class Context:
+    """One of_ctx (stream + pooled device buffers) on one device."""
+
+    def __init__(self, device: int = 0):
+        L = load()
+        h = C.c_void_p()
+        st = L.of_ctx_create(device, C.byref(h))
+        if st != A.OF_OK:
+            raise GpuUnavailable(f"of_ctx_create(device={device}) failed: {L.of_status_str(st).decode()}")
+        self._L = L
+        self.handle = h
+        self.device = device
+        self.lock = threading.Lock()
+
+    def check(self, status: int):
+        raise_for(status, self.handle)
+
+    @property
+    def sm_count(self) -> int:
+        return self._L.of_device_sm_count(self.handle)
+
+    def stream_ptr(self) -> int:
+        s = C.c_void_p()
+        self.check(self._L.of_ctx_get_stream(self.handle, C.byref(s)))
+        return s.value or 0
+
+    def set_stream(self, ptr: int):
+        self.check(self._L.of_ctx_set_stream(self.handle, C.c_void_p(ptr or None)))
+
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            self._L.of_ctx_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_contexts = {}
+
+
+def context(device: int = 0) -> Context:
+    with _lock:
+        ctx = _contexts.get(device)
+    if ctx is None:
+        ctx = Context(device)
+        with _lock:
+            _contexts.setdefault(device, ctx)
+            ctx = _contexts[device]
+    return ctx

@@ -1,0 +1,852 @@
+// mc_philox.cu - FP32 Philox Monte Carlo: the strike strip and the batched book.
+//
+// Generator: Philox4x32-10, counter {draw block, sample lo, sample hi, stream},
+// key = the 64-bit seed; one call yields 4 draws (4 GBM steps or 2 Heston
+// steps).  Paths live in registers (one path per thread at a time), payoff
+// sums are compensated FP32 per thread and FP64 from the warp level up.
+// Compiled with -use_fast_math: sqrt/exp/log/div map to single MUFU
+// operations; the few places that need more accuracy say so.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "of_internal.h"
+#include "path_fp32.cuh"
+
+using of::LegState;
+using of::StepConsts;
+
+namespace {
+
+constexpr uint32_t kStripStreamTag = 0x53545250u;  // "STRP"
+
+// FP32 constants of a model (computed in FP64, rounded once).
+StepConsts make_consts(const of_model* m) {
+  StepConsts c{};
+  const double dt = m->maturity / (double)m->steps;
+  const double sqdt = std::sqrt(dt);
+  c.drift = (float)((m->mu - 0.5 * m->sigma * m->sigma) * dt);
+  c.diff = (float)(m->sigma * sqdt);
+  c.mudt = (float)(m->mu * dt);
+  c.half_dt = (float)(0.5 * dt);
+  c.sqdt = (float)sqdt;
+  c.kdt = (float)(m->kappa * dt);
+  c.kdt_theta = (float)(m->kappa * m->theta * dt);
+  c.xi_sqdt = (float)(m->xi * sqdt);
+  c.rho = (float)m->rho;
+  c.rho_c = (float)std::sqrt(1.0 - m->rho * m->rho);
+  c.v0 = (float)m->v0;
+  c.y_floor = (float)std::log(1e-12 / m->s0);  // s.max(1e-12), simulation.rs:112
+  if (m->kind == OF_MODEL_HESTON_QE) {
+    const double e = std::exp(-m->kappa * dt);
+    c.qe_e = (float)e;
+    c.qe_c1 = (float)(m->xi * m->xi * e * (1.0 - e) / m->kappa);
+    c.qe_c2 = (float)(m->theta * m->xi * m->xi * (1.0 - e) * (1.0 - e) / (2.0 * m->kappa));
+    c.qe_theta = (float)m->theta;
+    const double g1 = 0.5, g2 = 0.5, kr = m->kappa * m->rho / m->xi - 0.5;
+    c.qe_k0 = (float)(-m->rho * m->kappa * m->theta * dt / m->xi);
+    c.qe_k1 = (float)(g1 * dt * kr - m->rho / m->xi);
+    c.qe_k2 = (float)(g2 * dt * kr + m->rho / m->xi);
+    c.qe_k3 = (float)(g1 * dt * (1.0 - m->rho * m->rho));
+    c.qe_k4 = (float)(g2 * dt * (1.0 - m->rho * m->rho));
+  }
+  return c;
+}
+
+// Simulates the terminal log-return of sample i (and of its antithetic twin).
+template <int MODEL, bool ANTI>
+__device__ __forceinline__ void simulate_terminal(const StepConsts& c, int32_t steps, uint64_t i, uint32_t stream,
+                                                  uint32_t k0, uint32_t k1, float& ya, float& yb) {
+  LegState a{0.0f, c.v0}, b{0.0f, c.v0};
+  const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
+  if (MODEL == OF_MODEL_GBM) {
+    float wa = 0.0f;  // sum of normals; y_T = steps*drift + diff*sum
+    for (int32_t j = 0; j < steps; j += 4) {
+      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo, hi, stream), k0, k1);
+      wa += of::normal_from_u32(r.x);
+      if (j + 1 < steps) wa += of::normal_from_u32(r.y);
+      if (j + 2 < steps) wa += of::normal_from_u32(r.z);
+      if (j + 3 < steps) wa += of::normal_from_u32(r.w);
+    }
+    const float base = (float)steps * c.drift;
+    ya = fmaf(c.diff, wa, base);
+    yb = fmaf(-c.diff, wa, base);
+  } else if (MODEL == OF_MODEL_HESTON_EULER) {
+    for (int32_t j = 0; j < steps; j += 2) {
+      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, stream), k0, k1);
+      float z1 = of::normal_from_u32(r.x), z2 = of::normal_from_u32(r.y);
+      of::heston_euler_step(a, c, z1, z2);
+      if (ANTI) of::heston_euler_step(b, c, -z1, -z2);
+      if (j + 1 < steps) {
+        z1 = of::normal_from_u32(r.z);
+        z2 = of::normal_from_u32(r.w);
+        of::heston_euler_step(a, c, z1, z2);
+        if (ANTI) of::heston_euler_step(b, c, -z1, -z2);
+      }
+    }
+    ya = a.y;
+    yb = b.y;
+  } else {
+    for (int32_t j = 0; j < steps; j += 2) {
+      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, stream), k0, k1);
+      float u = of::uniform_from_u32(r.x), zx = of::normal_from_u32(r.y);
+      of::heston_qe_step(a, c, u, 1.0f, zx, r.x);
+      if (ANTI) of::heston_qe_step(b, c, 1.0f - u, -1.0f, -zx, r.x);
+      if (j + 1 < steps) {
+        u = of::uniform_from_u32(r.z);
+        zx = of::normal_from_u32(r.w);
+        of::heston_qe_step(a, c, u, 1.0f, zx, r.z);
+        if (ANTI) of::heston_qe_step(b, c, 1.0f - u, -1.0f, -zx, r.z);
+      }
+    }
+    ya = a.y;
+    yb = b.y;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Strike strip: one shared path set, KPL strikes per lane.
+// ---------------------------------------------------------------------------
+struct StripParams {
+  StepConsts c;
+  int64_t samples;
+  int32_t steps, n_strikes, option_type, antithetic;
+  float s0;
+  uint32_t k0, k1;
+  const float* strikes;
+};
+
+template <int KPL, int MODEL, bool ANTI>
+__global__ void __launch_bounds__(256) strip_kernel(StripParams P, double* __restrict__ partials) {
+  extern __shared__ double sh_strip[];  // [warps][n_strikes][2]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  float K[KPL];
+  of::Kahan32 s1[KPL], s2[KPL];
+#pragma unroll
+  for (int q = 0; q < KPL; ++q) {
+    const int k = lane + 32 * q;
+    K[q] = k < P.n_strikes ? P.strikes[k] : 0.0f;
+  }
+  const bool call = P.option_type == OF_CALL;
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + warp * 32; base < P.samples; base += nthreads) {
+    const int64_t i = base + lane;
+    float sa = 0.0f, sb = 0.0f;
+    if (i < P.samples) {
+      float ya, yb;
+      simulate_terminal<MODEL, ANTI>(P.c, P.steps, (uint64_t)i, kStripStreamTag, P.k0, P.k1, ya, yb);
+      sa = P.s0 * __expf(ya);
+      sb = P.s0 * __expf(yb);
+    }
+    const int64_t rem = P.samples - base;
+    const int nvalid = rem < 32 ? (int)rem : 32;
+    for (int j = 0; j < nvalid; ++j) {
+      const float st = __shfl_sync(of::kFullMask, sa, j);
+      const float sta = ANTI ? __shfl_sync(of::kFullMask, sb, j) : 0.0f;
+#pragma unroll
+      for (int q = 0; q < KPL; ++q) {
+        float x = fmaxf(call ? st - K[q] : K[q] - st, 0.0f);
+        if (ANTI) x = 0.5f * (x + fmaxf(call ? sta - K[q] : K[q] - sta, 0.0f));
+        s1[q].add(x);
+        s2[q].add(x * x);
+      }
+    }
+  }
+  const int n = P.n_strikes;
+#pragma unroll
+  for (int q = 0; q < KPL; ++q) {
+    const int k = lane + 32 * q;
+    if (k < n) {
+      sh_strip[(warp * n + k) * 2] = s1[q].value();
+      sh_strip[(warp * n + k) * 2 + 1] = s2[q].value();
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 2 * n; t += blockDim.x) {
+    double acc = 0.0;
+    for (int w = 0; w < nw; ++w) acc += sh_strip[w * 2 * n + t];
+    partials[(int64_t)blockIdx.x * 2 * n + t] = acc;
+  }
+}
+
+typedef void (*StripKernelFn)(StripParams, double*);
+
+template <int KPL>
+StripKernelFn pick_strip(int model, bool anti) {
+  if (model == OF_MODEL_GBM) return anti ? strip_kernel<KPL, OF_MODEL_GBM, true> : strip_kernel<KPL, OF_MODEL_GBM, false>;
+  if (model == OF_MODEL_HESTON_EULER)
+    return anti ? strip_kernel<KPL, OF_MODEL_HESTON_EULER, true> : strip_kernel<KPL, OF_MODEL_HESTON_EULER, false>;
+  return anti ? strip_kernel<KPL, OF_MODEL_HESTON_QE, true> : strip_kernel<KPL, OF_MODEL_HESTON_QE, false>;
+}
+
+}  // namespace
+
+of_status of_validate_mc(of_ctx* ctx, const of_model* m, const of_payoff* p, const of_mc_config* c);
+void of_observation_weights(const of_payoff* p, int64_t steps, std::vector<double>& w, bool& terminal_only);
+
+static of_status validate_fp32_model(of_ctx* ctx, const of_model* m) {
+  if (m->steps > 2147483647LL) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_steps too large for FP32 mode");
+  if (m->kind == OF_MODEL_HESTON_QE && !(m->xi > 0.0 && m->theta > 0.0))
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "the QE scheme needs xi > 0 and theta > 0");
+  return OF_OK;
+}
+
+struct of_strip_plan {
+  of_ctx* ctx = nullptr;
+  StripParams P{};
+  int n_strikes = 0, grid = 0, block = 256;
+  size_t smem = 0;
+  StripKernelFn fn = nullptr;
+  double discount = 1.0;
+  int64_t samples = 0;
+  float* d_strikes = nullptr;
+  double* d_partials = nullptr;
+  double* d_sums = nullptr;
+  double* h_sums = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+static of_status strip_enqueue(of_strip_plan* pl, cudaStream_t s) {
+  pl->fn<<<pl->grid, pl->block, pl->smem, s>>>(pl->P, pl->d_partials);
+  const int64_t cols = 2 * (int64_t)pl->n_strikes;
+  of_launch_reduce_rows(pl->d_partials, pl->grid, cols, pl->d_sums, s);
+  cudaMemcpyAsync(pl->h_sums, pl->d_sums, cols * sizeof(double), cudaMemcpyDeviceToHost, s);
+  return OF_OK;
+}
+
+extern "C" void of_strip_plan_destroy(of_strip_plan* pl) {
+  if (!pl) return;
+  if (pl->ctx) cudaStreamSynchronize(pl->ctx->stream);
+  if (pl->exec) cudaGraphExecDestroy(pl->exec);
+  if (pl->graph) cudaGraphDestroy(pl->graph);
+  cudaFree(pl->d_strikes);
+  cudaFree(pl->d_partials);
+  cudaFree(pl->d_sums);
+  if (pl->h_sums) cudaFreeHost(pl->h_sums);
+  delete pl;
+}
+
+// Validates a strip request and fills the plan's parameters, kernel and
+// launch shape (no allocation).
+static of_status strip_setup(of_ctx* ctx, const of_model* m, int32_t option_type, const double* strikes,
+                             int64_t n_strikes, const of_mc_config* cfg, of_strip_plan* pl) {
+  of_payoff dummy{};
+  dummy.kind = OF_PAYOFF_VANILLA;
+  dummy.option_type = option_type;
+  dummy.strike = 1.0;
+  OF_TRY(of_validate_mc(ctx, m, &dummy, cfg));
+  OF_TRY(validate_fp32_model(ctx, m));
+  if (n_strikes <= 0 || !strikes) return of_fail(ctx, OF_ERR_INVALID_INPUT, "strip needs at least one strike");
+  if (n_strikes > 128) return of_fail(ctx, OF_ERR_UNSUPPORTED, "strip supports at most 128 strikes per call");
+  for (int64_t k = 0; k < n_strikes; ++k)
+    if (!(strikes[k] > 0.0) || !std::isfinite(strikes[k]))
+      return of_fail(ctx, OF_ERR_INVALID_INPUT, "strike %lld must be finite and > 0", (long long)k);
+  if (cfg->control_variate != OF_CV_NONE)
+    return of_fail(ctx, OF_ERR_UNSUPPORTED, "the strike strip has no control variate");
+  OF_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  pl->ctx = ctx;
+  pl->n_strikes = (int)n_strikes;
+  pl->discount = cfg->discount_factor;
+  pl->samples = cfg->antithetic ? (cfg->num_paths + 1) / 2 : cfg->num_paths;
+  StripParams& P = pl->P;
+  P.c = make_consts(m);
+  P.samples = pl->samples;
+  P.steps = (int32_t)m->steps;
+  P.n_strikes = (int32_t)n_strikes;
+  P.option_type = option_type;
+  P.antithetic = cfg->antithetic ? 1 : 0;
+  P.s0 = (float)m->s0;
+  P.k0 = (uint32_t)cfg->seed;
+  P.k1 = (uint32_t)(cfg->seed >> 32);
+  const int kpl = (int)((n_strikes + 31) / 32);
+  const int kpl_t = kpl <= 1 ? 1 : (kpl <= 2 ? 2 : 4);
+  pl->fn = kpl_t == 1 ? pick_strip<1>(m->kind, P.antithetic) : kpl_t == 2 ? pick_strip<2>(m->kind, P.antithetic)
+                                                                           : pick_strip<4>(m->kind, P.antithetic);
+  pl->smem = (size_t)(pl->block / 32) * n_strikes * 2 * sizeof(double);
+  const int per_sm = of_blocks_per_sm((const void*)pl->fn, pl->block, pl->smem);
+  const int64_t want = (pl->samples + pl->block - 1) / pl->block;
+  const int64_t cap = (int64_t)ctx->sm_count * per_sm;
+  pl->grid = (int)std::max<int64_t>(1, std::min(want, cap));
+  return OF_OK;
+}
+
+extern "C" of_status of_strip_plan_create(of_ctx* ctx, const of_model* m, int32_t option_type, const double* strikes,
+                                          int64_t n_strikes, const of_mc_config* cfg, of_strip_plan** out) {
+  if (!ctx || !out) return OF_ERR_INVALID_INPUT;
+  *out = nullptr;
+  of_strip_plan* pl = new of_strip_plan();
+  {
+    const of_status st = strip_setup(ctx, m, option_type, strikes, n_strikes, cfg, pl);
+    if (st != OF_OK) {
+      delete pl;
+      return st;
+    }
+  }
+  auto fail = [&](of_status st) {
+    of_strip_plan_destroy(pl);
+    return st;
+  };
+  std::vector<float> ks((size_t)n_strikes);
+  for (int64_t k = 0; k < n_strikes; ++k) ks[(size_t)k] = (float)strikes[k];
+  if (cudaMalloc(&pl->d_strikes, ks.size() * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&pl->d_partials, (size_t)pl->grid * 2 * n_strikes * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&pl->d_sums, 2 * n_strikes * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&pl->h_sums, 2 * n_strikes * sizeof(double)) != cudaSuccess)
+    return fail(of_fail(ctx, OF_ERR_ALLOC, "strip plan allocation failed"));
+  if (cudaMemcpy(pl->d_strikes, ks.data(), ks.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(of_fail(ctx, OF_ERR_CUDA, "strike upload failed"));
+  pl->P.strikes = pl->d_strikes;
+  // Capture kernel + reduction + readback once; launches replay the graph.
+  cudaStream_t cap_stream = nullptr;
+  if (cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(of_fail(ctx, OF_ERR_CUDA, "capture stream creation failed"));
+  cudaError_t e = cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    strip_enqueue(pl, cap_stream);
+    e = cudaStreamEndCapture(cap_stream, &pl->graph);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&pl->exec, pl->graph, 0);
+  cudaStreamDestroy(cap_stream);
+  if (e != cudaSuccess) return fail(of_fail(ctx, OF_ERR_CUDA, "strip graph capture failed: %s", cudaGetErrorString(e)));
+  *out = pl;
+  return OF_OK;
+}
+
+extern "C" of_status of_strip_plan_launch(of_strip_plan* pl) {
+  if (!pl) return OF_ERR_INVALID_INPUT;
+  OF_CUDA_TRY(pl->ctx, cudaGraphLaunch(pl->exec, pl->ctx->stream));
+  return OF_OK;
+}
+
+extern "C" of_status of_strip_plan_results(of_strip_plan* pl, of_mc_result* res) {
+  if (!pl || !res) return OF_ERR_INVALID_INPUT;
+  OF_CUDA_TRY(pl->ctx, cudaStreamSynchronize(pl->ctx->stream));
+  for (int k = 0; k < pl->n_strikes; ++k) {
+    const double s[5] = {pl->h_sums[2 * k], pl->h_sums[2 * k + 1], 0.0, 0.0, 0.0};
+    of_mc_finish(s, pl->samples, OF_CV_NONE, 0.0, pl->discount, &res[k]);
+    res[k].kernel_ms = 0.0;
+  }
+  return OF_OK;
+}
+
+// One-shot strip: the context's pooled buffers instead of a plan's own, no
+// graph (a single replay would not amortise the capture).
+extern "C" of_status of_mc_strip(of_ctx* ctx, const of_model* m, int32_t option_type, const double* strikes,
+                                 int64_t n_strikes, const of_mc_config* cfg, of_mc_result* results) {
+  if (!ctx || !results) return OF_ERR_INVALID_INPUT;
+  of_strip_plan pl;  // setup only; buffers come from the context
+  OF_TRY(strip_setup(ctx, m, option_type, strikes, n_strikes, cfg, &pl));
+  const int64_t cols = 2 * n_strikes;
+  void *d_k = nullptr, *d_part = nullptr, *d_sums = nullptr, *h = nullptr;
+  OF_TRY(of_scratch(ctx, SLOT_STRIKES, (size_t)n_strikes * sizeof(float), &d_k));
+  OF_TRY(of_scratch(ctx, SLOT_PARTIALS, (size_t)pl.grid * cols * sizeof(double), &d_part));
+  OF_TRY(of_scratch(ctx, SLOT_SUMS, (size_t)cols * sizeof(double), &d_sums));
+  OF_TRY(of_pinned(ctx, (size_t)cols * sizeof(double) + (size_t)n_strikes * sizeof(float), &h));
+  float* hk = (float*)((double*)h + cols);
+  for (int64_t k = 0; k < n_strikes; ++k) hk[k] = (float)strikes[k];
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(d_k, hk, (size_t)n_strikes * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  pl.P.strikes = (const float*)d_k;
+  pl.d_partials = (double*)d_part;
+  pl.d_sums = (double*)d_sums;
+  pl.h_sums = (double*)h;
+  OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+  strip_enqueue(&pl, ctx->stream);
+  OF_CUDA_TRY(ctx, cudaGetLastError());
+  OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+  OF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  float ms = 0.0f;
+  OF_CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+  for (int64_t k = 0; k < n_strikes; ++k) {
+    const double s[5] = {pl.h_sums[2 * k], pl.h_sums[2 * k + 1], 0.0, 0.0, 0.0};
+    of_mc_finish(s, pl.samples, OF_CV_NONE, 0.0, pl.discount, &results[k]);
+    results[k].kernel_ms = ms;
+  }
+  // The buffers belong to the context: detach them before `pl` goes out of scope.
+  pl.d_partials = nullptr;
+  pl.d_sums = nullptr;
+  pl.h_sums = nullptr;
+  return OF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched book: persistent kernel over (option, path-block) tiles.
+// ---------------------------------------------------------------------------
+namespace {
+
+enum : int32_t {
+  BF_ANTI = 1,
+  BF_UP = 2,
+  BF_IN = 4,
+  BF_GEOMETRIC = 8,
+  BF_FLOATING = 16,
+  BF_TERMINAL_ONLY = 32,
+  BF_DAILY = 64,        // every step 1..M observed once (daily fixings)
+  BF_NEED_ARITH = 128,
+  BF_NEED_GEO = 256,
+  BF_CALL = 512
+};
+
+struct BookOpt {
+  StepConsts c;
+  int32_t model, payoff, flags, cv_kind;
+  int32_t steps;
+  int32_t obs_offset;  // into the shared weight array, -1 when unused
+  float s0, strike, barrier_y, rebate, inv_nobs;
+  uint32_t stream;
+};
+
+struct BookTile {
+  int32_t opt;
+  int32_t count;
+  int64_t first;
+  int32_t slot;  // position of the tile's partials (option-major order)
+  int32_t reserved;
+};
+
+struct BookParams {
+  const BookOpt* opts;
+  const BookTile* tiles;
+  const float* obs_w;
+  int32_t n_tiles;
+  int32_t ppt;  // samples per thread per tile (tile = block * ppt samples)
+  uint32_t k0, k1;
+  int* counter;
+  double* partials;  // [slot][5]
+};
+
+struct PathObs {
+  float arith_sum, arith_comp, geo_sum;
+  bool hit;
+};
+
+__device__ __forceinline__ void book_observe(const BookOpt& o, PathObs& ob, float y, int32_t idx, const float* obs_w) {
+  const int f = o.flags;
+  if (o.payoff == OF_PAYOFF_BARRIER) ob.hit |= (f & BF_UP) ? (y >= o.barrier_y) : (y <= o.barrier_y);
+  if (f & (BF_NEED_ARITH | BF_NEED_GEO)) {
+    const float w = (f & BF_DAILY) ? (idx > 0 ? 1.0f : 0.0f) : __ldg(obs_w + o.obs_offset + idx);
+    if (w != 0.0f) {
+      if (f & BF_NEED_ARITH) {
+        const float add = w * __expf(y);
+        const float yk = add - ob.arith_comp;
+        const float t = ob.arith_sum + yk;
+        ob.arith_comp = (t - ob.arith_sum) - yk;
+        ob.arith_sum = t;
+      }
+      if (f & BF_NEED_GEO) ob.geo_sum = fmaf(w, y, ob.geo_sum);
+    }
+  }
+}
+
+__device__ __forceinline__ float vanilla32(bool call, float s, float k) { return fmaxf(call ? s - k : k - s, 0.0f); }
+
+__device__ __forceinline__ void book_payoff(const BookOpt& o, const PathObs& ob, float y, float& x, float& cv) {
+  const int f = o.flags;
+  const bool call = f & BF_CALL;
+  const float st = o.s0 * __expf(y);
+  switch (o.payoff) {
+    case OF_PAYOFF_VANILLA:
+      x = vanilla32(call, st, o.strike);
+      break;
+    case OF_PAYOFF_BARRIER: {
+      const bool active = (f & BF_IN) ? ob.hit : !ob.hit;
+      x = active ? vanilla32(call, st, o.strike) : o.rebate;
+      break;
+    }
+    default: {
+      float avg;
+      if (f & BF_TERMINAL_ONLY) avg = st;
+      else if (f & BF_GEOMETRIC) avg = o.s0 * __expf(ob.geo_sum * o.inv_nobs);
+      else avg = o.s0 * ((ob.arith_sum - ob.arith_comp) * o.inv_nobs);
+      x = (f & BF_FLOATING) ? vanilla32(call, st, avg) : vanilla32(call, avg, o.strike);
+    }
+  }
+  switch (o.cv_kind) {
+    case OF_CV_VANILLA_TERMINAL: cv = vanilla32(call, st, o.strike); break;
+    case OF_CV_GEOMETRIC_ASIAN:
+      cv = vanilla32(call, (f & BF_TERMINAL_ONLY) ? st : o.s0 * __expf(ob.geo_sum * o.inv_nobs), o.strike);
+      break;
+    case OF_CV_TERMINAL_SPOT: cv = st; break;
+    default: cv = 0.0f;
+  }
+}
+
+// One sample (and its antithetic twin) of option o; returns (x, y).
+template <int MODEL>
+__device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, uint32_t k0, uint32_t k1, const float* obs_w,
+                                            float& x, float& cvy) {
+  const bool anti = o.flags & BF_ANTI;
+  const StepConsts& c = o.c;
+  LegState a{0.0f, c.v0}, b{0.0f, c.v0};
+  PathObs oa{0.0f, 0.0f, 0.0f, false}, obb{0.0f, 0.0f, 0.0f, false};
+  book_observe(o, oa, 0.0f, 0, obs_w);
+  if (anti) book_observe(o, obb, 0.0f, 0, obs_w);
+  const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
+  const bool observe_each = (o.payoff != OF_PAYOFF_VANILLA) || (o.flags & (BF_NEED_ARITH | BF_NEED_GEO));
+  constexpr int SPC = MODEL == OF_MODEL_GBM ? 4 : 2;  // steps per Philox call
+  for (int32_t j = 0; j < o.steps; j += SPC) {
+    const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j / SPC), lo, hi, o.stream), k0, k1);
+    const uint32_t rr[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+    for (int q = 0; q < SPC; ++q) {
+      if (j + q >= o.steps) break;
+      if (MODEL == OF_MODEL_GBM) {
+        const float z = of::normal_from_u32(rr[q]);
+        a.y = fmaf(c.diff, z, a.y + c.drift);
+        if (anti) b.y = fmaf(-c.diff, z, b.y + c.drift);
+      } else if (MODEL == OF_MODEL_HESTON_EULER) {
+        const float z1 = of::normal_from_u32(rr[2 * q]), z2 = of::normal_from_u32(rr[2 * q + 1]);
+        of::heston_euler_step(a, c, z1, z2);
+        if (anti) of::heston_euler_step(b, c, -z1, -z2);
+      } else {
+        const float u = of::uniform_from_u32(rr[2 * q]), zx = of::normal_from_u32(rr[2 * q + 1]);
+        of::heston_qe_step(a, c, u, 1.0f, zx, rr[2 * q]);
+        if (anti) of::heston_qe_step(b, c, 1.0f - u, -1.0f, -zx, rr[2 * q]);
+      }
+      if (observe_each) {
+        book_observe(o, oa, a.y, j + q + 1, obs_w);
+        if (anti) book_observe(o, obb, b.y, j + q + 1, obs_w);
+      }
+    }
+  }
+  book_payoff(o, oa, a.y, x, cvy);
+  if (anti) {
+    float xb, yb;
+    book_payoff(o, obb, b.y, xb, yb);
+    x = 0.5f * (x + xb);
+    cvy = 0.5f * (cvy + yb);
+  }
+}
+
+__global__ void __launch_bounds__(256) book_kernel(BookParams P) {
+  __shared__ int tile_sh;
+  __shared__ double red_sh[5 * 8];
+  for (;;) {
+    if (threadIdx.x == 0) tile_sh = atomicAdd(P.counter, 1);
+    __syncthreads();
+    const int t = tile_sh;
+    if (t >= P.n_tiles) break;
+    const BookTile tile = P.tiles[t];
+    const BookOpt o = P.opts[tile.opt];
+    of::Kahan32 acc[5];
+    for (int k = 0; k < P.ppt; ++k) {
+      const int local = k * blockDim.x + threadIdx.x;
+      if (local >= tile.count) break;
+      const uint64_t i = (uint64_t)(tile.first + local);
+      float x, y;
+      if (o.model == OF_MODEL_GBM) book_sample<OF_MODEL_GBM>(o, i, P.k0, P.k1, P.obs_w, x, y);
+      else if (o.model == OF_MODEL_HESTON_EULER) book_sample<OF_MODEL_HESTON_EULER>(o, i, P.k0, P.k1, P.obs_w, x, y);
+      else book_sample<OF_MODEL_HESTON_QE>(o, i, P.k0, P.k1, P.obs_w, x, y);
+      acc[0].add(x);
+      acc[1].add(x * x);
+      acc[2].add(y);
+      acc[3].add(x * y);
+      acc[4].add(y * y);
+    }
+    double v[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) v[k] = acc[k].value();
+    of::block_sum<5>(v, red_sh);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < 5; ++k) P.partials[(int64_t)tile.slot * 5 + k] = v[k];
+    __syncthreads();
+  }
+}
+
+// Per-option sums over its tile slots [begin[o], begin[o+1]) in fixed order.
+__global__ void book_reduce_kernel(const double* __restrict__ partials, const int32_t* __restrict__ begin, int n_opts,
+                                   double* __restrict__ sums) {
+  const int o = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (o >= n_opts) return;
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int s = begin[o] + lane; s < begin[o + 1]; s += 32)
+    for (int k = 0; k < 5; ++k) acc[k] += partials[(int64_t)s * 5 + k];
+  for (int k = 0; k < 5; ++k) {
+    const double v = of::warp_sum(acc[k]);
+    if (lane == 0) sums[(int64_t)o * 5 + k] = v;
+  }
+}
+
+}  // namespace
+
+struct of_book_plan {
+  of_ctx* ctx = nullptr;
+  int64_t n = 0;
+  int block = 256, ppt = 4, grid = 0;
+  int64_t n_tiles = 0;
+  double path_steps = 0.0;
+  std::vector<int64_t> samples;
+  std::vector<int32_t> cv_kind;
+  std::vector<double> cv_expected, discount;
+  BookParams P{};
+  BookOpt* d_opts = nullptr;
+  BookTile* d_tiles = nullptr;
+  float* d_obs = nullptr;
+  int* d_counter = nullptr;
+  double* d_partials = nullptr;
+  int32_t* d_begin = nullptr;
+  double* d_sums = nullptr;
+  double* h_sums = nullptr;
+  bool use_graph = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+static void book_enqueue(of_book_plan* pl, cudaStream_t s) {
+  cudaMemsetAsync(pl->d_counter, 0, sizeof(int), s);
+  book_kernel<<<pl->grid, pl->block, 0, s>>>(pl->P);
+  book_reduce_kernel<<<(unsigned)((pl->n + 7) / 8), 256, 0, s>>>(pl->d_partials, pl->d_begin, (int)pl->n, pl->d_sums);
+  cudaMemcpyAsync(pl->h_sums, pl->d_sums, (size_t)pl->n * 5 * sizeof(double), cudaMemcpyDeviceToHost, s);
+}
+
+extern "C" void of_book_plan_destroy(of_book_plan* pl) {
+  if (!pl) return;
+  if (pl->ctx) cudaStreamSynchronize(pl->ctx->stream);
+  if (pl->exec) cudaGraphExecDestroy(pl->exec);
+  if (pl->graph) cudaGraphDestroy(pl->graph);
+  cudaFree(pl->d_opts);
+  cudaFree(pl->d_tiles);
+  cudaFree(pl->d_obs);
+  cudaFree(pl->d_counter);
+  cudaFree(pl->d_partials);
+  cudaFree(pl->d_begin);
+  cudaFree(pl->d_sums);
+  if (pl->h_sums) cudaFreeHost(pl->h_sums);
+  delete pl;
+}
+
+extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, int64_t n, const of_book_config* cfg,
+                                         of_book_plan** out) {
+  if (!ctx || !out || !cfg) return OF_ERR_INVALID_INPUT;
+  *out = nullptr;
+  if (n <= 0 || !e) return of_fail(ctx, OF_ERR_INVALID_INPUT, "book must hold at least one option");
+  if (n > (1 << 24)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "book too large");
+  OF_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  of_book_plan* pl = new of_book_plan();
+  pl->ctx = ctx;
+  pl->n = n;
+  pl->block = cfg->block > 0 ? cfg->block : 256;
+  pl->ppt = cfg->paths_per_thread > 0 ? cfg->paths_per_thread : 4;
+  pl->use_graph = cfg->use_graph != 0;
+  if (pl->block % 32 != 0 || pl->block > 256) {
+    of_book_plan_destroy(pl);
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "block must be a multiple of 32 and <= 256");
+  }
+  auto fail = [&](of_status st) {
+    of_book_plan_destroy(pl);
+    return st;
+  };
+  std::vector<BookOpt> opts((size_t)n);
+  std::vector<float> obs;
+  pl->samples.resize((size_t)n);
+  pl->cv_kind.resize((size_t)n);
+  pl->cv_expected.resize((size_t)n);
+  pl->discount.resize((size_t)n);
+  struct Pending {
+    int32_t opt;
+    int64_t first;
+    int32_t count;
+    double cost;
+  };
+  std::vector<Pending> pend;
+  const int64_t tile_samples = (int64_t)pl->block * pl->ppt;
+  for (int64_t o = 0; o < n; ++o) {
+    const of_book_entry& b = e[o];
+    of_mc_config c{};
+    c.num_paths = b.num_paths;
+    c.antithetic = b.antithetic;
+    c.control_variate = b.control_variate;
+    c.discount_factor = b.discount_factor;
+    c.precision = OF_PREC_FP32_PHILOX;
+    of_status st = of_validate_mc(ctx, &b.model, &b.payoff, &c);
+    if (st == OF_OK) st = validate_fp32_model(ctx, &b.model);
+    if (st != OF_OK) {
+      ctx->last_error = "book entry " + std::to_string(o) + ": " + ctx->last_error;
+      return fail(st);
+    }
+    BookOpt& d = opts[(size_t)o];
+    d.c = make_consts(&b.model);
+    d.model = b.model.kind;
+    d.payoff = b.payoff.kind;
+    d.cv_kind = b.control_variate;
+    d.steps = (int32_t)b.model.steps;
+    d.s0 = (float)b.model.s0;
+    d.strike = (float)b.payoff.strike;
+    d.rebate = (float)b.payoff.rebate;
+    d.barrier_y = (float)std::log(b.payoff.barrier_level / b.model.s0);
+    if (!(b.payoff.barrier_level > 0.0)) d.barrier_y = b.payoff.barrier_direction == OF_BARRIER_UP ? INFINITY : -INFINITY;
+    d.stream = (uint32_t)o;
+    d.obs_offset = -1;
+    int32_t f = 0;
+    if (b.antithetic) f |= BF_ANTI;
+    if (b.payoff.barrier_direction == OF_BARRIER_UP) f |= BF_UP;
+    if (b.payoff.barrier_style == OF_BARRIER_IN) f |= BF_IN;
+    if (b.payoff.averaging == OF_AVG_GEOMETRIC) f |= BF_GEOMETRIC;
+    if (b.payoff.strike_type == OF_STRIKE_FLOATING) f |= BF_FLOATING;
+    if (b.payoff.option_type == OF_CALL) f |= BF_CALL;
+    const bool asian = b.payoff.kind == OF_PAYOFF_ASIAN;
+    bool need_arith = asian && b.payoff.averaging == OF_AVG_ARITHMETIC;
+    bool need_geo = (asian && b.payoff.averaging == OF_AVG_GEOMETRIC) || b.control_variate == OF_CV_GEOMETRIC_ASIAN;
+    if (need_arith || need_geo) {
+      std::vector<double> w;
+      bool terminal_only = true;
+      of_observation_weights(&b.payoff, b.model.steps, w, terminal_only);
+      if (terminal_only) {
+        f |= BF_TERMINAL_ONLY;
+        need_arith = need_geo = false;
+      } else {
+        bool daily = w[0] == 0.0;
+        for (size_t k = 1; k < w.size() && daily; ++k) daily = w[k] == 1.0;
+        if (daily) {
+          f |= BF_DAILY;
+        } else {
+          d.obs_offset = (int32_t)obs.size();
+          for (double x : w) obs.push_back((float)x);
+        }
+        d.inv_nobs = (float)(1.0 / (double)b.payoff.n_observations);
+      }
+    }
+    if (need_arith) f |= BF_NEED_ARITH;
+    if (need_geo) f |= BF_NEED_GEO;
+    if (asian && !need_arith && !need_geo) f |= BF_TERMINAL_ONLY;
+    d.flags = f;
+    const int64_t samples = b.antithetic ? (b.num_paths + 1) / 2 : b.num_paths;
+    pl->samples[(size_t)o] = samples;
+    pl->cv_kind[(size_t)o] = b.control_variate;
+    pl->cv_expected[(size_t)o] = b.cv_expected;
+    pl->discount[(size_t)o] = b.discount_factor;
+    pl->path_steps += (double)b.num_paths * (double)b.model.steps;
+    for (int64_t first = 0; first < samples; first += tile_samples) {
+      const int32_t cnt = (int32_t)std::min<int64_t>(tile_samples, samples - first);
+      const double legs = b.antithetic ? 2.0 : 1.0;
+      pend.push_back({(int32_t)o, first, cnt, (double)cnt * legs * (double)b.model.steps});
+    }
+  }
+  if (pend.size() > (size_t)2147483647) return fail(of_fail(ctx, OF_ERR_INVALID_INPUT, "too many tiles"));
+  // Slots in option-major order, schedule longest tile first.
+  std::vector<int32_t> begin((size_t)n + 1, 0);
+  for (size_t k = 0; k < pend.size(); ++k) begin[(size_t)pend[k].opt + 1]++;
+  for (int64_t o = 0; o < n; ++o) begin[(size_t)o + 1] += begin[(size_t)o];
+  std::vector<BookTile> tiles(pend.size());
+  for (size_t k = 0; k < pend.size(); ++k) tiles[k] = {pend[k].opt, pend[k].count, pend[k].first, (int32_t)k, 0};
+  std::vector<size_t> order(pend.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return pend[a].cost > pend[b].cost; });
+  std::vector<BookTile> sorted(pend.size());
+  for (size_t k = 0; k < order.size(); ++k) sorted[k] = tiles[order[k]];
+  pl->n_tiles = (int64_t)sorted.size();
+
+  const size_t nt = sorted.size();
+  if (cudaMalloc(&pl->d_opts, opts.size() * sizeof(BookOpt)) != cudaSuccess ||
+      cudaMalloc(&pl->d_tiles, nt * sizeof(BookTile)) != cudaSuccess ||
+      cudaMalloc(&pl->d_obs, std::max<size_t>(1, obs.size()) * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&pl->d_counter, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&pl->d_partials, nt * 5 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&pl->d_begin, begin.size() * sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(&pl->d_sums, (size_t)n * 5 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&pl->h_sums, (size_t)n * 5 * sizeof(double)) != cudaSuccess)
+    return fail(of_fail(ctx, OF_ERR_ALLOC, "book plan allocation failed"));
+  if (cudaMemcpy(pl->d_opts, opts.data(), opts.size() * sizeof(BookOpt), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(pl->d_tiles, sorted.data(), nt * sizeof(BookTile), cudaMemcpyHostToDevice) != cudaSuccess ||
+      (!obs.empty() && cudaMemcpy(pl->d_obs, obs.data(), obs.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) ||
+      cudaMemcpy(pl->d_begin, begin.data(), begin.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(of_fail(ctx, OF_ERR_CUDA, "book upload failed"));
+  BookParams& P = pl->P;
+  P.opts = pl->d_opts;
+  P.tiles = pl->d_tiles;
+  P.obs_w = pl->d_obs;
+  P.n_tiles = (int32_t)nt;
+  P.ppt = pl->ppt;
+  P.k0 = (uint32_t)cfg->seed;
+  P.k1 = (uint32_t)(cfg->seed >> 32);
+  P.counter = pl->d_counter;
+  P.partials = pl->d_partials;
+  const int per_sm = of_blocks_per_sm((const void*)book_kernel, pl->block, 0);
+  const int64_t cap = (int64_t)ctx->sm_count * per_sm;
+  pl->grid = (int)std::max<int64_t>(1, std::min<int64_t>(cap, (int64_t)nt));
+  if (pl->use_graph) {
+    cudaStream_t cs = nullptr;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(of_fail(ctx, OF_ERR_CUDA, "capture stream creation failed"));
+    cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (err == cudaSuccess) {
+      book_enqueue(pl, cs);
+      err = cudaStreamEndCapture(cs, &pl->graph);
+    }
+    if (err == cudaSuccess) err = cudaGraphInstantiate(&pl->exec, pl->graph, 0);
+    cudaStreamDestroy(cs);
+    if (err != cudaSuccess) return fail(of_fail(ctx, OF_ERR_CUDA, "book graph capture failed: %s", cudaGetErrorString(err)));
+  }
+  *out = pl;
+  return OF_OK;
+}
+
+extern "C" of_status of_book_plan_launch(of_book_plan* pl) {
+  if (!pl) return OF_ERR_INVALID_INPUT;
+  if (pl->use_graph) {
+    OF_CUDA_TRY(pl->ctx, cudaGraphLaunch(pl->exec, pl->ctx->stream));
+  } else {
+    book_enqueue(pl, pl->ctx->stream);
+    OF_CUDA_TRY(pl->ctx, cudaGetLastError());
+  }
+  return OF_OK;
+}
+
+extern "C" of_status of_book_plan_results(of_book_plan* pl, of_mc_result* res) {
+  if (!pl || !res) return OF_ERR_INVALID_INPUT;
+  OF_CUDA_TRY(pl->ctx, cudaStreamSynchronize(pl->ctx->stream));
+  for (int64_t o = 0; o < pl->n; ++o) {
+    of_mc_finish(pl->h_sums + o * 5, pl->samples[(size_t)o], pl->cv_kind[(size_t)o], pl->cv_expected[(size_t)o],
+                 pl->discount[(size_t)o], &res[o]);
+    res[o].kernel_ms = 0.0;
+  }
+  return OF_OK;
+}
+
+extern "C" of_status of_book_plan_info(of_book_plan* pl, int32_t* block, int32_t* ppt, int64_t* n_tiles,
+                                       double* path_steps) {
+  if (!pl) return OF_ERR_INVALID_INPUT;
+  if (block) *block = pl->block;
+  if (ppt) *ppt = pl->ppt;
+  if (n_tiles) *n_tiles = pl->n_tiles;
+  if (path_steps) *path_steps = pl->path_steps;
+  return OF_OK;
+}
+
+extern "C" of_status of_mc_price_book(of_ctx* ctx, const of_book_entry* e, int64_t n, const of_book_config* cfg,
+                                      of_mc_result* res) {
+  if (!ctx || !res) return OF_ERR_INVALID_INPUT;
+  of_book_plan* pl = nullptr;
+  OF_TRY(of_book_plan_create(ctx, e, n, cfg, &pl));
+  cudaEventRecord(ctx->ev_start, ctx->stream);
+  of_status st = of_book_plan_launch(pl);
+  cudaEventRecord(ctx->ev_stop, ctx->stream);
+  if (st == OF_OK) st = of_book_plan_results(pl, res);
+  float ms = 0.0f;
+  if (st == OF_OK && cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess)
+    for (int64_t o = 0; o < n; ++o) res[o].kernel_ms = ms;
+  of_book_plan_destroy(pl);
+  return st;
+}
+
+// FP32 branch of of_mc_run: a one-option book.
+of_status of_mc_run_fp32(of_ctx* ctx, const of_model* m, const of_payoff* p, const of_mc_config* c,
+                         of_mc_result* out) {
+  if (c->injected_normals)
+    return of_fail(ctx, OF_ERR_UNSUPPORTED, "injected normals are a FP64 reference-mode test hook");
+  of_book_entry b{};
+  b.model = *m;
+  b.payoff = *p;
+  b.num_paths = c->num_paths;
+  b.antithetic = c->antithetic;
+  b.control_variate = c->control_variate;
+  b.cv_expected = c->cv_expected;
+  b.discount_factor = c->discount_factor;
+  of_book_config bc{};
+  bc.seed = c->seed;
+  bc.use_graph = 0;
+  return of_mc_price_book(ctx, &b, 1, &bc, out);
+}

@@ -1,0 +1,179 @@
+// of_device.cuh - device-side generators and reductions shared by the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "invnorm_coeffs.h"
+
+namespace of {
+
+constexpr unsigned kFullMask = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// openferric's reference stream (FP64 reference mode).
+// xoshiro256++ seeded by SplitMix64: src/math/fast_rng.rs:30-81,181-200.
+// ---------------------------------------------------------------------------
+struct Xoshiro256pp {
+  uint64_t s0, s1, s2, s3;
+
+  __device__ __forceinline__ static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+
+  __device__ __forceinline__ void seed(uint64_t seed) {
+    uint64_t sm = seed;
+    uint64_t st[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      sm += 0x9E3779B97F4A7C15ULL;
+      uint64_t z = sm;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+      st[i] = z ^ (z >> 31);
+    }
+    if ((st[0] | st[1] | st[2] | st[3]) == 0) st[0] = 1;
+    s0 = st[0];
+    s1 = st[1];
+    s2 = st[2];
+    s3 = st[3];
+  }
+
+  __device__ __forceinline__ uint64_t next_u64() {
+    const uint64_t result = rotl(s0 + s3, 23) + s0;
+    const uint64_t t = s1 << 17;
+    s2 ^= s0;
+    s3 ^= s1;
+    s1 ^= s2;
+    s0 ^= s3;
+    s2 ^= t;
+    s3 = rotl(s3, 45);
+    return result;
+  }
+
+  // next_f64, fast_rng.rs:70-73
+  __device__ __forceinline__ double next_f64() { return (double)(next_u64() >> 11) * (1.0 / 9007199254740992.0); }
+};
+
+// uniform_open01 (fast_rng.rs:219-221) then the Acklam inverse
+// (beasley_springer_moro_inv_cdf, src/math/fast_norm.rs:54-139), FP64.
+// Translation units using this must be compiled with --fmad=false so that
+// only the explicit fma() calls (the reference's mul_add) contract.
+__device__ __forceinline__ double acklam_inv_cdf(double p) {
+  const double eps = 2.220446049250313080847263336181640625e-16;
+  p = p < eps ? eps : (p > 1.0 - eps ? 1.0 - eps : p);
+  const double a0 = -3.969683028665376e1, a1 = 2.209460984245205e2, a2 = -2.759285104469687e2,
+               a3 = 1.38357751867269e2, a4 = -3.066479806614716e1, a5 = 2.506628277459239;
+  const double b0 = -5.447609879822406e1, b1 = 1.615858368580409e2, b2 = -1.556989798598866e2,
+               b3 = 6.680131188771972e1, b4 = -1.328068155288572e1;
+  const double c0 = -7.784894002430293e-3, c1 = -3.223964580411365e-1, c2 = -2.400758277161838,
+               c3 = -2.549732539343734, c4 = 4.374664141464968, c5 = 2.938163982698783;
+  const double d0 = 7.784695709041462e-3, d1 = 3.224671290700398e-1, d2 = 2.445134137142996,
+               d3 = 3.754408661907416;
+  const double p_low = 0.02425, p_high = 1.0 - 0.02425;
+  if (p < p_low) {
+    const double q = sqrt(-2.0 * log(p));
+    return fma(fma(fma(fma(fma(c0, q, c1), q, c2), q, c3), q, c4), q, c5) /
+           fma(fma(fma(fma(d0, q, d1), q, d2), q, d3), q, 1.0);
+  } else if (p <= p_high) {
+    const double q = p - 0.5;
+    const double r = q * q;
+    return fma(fma(fma(fma(fma(a0, r, a1), r, a2), r, a3), r, a4), r, a5) * q /
+           fma(fma(fma(fma(fma(b0, r, b1), r, b2), r, b3), r, b4), r, 1.0);
+  } else {
+    const double q = sqrt(-2.0 * log(1.0 - p));
+    return -fma(fma(fma(fma(fma(c0, q, c1), q, c2), q, c3), q, c4), q, c5) /
+           fma(fma(fma(fma(d0, q, d1), q, d2), q, d3), q, 1.0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) - FP32 mode generator.
+// Counter layout used by every kernel: {draw block, path lo, path hi, stream tag}.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// u32 -> standard normal in FP32: u = (k + 0.5) 2^-23 with k the top 23 bits,
+// then Phi^-1(u) = x P(w), x = 2u-1, w = -log2((1+x)(1-x)) with the fitted
+// polynomials of invnorm_coeffs.h (one MUFU lg2 per draw; the tail branch,
+// w >= OF_INVN_W_SPLIT, is taken with probability 0.34 %).
+__device__ __forceinline__ float normal_from_u32(uint32_t r) {
+  const float f = __uint_as_float(0x3F800000u | (r >> 9));  // 1 + k 2^-23, exact
+  const float x = fmaf(2.0f, f, -3.0f) + 1.1920928955078125e-7f;  // (2k + 1 - 2^23) 2^-23, exact
+  const float t = (1.0f + x) * (1.0f - x);
+  const float w = -__log2f(t);
+  float p;
+  if (w < OF_INVN_W_SPLIT) {
+    const float s = w - OF_INVN_C_CENTER;
+    p = kInvnCentral[OF_INVN_DEG_C];
+#pragma unroll
+    for (int i = OF_INVN_DEG_C - 1; i >= 0; --i) p = fmaf(p, s, kInvnCentral[i]);
+  } else {
+    const float s = sqrtf(w) - OF_INVN_T_CENTER;
+    p = kInvnTail[OF_INVN_DEG_T];
+#pragma unroll
+    for (int i = OF_INVN_DEG_T - 1; i >= 0; --i) p = fmaf(p, s, kInvnTail[i]);
+  }
+  return x * p;
+}
+
+// u32 -> uniform in (0,1), the same grid as normal_from_u32: (k + 0.5) 2^-23.
+__device__ __forceinline__ float uniform_from_u32(uint32_t r) {
+  const float f = __uint_as_float(0x3F800000u | (r >> 9));
+  return (f - 1.0f) + 5.9604644775390625e-8f;
+}
+
+// ---------------------------------------------------------------------------
+// Reductions
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFullMask, v, o);
+  return v;
+}
+
+// Block-wide sum of N doubles per thread; result valid in thread 0 (out[]).
+// `sh` must hold N * (blockDim.x / 32) doubles.
+template <int N>
+__device__ __forceinline__ void block_sum(double (&v)[N], double* sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < N; ++k) v[k] = warp_sum(v[k]);
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) sh[warp * N + k] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      double acc = 0.0;
+      for (int w = 0; w < nw; ++w) acc += sh[w * N + k];
+      v[k] = acc;
+    }
+  }
+}
+
+// Compensated FP32 accumulator (Kahan); flushed to FP64 as sum - comp.
+struct Kahan32 {
+  float sum = 0.0f, comp = 0.0f;
+  __device__ __forceinline__ void add(float v) {
+    const float y = v - comp;
+    const float t = sum + y;
+    comp = (t - sum) - y;
+    sum = t;
+  }
+  __device__ __forceinline__ double value() const { return (double)sum - (double)comp; }
+};
+
+}  // namespace of

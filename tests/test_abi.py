@@ -1,0 +1,79 @@
+"""The C-ABI library: loads without a GPU, exports every declared symbol, and
+its structs have the layout the ctypes mirror assumes."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from conftest import ROOT
+from openferric_b200 import _abi as A
+from openferric_b200 import _lib
+
+HEADER = os.path.join(ROOT, "include", "of_gpu.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(of_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declarations_match_binding_list():
+    assert declared_functions() == sorted(_lib.EXPORTED)
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.load()
+    for name in declared_functions():
+        assert hasattr(L, name), name
+    assert L.of_abi_version() == 1
+    assert L.of_status_str(A.OF_ERR_INVALID_INPUT).decode() == "invalid input"
+
+
+STRUCTS = {
+    "of_model": A.OfModel,
+    "of_payoff": A.OfPayoff,
+    "of_mc_config": A.OfMcConfig,
+    "of_mc_result": A.OfMcResult,
+    "of_book_entry": A.OfBookEntry,
+    "of_book_config": A.OfBookConfig,
+}
+
+
+def test_struct_layout_matches_ctypes():
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
+    for cname, py in STRUCTS.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0;}")
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "probe.c")
+        exe = os.path.join(d, "probe")
+        open(src, "w").write("\n".join(lines))
+        subprocess.run(["/usr/bin/gcc", "-std=c11", "-o", exe, src], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    got = dict(line.rsplit(" ", 1) for line in out.strip().splitlines())
+    for cname, py in STRUCTS.items():
+        assert int(got[cname]) == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(py, fname).offset, f"{cname}.{fname}"
+
+
+def _gpu_present():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_gpu_present(), reason="checks the no-GPU failure path")
+def test_no_gpu_fails_loudly_without_cpu_fallback():
+    from openferric_b200 import MonteCarloPricingEngine, Market, VanillaOption
+    market = Market.builder().spot(100).rate(0.05).flat_vol(0.2).build()
+    with pytest.raises(_lib.GpuUnavailable):
+        MonteCarloPricingEngine(1000, 10, 1).price(VanillaOption.european_call(100, 1.0), market)
