@@ -209,6 +209,119 @@ of_status of_book_plan_info(of_book_plan* plan, int32_t* block, int32_t* paths_p
                             int64_t* n_tiles, double* path_steps);
 void of_book_plan_destroy(of_book_plan* plan);
 
+/* ---- Monte Carlo Greeks on the reference streams (FP64) ----------------- */
+typedef struct of_greeks_params {
+  int32_t option_type; /* OF_CALL / OF_PUT */
+  int32_t antithetic;
+  double spot, strike, rate, dividend_yield, vol, expiry;
+  int64_t num_paths, num_steps;
+  uint64_t seed;
+  double spot_bump_rel; /* MonteCarloGreeksEngine gamma bump (>= 1e-6) */
+  /* Heston dynamics for of_heston_price_delta_aad (mu = spot drift) */
+  double mu, kappa, theta, xi, rho, v0;
+} of_greeks_params;
+
+typedef struct of_greeks_result {
+  double price, stderr_;
+  double delta, gamma, vega, theta, rho;
+  double lr_delta, lr_gamma, lr_vega; /* likelihood-ratio estimators */
+  int64_t samples;
+  double kernel_ms;
+} of_greeks_result;
+
+/* Pathwise reverse-mode Greeks of a European vanilla under GBM:
+ * mc_european_pathwise_aad (src/engines/monte_carlo/mc_aad.rs:75-219).
+ * Fills price, stderr_, delta, vega, theta, rho (gamma = 0). */
+of_status of_mc_european_pathwise_aad(of_ctx* ctx, const of_greeks_params* p, of_greeks_result* out);
+/* Forward-mode Heston Euler delta: heston_price_delta_aad
+ * (src/engines/monte_carlo/mc_aad.rs:280-342).  Fills price (plain mean) and delta. */
+of_status of_heston_price_delta_aad(of_ctx* ctx, const of_greeks_params* p, of_greeks_result* out);
+/* Terminal-value estimators of MonteCarloGreeksEngine (src/engines/monte_carlo/mc_greeks.rs:95-342):
+ * delta/gamma = pathwise, lr_delta/lr_gamma/lr_vega = likelihood ratio. */
+of_status of_mc_greek_estimators(of_ctx* ctx, const of_greeks_params* p, of_greeks_result* out);
+
+/* ---- Longstaff-Schwartz (HBM-resident path store) ----------------------- */
+enum { OF_EXERCISE_EUROPEAN = 0, OF_EXERCISE_AMERICAN = 1, OF_EXERCISE_BERMUDAN = 2 };
+
+typedef struct of_lsm_contract {
+  int32_t option_type; /* OF_CALL / OF_PUT */
+  int32_t exercise;    /* OF_EXERCISE_* (ExerciseStyle, src/core/types.rs:41-49) */
+  double spot, strike, rate, dividend_yield, vol, expiry;
+  int64_t num_steps;
+  const double* exercise_dates; /* Bermudan dates in years (host), else NULL */
+  int64_t n_exercise_dates;
+} of_lsm_contract;
+
+typedef struct of_lsm_config {
+  int64_t num_paths;
+  uint64_t seed;
+  int32_t precision;    /* FP64_REFERENCE: the reference's single xoshiro256++ stream, FP64
+                           paths; FP32_PHILOX: Philox normals, FP32 path store */
+  int32_t basis_degree; /* 2: {1,S,S^2} + LU (the reference); 3: {1,x,x^2,x^3}, x=S/K, Cholesky */
+  int32_t want_delta;   /* also return the pathwise delta under the fitted exercise policy */
+  int32_t reserved0;
+  /* Test hook: [contract][path][step] normals replacing the device stream
+   * (FP64_REFERENCE only), NULL to draw on the device. */
+  const double* injected_normals;
+  int64_t n_injected;
+} of_lsm_config;
+
+typedef struct of_lsm_result {
+  double price, stderr_, delta;
+  int64_t regressions; /* exercise dates with >= 3 in-the-money paths */
+  double kernel_ms;
+} of_lsm_result;
+
+/* LongstaffSchwartzEngine::price(VanillaOption) for a batch of contracts
+ * (src/engines/lsm/longstaff_schwartz.rs:421-618): paths in HBM time-major
+ * [step][path], per exercise date one fused pass (apply the previous date's
+ * exercise, discount, in-the-money basis moments in FP64) whose last block
+ * solves the normal equations on the device. */
+of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* contracts, int64_t n,
+                       const of_lsm_config* cfg, of_lsm_result* results);
+
+/* xoshiro256++ jump-ahead: the state of the stream seeded with `seed`
+ * (Xoshiro256PlusPlus::seed_from_u64, src/math/fast_rng.rs:36-48) after
+ * `draws` calls of next_u64, computed on the device by GF(2) matrix powers.
+ * Exposed for tests of the LSM reference stream. */
+of_status of_xoshiro_jump(of_ctx* ctx, uint64_t seed, const uint64_t* draws, int64_t n, uint64_t* states_out);
+
+/* ---- Heston pathwise adjoint (FP32, checkpointed) ------------------------ */
+typedef struct of_heston_adjoint_params {
+  double spot, strike, rate, dividend_yield, expiry;
+  double kappa, theta, xi, rho, v0;
+  int64_t num_paths, num_steps;
+  uint64_t seed;
+  int32_t option_type;      /* OF_CALL / OF_PUT */
+  int32_t payoff;           /* OF_PAYOFF_VANILLA, or OF_PAYOFF_ASIAN: arithmetic average of
+                               the spot at every step 1..num_steps */
+  int32_t scheme;           /* OF_MODEL_HESTON_QE or OF_MODEL_HESTON_EULER */
+  int32_t checkpoint_every; /* path-state checkpoint interval (32) */
+  int32_t forward_only;     /* 1: price only, same random numbers (bump-and-revalue) */
+  int32_t reserved0;
+} of_heston_adjoint_params;
+
+enum {
+  OF_ADJ_SPOT = 0, OF_ADJ_RATE = 1, OF_ADJ_V0 = 2, OF_ADJ_KAPPA = 3,
+  OF_ADJ_THETA = 4, OF_ADJ_XI = 5, OF_ADJ_RHO = 6, OF_ADJ_COUNT = 7
+};
+
+typedef struct of_adjoint_result {
+  double price, stderr_;
+  double greeks[OF_ADJ_COUNT];        /* d price / d(S0, r, v0, kappa, theta, xi, rho) */
+  double greeks_stderr[OF_ADJ_COUNT]; /* Monte Carlo standard error of each */
+  int64_t samples;
+  double kernel_ms;
+} of_adjoint_result;
+
+/* Price and all seven Heston sensitivities from one forward pass (path state
+ * checkpointed every `checkpoint_every` steps) and one backward sweep that
+ * recomputes each segment and regenerates its counter-based draws.  The
+ * reference has forward-mode Heston delta only (heston_price_delta_aad,
+ * src/engines/monte_carlo/mc_aad.rs:280-342); the other six have no
+ * reference counterpart. */
+of_status of_heston_price_adjoint(of_ctx* ctx, const of_heston_adjoint_params* p, of_adjoint_result* out);
+
 #ifdef __cplusplus
 }
 #endif

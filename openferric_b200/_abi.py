@@ -96,6 +96,126 @@ class OfBookConfig(C.Structure):
     ]
 
 
+class OfGreeksParams(C.Structure):
+    _fields_ = [
+        ("option_type", C.c_int32),
+        ("antithetic", C.c_int32),
+        ("spot", C.c_double),
+        ("strike", C.c_double),
+        ("rate", C.c_double),
+        ("dividend_yield", C.c_double),
+        ("vol", C.c_double),
+        ("expiry", C.c_double),
+        ("num_paths", C.c_int64),
+        ("num_steps", C.c_int64),
+        ("seed", C.c_uint64),
+        ("spot_bump_rel", C.c_double),
+        ("mu", C.c_double),
+        ("kappa", C.c_double),
+        ("theta", C.c_double),
+        ("xi", C.c_double),
+        ("rho", C.c_double),
+        ("v0", C.c_double),
+    ]
+
+
+class OfGreeksResult(C.Structure):
+    _fields_ = [
+        ("price", C.c_double),
+        ("stderr_", C.c_double),
+        ("delta", C.c_double),
+        ("gamma", C.c_double),
+        ("vega", C.c_double),
+        ("theta", C.c_double),
+        ("rho", C.c_double),
+        ("lr_delta", C.c_double),
+        ("lr_gamma", C.c_double),
+        ("lr_vega", C.c_double),
+        ("samples", C.c_int64),
+        ("kernel_ms", C.c_double),
+    ]
+
+
+OF_EXERCISE_EUROPEAN, OF_EXERCISE_AMERICAN, OF_EXERCISE_BERMUDAN = 0, 1, 2
+
+
+class OfLsmContract(C.Structure):
+    _fields_ = [
+        ("option_type", C.c_int32),
+        ("exercise", C.c_int32),
+        ("spot", C.c_double),
+        ("strike", C.c_double),
+        ("rate", C.c_double),
+        ("dividend_yield", C.c_double),
+        ("vol", C.c_double),
+        ("expiry", C.c_double),
+        ("num_steps", C.c_int64),
+        ("exercise_dates", C.POINTER(C.c_double)),
+        ("n_exercise_dates", C.c_int64),
+    ]
+
+
+class OfLsmConfig(C.Structure):
+    _fields_ = [
+        ("num_paths", C.c_int64),
+        ("seed", C.c_uint64),
+        ("precision", C.c_int32),
+        ("basis_degree", C.c_int32),
+        ("want_delta", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("injected_normals", C.POINTER(C.c_double)),
+        ("n_injected", C.c_int64),
+    ]
+
+
+class OfLsmResult(C.Structure):
+    _fields_ = [
+        ("price", C.c_double),
+        ("stderr_", C.c_double),
+        ("delta", C.c_double),
+        ("regressions", C.c_int64),
+        ("kernel_ms", C.c_double),
+    ]
+
+
+OF_ADJ_NAMES = ("spot", "rate", "v0", "kappa", "theta", "xi", "rho")
+
+
+class OfHestonAdjointParams(C.Structure):
+    _fields_ = [
+        ("spot", C.c_double),
+        ("strike", C.c_double),
+        ("rate", C.c_double),
+        ("dividend_yield", C.c_double),
+        ("expiry", C.c_double),
+        ("kappa", C.c_double),
+        ("theta", C.c_double),
+        ("xi", C.c_double),
+        ("rho", C.c_double),
+        ("v0", C.c_double),
+        ("num_paths", C.c_int64),
+        ("num_steps", C.c_int64),
+        ("seed", C.c_uint64),
+        ("option_type", C.c_int32),
+        ("payoff", C.c_int32),
+        ("scheme", C.c_int32),
+        ("checkpoint_every", C.c_int32),
+        ("forward_only", C.c_int32),
+        ("reserved0", C.c_int32),
+    ]
+
+
+class OfAdjointResult(C.Structure):
+    _fields_ = [
+        ("price", C.c_double),
+        ("stderr_", C.c_double),
+        ("greeks", C.c_double * 7),
+        ("greeks_stderr", C.c_double * 7),
+        ("samples", C.c_int64),
+        ("kernel_ms", C.c_double),
+    ]
+
+
 class OfMcResult(C.Structure):
     _fields_ = [
         ("price", C.c_double),

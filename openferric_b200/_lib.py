@@ -21,7 +21,8 @@ EXPORTED = [
     "of_ctx_get_stream", "of_device_sm_count", "of_mc_run", "of_mc_strip", "of_strip_plan_create",
     "of_strip_plan_launch", "of_strip_plan_results", "of_strip_plan_destroy", "of_mc_price_book",
     "of_book_plan_create", "of_book_plan_launch", "of_book_plan_results", "of_book_plan_info",
-    "of_book_plan_destroy",
+    "of_book_plan_destroy", "of_mc_european_pathwise_aad", "of_heston_price_delta_aad", "of_mc_greek_estimators",
+    "of_lsm_price", "of_xoshiro_jump", "of_heston_price_adjoint",
 ]
 
 
@@ -71,6 +72,15 @@ def _declare(L):
     L.of_book_plan_info.argtypes = [vp, P(C.c_int32), P(C.c_int32), P(C.c_int64), P(C.c_double)]
     L.of_book_plan_destroy.argtypes = [vp]
     L.of_book_plan_destroy.restype = None
+    for name in ["of_mc_european_pathwise_aad", "of_heston_price_delta_aad", "of_mc_greek_estimators"]:
+        getattr(L, name).argtypes = [vp, P(A.OfGreeksParams), P(A.OfGreeksResult)]
+        getattr(L, name).restype = C.c_int
+    L.of_lsm_price.argtypes = [vp, P(A.OfLsmContract), C.c_int64, P(A.OfLsmConfig), P(A.OfLsmResult)]
+    L.of_lsm_price.restype = C.c_int
+    L.of_xoshiro_jump.argtypes = [vp, C.c_uint64, P(C.c_uint64), C.c_int64, P(C.c_uint64)]
+    L.of_xoshiro_jump.restype = C.c_int
+    L.of_heston_price_adjoint.argtypes = [vp, P(A.OfHestonAdjointParams), P(A.OfAdjointResult)]
+    L.of_heston_price_adjoint.restype = C.c_int
     for name in ["of_ctx_create", "of_ctx_set_stream", "of_ctx_get_stream", "of_mc_run", "of_mc_strip",
                  "of_strip_plan_create", "of_strip_plan_launch", "of_strip_plan_results", "of_mc_price_book",
                  "of_book_plan_create", "of_book_plan_launch", "of_book_plan_results", "of_book_plan_info"]:

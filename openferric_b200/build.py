@@ -31,7 +31,9 @@ UNIT_FLAGS = {
     "greeks_reference.cu": ["--fmad=false"],
     "lsm.cu": ["--fmad=false"],
     "mc_philox.cu": ["-use_fast_math"],
-    "adjoint.cu": ["-use_fast_math"],
+    # explicit fmaf only, so the forward pass and the backward-sweep recompute
+    # are bit-identical; MUFU approximations are written as intrinsics
+    "adjoint.cu": ["--fmad=false", "-ftz=true"],
     "wgsl_port.cu": [],
 }
 

@@ -1,0 +1,765 @@
+// lsm.cu - Longstaff-Schwartz with an HBM-resident, time-major path store.
+//
+// Replaces LongstaffSchwartzEngine::price(VanillaOption)
+// (src/engines/lsm/longstaff_schwartz.rs:421-618) for a batch of contracts.
+//
+// Layout: S[contract][step-1][path] (time-major: a date's column is one
+// contiguous, coalesced read), cash flows V[contract][path] and their pathwise
+// spot derivatives dV.  One kernel per exercise date does
+//   exercise(t+1) with the betas of the previous pass -> discount -> FP64
+//   in-the-money basis moments at t -> block partials,
+// and the last block of each contract (last-block-done counter, no spin)
+// reduces the partials in a fixed order and solves the normal equations:
+// degree 2 = the reference's {1,S,S^2} with partially pivoted LU (nalgebra),
+// degree 3 = {1,x,x^2,x^3}, x = S/K, with Cholesky.
+//
+// FP64 reference mode reproduces the reference's draws: ONE xoshiro256++
+// stream seeded with `seed` feeds all paths in path-major order
+// (longstaff_schwartz.rs:467-509).  A thread owns a chunk of consecutive paths
+// and jumps its copy of the stream to the chunk's first draw with GF(2)
+// matrix powers of the (linear) xoshiro state transition.
+// FP32 Philox mode: counter-based normals, FP32 path store.
+//
+// Compiled with --fmad=false; FP32 code uses explicit fmaf.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "of_device.cuh"
+#include "of_internal.h"
+
+namespace {
+
+constexpr uint32_t kLsmStreamTag = 0x4C534D31u;  // "LSM1"
+constexpr int kPassThreads = 256;
+constexpr int kPathsPerThread = 4;
+constexpr int kPathsPerBlock = kPassThreads * kPathsPerThread;
+constexpr int kMaxMoments = 12;  // degree 3: x^0..x^6 (7) + y x^0..x^3 (4) ; degree 2: 8
+
+// ---------------------------------------------------------------------------
+// xoshiro256++ jump-ahead over GF(2)
+// ---------------------------------------------------------------------------
+void xoshiro_linear_step(uint64_t s[4]) {  // the state update of next_u64 (fast_rng.rs:58-66)
+  const uint64_t t = s[1] << 17;
+  s[2] ^= s[0];
+  s[3] ^= s[1];
+  s[1] ^= s[2];
+  s[0] ^= s[3];
+  s[2] ^= t;
+  s[3] = (s[3] << 45) | (s[3] >> 19);
+}
+
+void gf2_apply_host(const uint64_t* M, const uint64_t v[4], uint64_t out[4]) {
+  uint64_t r[4] = {0, 0, 0, 0};
+  for (int w = 0; w < 4; ++w)
+    for (int b = 0; b < 64; ++b)
+      if ((v[w] >> b) & 1ULL) {
+        const uint64_t* c = M + (size_t)(w * 64 + b) * 4;
+        for (int k = 0; k < 4; ++k) r[k] ^= c[k];
+      }
+  for (int k = 0; k < 4; ++k) out[k] = r[k];
+}
+
+// tables[k] = columns of T^(2^k), k = 0..63; column j = T^(2^k) e_j.
+const std::vector<uint64_t>& jump_tables() {
+  static std::vector<uint64_t> tab;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    tab.assign((size_t)64 * 256 * 4, 0);
+    for (int j = 0; j < 256; ++j) {
+      uint64_t s[4] = {0, 0, 0, 0};
+      s[j / 64] = 1ULL << (j % 64);
+      xoshiro_linear_step(s);
+      for (int k = 0; k < 4; ++k) tab[(size_t)j * 4 + k] = s[k];
+    }
+    for (int p = 1; p < 64; ++p) {
+      const uint64_t* prev = tab.data() + (size_t)(p - 1) * 1024;
+      uint64_t* cur = tab.data() + (size_t)p * 1024;
+      for (int j = 0; j < 256; ++j) gf2_apply_host(prev, prev + (size_t)j * 4, cur + (size_t)j * 4);
+    }
+  });
+  return tab;
+}
+
+__device__ void gf2_apply(const uint64_t* __restrict__ M, uint64_t s[4]) {
+  uint64_t r0 = 0, r1 = 0, r2 = 0, r3 = 0;
+#pragma unroll 1
+  for (int w = 0; w < 4; ++w) {
+    const uint64_t word = s[w];
+#pragma unroll 8
+    for (int b = 0; b < 64; ++b) {
+      const uint64_t m = 0ULL - ((word >> b) & 1ULL);
+      const ulonglong2* c = reinterpret_cast<const ulonglong2*>(M + (size_t)(w * 64 + b) * 4);
+      const ulonglong2 c01 = __ldg(c), c23 = __ldg(c + 1);
+      r0 ^= c01.x & m;
+      r1 ^= c01.y & m;
+      r2 ^= c23.x & m;
+      r3 ^= c23.y & m;
+    }
+  }
+  s[0] = r0;
+  s[1] = r1;
+  s[2] = r2;
+  s[3] = r3;
+}
+
+__device__ void xoshiro_jump(of::Xoshiro256pp& x, uint64_t n, const uint64_t* __restrict__ tables) {
+  uint64_t s[4] = {x.s0, x.s1, x.s2, x.s3};
+  for (int k = 0; k < 64 && n; ++k, n >>= 1)
+    if (n & 1ULL) gf2_apply(tables + (size_t)k * 1024, s);
+  x.s0 = s[0];
+  x.s1 = s[1];
+  x.s2 = s[2];
+  x.s3 = s[3];
+}
+
+__global__ void jump_test_kernel(uint64_t seed, const uint64_t* draws, int64_t n, const uint64_t* tables,
+                                 uint64_t* out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  of::Xoshiro256pp x;
+  x.seed(seed);
+  xoshiro_jump(x, draws[i], tables);
+  out[i * 4 + 0] = x.s0;
+  out[i * 4 + 1] = x.s1;
+  out[i * 4 + 2] = x.s2;
+  out[i * 4 + 3] = x.s3;
+}
+
+// ---------------------------------------------------------------------------
+// Contract constants
+// ---------------------------------------------------------------------------
+struct LsmC {
+  int32_t put;
+  int32_t steps;
+  double spot, strike, inv_strike, drift, step_vol, disc, inv_spot;
+  float fdrift, fstep_vol, fspot;
+};
+
+struct LsmBatch {
+  const LsmC* c;             // [nc]
+  const uint8_t* can_ex;     // [nc][steps+1]
+  int32_t nc, steps;
+  int64_t n, npad;           // paths, padded path stride
+  void* S;                   // [nc][steps][npad] (T)
+  void* V;                   // [nc][npad]
+  void* dV;                  // [nc][npad]
+  double* partials;          // [nc][blocks][kMaxMoments]
+  double* betas;             // [2][nc][4] + valid flag in [2][nc] (separate)
+  int32_t* beta_ok;          // [2][nc]
+  int32_t* regress_count;    // [nc]
+  uint32_t* counters;        // [nc]
+  double* results;           // [nc][3]: price, stderr, delta
+  int32_t blocks;            // blocks per contract
+  int32_t degree;
+  int32_t want_delta;
+  uint64_t seed;
+  uint32_t k0, k1, contract_base;
+  const double* inj;         // [nc][n][steps] or null
+  const uint64_t* jump;      // jump tables
+  int32_t chunk;             // paths per thread in the reference generator
+};
+
+template <typename T>
+__device__ __forceinline__ T intrinsic_v(bool put, T s, T k) {
+  const T v = put ? k - s : s - k;
+  return v > T(0) ? v : T(0);
+}
+
+// FP64 reference generator: chunk of consecutive paths per thread.
+__global__ void __launch_bounds__(128) lsm_gen_ref(LsmBatch B) {
+  const int c = blockIdx.y;
+  const LsmC C = B.c[c];
+  const int64_t chunk0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * B.chunk;
+  if (chunk0 >= B.n) return;
+  double* S = (double*)B.S + (size_t)c * B.steps * B.npad;
+  double* V = (double*)B.V + (size_t)c * B.npad;
+  double* dV = (double*)B.dV + (size_t)c * B.npad;
+  of::Xoshiro256pp rng;
+  if (!B.inj) {
+    rng.seed(B.seed);
+    xoshiro_jump(rng, (uint64_t)chunk0 * (uint64_t)B.steps, B.jump);
+  }
+  const int64_t end = chunk0 + B.chunk < B.n ? chunk0 + B.chunk : B.n;
+  for (int64_t p = chunk0; p < end; ++p) {
+    double s = C.spot;
+    const double* z = B.inj ? B.inj + ((size_t)c * B.n + p) * B.steps : nullptr;
+    for (int t = 1; t <= B.steps; ++t) {
+      const double zz = z ? z[t - 1] : of::acklam_inv_cdf(rng.next_f64());
+      s = s * exp(fma(C.step_vol, zz, C.drift));  // longstaff_schwartz.rs:507
+      S[(size_t)(t - 1) * B.npad + p] = s;
+    }
+    const double v = intrinsic_v<double>(C.put, s, C.strike);
+    V[p] = v;
+    dV[p] = v > 0.0 ? (C.put ? -s * C.inv_spot : s * C.inv_spot) : 0.0;
+  }
+}
+
+// FP32 Philox generator: 4 consecutive paths per thread, float4 stores.
+__global__ void __launch_bounds__(256) lsm_gen_philox(LsmBatch B) {
+  const int c = blockIdx.y;
+  const LsmC C = B.c[c];
+  const int64_t p0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (p0 >= B.npad) return;
+  float* S = (float*)B.S + (size_t)c * B.steps * B.npad;
+  float y[4] = {0.f, 0.f, 0.f, 0.f};
+  uint4 r[4];
+  const uint32_t cid = B.contract_base + (uint32_t)c;
+  for (int t = 0; t < B.steps; ++t) {
+    if ((t & 3) == 0) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        r[q] = of::philox4x32_10(make_uint4((uint32_t)(t >> 2), (uint32_t)(p0 + q), cid, kLsmStreamTag), B.k0, B.k1);
+    }
+    float4 out;
+    float* o = &out.x;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t bits = (t & 3) == 0 ? r[q].x : (t & 3) == 1 ? r[q].y : (t & 3) == 2 ? r[q].z : r[q].w;
+      const float z = of::normal_from_u32(bits);
+      y[q] = fmaf(C.fstep_vol, z, y[q] + C.fdrift);
+      o[q] = C.fspot * __expf(y[q]);
+    }
+    *reinterpret_cast<float4*>(S + (size_t)t * B.npad + p0) = out;
+  }
+  float* V = (float*)B.V + (size_t)c * B.npad;
+  float* dV = (float*)B.dV + (size_t)c * B.npad;
+  const float* last = S + (size_t)(B.steps - 1) * B.npad + p0;
+  const float fk = (float)C.strike, finv = (float)C.inv_spot;
+  for (int q = 0; q < 4; ++q) {
+    const float s = last[q];
+    const float v = intrinsic_v<float>(C.put, s, fk);
+    V[p0 + q] = (p0 + q < B.n) ? v : 0.0f;
+    dV[p0 + q] = (p0 + q < B.n && v > 0.0f) ? (C.put ? -s * finv : s * finv) : 0.0f;
+  }
+}
+
+// Continuation value of the fitted basis, FP64 (longstaff_schwartz.rs:597).
+__device__ __forceinline__ double continuation(int degree, const double* b, double s, double inv_k) {
+  if (degree == 2) return b[0] + b[1] * s + b[2] * s * s;
+  const double x = s * inv_k;
+  return b[0] + x * (b[1] + x * (b[2] + x * b[3]));
+}
+
+// Solves the normal equations from the reduced moments (thread 0 of the last block).
+__device__ void solve_beta(int degree, const double* m, double* beta, int32_t* ok) {
+  if (m[0] < 3.0) {  // fewer than 3 in-the-money paths: no regression (:561-563)
+    *ok = 0;
+    return;
+  }
+  *ok = 1;
+  beta[0] = beta[1] = beta[2] = beta[3] = 0.0;
+  if (degree == 2) {
+    // m = {s1, S, S^2, S^3, S^4, y, Sy, S^2y}; nalgebra LU with partial pivoting
+    double a[3][3] = {{m[0], m[1], m[2]}, {m[1], m[2], m[3]}, {m[2], m[3], m[4]}};
+    double b[3] = {m[5], m[6], m[7]};
+    for (int i = 0; i < 3; ++i) {
+      int piv = i;
+      double best = fabs(a[i][i]);
+      for (int k = i + 1; k < 3; ++k)
+        if (fabs(a[k][i]) > best) {
+          best = fabs(a[k][i]);
+          piv = k;
+        }
+      if (best == 0.0) continue;
+      if (piv != i) {
+        for (int j = 0; j < 3; ++j) {
+          const double t = a[i][j];
+          a[i][j] = a[piv][j];
+          a[piv][j] = t;
+        }
+        const double tb = b[i];
+        b[i] = b[piv];
+        b[piv] = tb;
+      }
+      for (int k = i + 1; k < 3; ++k) {
+        const double f = a[k][i] / a[i][i];
+        a[k][i] = f;
+        for (int j = i + 1; j < 3; ++j) a[k][j] -= f * a[i][j];
+        b[k] -= f * b[i];
+      }
+    }
+    for (int i = 0; i < 3; ++i)
+      if (a[i][i] == 0.0) return;  // singular: beta = 0 (:592)
+    double x[3];
+    for (int i = 2; i >= 0; --i) {
+      double s = b[i];
+      for (int j = i + 1; j < 3; ++j) s -= a[i][j] * x[j];
+      x[i] = s / a[i][i];
+    }
+    beta[0] = x[0];
+    beta[1] = x[1];
+    beta[2] = x[2];
+  } else {
+    // m = {x^0..x^6, y x^0..x^3}; Cholesky of the 4x4 Gram matrix
+    double a[4][4], l[4][4] = {{0}};
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) a[i][j] = m[i + j];
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j <= i; ++j) {
+        double s = a[i][j];
+        for (int k = 0; k < j; ++k) s -= l[i][k] * l[j][k];
+        if (i == j) {
+          if (!(s > 0.0)) return;
+          l[i][i] = sqrt(s);
+        } else {
+          l[i][j] = s / l[j][j];
+        }
+      }
+    double y[4], x[4];
+    for (int i = 0; i < 4; ++i) {
+      double s = m[7 + i];
+      for (int k = 0; k < i; ++k) s -= l[i][k] * y[k];
+      y[i] = s / l[i][i];
+    }
+    for (int i = 3; i >= 0; --i) {
+      double s = y[i];
+      for (int k = i + 1; k < 4; ++k) s -= l[k][i] * x[k];
+      x[i] = s / l[i][i];
+    }
+    for (int i = 0; i < 4; ++i) beta[i] = x[i];
+  }
+}
+
+// Fixed-order reduction of the per-block partials of one contract by the
+// block that finished last; thread 0 then solves for the betas.
+__device__ void last_block_reduce(const LsmBatch& B, int c, int nm, double* moments_sh, double* red_sh,
+                                  int t_pass) {
+  const double* part = B.partials + (size_t)c * B.blocks * kMaxMoments;
+  for (int k = 0; k < nm; ++k) {
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < B.blocks; b += blockDim.x) acc += part[(size_t)b * kMaxMoments + k];
+    red_sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if ((int)threadIdx.x < s) red_sh[threadIdx.x] += red_sh[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) moments_sh[k] = red_sh[0];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int buf = t_pass & 1;
+    double* beta = B.betas + ((size_t)buf * B.nc + c) * 4;
+    int32_t* ok = B.beta_ok + (size_t)buf * B.nc + c;
+    solve_beta(B.degree, moments_sh, beta, ok);
+    if (*ok) B.regress_count[c] += 1;
+  }
+}
+
+// One exercise date t (1 <= t <= steps-1): exercise(t+1), discount, moments(t).
+template <typename T>
+__global__ void __launch_bounds__(kPassThreads) lsm_pass(LsmBatch B, int t) {
+  __shared__ double red_sh[kPassThreads];
+  __shared__ double mom_sh[kMaxMoments];
+  __shared__ bool is_last;
+  const int c = blockIdx.y;
+  const LsmC C = B.c[c];
+  const T* S = (const T*)B.S + (size_t)c * B.steps * B.npad;
+  T* V = (T*)B.V + (size_t)c * B.npad;
+  T* dV = (T*)B.dV + (size_t)c * B.npad;
+  const bool ex_next = (t + 1 < B.steps) && B.can_ex[(size_t)c * (B.steps + 1) + t + 1];
+  const bool ex_now = B.can_ex[(size_t)c * (B.steps + 1) + t];
+  const int nb = (t + 1) & 1;  // betas of date t+1 were written by the previous pass
+  const bool have_beta = ex_next && B.beta_ok[(size_t)nb * B.nc + c];
+  double beta[4] = {0, 0, 0, 0};
+  if (have_beta)
+    for (int k = 0; k < 4; ++k) beta[k] = B.betas[((size_t)nb * B.nc + c) * 4 + k];
+  const int nm = B.degree == 2 ? 8 : 11;
+  double mom[kMaxMoments];
+#pragma unroll
+  for (int k = 0; k < kMaxMoments; ++k) mom[k] = 0.0;
+  const int64_t base = (int64_t)blockIdx.x * kPathsPerBlock;
+#pragma unroll
+  for (int q = 0; q < kPathsPerThread; ++q) {
+    const int64_t p = base + q * kPassThreads + threadIdx.x;
+    if (p >= B.n) break;
+    double v = (double)V[p], dv = (double)dV[p];
+    if (have_beta) {
+      const double s1 = (double)S[(size_t)t * B.npad + p];  // spot at date t+1
+      const double ex = intrinsic_v<double>(C.put, s1, C.strike);
+      if (ex > 0.0 && ex > continuation(B.degree, beta, s1, C.inv_strike)) {
+        v = ex;
+        dv = C.put ? -s1 * C.inv_spot : s1 * C.inv_spot;
+      }
+    }
+    v *= C.disc;
+    dv *= C.disc;
+    if (ex_now) {
+      const double s0 = (double)S[(size_t)(t - 1) * B.npad + p];  // spot at date t
+      if (intrinsic_v<double>(C.put, s0, C.strike) > 0.0) {
+        if (B.degree == 2) {
+          const double s2 = s0 * s0;
+          mom[0] += 1.0;
+          mom[1] += s0;
+          mom[2] += s2;
+          mom[3] += s2 * s0;
+          mom[4] += s2 * s2;
+          mom[5] += v;
+          mom[6] += s0 * v;
+          mom[7] += s2 * v;
+        } else {
+          const double x = s0 * C.inv_strike;
+          double pw = 1.0;
+#pragma unroll
+          for (int e = 0; e < 7; ++e) {
+            mom[e] += pw;
+            if (e < 4) mom[7 + e] += pw * v;
+            pw *= x;
+          }
+        }
+      }
+    }
+    V[p] = (T)v;
+    dV[p] = (T)dv;
+  }
+  if (!ex_now) return;
+  // block reduction of the moments (fixed order) -> partials
+  double* part = B.partials + ((size_t)c * B.blocks + blockIdx.x) * kMaxMoments;
+  for (int k = 0; k < nm; ++k) {
+    double w = of::warp_sum(mom[k]);
+    if ((threadIdx.x & 31) == 0) red_sh[threadIdx.x >> 5] = w;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double acc = 0.0;
+      for (int i = 0; i < kPassThreads / 32; ++i) acc += red_sh[i];
+      part[k] = acc;
+    }
+    __syncthreads();
+  }
+  __threadfence();
+  if (threadIdx.x == 0) {
+    const uint32_t done = atomicAdd(B.counters + c, 1u);
+    is_last = done == (uint32_t)B.blocks - 1;
+  }
+  __syncthreads();
+  if (is_last) {
+    __threadfence();
+    last_block_reduce(B, c, nm, mom_sh, red_sh, t);
+    if (threadIdx.x == 0) B.counters[c] = 0;
+  }
+}
+
+// Exercise at date 1, final discount, price/stderr/delta sums
+// (longstaff_schwartz.rs:604-605, mean_and_stderr :125-140).
+template <typename T>
+__global__ void __launch_bounds__(kPassThreads) lsm_final(LsmBatch B) {
+  __shared__ double red_sh[kPassThreads];
+  __shared__ double mom_sh[kMaxMoments];
+  __shared__ bool is_last;
+  const int c = blockIdx.y;
+  const LsmC C = B.c[c];
+  const T* S = (const T*)B.S + (size_t)c * B.steps * B.npad;
+  const T* V = (const T*)B.V + (size_t)c * B.npad;
+  const T* dV = (const T*)B.dV + (size_t)c * B.npad;
+  const bool ex1 = (1 < B.steps) && B.can_ex[(size_t)c * (B.steps + 1) + 1];
+  const int nb = 1 & 1;
+  const bool have_beta = ex1 && B.beta_ok[(size_t)nb * B.nc + c];
+  double beta[4] = {0, 0, 0, 0};
+  if (have_beta)
+    for (int k = 0; k < 4; ++k) beta[k] = B.betas[((size_t)nb * B.nc + c) * 4 + k];
+  double acc[3] = {0, 0, 0};
+  const int64_t base = (int64_t)blockIdx.x * kPathsPerBlock;
+  for (int q = 0; q < kPathsPerThread; ++q) {
+    const int64_t p = base + q * kPassThreads + threadIdx.x;
+    if (p >= B.n) break;
+    double v = (double)V[p], dv = (double)dV[p];
+    if (have_beta) {
+      const double s1 = (double)S[p];  // spot at date 1
+      const double ex = intrinsic_v<double>(C.put, s1, C.strike);
+      if (ex > 0.0 && ex > continuation(B.degree, beta, s1, C.inv_strike)) {
+        v = ex;
+        dv = C.put ? -s1 * C.inv_spot : s1 * C.inv_spot;
+      }
+    }
+    v *= C.disc;
+    dv *= C.disc;
+    acc[0] += v;
+    acc[1] += v * v;
+    acc[2] += dv;
+  }
+  double* part = B.partials + ((size_t)c * B.blocks + blockIdx.x) * kMaxMoments;
+  for (int k = 0; k < 3; ++k) {
+    double w = of::warp_sum(acc[k]);
+    if ((threadIdx.x & 31) == 0) red_sh[threadIdx.x >> 5] = w;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0;
+      for (int i = 0; i < kPassThreads / 32; ++i) a += red_sh[i];
+      part[k] = a;
+    }
+    __syncthreads();
+  }
+  __threadfence();
+  if (threadIdx.x == 0) {
+    const uint32_t done = atomicAdd(B.counters + c, 1u);
+    is_last = done == (uint32_t)B.blocks - 1;
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  const double* pp = B.partials + (size_t)c * B.blocks * kMaxMoments;
+  for (int k = 0; k < 3; ++k) {
+    double a = 0.0;
+    for (int b = threadIdx.x; b < B.blocks; b += blockDim.x) a += pp[(size_t)b * kMaxMoments + k];
+    red_sh[threadIdx.x] = a;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if ((int)threadIdx.x < s) red_sh[threadIdx.x] += red_sh[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) mom_sh[k] = red_sh[0];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double n = (double)B.n;
+    const double mean = mom_sh[0] / n;
+    const double var = B.n > 1 ? (mom_sh[1] - mom_sh[0] * mom_sh[0] / n) / (n - 1.0) : 0.0;
+    B.results[c * 3 + 0] = mean;
+    B.results[c * 3 + 1] = sqrt(var / n);
+    B.results[c * 3 + 2] = mom_sh[2] / n;
+    B.counters[c] = 0;
+  }
+}
+
+}  // namespace
+
+static of_status lsm_validate(of_ctx* ctx, const of_lsm_contract* k, int64_t paths) {
+  if (k->option_type != OF_CALL && k->option_type != OF_PUT)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown option type %d", k->option_type);
+  if (!(k->strike > 0.0)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "vanilla strike must be > 0");
+  if (!(k->expiry >= 0.0)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "vanilla expiry must be >= 0");
+  if (k->exercise == OF_EXERCISE_BERMUDAN) {
+    if (k->n_exercise_dates <= 0 || !k->exercise_dates)
+      return of_fail(ctx, OF_ERR_INVALID_INPUT, "bermudan exercise dates cannot be empty");
+    for (int64_t d = 0; d < k->n_exercise_dates; ++d)
+      if (k->exercise_dates[d] <= 0.0 || k->exercise_dates[d] > k->expiry)
+        return of_fail(ctx, OF_ERR_INVALID_INPUT, "bermudan exercise dates must lie in (0, expiry]");
+  } else if (k->exercise != OF_EXERCISE_EUROPEAN && k->exercise != OF_EXERCISE_AMERICAN) {
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown exercise style %d", k->exercise);
+  }
+  if (k->num_steps < 2) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_steps must be >= 2 for Longstaff-Schwartz");
+  if (k->num_steps > (1 << 20)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_steps too large");
+  if (paths < 3) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_paths must be >= 3 for Longstaff-Schwartz");
+  if (k->expiry > 0.0 && !(k->vol > 0.0)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "market volatility must be > 0");
+  if (!(k->spot > 0.0)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "market spot must be > 0");
+  return OF_OK;
+}
+
+static of_status upload_jump_tables(of_ctx* ctx, const uint64_t** out) {
+  const std::vector<uint64_t>& t = jump_tables();
+  const size_t bytes = t.size() * sizeof(uint64_t);
+  const bool fresh = ctx->slot_bytes[SLOT_JUMP] < bytes;
+  void* d = nullptr;
+  OF_TRY(of_scratch(ctx, SLOT_JUMP, bytes, &d));
+  if (fresh) OF_CUDA_TRY(ctx, cudaMemcpy(d, t.data(), bytes, cudaMemcpyHostToDevice));
+  *out = (const uint64_t*)d;
+  return OF_OK;
+}
+
+extern "C" of_status of_xoshiro_jump(of_ctx* ctx, uint64_t seed, const uint64_t* draws, int64_t n,
+                                     uint64_t* states_out) {
+  if (!ctx || !draws || !states_out || n <= 0) return OF_ERR_INVALID_INPUT;
+  OF_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const uint64_t* tab = nullptr;
+  OF_TRY(upload_jump_tables(ctx, &tab));
+  void *d_in = nullptr, *d_out = nullptr;
+  OF_TRY(of_scratch(ctx, SLOT_MISC, (size_t)n * 5 * sizeof(uint64_t), &d_in));
+  d_out = (uint64_t*)d_in + n;
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(d_in, draws, (size_t)n * sizeof(uint64_t), cudaMemcpyHostToDevice, ctx->stream));
+  jump_test_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(seed, (const uint64_t*)d_in, n, tab,
+                                                                       (uint64_t*)d_out);
+  OF_CUDA_TRY(ctx, cudaGetLastError());
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(states_out, d_out, (size_t)n * 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+  OF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return OF_OK;
+}
+
+extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_t n, const of_lsm_config* cfg,
+                                  of_lsm_result* res) {
+  if (!ctx || !ks || !cfg || !res || n <= 0) return OF_ERR_INVALID_INPUT;
+  if (cfg->basis_degree != 2 && cfg->basis_degree != 3)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "basis_degree must be 2 or 3");
+  const bool fp64 = cfg->precision == OF_PREC_FP64_REFERENCE;
+  if (!fp64 && cfg->precision != OF_PREC_FP32_PHILOX)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown precision %d", cfg->precision);
+  if (cfg->injected_normals && !fp64)
+    return of_fail(ctx, OF_ERR_UNSUPPORTED, "injected normals are a FP64 reference-mode test hook");
+  const int64_t N = cfg->num_paths;
+  for (int64_t i = 0; i < n; ++i) OF_TRY(lsm_validate(ctx, &ks[i], N));
+  if (cfg->injected_normals) {
+    int64_t need = 0;
+    for (int64_t i = 0; i < n; ++i) need += N * ks[i].num_steps;
+    if (cfg->n_injected < need)
+      return of_fail(ctx, OF_ERR_INVALID_INPUT, "injected normals: need %lld values, got %lld", (long long)need,
+                     (long long)cfg->n_injected);
+  }
+  OF_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  std::memset(res, 0, sizeof(of_lsm_result) * (size_t)n);
+  const uint64_t* jump = nullptr;
+  if (fp64 && !cfg->injected_normals) OF_TRY(upload_jump_tables(ctx, &jump));
+
+  const size_t esz = fp64 ? sizeof(double) : sizeof(float);
+  const int64_t npad = (N + kPathsPerBlock - 1) / kPathsPerBlock * kPathsPerBlock;
+  const int blocks = (int)(npad / kPathsPerBlock);
+  // Contracts sharing a step count go through the date loop together, in
+  // batches bounded by a path-store budget.
+  const size_t budget = (size_t)24 << 30;
+  std::vector<int64_t> order((size_t)n);
+  for (int64_t i = 0; i < n; ++i) order[(size_t)i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return ks[a].num_steps < ks[b].num_steps; });
+  // injected-normal offsets in the caller's contract order
+  std::vector<int64_t> inj_off((size_t)n, 0);
+  for (int64_t i = 1; i < n; ++i) inj_off[(size_t)i] = inj_off[(size_t)i - 1] + N * ks[i - 1].num_steps;
+
+  float total_ms = 0.0f;
+  size_t pos = 0;
+  while (pos < order.size()) {
+    // trivial contracts (expiry == 0): intrinsic, stderr 0 (longstaff_schwartz.rs:440-447)
+    const of_lsm_contract& k0 = ks[order[pos]];
+    if (k0.expiry == 0.0) {
+      const double v = k0.option_type == OF_CALL ? k0.spot - k0.strike : k0.strike - k0.spot;
+      res[order[pos]].price = v > 0.0 ? v : 0.0;
+      ++pos;
+      continue;
+    }
+    const int64_t steps = k0.num_steps;
+    const size_t per = (size_t)steps * npad * esz;
+    size_t cap = std::max<size_t>(1, budget / per);
+    if (cfg->injected_normals) cap = 1;  // one contract per batch keeps the injected layout simple
+    std::vector<int64_t> batch;
+    while (pos < order.size() && batch.size() < cap && ks[order[pos]].num_steps == steps &&
+           ks[order[pos]].expiry != 0.0)
+      batch.push_back(order[pos++]);
+    const int nc = (int)batch.size();
+    std::vector<LsmC> hc((size_t)nc);
+    std::vector<uint8_t> can((size_t)nc * (steps + 1), 0);
+    for (int c = 0; c < nc; ++c) {
+      const of_lsm_contract& k = ks[batch[(size_t)c]];
+      LsmC& C = hc[(size_t)c];
+      const double dt = k.expiry / (double)steps;
+      C.put = k.option_type == OF_PUT;
+      C.steps = (int32_t)steps;
+      C.spot = k.spot;
+      C.strike = k.strike;
+      C.inv_strike = 1.0 / k.strike;
+      C.inv_spot = 1.0 / k.spot;
+      C.drift = (k.rate - k.dividend_yield - 0.5 * k.vol * k.vol) * dt;  // :452
+      C.step_vol = k.vol * std::sqrt(dt);
+      C.disc = std::exp(-k.rate * dt);
+      C.fdrift = (float)C.drift;
+      C.fstep_vol = (float)C.step_vol;
+      C.fspot = (float)k.spot;
+      uint8_t* ce = can.data() + (size_t)c * (steps + 1);
+      if (k.exercise == OF_EXERCISE_EUROPEAN) {
+        ce[steps] = 1;
+      } else if (k.exercise == OF_EXERCISE_AMERICAN) {
+        for (int64_t t = 1; t <= steps; ++t) ce[t] = 1;
+      } else {
+        for (int64_t d = 0; d < k.n_exercise_dates; ++d) {
+          const double idx = std::round((k.exercise_dates[d] / k.expiry) * (double)steps);
+          int64_t i = (std::isnan(idx) || idx <= 0.0) ? 0 : (int64_t)idx;
+          ce[i < steps ? i : steps] = 1;
+        }
+        ce[steps] = 1;
+      }
+    }
+    // device buffers
+    void *dS = nullptr, *dV = nullptr, *dAux = nullptr, *dInj = nullptr;
+    OF_TRY(of_scratch(ctx, SLOT_LSM_PATHS, (size_t)nc * per, &dS));
+    OF_TRY(of_scratch(ctx, SLOT_LSM_VALUES, (size_t)nc * npad * esz * 2, &dV));
+    const size_t part_bytes = (size_t)nc * blocks * kMaxMoments * sizeof(double);
+    const size_t aux_bytes = part_bytes + (size_t)nc * (sizeof(LsmC) + 2 * 4 * sizeof(double) + 3 * sizeof(double) +
+                                                        2 * sizeof(int32_t) + sizeof(int32_t) + sizeof(uint32_t)) +
+                             can.size() + 1024;
+    OF_TRY(of_scratch(ctx, SLOT_LSM_AUX, aux_bytes, &dAux));
+    char* a = (char*)dAux;
+    LsmBatch B{};
+    B.partials = (double*)a;
+    a += part_bytes;
+    B.betas = (double*)a;
+    a += (size_t)nc * 8 * sizeof(double);
+    B.results = (double*)a;
+    a += (size_t)nc * 3 * sizeof(double);
+    LsmC* dC = (LsmC*)a;
+    a += (size_t)nc * sizeof(LsmC);
+    B.beta_ok = (int32_t*)a;
+    a += (size_t)nc * 2 * sizeof(int32_t);
+    B.regress_count = (int32_t*)a;
+    a += (size_t)nc * sizeof(int32_t);
+    B.counters = (uint32_t*)a;
+    a += (size_t)nc * sizeof(uint32_t);
+    uint8_t* dCan = (uint8_t*)a;
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(dC, hc.data(), hc.size() * sizeof(LsmC), cudaMemcpyHostToDevice, ctx->stream));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(dCan, can.data(), can.size(), cudaMemcpyHostToDevice, ctx->stream));
+    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.beta_ok, 0, (size_t)nc * 4 * sizeof(int32_t), ctx->stream));
+    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.regress_count, 0, (size_t)nc * sizeof(int32_t), ctx->stream));
+    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.counters, 0, (size_t)nc * sizeof(uint32_t), ctx->stream));
+    if (cfg->injected_normals) {
+      const size_t cnt = (size_t)N * steps;
+      OF_TRY(of_scratch(ctx, SLOT_INJECT, cnt * sizeof(double), &dInj));
+      OF_CUDA_TRY(ctx, cudaMemcpyAsync(dInj, cfg->injected_normals + inj_off[(size_t)batch[0]], cnt * sizeof(double),
+                                       cudaMemcpyHostToDevice, ctx->stream));
+    }
+    B.c = dC;
+    B.can_ex = dCan;
+    B.nc = nc;
+    B.steps = (int32_t)steps;
+    B.n = N;
+    B.npad = npad;
+    B.S = dS;
+    B.V = dV;
+    B.dV = (char*)dV + (size_t)nc * npad * esz;
+    B.blocks = blocks;
+    B.degree = cfg->basis_degree;
+    B.want_delta = cfg->want_delta;
+    B.seed = cfg->seed;
+    B.k0 = (uint32_t)cfg->seed;
+    B.k1 = (uint32_t)(cfg->seed >> 32);
+    B.contract_base = (uint32_t)batch[0];
+    B.inj = (const double*)dInj;
+    B.jump = jump;
+    B.chunk = 8;
+    if (!fp64) OF_CUDA_TRY(ctx, cudaMemsetAsync(dV, 0, (size_t)nc * npad * esz * 2, ctx->stream));
+    OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+    if (fp64) {
+      const int64_t chunks = (N + B.chunk - 1) / B.chunk;
+      lsm_gen_ref<<<dim3((unsigned)((chunks + 127) / 128), nc), 128, 0, ctx->stream>>>(B);
+    } else {
+      const int64_t quads = npad / 4;
+      lsm_gen_philox<<<dim3((unsigned)((quads + 255) / 256), nc), 256, 0, ctx->stream>>>(B);
+    }
+    OF_CUDA_TRY(ctx, cudaGetLastError());
+    const dim3 grid((unsigned)blocks, nc);
+    for (int t = (int)steps - 1; t >= 1; --t) {
+      if (fp64) lsm_pass<double><<<grid, kPassThreads, 0, ctx->stream>>>(B, t);
+      else lsm_pass<float><<<grid, kPassThreads, 0, ctx->stream>>>(B, t);
+    }
+    if (fp64) lsm_final<double><<<grid, kPassThreads, 0, ctx->stream>>>(B);
+    else lsm_final<float><<<grid, kPassThreads, 0, ctx->stream>>>(B);
+    OF_CUDA_TRY(ctx, cudaGetLastError());
+    OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+    std::vector<double> hres((size_t)nc * 3);
+    std::vector<int32_t> hreg((size_t)nc);
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(hres.data(), B.results, hres.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(hreg.data(), B.regress_count, hreg.size() * sizeof(int32_t),
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    OF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    float ms = 0.0f;
+    OF_CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+    total_ms += ms;
+    for (int c = 0; c < nc; ++c) {
+      of_lsm_result& r = res[batch[(size_t)c]];
+      r.price = hres[(size_t)c * 3];
+      r.stderr_ = hres[(size_t)c * 3 + 1];
+      r.delta = cfg->want_delta ? hres[(size_t)c * 3 + 2] : 0.0;
+      r.regressions = hreg[(size_t)c];
+    }
+  }
+  for (int64_t i = 0; i < n; ++i) res[i].kernel_ms = total_ms;
+  return OF_OK;
+}

@@ -29,6 +29,7 @@ enum OfSlot {
   SLOT_ADJ_AUX = 12,
   SLOT_STATUS = 13,    // device error word + counters
   SLOT_MISC = 14,
+  SLOT_JUMP = 15,      // xoshiro256++ GF(2) jump tables
   SLOT_COUNT = 16
 };
 

@@ -169,29 +169,51 @@ class BarrierOptionBuilder:
 
 @dataclass
 class BermudanOption:
-    """instruments::BermudanOption (src/instruments/bermudan.rs:19-106): a
-    schedule of (exercise time, strike) pairs."""
+    """instruments::BermudanOption (src/instruments/bermudan.rs:19-150): exercise
+    dates with a strike per date."""
 
     option_type: OptionType
     expiry: float
-    exercise_schedule: List[Tuple[float, float]]
+    exercise_dates: List[float]
+    strike_schedule: List[float]
+
+    @staticmethod
+    def new(option_type: OptionType, expiry: float, exercise_dates: Sequence[float],
+            strike_schedule: Sequence[float]) -> "BermudanOption":
+        return BermudanOption(option_type, float(expiry), [float(t) for t in exercise_dates],
+                              [float(k) for k in strike_schedule])
+
+    @staticmethod
+    def with_constant_strike(option_type: OptionType, strike: float, expiry: float,
+                             exercise_dates: Sequence[float]) -> "BermudanOption":
+        return BermudanOption.new(option_type, expiry, exercise_dates, [float(strike)] * len(exercise_dates))
 
     def instrument_type(self) -> str:
         return "BermudanOption"
 
     def validate(self) -> None:
-        if self.expiry <= 0.0:
-            raise PricingError.InvalidInput("bermudan expiry must be > 0")
-        if not self.exercise_schedule:
-            raise PricingError.InvalidInput("bermudan schedule cannot be empty")
-        for t, k in self.exercise_schedule:
-            if t <= 0.0 or t > self.expiry:
-                raise PricingError.InvalidInput("bermudan exercise times must lie in (0, expiry]")
-            if k <= 0.0:
-                raise PricingError.InvalidInput("bermudan strikes must be > 0")
+        import math
+        if self.expiry <= 0.0 or not math.isfinite(self.expiry):
+            raise PricingError.InvalidInput("bermudan expiry must be finite and > 0")
+        if not self.exercise_dates:
+            raise PricingError.InvalidInput("bermudan exercise_dates cannot be empty")
+        if len(self.exercise_dates) != len(self.strike_schedule):
+            raise PricingError.InvalidInput("bermudan strike_schedule must match exercise_dates length")
+        if any((not math.isfinite(t)) or t <= 0.0 or t > self.expiry for t in self.exercise_dates):
+            raise PricingError.InvalidInput("bermudan exercise_dates must be finite and in (0, expiry]")
+        if any(b <= a for a, b in zip(self.exercise_dates, self.exercise_dates[1:])):
+            raise PricingError.InvalidInput("bermudan exercise_dates must be strictly increasing")
+        if any((not math.isfinite(k)) or k <= 0.0 for k in self.strike_schedule):
+            raise PricingError.InvalidInput("bermudan strike_schedule entries must be finite and > 0")
 
     def effective_schedule(self) -> List[Tuple[float, float]]:
-        return sorted(self.exercise_schedule)
+        """(time, strike) pairs, with (expiry, last strike) appended when the
+        last date is before expiry (bermudan.rs:82-101)."""
+        self.validate()
+        out = list(zip(self.exercise_dates, self.strike_schedule))
+        if self.expiry - out[-1][0] > 1.0e-12:
+            out.append((self.expiry, out[-1][1]))
+        return out
 
 
 def daily_fixings(expiry: float, steps: int) -> List[float]:

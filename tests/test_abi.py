@@ -40,6 +40,11 @@ STRUCTS = {
     "of_mc_result": A.OfMcResult,
     "of_book_entry": A.OfBookEntry,
     "of_book_config": A.OfBookConfig,
+    "of_greeks_params": A.OfGreeksParams,
+    "of_greeks_result": A.OfGreeksResult,
+    "of_lsm_contract": A.OfLsmContract,
+    "of_lsm_config": A.OfLsmConfig,
+    "of_lsm_result": A.OfLsmResult,
 }
 
 
