@@ -177,7 +177,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--paths", type=int, default=PATHS,
+                    help="paths per strip (profiling a smaller case; the benchmark workload is 2^20)")
     args = ap.parse_args()
+    global PATH_STEPS
+    PATH_STEPS = float(args.paths) * STEPS
+    CONFIG["paths"] = args.paths
     rank, world, local_rank = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         return run_reference(args, rank, world)
@@ -197,7 +202,7 @@ def main():
     gen = of.HestonPathGenerator(of.Heston(**HESTON), S0, T, STEPS)
     df = math.exp(-RATE * T)
     seed = SEED + rank
-    plan = StripPlan(gen, of.OptionType.Call, STRIKES, PATHS, seed, df)
+    plan = StripPlan(gen, of.OptionType.Call, STRIKES, args.paths, seed, df)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", local_rank))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
 
@@ -231,12 +236,12 @@ def main():
 
     # End to end through the public API (host wall clock, sync inside each call).
     for _ in range(2):
-        of.price_strike_strip(gen, of.OptionType.Call, STRIKES, PATHS, seed, df)
+        of.price_strike_strip(gen, of.OptionType.Call, STRIKES, args.paths, seed, df)
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        e2e_prices = of.price_strike_strip(gen, of.OptionType.Call, STRIKES, PATHS, seed, df)
+        e2e_prices = of.price_strike_strip(gen, of.OptionType.Call, STRIKES, args.paths, seed, df)
     e2e_s = time.perf_counter() - t0
     if dist:
         t = torch.tensor([e2e_s], device=f"cuda:{local_rank}", dtype=torch.float64)

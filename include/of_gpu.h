@@ -322,6 +322,14 @@ typedef struct of_adjoint_result {
  * reference counterpart. */
 of_status of_heston_price_adjoint(of_ctx* ctx, const of_heston_adjoint_params* p, of_adjoint_result* out);
 
+/* ---- the reference's GPU European kernel ---------------------------------- */
+/* mc_european_gpu (src/engines/gpu/gpu_mc.rs:322-349, shader
+ * src/engines/gpu/mc_shader.wgsl:28-142) on CUDA: f32 GBM paths, xoshiro128++,
+ * Box-Muller, 256-wide block reduction, FP64 host sum. */
+of_status of_mc_european_gpu(of_ctx* ctx, double spot, double strike, double rate, double vol, double expiry,
+                             int64_t num_paths, int64_t num_steps, uint32_t seed, int32_t is_call,
+                             double* price, double* stderr_);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,20 @@ def close(a, b, rtol):
     return abs(a - b) <= rtol * max(abs(a), abs(b), 1e-300) or abs(a - b) <= 1e-300
 
 
+def se_close(a, b, rtol, price):
+    """Standard errors agree, or both are zero variance.  With a control
+    variate identical to the payoff the adjusted variance is a difference of
+    sums that cancels to rounding level (the reference returns NaN, 0 or a
+    few 1e-9 there, depending on summation order): any NaN or value below
+    1e-7 of the price on both sides is the same zero variance."""
+    zero = 1e-7 * max(1.0, abs(price))
+    za = math.isnan(a) or abs(a) <= zero
+    zb = math.isnan(b) or abs(b) <= zero
+    if za or zb:
+        return za and zb
+    return close(a, b, rtol)
+
+
 def _market(spot=100.0, r=0.05, q=0.0, vol=0.2):
     return Market.builder().spot(spot).rate(r).dividend_yield(q).flat_vol(vol).build()
 
@@ -95,7 +109,7 @@ def test_fp64_reference_mode_matches_oracle(orc, model, name, anti, use_cv):
     ref = _oracle_run(orc, gen, inst, anti, cv, df, paths, seed)
     assert gpu.samples == ref.samples
     assert close(gpu.price, ref.price, PRICE_RTOL), (gpu.price, ref.price)
-    assert close(gpu.stderr_, ref.stderr_, SE_RTOL), (gpu.stderr_, ref.stderr_)
+    assert se_close(gpu.stderr_, ref.stderr_, SE_RTOL, ref.price), (gpu.stderr_, ref.stderr_)
     for f in ("sum_x", "sum_x2", "sum_y", "sum_xy", "sum_y2"):
         assert close(getattr(gpu, f), getattr(ref, f), 1e-12), f
 

@@ -1,0 +1,26 @@
+"""The reference's GPU European kernel (WGSL semantics) on CUDA vs the oracle's
+C float restatement of the shader math.  Both run f32 arithmetic with
+different libm implementations of exp/log/sin/cos, so agreement is at f32
+rounding level, not bit level."""
+import pytest
+
+from openferric_b200.analytic import bs_price
+from openferric_b200.core import OptionType
+from openferric_b200.gpu_mc import mc_european_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("steps", [1, 2, 63, 64])
+@pytest.mark.parametrize("is_call", [True, False])
+def test_wgsl_port_matches_c_restatement(orc, steps, is_call):
+    g = mc_european_gpu(100.0, 105.0, 0.03, 0.25, 1.0, 50_000, steps, 17, is_call)
+    p, s = orc.wgsl_european(100.0, 105.0, 0.03, 0.25, 1.0, 50_000, steps, 17, is_call)
+    assert abs(g.price - p) <= 2e-5 * abs(p) + 1e-6, (g.price, p)
+    assert abs(g.stderr - s) <= 2e-4 * abs(s)
+
+
+def test_wgsl_port_prices_near_black_scholes():
+    r = mc_european_gpu(100.0, 100.0, 0.05, 0.2, 1.0, 1 << 20, 64, 3, True)
+    bs = bs_price(OptionType.Call, 100.0, 100.0, 0.05, 0.0, 0.2, 1.0)
+    assert abs(r.price - bs) <= 4 * r.stderr + 0.01
