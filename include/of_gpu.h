@@ -297,7 +297,10 @@ typedef struct of_heston_adjoint_params {
                                the spot at every step 1..num_steps */
   int32_t scheme;           /* OF_MODEL_HESTON_QE or OF_MODEL_HESTON_EULER */
   int32_t checkpoint_every; /* path-state checkpoint interval (32) */
-  int32_t forward_only;     /* 1: price only, same random numbers (bump-and-revalue) */
+  int32_t forward_only;     /* 0: price + adjoint Greeks; 1: price only (FP32); 2: price only
+                               in FP64 arithmetic on the same draws (bump-and-revalue with
+                               common random numbers: a 1e-4 relative bump is below the FP32
+                               resolution of the path state) */
   int32_t reserved0;
 } of_heston_adjoint_params;
 

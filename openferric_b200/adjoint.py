@@ -58,7 +58,10 @@ def _params(spec: HestonAdjointSpec, spot, rate, v0, kappa, theta, xi, rho, forw
 
 
 def heston_adjoint(spec: HestonAdjointSpec, spot: float, rate: float, v0: float, kappa: float, theta: float,
-                   xi: float, rho: float, forward_only: bool = False, device: int = 0) -> AdjointResult:
+                   xi: float, rho: float, forward_only: int = 0, device: int = 0) -> AdjointResult:
+    """forward_only: 0 price + adjoint Greeks, 1 price only (FP32), 2 price
+    only in FP64 on the same draws (for bump-and-revalue with common random
+    numbers)."""
     ctx = context(device)
     p = _params(spec, spot, rate, v0, kappa, theta, xi, rho, forward_only)
     out = A.OfAdjointResult()
@@ -82,7 +85,7 @@ def price_with_adjoint(instrument, market: Market, model: Heston, num_paths: int
         s = instrument.asian
         if s.averaging is not Averaging.Arithmetic or s.strike_type is not StrikeType.Fixed:
             raise PricingError.InvalidInput("adjoint pricing supports fixed-strike arithmetic Asians")
-        expected = [instrument.expiry * j / num_steps for j in range(1, num_steps + 1)]
+        expected = [instrument.expiry * (j / num_steps) for j in range(1, num_steps + 1)]
         if len(s.observation_times) != num_steps or any(
                 abs(a - b) > 1e-12 * max(1.0, instrument.expiry) for a, b in zip(s.observation_times, expected)):
             raise PricingError.InvalidInput("adjoint Asian pricing needs a fixing at every simulation step")

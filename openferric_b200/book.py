@@ -140,7 +140,7 @@ def synthetic_book(n: int = 4096, seed: int = 20261203, steps_per_year: int = 25
         if kind == 0:
             inst = VanillaOption.european_call(k[i], T[i])
         elif kind == 1:
-            obs = [T[i] * j / steps for j in range(1, steps + 1)]
+            obs = [T[i] * (j / steps) for j in range(1, steps + 1)]  # last fixing == T exactly
             inst = AsianOption(OptionType.Call, k[i], T[i], AsianSpec(Averaging.Arithmetic, StrikeType.Fixed, obs))
         else:
             inst = BarrierOption(OptionType.Call, k[i], T[i],

@@ -45,7 +45,7 @@ struct AdjC {
   double disc, T;
   int32_t steps, seg_len, n_seg, call, asian, forward_only;
   int64_t paths;
-  uint32_t k0, k1;
+  of::PhiloxKeys keys;
 };
 
 struct QeDraw {
@@ -144,7 +144,8 @@ __device__ __forceinline__ StepJac qe_jacobian(const AdjC& c, float v, float vn,
 }
 
 template <int C>
-__global__ void __launch_bounds__(128) adjoint_kernel(AdjC c, double* __restrict__ partials) {
+__global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ AdjC c,
+                                                      double* __restrict__ partials) {
   __shared__ double sh[16 * 4];
   double acc[16];
 #pragma unroll
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(AdjC c, double* __restrict
       for (int k = 0; k < C; k += 2) {
         const int j = j0 + k;
         if (j >= c.steps) break;
-        const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, kAdjStreamTag), c.k0, c.k1);
+        const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, kAdjStreamTag), c.keys);
 #pragma unroll
         for (int o = 0; o < 2; ++o) {
           if (j + o < c.steps) {
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(AdjC c, double* __restrict
       for (int k = 0; k < C; k += 2) {
         if (k < len) {
           const int j = j0 + k;
-          const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, kAdjStreamTag), c.k0, c.k1);
+          const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, kAdjStreamTag), c.keys);
 #pragma unroll
           for (int o = 0; o < 2; ++o) {
             if (k + o < len) {
@@ -219,7 +220,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(AdjC c, double* __restrict
       for (int k = C - 2; k >= 0; k -= 2) {
         if (k < len) {
           const int j = j0 + k;
-          const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, kAdjStreamTag), c.k0, c.k1);
+          const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, kAdjStreamTag), c.keys);
 #pragma unroll
           for (int o = 1; o >= 0; --o) {
             if (k + o < len) {
@@ -250,6 +251,63 @@ __global__ void __launch_bounds__(128) adjoint_kernel(AdjC c, double* __restrict
     for (int k = 0; k < 16; ++k) partials[(int64_t)blockIdx.x * 16 + k] = acc[k];
 }
 
+// Price-only FP64 pass over the same draws (the bits of each Philox counter
+// give the same U, Zv, Zx), for bump-and-revalue with common random numbers:
+// a relative bump of 1e-4 moves a step's log-increment by ~1e-8, below the
+// FP32 resolution of the path state, so the revaluation runs in FP64.
+struct AdjC64 {
+  double e, c1, c2, theta, c0, K1, K2, k34, s0, strike, inv_steps, disc, v0;
+  int32_t steps, call, asian;
+  int64_t paths;
+  of::PhiloxKeys keys;
+};
+
+__global__ void __launch_bounds__(128) forward64_kernel(const __grid_constant__ AdjC64 c,
+                                                        double* __restrict__ partials) {
+  __shared__ double sh[16 * 4];
+  double acc[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) acc[k] = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < c.paths; i += stride) {
+    const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
+    double v = c.v0, y = 0.0, sum_s = 0.0;
+    for (int j = 0; j < c.steps; j += 2) {
+      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, kAdjStreamTag), c.keys);
+      for (int o = 0; o < 2 && j + o < c.steps; ++o) {
+        const uint32_t ub = o ? r.z : r.x;
+        const double u = (double)of::uniform_from_u32(ub);
+        const double zx = (double)of::normal_from_u32(o ? r.w : r.y);
+        const double m = c.theta + (v - c.theta) * c.e;
+        const double s2 = v * c.c1 + c.c2;
+        const double psi = s2 / (m * m);
+        double vn;
+        if (psi <= 1.5) {
+          const double t = 2.0 / psi;
+          const double b2 = (t - 1.0) + sqrt(t * (t - 1.0));
+          const double a = m / (1.0 + b2);
+          const double bz = sqrt(b2) + (double)of::normal_from_u32(ub);
+          vn = a * bz * bz;
+        } else {
+          const double p = (psi - 1.0) / (psi + 1.0);
+          vn = (u <= p) ? 0.0 : m * log((1.0 - p) / (1.0 - u)) / (1.0 - p);
+        }
+        y = y + c.c0 + c.K1 * v + c.K2 * vn + sqrt(c.k34 * (v + vn)) * zx;
+        v = vn;
+        if (c.asian) sum_s += exp(y);
+      }
+    }
+    const double und = c.asian ? c.s0 * sum_s * c.inv_steps : c.s0 * exp(y);
+    const double intr = c.call ? und - c.strike : c.strike - und;
+    const double pv = intr > 0.0 ? c.disc * intr : 0.0;
+    acc[0] += pv;
+    acc[1] += pv * pv;
+  }
+  of::block_sum<16>(acc, sh);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 16; ++k) partials[(int64_t)blockIdx.x * 16 + k] = acc[k];
+}
+
 }  // namespace
 
 extern "C" of_status of_heston_price_adjoint(of_ctx* ctx, const of_heston_adjoint_params* p, of_adjoint_result* out) {
@@ -264,6 +322,8 @@ extern "C" of_status of_heston_price_adjoint(of_ctx* ctx, const of_heston_adjoin
   if (p->num_paths <= 0) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_paths must be > 0");
   if (p->num_steps <= 0) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_steps must be > 0");
   if (p->checkpoint_every != 32) return of_fail(ctx, OF_ERR_UNSUPPORTED, "checkpoint interval must be 32");
+  if (p->forward_only < 0 || p->forward_only > 2)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "forward_only must be 0, 1 or 2");
   if (p->num_steps > (int64_t)kMaxSegments * 32)
     return of_fail(ctx, OF_ERR_UNSUPPORTED, "at most %d steps", kMaxSegments * 32);
   if (!(p->spot > 0.0) || !(p->strike > 0.0) || !(p->expiry > 0.0))
@@ -321,8 +381,7 @@ extern "C" of_status of_heston_price_adjoint(of_ctx* ctx, const of_heston_adjoin
   c.asian = p->payoff == OF_PAYOFF_ASIAN;
   c.forward_only = p->forward_only ? 1 : 0;
   c.paths = p->num_paths;
-  c.k0 = (uint32_t)p->seed;
-  c.k1 = (uint32_t)(p->seed >> 32);
+  c.keys = of::philox_keys(p->seed);
 
   const int block = 128;
   const int64_t want = (p->num_paths + block - 1) / block;
@@ -333,7 +392,30 @@ extern "C" of_status of_heston_price_adjoint(of_ctx* ctx, const of_heston_adjoin
   OF_TRY(of_scratch(ctx, SLOT_SUMS, 16 * sizeof(double), &d_sums));
   OF_TRY(of_pinned(ctx, 16 * sizeof(double), &h));
   OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
-  adjoint_kernel<32><<<grid, block, 0, ctx->stream>>>(c, (double*)d_part);
+  if (p->forward_only == 2) {
+    AdjC64 d{};
+    d.e = e;
+    d.c1 = c1;
+    d.c2 = c2;
+    d.theta = th;
+    d.c0 = (p->rate - p->dividend_yield) * dt + K0;
+    d.K1 = K1;
+    d.K2 = K2;
+    d.k34 = k34;
+    d.s0 = p->spot;
+    d.strike = p->strike;
+    d.inv_steps = 1.0 / (double)p->num_steps;
+    d.disc = std::exp(-p->rate * p->expiry);
+    d.v0 = p->v0;
+    d.steps = (int32_t)p->num_steps;
+    d.call = c.call;
+    d.asian = c.asian;
+    d.paths = p->num_paths;
+    d.keys = c.keys;
+    forward64_kernel<<<grid, block, 0, ctx->stream>>>(d, (double*)d_part);
+  } else {
+    adjoint_kernel<32><<<grid, block, 0, ctx->stream>>>(c, (double*)d_part);
+  }
   OF_CUDA_TRY(ctx, cudaGetLastError());
   OF_TRY(of_reduce_rows(ctx, (const double*)d_part, grid, 16, (double*)d_sums));
   OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));

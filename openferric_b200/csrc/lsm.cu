@@ -156,7 +156,8 @@ struct LsmBatch {
   int32_t degree;
   int32_t want_delta;
   uint64_t seed;
-  uint32_t k0, k1, contract_base;
+  of::PhiloxKeys keys;
+  uint32_t contract_base;
   const double* inj;         // [nc][n][steps] or null
   const uint64_t* jump;      // jump tables
   int32_t chunk;             // paths per thread in the reference generator
@@ -198,7 +199,7 @@ __global__ void __launch_bounds__(128) lsm_gen_ref(LsmBatch B) {
 }
 
 // FP32 Philox generator: 4 consecutive paths per thread, float4 stores.
-__global__ void __launch_bounds__(256) lsm_gen_philox(LsmBatch B) {
+__global__ void __launch_bounds__(256) lsm_gen_philox(const __grid_constant__ LsmBatch B) {
   const int c = blockIdx.y;
   const LsmC C = B.c[c];
   const int64_t p0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
@@ -211,7 +212,7 @@ __global__ void __launch_bounds__(256) lsm_gen_philox(LsmBatch B) {
     if ((t & 3) == 0) {
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        r[q] = of::philox4x32_10(make_uint4((uint32_t)(t >> 2), (uint32_t)(p0 + q), cid, kLsmStreamTag), B.k0, B.k1);
+        r[q] = of::philox4x32_10(make_uint4((uint32_t)(t >> 2), (uint32_t)(p0 + q), cid, kLsmStreamTag), B.keys);
     }
     float4 out;
     float* o = &out.x;
@@ -717,8 +718,7 @@ extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_
     B.degree = cfg->basis_degree;
     B.want_delta = cfg->want_delta;
     B.seed = cfg->seed;
-    B.k0 = (uint32_t)cfg->seed;
-    B.k1 = (uint32_t)(cfg->seed >> 32);
+    B.keys = of::philox_keys(cfg->seed);
     B.contract_base = (uint32_t)batch[0];
     B.inj = (const double*)dInj;
     B.jump = jump;

@@ -58,13 +58,13 @@ StepConsts make_consts(const of_model* m) {
 // Simulates the terminal log-return of sample i (and of its antithetic twin).
 template <int MODEL, bool ANTI>
 __device__ __forceinline__ void simulate_terminal(const StepConsts& c, int32_t steps, uint64_t i, uint32_t stream,
-                                                  uint32_t k0, uint32_t k1, float& ya, float& yb) {
+                                                  const of::PhiloxKeys& K, float& ya, float& yb) {
   LegState a{0.0f, c.v0}, b{0.0f, c.v0};
   const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
   if (MODEL == OF_MODEL_GBM) {
     float wa = 0.0f;  // sum of normals; y_T = steps*drift + diff*sum
     for (int32_t j = 0; j < steps; j += 4) {
-      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo, hi, stream), k0, k1);
+      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo, hi, stream), K);
       wa += of::normal_from_u32(r.x);
       if (j + 1 < steps) wa += of::normal_from_u32(r.y);
       if (j + 2 < steps) wa += of::normal_from_u32(r.z);
@@ -75,7 +75,7 @@ __device__ __forceinline__ void simulate_terminal(const StepConsts& c, int32_t s
     yb = fmaf(-c.diff, wa, base);
   } else if (MODEL == OF_MODEL_HESTON_EULER) {
     for (int32_t j = 0; j < steps; j += 2) {
-      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, stream), k0, k1);
+      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, stream), K);
       float z1 = of::normal_from_u32(r.x), z2 = of::normal_from_u32(r.y);
       of::heston_euler_step(a, c, z1, z2);
       if (ANTI) of::heston_euler_step(b, c, -z1, -z2);
@@ -90,7 +90,7 @@ __device__ __forceinline__ void simulate_terminal(const StepConsts& c, int32_t s
     yb = b.y;
   } else {
     for (int32_t j = 0; j < steps; j += 2) {
-      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, stream), k0, k1);
+      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, stream), K);
       float u = of::uniform_from_u32(r.x), zx = of::normal_from_u32(r.y);
       of::heston_qe_step(a, c, u, 1.0f, zx, r.x);
       if (ANTI) of::heston_qe_step(b, c, 1.0f - u, -1.0f, -zx, r.x);
@@ -114,12 +114,13 @@ struct StripParams {
   int64_t samples;
   int32_t steps, n_strikes, option_type, antithetic;
   float s0;
-  uint32_t k0, k1;
+  of::PhiloxKeys keys;
   const float* strikes;
 };
 
 template <int KPL, int MODEL, bool ANTI>
-__global__ void __launch_bounds__(256) strip_kernel(StripParams P, double* __restrict__ partials) {
+__global__ void __launch_bounds__(256) strip_kernel(const __grid_constant__ StripParams P,
+                                                    double* __restrict__ partials) {
   extern __shared__ double sh_strip[];  // [warps][n_strikes][2]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   float K[KPL];
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(256) strip_kernel(StripParams P, double* __res
     float sa = 0.0f, sb = 0.0f;
     if (i < P.samples) {
       float ya, yb;
-      simulate_terminal<MODEL, ANTI>(P.c, P.steps, (uint64_t)i, kStripStreamTag, P.k0, P.k1, ya, yb);
+      simulate_terminal<MODEL, ANTI>(P.c, P.steps, (uint64_t)i, kStripStreamTag, P.keys, ya, yb);
       sa = P.s0 * __expf(ya);
       sb = P.s0 * __expf(yb);
     }
@@ -259,8 +260,7 @@ static of_status strip_setup(of_ctx* ctx, const of_model* m, int32_t option_type
   P.option_type = option_type;
   P.antithetic = cfg->antithetic ? 1 : 0;
   P.s0 = (float)m->s0;
-  P.k0 = (uint32_t)cfg->seed;
-  P.k1 = (uint32_t)(cfg->seed >> 32);
+  P.keys = of::philox_keys(cfg->seed);
   const int kpl = (int)((n_strikes + 31) / 32);
   const int kpl_t = kpl <= 1 ? 1 : (kpl <= 2 ? 2 : 4);
   pl->fn = kpl_t == 1 ? pick_strip<1>(m->kind, P.antithetic) : kpl_t == 2 ? pick_strip<2>(m->kind, P.antithetic)
@@ -412,7 +412,7 @@ struct BookParams {
   const float* obs_w;
   int32_t n_tiles;
   int32_t ppt;  // samples per thread per tile (tile = block * ppt samples)
-  uint32_t k0, k1;
+  of::PhiloxKeys keys;
   int* counter;
   double* partials;  // [slot][5]
 };
@@ -475,7 +475,7 @@ __device__ __forceinline__ void book_payoff(const BookOpt& o, const PathObs& ob,
 
 // One sample (and its antithetic twin) of option o; returns (x, y).
 template <int MODEL>
-__device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, uint32_t k0, uint32_t k1, const float* obs_w,
+__device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, const of::PhiloxKeys& K, const float* obs_w,
                                             float& x, float& cvy) {
   const bool anti = o.flags & BF_ANTI;
   const StepConsts& c = o.c;
@@ -487,7 +487,7 @@ __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, uint32
   const bool observe_each = (o.payoff != OF_PAYOFF_VANILLA) || (o.flags & (BF_NEED_ARITH | BF_NEED_GEO));
   constexpr int SPC = MODEL == OF_MODEL_GBM ? 4 : 2;  // steps per Philox call
   for (int32_t j = 0; j < o.steps; j += SPC) {
-    const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j / SPC), lo, hi, o.stream), k0, k1);
+    const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j / SPC), lo, hi, o.stream), K);
     const uint32_t rr[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
     for (int q = 0; q < SPC; ++q) {
@@ -520,7 +520,7 @@ __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, uint32
   }
 }
 
-__global__ void __launch_bounds__(256) book_kernel(BookParams P) {
+__global__ void __launch_bounds__(256) book_kernel(const __grid_constant__ BookParams P) {
   __shared__ int tile_sh;
   __shared__ double red_sh[5 * 8];
   for (;;) {
@@ -536,9 +536,9 @@ __global__ void __launch_bounds__(256) book_kernel(BookParams P) {
       if (local >= tile.count) break;
       const uint64_t i = (uint64_t)(tile.first + local);
       float x, y;
-      if (o.model == OF_MODEL_GBM) book_sample<OF_MODEL_GBM>(o, i, P.k0, P.k1, P.obs_w, x, y);
-      else if (o.model == OF_MODEL_HESTON_EULER) book_sample<OF_MODEL_HESTON_EULER>(o, i, P.k0, P.k1, P.obs_w, x, y);
-      else book_sample<OF_MODEL_HESTON_QE>(o, i, P.k0, P.k1, P.obs_w, x, y);
+      if (o.model == OF_MODEL_GBM) book_sample<OF_MODEL_GBM>(o, i, P.keys, P.obs_w, x, y);
+      else if (o.model == OF_MODEL_HESTON_EULER) book_sample<OF_MODEL_HESTON_EULER>(o, i, P.keys, P.obs_w, x, y);
+      else book_sample<OF_MODEL_HESTON_QE>(o, i, P.keys, P.obs_w, x, y);
       acc[0].add(x);
       acc[1].add(x * x);
       acc[2].add(y);
@@ -760,8 +760,7 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
   P.obs_w = pl->d_obs;
   P.n_tiles = (int32_t)nt;
   P.ppt = pl->ppt;
-  P.k0 = (uint32_t)cfg->seed;
-  P.k1 = (uint32_t)(cfg->seed >> 32);
+  P.keys = of::philox_keys(cfg->seed);
   P.counter = pl->d_counter;
   P.partials = pl->d_partials;
   const int per_sm = of_blocks_per_sm((const void*)book_kernel, pl->block, 0);

@@ -103,6 +103,36 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1
   return c;
 }
 
+// The ten round keys of a 64-bit seed, computed once on the host.  Kernels
+// carry them in their (constant-bank) parameters, so a round is two wide
+// multiplies and two three-input XORs with no key arithmetic.
+struct PhiloxKeys {
+  uint32_t k0[10], k1[10];
+};
+
+__host__ __device__ inline PhiloxKeys philox_keys(uint64_t seed) {
+  PhiloxKeys K;
+  uint32_t a = (uint32_t)seed, b = (uint32_t)(seed >> 32);
+  for (int r = 0; r < 10; ++r) {
+    K.k0[r] = a;
+    K.k1[r] = b;
+    a += 0x9E3779B9u;
+    b += 0xBB67AE85u;
+  }
+  return K;
+}
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, const PhiloxKeys& K) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+    c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ K.k0[r], (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ K.k1[r],
+                   (uint32_t)p0);
+  }
+  return c;
+}
+
 // u32 -> standard normal in FP32: u = (k + 0.5) 2^-23 with k the top 23 bits,
 // then Phi^-1(u) = x P(w), x = 2u-1, w = -log2((1+x)(1-x)) with the fitted
 // polynomials of invnorm_coeffs.h (one MUFU lg2 per draw; the tail branch,

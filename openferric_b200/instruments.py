@@ -217,8 +217,9 @@ class BermudanOption:
 
 
 def daily_fixings(expiry: float, steps: int) -> List[float]:
-    """Observation times at every simulation step 1..steps (daily fixings)."""
-    return [expiry * j / steps for j in range(1, steps + 1)]
+    """Observation times at every simulation step 1..steps (daily fixings);
+    the last one is the expiry exactly."""
+    return [expiry * (j / steps) for j in range(1, steps + 1)]
 
 
 __all__ = ["VanillaOption", "AsianOption", "BarrierOption", "BarrierOptionBuilder", "BermudanOption", "AsianSpec",

@@ -16,13 +16,15 @@ BASE = dict(spot=100.0, rate=0.03, v0=0.04, kappa=2.0, theta=0.04, xi=0.5, rho=-
 
 
 def crn_fd(spec, name, rel_bump=1e-4):
+    """Central difference with common random numbers: the FP64 price-only pass
+    on the same Philox draws (forward_only=2)."""
     p = dict(BASE)
     h = rel_bump * abs(p[name])
     up, dn = dict(p), dict(p)
     up[name] += h
     dn[name] -= h
-    pu = heston_adjoint(spec, forward_only=True, **up).price
-    pd = heston_adjoint(spec, forward_only=True, **dn).price
+    pu = heston_adjoint(spec, forward_only=2, **up).price
+    pd = heston_adjoint(spec, forward_only=2, **dn).price
     return (pu - pd) / (2 * h)
 
 
@@ -31,8 +33,10 @@ def test_adjoint_greeks_match_crn_central_differences(asian):
     spec = HestonAdjointSpec(strike=100.0, expiry=2.0 if asian else 1.0, num_paths=1 << 18,
                              num_steps=512 if asian else 256, seed=7, asian=asian)
     res = heston_adjoint(spec, **BASE)
-    fwd = heston_adjoint(spec, forward_only=True, **BASE)
+    fwd = heston_adjoint(spec, forward_only=1, **BASE)
+    fwd64 = heston_adjoint(spec, forward_only=2, **BASE)
     assert res.price == fwd.price  # the adjoint run prices the same paths
+    assert abs(fwd64.price - res.price) <= 1e-4 * abs(res.price)  # FP32 path error
     report = {}
     for name in A.OF_ADJ_NAMES:
         fd = crn_fd(spec, name)

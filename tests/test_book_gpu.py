@@ -37,9 +37,11 @@ def test_tile_shape_does_not_change_the_paths():
     a = price_book(book, seed=9, block=256, paths_per_thread=4)
     b = price_book(book, seed=9, block=128, paths_per_thread=1)
     c = price_book(book, seed=9, block=64, paths_per_thread=8)
+    # same per-sample draws; only the compensated-FP32 per-thread partial sums
+    # regroup, which moves the result at the FP32 rounding level
     for x, y, z in zip(a, b, c):
-        assert abs(x.price - y.price) <= 1e-9 * abs(x.price) + 1e-12
-        assert abs(x.price - z.price) <= 1e-9 * abs(x.price) + 1e-12
+        assert abs(x.price - y.price) <= 1e-6 * abs(x.price) + 1e-9
+        assert abs(x.price - z.price) <= 1e-6 * abs(x.price) + 1e-9
 
 
 def test_graph_replay_is_deterministic():
@@ -57,17 +59,32 @@ def test_graph_replay_is_deterministic():
 
 
 def test_book_control_variate_and_antithetic():
+    from openferric_b200.analytic import bs_price
+    from openferric_b200.core import OptionType
     book = synthetic_book(n=9, seed=4, min_log2_paths=15, max_log2_paths=15)
     plain = price_book(book, seed=2)
-    for vr in (VarianceReduction.Antithetic, VarianceReduction.ControlVariate):
-        b2 = [BookEntry(e.instrument, e.market, e.num_paths, e.num_steps, vr) for e in book]
-        res = price_book(b2, seed=2)
-        for p, r in zip(plain, res):
+    anti = price_book([BookEntry(e.instrument, e.market, e.num_paths, e.num_steps, VarianceReduction.Antithetic)
+                       for e in book], seed=2)
+    for p, r in zip(plain, anti):
+        assert abs(p.price - r.price) <= 5 * math.hypot(p.stderr, r.stderr) + 1e-3
+    cv = price_book([BookEntry(e.instrument, e.market, e.num_paths, e.num_steps, VarianceReduction.ControlVariate)
+                     for e in book], seed=2)
+    for k, (e, p, r) in enumerate(zip(book, plain, cv)):
+        if k % 3 == 0:
+            # The European's control variate is its own payoff (mc_engine.rs:458-485): the
+            # estimate collapses to the closed form and the variance to rounding level.
+            m = e.market
+            bs = bs_price(OptionType.Call, m.spot, e.instrument.strike, m.rate, 0.0,
+                          m.vol_for(e.instrument.strike, e.instrument.expiry), e.instrument.expiry)
+            assert abs(r.price - bs) <= 1e-6 * bs + 1e-9
+            assert math.isnan(r.stderr) or r.stderr <= 1e-4 * max(bs, 1.0)
+        elif k % 3 == 1:
+            # Asian: geometric control variate, much tighter than plain
             assert abs(p.price - r.price) <= 5 * math.hypot(p.stderr, r.stderr) + 1e-3
-        if vr is VarianceReduction.ControlVariate:
-            # European and Asian entries carry a control variate: tighter errors
-            for k in (0, 1, 3, 4):
-                assert res[k].stderr < plain[k].stderr
+            assert r.stderr < 0.5 * p.stderr
+        else:
+            # the barrier option has no control variate: same draws, same estimate
+            assert r.price == p.price
 
 
 def test_full_book_plan_info():
