@@ -325,6 +325,39 @@ typedef struct of_adjoint_result {
  * reference counterpart. */
 of_status of_heston_price_adjoint(of_ctx* ctx, const of_heston_adjoint_params* p, of_adjoint_result* out);
 
+/* ---- strike strip without any allocation --------------------------------- */
+/* No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory at call time.  Examples: a process whose HBM is
+ * already reserved in full by another allocator (a framework's caching pool),
+ * where a cudaMalloc would fail or fragment that pool; and latency-bound
+ * callers that cannot take cudaFree's implicit device-wide synchronisation.
+ * It creates no context, stream or event either.
+ *
+ * Same computation as of_mc_strip (FP32 Philox, one shared path set), with
+ * its scratch (strikes, per-block partial sums, final sums) in one static
+ * device array of OF_STRIP_NOALLOC_SCRATCH_BYTES that every GPU loading the
+ * library holds until the process exits.  Limits: at most
+ * OF_STRIP_NOALLOC_MAX_STRIKES strikes and OF_STRIP_NOALLOC_MAX_BLOCKS blocks
+ * (larger requests are rejected with OF_ERR_INVALID_INPUT and a message).
+ *
+ * Runs on the calling thread's current device and on `cuda_stream` (NULL =
+ * the legacy default stream), and returns when the results are on the host.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) once: make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams, other threads) race and must be serialised by the caller.  Every
+ * call overwrites all of the scratch it reads, so nothing needs clearing
+ * between calls.  `err`/`err_len` (may be NULL/0) receive the message of a
+ * failure; kernel_ms is not measured (0). */
+#define OF_STRIP_NOALLOC_MAX_STRIKES 64
+#define OF_STRIP_NOALLOC_MAX_BLOCKS 1024
+#define OF_STRIP_NOALLOC_SCRATCH_BYTES                            \
+  (OF_STRIP_NOALLOC_MAX_STRIKES * 4 + OF_STRIP_NOALLOC_MAX_STRIKES * 2 * 8 + \
+   OF_STRIP_NOALLOC_MAX_BLOCKS * OF_STRIP_NOALLOC_MAX_STRIKES * 2 * 8)
+of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* model, int32_t option_type,
+                              const double* strikes, int64_t n_strikes, const of_mc_config* cfg,
+                              of_mc_result* results, char* err, size_t err_len);
+
 /* ---- the reference's GPU European kernel ---------------------------------- */
 /* mc_european_gpu (src/engines/gpu/gpu_mc.rs:322-349, shader
  * src/engines/gpu/mc_shader.wgsl:28-142) on CUDA: f32 GBM paths, xoshiro128++,

@@ -22,7 +22,7 @@ EXPORTED = [
     "of_strip_plan_launch", "of_strip_plan_results", "of_strip_plan_destroy", "of_mc_price_book",
     "of_book_plan_create", "of_book_plan_launch", "of_book_plan_results", "of_book_plan_info",
     "of_book_plan_destroy", "of_mc_european_pathwise_aad", "of_heston_price_delta_aad", "of_mc_greek_estimators",
-    "of_lsm_price", "of_xoshiro_jump", "of_heston_price_adjoint", "of_mc_european_gpu",
+    "of_lsm_price", "of_xoshiro_jump", "of_heston_price_adjoint", "of_mc_european_gpu", "of_mc_strip_noalloc",
 ]
 
 
@@ -84,6 +84,9 @@ def _declare(L):
     L.of_mc_european_gpu.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int64,
                                      C.c_int64, C.c_uint32, C.c_int32, P(C.c_double), P(C.c_double)]
     L.of_mc_european_gpu.restype = C.c_int
+    L.of_mc_strip_noalloc.argtypes = [vp, P(A.OfModel), C.c_int32, P(C.c_double), C.c_int64, P(A.OfMcConfig),
+                                      P(A.OfMcResult), C.c_char_p, C.c_size_t]
+    L.of_mc_strip_noalloc.restype = C.c_int
     for name in ["of_ctx_create", "of_ctx_set_stream", "of_ctx_get_stream", "of_mc_run", "of_mc_strip",
                  "of_strip_plan_create", "of_strip_plan_launch", "of_strip_plan_results", "of_mc_price_book",
                  "of_book_plan_create", "of_book_plan_launch", "of_book_plan_results", "of_book_plan_info"]:

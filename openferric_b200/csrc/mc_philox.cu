@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -848,4 +849,152 @@ of_status of_mc_run_fp32(of_ctx* ctx, const of_model* m, const of_payoff* p, con
   bc.seed = c->seed;
   bc.use_graph = 0;
   return of_mc_price_book(ctx, &b, 1, &bc, out);
+}
+
+// ---------------------------------------------------------------------------
+// Strike strip without any allocation (of_mc_strip_noalloc).
+//
+// For callers that cannot allocate device memory when they price: every
+// byte of scratch the strip kernel needs lives in the static array below,
+// which each GPU that loads this library holds until the process exits.
+// Layout: [strikes: MAX_STRIKES floats][sums: 2*MAX_STRIKES doubles]
+//         [per-block partials: MAX_BLOCKS * 2*MAX_STRIKES doubles].
+// In host code `g_strip_noalloc_scratch` names a host-side stand-in, not the
+// device array: its device address is looked up with cudaGetSymbolAddress,
+// once per device with that device current, and that address is what the
+// kernels get.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_strip_noalloc_scratch[OF_STRIP_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+void* g_noalloc_addr[kNoallocMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+
+void noalloc_msg(char* err, size_t len, const char* fmt, ...) {
+  if (!err || len == 0) return;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(err, len, fmt, ap);
+  va_end(ap);
+}
+
+}  // namespace
+
+extern "C" of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* m, int32_t option_type,
+                                         const double* strikes, int64_t n_strikes, const of_mc_config* cfg,
+                                         of_mc_result* results, char* err, size_t err_len) {
+  if (err && err_len) err[0] = '\0';
+  if (!m || !cfg || !results || !strikes) {
+    noalloc_msg(err, err_len, "null argument");
+    return OF_ERR_INVALID_INPUT;
+  }
+  if (n_strikes <= 0 || n_strikes > OF_STRIP_NOALLOC_MAX_STRIKES) {
+    noalloc_msg(err, err_len, "n_strikes must be in [1, %d] (static scratch limit), got %lld",
+                OF_STRIP_NOALLOC_MAX_STRIKES, (long long)n_strikes);
+    return OF_ERR_INVALID_INPUT;
+  }
+  // Validation of of_mc_strip, restated without a context.
+  if (cfg->num_paths <= 0) return noalloc_msg(err, err_len, "num_paths must be > 0"), OF_ERR_INVALID_INPUT;
+  if (m->steps <= 0 || m->steps > 2147483647LL)
+    return noalloc_msg(err, err_len, "num_steps must be in [1, 2^31-1]"), OF_ERR_INVALID_INPUT;
+  if (!(m->maturity > 0.0) || !std::isfinite(m->maturity))
+    return noalloc_msg(err, err_len, "maturity must be finite and > 0"), OF_ERR_INVALID_INPUT;
+  if (!(m->s0 > 0.0) || !std::isfinite(m->s0) || !std::isfinite(m->mu))
+    return noalloc_msg(err, err_len, "spot must be > 0 and drift finite"), OF_ERR_INVALID_INPUT;
+  if (m->kind == OF_MODEL_GBM) {
+    if (!(m->sigma > 0.0) || !std::isfinite(m->sigma))
+      return noalloc_msg(err, err_len, "market volatility must be > 0"), OF_ERR_INVALID_INPUT;
+  } else if (m->kind == OF_MODEL_HESTON_EULER || m->kind == OF_MODEL_HESTON_QE) {
+    if (!(m->kappa > 0.0 && m->theta >= 0.0 && m->xi >= 0.0 && m->v0 >= 0.0 && m->rho > -1.0 && m->rho < 1.0))
+      return noalloc_msg(err, err_len, "invalid Heston parameters"), OF_ERR_INVALID_INPUT;
+    if (m->kind == OF_MODEL_HESTON_QE && !(m->xi > 0.0 && m->theta > 0.0))
+      return noalloc_msg(err, err_len, "the QE scheme needs xi > 0 and theta > 0"), OF_ERR_INVALID_INPUT;
+  } else {
+    return noalloc_msg(err, err_len, "unknown model kind %d", m->kind), OF_ERR_INVALID_INPUT;
+  }
+  if (option_type != OF_CALL && option_type != OF_PUT)
+    return noalloc_msg(err, err_len, "unknown option type %d", option_type), OF_ERR_INVALID_INPUT;
+  if (cfg->control_variate != OF_CV_NONE || cfg->injected_normals)
+    return noalloc_msg(err, err_len, "the strip has no control variate and no injected normals"),
+           OF_ERR_INVALID_INPUT;
+  if (!std::isfinite(cfg->discount_factor))
+    return noalloc_msg(err, err_len, "discount factor must be finite"), OF_ERR_INVALID_INPUT;
+  float hk[OF_STRIP_NOALLOC_MAX_STRIKES];
+  for (int64_t k = 0; k < n_strikes; ++k) {
+    if (!(strikes[k] > 0.0) || !std::isfinite(strikes[k]))
+      return noalloc_msg(err, err_len, "strike %lld must be finite and > 0", (long long)k), OF_ERR_INVALID_INPUT;
+    hk[k] = (float)strikes[k];
+  }
+
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) {
+    noalloc_msg(err, err_len, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+    return OF_ERR_CUDA;
+  }
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> guard(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_strip_noalloc_scratch);
+      if (e != cudaSuccess || !p) {
+        noalloc_msg(err, err_len, "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        return OF_ERR_CUDA;
+      }
+      g_noalloc_addr[dev] = p;
+    }
+    base = g_noalloc_addr[dev];
+  }
+  float* d_strikes = (float*)base;
+  double* d_sums = (double*)((char*)base + OF_STRIP_NOALLOC_MAX_STRIKES * 4);
+  double* d_partials = d_sums + OF_STRIP_NOALLOC_MAX_STRIKES * 2;
+
+  StripParams P{};
+  P.c = make_consts(m);
+  P.samples = cfg->antithetic ? (cfg->num_paths + 1) / 2 : cfg->num_paths;
+  P.steps = (int32_t)m->steps;
+  P.n_strikes = (int32_t)n_strikes;
+  P.option_type = option_type;
+  P.antithetic = cfg->antithetic ? 1 : 0;
+  P.s0 = (float)m->s0;
+  P.keys = of::philox_keys(cfg->seed);
+  P.strikes = d_strikes;
+  const StripKernelFn fn = n_strikes <= 32 ? pick_strip<1>(m->kind, P.antithetic) : pick_strip<2>(m->kind, P.antithetic);
+  const int block = 256;
+  const size_t smem = (size_t)(block / 32) * n_strikes * 2 * sizeof(double);
+  int sms = 0, per_sm = 0;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, block, smem)) != cudaSuccess) {
+    noalloc_msg(err, err_len, "device query failed: %s", cudaGetErrorString(e));
+    return OF_ERR_CUDA;
+  }
+  const int64_t want = (P.samples + block - 1) / block;
+  int64_t grid = std::min<int64_t>(want, (int64_t)sms * std::max(per_sm, 1));
+  grid = std::max<int64_t>(1, std::min<int64_t>(grid, OF_STRIP_NOALLOC_MAX_BLOCKS));
+
+  cudaStream_t s = (cudaStream_t)cuda_stream;
+  const int64_t cols = 2 * n_strikes;
+  double hs[2 * OF_STRIP_NOALLOC_MAX_STRIKES];
+  if ((e = cudaMemcpyAsync(d_strikes, hk, (size_t)n_strikes * sizeof(float), cudaMemcpyHostToDevice, s)) !=
+      cudaSuccess) {
+    noalloc_msg(err, err_len, "strike upload failed: %s", cudaGetErrorString(e));
+    return OF_ERR_CUDA;
+  }
+  fn<<<(unsigned)grid, block, smem, s>>>(P, d_partials);
+  of_launch_reduce_rows(d_partials, grid, cols, d_sums, s);
+  if ((e = cudaGetLastError()) != cudaSuccess ||
+      (e = cudaMemcpyAsync(hs, d_sums, (size_t)cols * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+    noalloc_msg(err, err_len, "strip launch failed: %s", cudaGetErrorString(e));
+    return OF_ERR_CUDA;
+  }
+  for (int64_t k = 0; k < n_strikes; ++k) {
+    const double sums[5] = {hs[2 * k], hs[2 * k + 1], 0.0, 0.0, 0.0};
+    of_mc_finish(sums, P.samples, OF_CV_NONE, 0.0, cfg->discount_factor, &results[k]);
+    results[k].kernel_ms = 0.0;
+  }
+  return OF_OK;
 }

@@ -1,0 +1,55 @@
+"""The no-allocation strike strip (of_mc_strip_noalloc), called through the C ABI.
+
+Some callers cannot allocate device memory when they price: their HBM is
+already reserved in full by another allocator, or they cannot take the
+device-wide synchronisation of cudaFree.  This entry point serves them from a
+static device array instead.  The test checks its output against the existing
+entry point (of_mc_strip, which draws its scratch from the context's pool) on
+two calls in a row, so that the second call also sees the array the first one
+left behind.  It runs last (file name) and passes alone or after the rest of
+the suite.
+"""
+import ctypes as C
+import math
+
+import pytest
+
+from openferric_b200 import Heston, HestonPathGenerator, OptionType, price_strike_strip
+from openferric_b200 import _abi as A
+from openferric_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+STRIKES = [80.0 + 2.0 * k for k in range(21)]
+
+
+def noalloc_strip(model, option_type, strikes, num_paths, seed, df):
+    L = _lib.load()
+    ks =(C.c_double * len(strikes))(*strikes)
+    cfg = A.OfMcConfig(num_paths=num_paths, seed=seed, precision=A.OF_PREC_FP32_PHILOX, discount_factor=df)
+    out = (A.OfMcResult * len(strikes))()
+    err = C.create_string_buffer(256)
+    st = L.of_mc_strip_noalloc(None, C.byref(model), option_type, ks, len(strikes), C.byref(cfg), out, err,
+                               len(err))
+    return st, err.value.decode(), [(r.price, r.stderr_) for r in out]
+
+
+def test_noalloc_strip_matches_existing_entry_point_on_two_calls():
+    gen = HestonPathGenerator(Heston(0.03, 2.0, 0.04, 0.5, -0.7, 0.04), 100.0, 1.0, 64)
+    df = math.exp(-0.03)
+    ref = price_strike_strip(gen, OptionType.Call, STRIKES, 1 << 18, 7, df)
+    for _ in range(2):
+        st, msg, got = noalloc_strip(gen.to_abi(), A.OF_CALL, STRIKES, 1 << 18, 7, df)
+        assert st == A.OF_OK, msg
+        for (p, s), (rp, rs) in zip(got, ref):
+            # same kernel, same draws: equal up to the FP32 partial-sum grouping
+            assert abs(p - rp) <= 1e-9 * abs(rp) + 1e-12, (p, rp)
+            assert abs(s - rs) <= 1e-9 * abs(rs) + 1e-12
+
+
+def test_noalloc_strip_rejects_sizes_beyond_its_static_scratch():
+    gen = HestonPathGenerator(Heston(0.03, 2.0, 0.04, 0.5, -0.7, 0.04), 100.0, 1.0, 8)
+    too_many = [90.0 + 0.1 * k for k in range(65)]
+    st, msg, _ = noalloc_strip(gen.to_abi(), A.OF_CALL, too_many, 1 << 10, 1, 1.0)
+    assert st == A.OF_ERR_INVALID_INPUT
+    assert "64" in msg
