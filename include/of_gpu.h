@@ -302,6 +302,12 @@ typedef struct of_heston_adjoint_params {
                                common random numbers: a 1e-4 relative bump is below the FP32
                                resolution of the path state) */
   int32_t reserved0;
+  /* Half-width of the band around psi_c = 1.5 in which the QE step blends its
+   * quadratic and exponential branches (smoothstep).  0 = Andersen's hard
+   * switch, whose jump in v' a pathwise derivative cannot see; > 0 makes the
+   * step continuous, so the adjoint Greeks are unbiased for the scheme they
+   * differentiate.  At most 0.25. */
+  double qe_switch_band;
 } of_heston_adjoint_params;
 
 enum {

@@ -202,6 +202,7 @@ class OfHestonAdjointParams(C.Structure):
         ("checkpoint_every", C.c_int32),
         ("forward_only", C.c_int32),
         ("reserved0", C.c_int32),
+        ("qe_switch_band", C.c_double),
     ]
 
 

@@ -45,6 +45,9 @@ class HestonAdjointSpec:
     asian: bool = True
     dividend_yield: float = 0.0
     checkpoint_every: int = 32
+    # Half-width of the smoothed QE branch switch around psi_c = 1.5 (0 = hard switch,
+    # whose jump a pathwise derivative cannot see; see include/of_gpu.h).
+    qe_switch_band: float = 0.05
 
 
 def _params(spec: HestonAdjointSpec, spot, rate, v0, kappa, theta, xi, rho, forward_only=False):
@@ -54,7 +57,8 @@ def _params(spec: HestonAdjointSpec, spot, rate, v0, kappa, theta, xi, rho, forw
         v0=float(v0), num_paths=int(spec.num_paths), num_steps=int(spec.num_steps),
         seed=int(spec.seed) & 0xFFFFFFFFFFFFFFFF, option_type=spec.option_type.value,
         payoff=A.OF_PAYOFF_ASIAN if spec.asian else A.OF_PAYOFF_VANILLA, scheme=A.OF_MODEL_HESTON_QE,
-        checkpoint_every=int(spec.checkpoint_every), forward_only=int(forward_only))
+        checkpoint_every=int(spec.checkpoint_every), forward_only=int(forward_only),
+        qe_switch_band=float(spec.qe_switch_band))
 
 
 def heston_adjoint(spec: HestonAdjointSpec, spot: float, rate: float, v0: float, kappa: float, theta: float,

@@ -62,7 +62,8 @@ def main():
                                   2 ** 23 - 1 - np.arange(0, 2 ** 16)]))
     u = ((k.astype(np.float64) + 0.5) * 2.0 ** -23).astype(np.float32)
     x = (np.float32(2.0) * u - np.float32(1.0)).astype(np.float32)
-    tt = (np.float32(4.0) * u * (np.float32(1.0) - u)).astype(np.float32)
+    # the kernel forms t = fmaf(-x, x, 1): 1 - x^2 rounded once from the exact value
+    tt = (1.0 - x.astype(np.float64) ** 2).astype(np.float32)
     w = (-np.log2(tt.astype(np.float64))).astype(np.float32)
     p = np.where(w < W_SPLIT, horner32(cc, (w - np.float32(c_center)).astype(np.float32)),
                  horner32(tc, (np.sqrt(w) - np.float32(t_center)).astype(np.float32)))

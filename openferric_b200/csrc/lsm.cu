@@ -34,7 +34,7 @@ namespace {
 
 constexpr uint32_t kLsmStreamTag = 0x4C534D31u;  // "LSM1"
 constexpr int kPassThreads = 256;
-constexpr int kPathsPerThread = 4;
+constexpr int kPathsPerThread = 16;
 constexpr int kPathsPerBlock = kPassThreads * kPathsPerThread;
 constexpr int kMaxMoments = 12;  // degree 3: x^0..x^6 (7) + y x^0..x^3 (4) ; degree 2: 8
 
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(kPassThreads) lsm_pass(LsmBatch B, int t) {
   for (int q = 0; q < kPathsPerThread; ++q) {
     const int64_t p = base + q * kPassThreads + threadIdx.x;
     if (p >= B.n) break;
-    double v = (double)V[p], dv = (double)dV[p];
+    double v = (double)V[p], dv = B.want_delta ? (double)dV[p] : 0.0;
     if (have_beta) {
       const double s1 = (double)S[(size_t)t * B.npad + p];  // spot at date t+1
       const double ex = intrinsic_v<double>(C.put, s1, C.strike);
@@ -414,23 +414,27 @@ __global__ void __launch_bounds__(kPassThreads) lsm_pass(LsmBatch B, int t) {
       }
     }
     V[p] = (T)v;
-    dV[p] = (T)dv;
+    if (B.want_delta) dV[p] = (T)dv;
   }
   if (!ex_now) return;
-  // block reduction of the moments (fixed order) -> partials
+  // block reduction of all moments with one barrier: warp shuffles, then one
+  // thread per moment sums the warps in a fixed order -> partials
   double* part = B.partials + ((size_t)c * B.blocks + blockIdx.x) * kMaxMoments;
-  for (int k = 0; k < nm; ++k) {
-    double w = of::warp_sum(mom[k]);
-    if ((threadIdx.x & 31) == 0) red_sh[threadIdx.x >> 5] = w;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double acc = 0.0;
-      for (int i = 0; i < kPassThreads / 32; ++i) acc += red_sh[i];
-      part[k] = acc;
+#pragma unroll
+  for (int k = 0; k < kMaxMoments; ++k) {
+    if (k < nm) {
+      const double w = of::warp_sum(mom[k]);
+      if ((threadIdx.x & 31) == 0) red_sh[(threadIdx.x >> 5) * kMaxMoments + k] = w;
     }
-    __syncthreads();
   }
-  __threadfence();
+  __syncthreads();
+  if ((int)threadIdx.x < nm) {
+    double acc = 0.0;
+    for (int i = 0; i < kPassThreads / 32; ++i) acc += red_sh[i * kMaxMoments + threadIdx.x];
+    part[threadIdx.x] = acc;
+    __threadfence();
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
     const uint32_t done = atomicAdd(B.counters + c, 1u);
     is_last = done == (uint32_t)B.blocks - 1;
@@ -466,7 +470,7 @@ __global__ void __launch_bounds__(kPassThreads) lsm_final(LsmBatch B) {
   for (int q = 0; q < kPathsPerThread; ++q) {
     const int64_t p = base + q * kPassThreads + threadIdx.x;
     if (p >= B.n) break;
-    double v = (double)V[p], dv = (double)dV[p];
+    double v = (double)V[p], dv = B.want_delta ? (double)dV[p] : 0.0;
     if (have_beta) {
       const double s1 = (double)S[p];  // spot at date 1
       const double ex = intrinsic_v<double>(C.put, s1, C.strike);

@@ -35,6 +35,7 @@ StepConsts make_consts(const of_model* m) {
   c.sqdt = (float)sqdt;
   c.kdt = (float)(m->kappa * dt);
   c.kdt_theta = (float)(m->kappa * m->theta * dt);
+  c.one_m_kdt = (float)(1.0 - m->kappa * dt);
   c.xi_sqdt = (float)(m->xi * sqdt);
   c.rho = (float)m->rho;
   c.rho_c = (float)std::sqrt(1.0 - m->rho * m->rho);
@@ -75,17 +76,22 @@ __device__ __forceinline__ void simulate_terminal(const StepConsts& c, int32_t s
     ya = fmaf(c.diff, wa, base);
     yb = fmaf(-c.diff, wa, base);
   } else if (MODEL == OF_MODEL_HESTON_EULER) {
-    for (int32_t j = 0; j < steps; j += 2) {
-      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, stream), K);
+    const int32_t pairs = steps >> 1;  // full Philox calls; an odd last step below
+    for (int32_t q = 0; q < pairs; ++q) {
+      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)q, lo, hi, stream), K);
       float z1 = of::normal_from_u32(r.x), z2 = of::normal_from_u32(r.y);
       of::heston_euler_step(a, c, z1, z2);
       if (ANTI) of::heston_euler_step(b, c, -z1, -z2);
-      if (j + 1 < steps) {
-        z1 = of::normal_from_u32(r.z);
-        z2 = of::normal_from_u32(r.w);
-        of::heston_euler_step(a, c, z1, z2);
-        if (ANTI) of::heston_euler_step(b, c, -z1, -z2);
-      }
+      z1 = of::normal_from_u32(r.z);
+      z2 = of::normal_from_u32(r.w);
+      of::heston_euler_step(a, c, z1, z2);
+      if (ANTI) of::heston_euler_step(b, c, -z1, -z2);
+    }
+    if (steps & 1) {
+      const uint4 r = of::philox4x32_10(make_uint4((uint32_t)pairs, lo, hi, stream), K);
+      const float z1 = of::normal_from_u32(r.x), z2 = of::normal_from_u32(r.y);
+      of::heston_euler_step(a, c, z1, z2);
+      if (ANTI) of::heston_euler_step(b, c, -z1, -z2);
     }
     ya = a.y;
     yb = b.y;

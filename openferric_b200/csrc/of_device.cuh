@@ -140,7 +140,7 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, const PhiloxKeys& K) {
 __device__ __forceinline__ float normal_from_u32(uint32_t r) {
   const float f = __uint_as_float(0x3F800000u | (r >> 9));  // 1 + k 2^-23, exact
   const float x = fmaf(2.0f, f, -3.0f) + 1.1920928955078125e-7f;  // (2k + 1 - 2^23) 2^-23, exact
-  const float t = (1.0f + x) * (1.0f - x);
+  const float t = fmaf(-x, x, 1.0f);  // 1 - x^2 = 4u(1-u), one rounding of the exact value
   const float w = -__log2f(t);
   float p;
   if (w < OF_INVN_W_SPLIT) {

@@ -16,7 +16,7 @@ struct StepConsts {
   // Heston Euler of the reference (src/models/stochastic.rs:56-71, with the
   // variance floored after every step as src/mc/simulation.rs:111-113 does):
   // y += mudt - half_dt v + sqdt sqrt(v) zs ; v = max(v + kdt_theta - kdt v + xi_sqdt sqrt(v) z1, 0)
-  float mudt, half_dt, sqdt, kdt, kdt_theta, xi_sqdt, rho, rho_c, v0, y_floor;
+  float mudt, half_dt, sqdt, kdt, kdt_theta, xi_sqdt, rho, rho_c, v0, y_floor, one_m_kdt;
   // Heston QE (Andersen 2008, gamma1 = gamma2 = 1/2, psi_c = 1.5)
   float qe_e, qe_c1, qe_c2, qe_theta, qe_k0, qe_k1, qe_k2, qe_k3, qe_k4;
 };
@@ -30,7 +30,8 @@ __device__ __forceinline__ void heston_euler_step(LegState& L, const StepConsts&
   const float sq = sqrtf(L.v);
   const float zs = fmaf(c.rho, z1, c.rho_c * z2);
   const float y = fmaf(c.sqdt * sq, zs, fmaf(-c.half_dt, L.v, L.y + c.mudt));
-  const float vn = fmaf(c.xi_sqdt * sq, z1, fmaf(-c.kdt, L.v, L.v + c.kdt_theta));
+  // v + kappa (theta - v) dt = (1 - kappa dt) v + kappa theta dt
+  const float vn = fmaf(c.xi_sqdt * sq, z1, fmaf(c.one_m_kdt, L.v, c.kdt_theta));
   L.v = fmaxf(vn, 0.0f);
   L.y = fmaxf(y, c.y_floor);
 }
