@@ -170,6 +170,108 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+ADJ_HESTON = dict(spot=100.0, rate=0.03, v0=0.04, kappa=2.0, theta=0.04, xi=0.5, rho=-0.7)
+
+
+def greeks_comparison(paths=PATHS, steps=512, reps=3):
+    """Priced + full-Greeks options/s for one Heston arithmetic Asian call
+    (K=100, T=2, daily fixings at all 512 steps, the parameters of the strip):
+    FP32 QE + checkpointed adjoint (one call) against the plain FP64 engine
+    (the reference-stream Euler engine) with the 7 Greeks by central bumps
+    with common random numbers (15 runs).  Both at the same path count; the
+    standard error of both is below 1e-4 S0 = 0.01."""
+    import openferric_b200 as of
+    from openferric_b200.adjoint import HestonAdjointSpec, heston_adjoint
+    spec = HestonAdjointSpec(strike=100.0, expiry=2.0, num_paths=paths, num_steps=steps, seed=SEED, asian=True)
+    heston_adjoint(spec, **ADJ_HESTON)
+    adj = [heston_adjoint(spec, **ADJ_HESTON) for _ in range(reps)]
+    t_adj = min(a.kernel_ms for a in adj)
+    obs = [2.0 * (j / steps) for j in range(1, steps + 1)]
+    opt = of.AsianOption(of.OptionType.Call, 100.0, 2.0, of.AsianSpec(of.Averaging.Arithmetic, of.StrikeType.Fixed, obs))
+
+    def fp64_run(p):
+        gen = of.HestonPathGenerator(of.Heston(p["rate"], p["kappa"], p["theta"], p["xi"], p["rho"], p["v0"]),
+                                     p["spot"], 2.0, steps)
+        eng = of.MonteCarloEngine(paths, SEED)
+        r = eng.run_full(gen, opt, math.exp(-2.0 * p["rate"]))
+        return r.price, r.stderr_, r.kernel_ms
+
+    fp64_run(ADJ_HESTON)
+    t64, base_se = 0.0, None
+    for name in [None] + list(ADJ_HESTON):
+        for sgn in ((0,) if name is None else (1, -1)):
+            p = dict(ADJ_HESTON)
+            if name is not None:
+                p[name] *= 1.0 + sgn * 1e-4
+            price, se, ms = fp64_run(p)
+            t64 += ms
+            if name is None:
+                base_se = se
+    return {"workload": "heston_qe_asian_adjoint", "paths": paths, "steps": steps, "strike": 100.0, "T": 2.0,
+            "fp32_adjoint_ms": t_adj, "fp32_adjoint_options_per_s": 1e3 / t_adj,
+            "fp32_adjoint_price": adj[0].price, "fp32_adjoint_se": adj[0].stderr,
+            "fp64_plain_bump_ms": t64, "fp64_plain_bump_options_per_s": 1e3 / t64, "fp64_plain_se": base_se,
+            "speedup": t64 / t_adj, "greeks": adj[0].greeks}
+
+
+def run_workload(args, local_rank):
+    """Single-GPU lines for configurations 3-5 (not the headline)."""
+    import torch
+    import numpy as np
+    import openferric_b200 as of
+    torch.cuda.set_device(local_rank)
+    if args.workload == "adjoint":
+        g = greeks_comparison(args.paths)
+        line = {"metric": "priced+Greeks options/s at SE<=1e-4*S0", "value": g["fp32_adjoint_options_per_s"],
+                "unit": "options/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+                "config": g}
+    elif args.workload == "book":
+        from openferric_b200.book import BookPlan, synthetic_book
+        plan = BookPlan(synthetic_book(), seed=20261203)
+        info = plan.info()
+        for _ in range(max(1, args.warmup)):
+            plan.launch()
+        plan.raw_results()
+        ctx = of.context(local_rank)
+        stream = torch.cuda.ExternalStream(ctx.stream_ptr())
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for s, e in ev:
+            s.record(stream)
+            plan.launch()
+            e.record(stream)
+        stream.synchronize()
+        ms = statistics.median(s.elapsed_time(e) for s, e in ev)
+        plan.close()
+        line = {"metric": "path-steps/s", "value": info["path_steps"] / (ms / 1e3), "unit": "path-steps/s",
+                "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic", "ms_per_step": ms,
+                "config": {"workload": "batched_book_4096", "tiles": info["tiles"], "block": info["block"],
+                           "paths_per_thread": info["paths_per_thread"], "path_steps": info["path_steps"],
+                           "options_per_s": 4096 / (ms / 1e3), "cuda_graph": True}}
+    else:  # lsm
+        from openferric_b200.lsm import LongstaffSchwartzEngine
+        rng = np.random.default_rng(20261203)
+        items = []
+        for i in range(256):
+            vol, T = (0.2, 0.4)[i % 2], (1.0, 2.0)[(i // 2) % 2]
+            m = of.Market.builder().spot(rng.uniform(30.0, 50.0)).rate(0.06).flat_vol(vol).build()
+            items.append((of.VanillaOption.american_put(40.0, T), m))
+        total_ms, alg_bytes = 0.0, 0.0
+        for T in (1.0, 2.0):
+            sub = [it for it in items if it[0].expiry == T]
+            eng = LongstaffSchwartzEngine(args.paths, int(50 * T), SEED).with_precision(
+                of.Precision.Fp32Philox).with_basis_degree(3)
+            eng.price_batch(sub[:2], with_delta=True)
+            eng.price_batch(sub, with_delta=True)
+            total_ms += eng.last_kernel_ms
+            alg_bytes += len(sub) * float(args.paths) * int(50 * T) * 16.0
+        line = {"metric": "LSM contracts/s (price + delta)", "value": 256 / (total_ms / 1e3), "unit": "contracts/s",
+                "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic", "ms_per_step": total_ms,
+                "config": {"workload": "lsm_american_put_256", "paths": args.paths, "dates_per_year": 50,
+                           "basis": "1,x,x^2,x^3 (x=S/K), Cholesky", "algorithmic_bytes": alg_bytes,
+                           "algorithmic_GBps": alg_bytes / (total_ms / 1e3) / 1e9}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -177,6 +279,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-greeks", action="store_true", help="skip the adjoint vs FP64-bump comparison")
+    ap.add_argument("--workload", default="strip", choices=["strip", "adjoint", "book", "lsm"],
+                    help="strip is the benchmark line; the others are single-GPU lines for configurations 3-5")
     ap.add_argument("--paths", type=int, default=PATHS,
                     help="paths per strip (profiling a smaller case; the benchmark workload is 2^20)")
     args = ap.parse_args()
@@ -186,6 +291,8 @@ def main():
     rank, world, local_rank = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload != "strip":
+        return run_workload(args, local_rank) if rank == 0 else None
 
     import torch
     import openferric_b200 as of
@@ -272,6 +379,9 @@ def main():
         "check": {"price_K100": prices[20][0], "stderr_K100": prices[20][1],
                   "e2e_price_K100": e2e_prices[20][0]},
     }
+    if rank == 0 and not args.no_greeks:
+        # the priced+Greeks part of the metric (outside the timed region)
+        line["greeks"] = greeks_comparison()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, sample = cpu_sample(os.cpu_count() or 1, 10.0)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",

@@ -34,7 +34,7 @@ namespace {
 
 constexpr uint32_t kLsmStreamTag = 0x4C534D31u;  // "LSM1"
 constexpr int kPassThreads = 256;
-constexpr int kPathsPerThread = 16;
+constexpr int kPathsPerThread = 8;
 constexpr int kPathsPerBlock = kPassThreads * kPathsPerThread;
 constexpr int kMaxMoments = 12;  // degree 3: x^0..x^6 (7) + y x^0..x^3 (4) ; degree 2: 8
 
@@ -350,6 +350,45 @@ __device__ void last_block_reduce(const LsmBatch& B, int c, int nm, double* mome
   }
 }
 
+// One path of a pass: exercise at date t+1 (spot s1) with the betas of that
+// date, discount one step, and the in-the-money basis moments at date t
+// (spot s0, longstaff_schwartz.rs:543-601).
+__device__ __forceinline__ void lsm_path_update(const LsmBatch& B, const LsmC& C, const double* beta, bool have_beta,
+                                                bool ex_now, double s1, double s0, double& v, double& dv,
+                                                double* mom) {
+  if (have_beta) {
+    const double ex = intrinsic_v<double>(C.put, s1, C.strike);
+    if (ex > 0.0 && ex > continuation(B.degree, beta, s1, C.inv_strike)) {
+      v = ex;
+      dv = C.put ? -s1 * C.inv_spot : s1 * C.inv_spot;
+    }
+  }
+  v *= C.disc;
+  dv *= C.disc;
+  if (ex_now && intrinsic_v<double>(C.put, s0, C.strike) > 0.0) {
+    if (B.degree == 2) {
+      const double s2 = s0 * s0;
+      mom[0] += 1.0;
+      mom[1] += s0;
+      mom[2] += s2;
+      mom[3] += s2 * s0;
+      mom[4] += s2 * s2;
+      mom[5] += v;
+      mom[6] += s0 * v;
+      mom[7] += s2 * v;
+    } else {
+      const double x = s0 * C.inv_strike;
+      double pw = 1.0;
+#pragma unroll
+      for (int e = 0; e < 7; ++e) {
+        mom[e] += pw;
+        if (e < 4) mom[7 + e] += pw * v;
+        pw *= x;
+      }
+    }
+  }
+}
+
 // One exercise date t (1 <= t <= steps-1): exercise(t+1), discount, moments(t).
 template <typename T>
 __global__ void __launch_bounds__(kPassThreads) lsm_pass(LsmBatch B, int t) {
@@ -373,48 +412,54 @@ __global__ void __launch_bounds__(kPassThreads) lsm_pass(LsmBatch B, int t) {
 #pragma unroll
   for (int k = 0; k < kMaxMoments; ++k) mom[k] = 0.0;
   const int64_t base = (int64_t)blockIdx.x * kPathsPerBlock;
+  if constexpr (sizeof(T) == 4) {
+    // FP32 store: 4 groups of 4 consecutive paths per thread; every float4
+    // load of the pass is issued before any of them is used.
+    constexpr int G = kPathsPerThread / 4;
+    const float4* S1 = reinterpret_cast<const float4*>(S + (size_t)t * B.npad);
+    const float4* S0 = reinterpret_cast<const float4*>(S + (size_t)(t - 1) * B.npad);
+    float4* V4 = reinterpret_cast<float4*>(V);
+    float4* D4 = reinterpret_cast<float4*>(dV);
+    float4 v4[G], d4[G], a4[G], b4[G];
 #pragma unroll
-  for (int q = 0; q < kPathsPerThread; ++q) {
-    const int64_t p = base + q * kPassThreads + threadIdx.x;
-    if (p >= B.n) break;
-    double v = (double)V[p], dv = B.want_delta ? (double)dV[p] : 0.0;
-    if (have_beta) {
-      const double s1 = (double)S[(size_t)t * B.npad + p];  // spot at date t+1
-      const double ex = intrinsic_v<double>(C.put, s1, C.strike);
-      if (ex > 0.0 && ex > continuation(B.degree, beta, s1, C.inv_strike)) {
-        v = ex;
-        dv = C.put ? -s1 * C.inv_spot : s1 * C.inv_spot;
-      }
+    for (int g = 0; g < G; ++g) {
+      const int64_t q = base / 4 + g * kPassThreads + threadIdx.x;
+      v4[g] = V4[q];
+      d4[g] = B.want_delta ? D4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+      a4[g] = have_beta ? S1[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+      b4[g] = ex_now ? S0[q] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    v *= C.disc;
-    dv *= C.disc;
-    if (ex_now) {
-      const double s0 = (double)S[(size_t)(t - 1) * B.npad + p];  // spot at date t
-      if (intrinsic_v<double>(C.put, s0, C.strike) > 0.0) {
-        if (B.degree == 2) {
-          const double s2 = s0 * s0;
-          mom[0] += 1.0;
-          mom[1] += s0;
-          mom[2] += s2;
-          mom[3] += s2 * s0;
-          mom[4] += s2 * s2;
-          mom[5] += v;
-          mom[6] += s0 * v;
-          mom[7] += s2 * v;
-        } else {
-          const double x = s0 * C.inv_strike;
-          double pw = 1.0;
 #pragma unroll
-          for (int e = 0; e < 7; ++e) {
-            mom[e] += pw;
-            if (e < 4) mom[7 + e] += pw * v;
-            pw *= x;
-          }
-        }
+    for (int g = 0; g < G; ++g) {
+      const int64_t p0 = base + ((int64_t)g * kPassThreads + threadIdx.x) * 4;
+      float* vv = &v4[g].x;
+      float* dd = &d4[g].x;
+      const float* s1 = &a4[g].x;
+      const float* s0 = &b4[g].x;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (p0 + e >= B.n) continue;  // padding
+        double v = vv[e], dv = dd[e];
+        lsm_path_update(B, C, beta, have_beta, ex_now, s1[e], s0[e], v, dv, mom);
+        vv[e] = (float)v;
+        dd[e] = (float)dv;
       }
+      const int64_t q = base / 4 + g * kPassThreads + threadIdx.x;
+      V4[q] = v4[g];
+      if (B.want_delta) D4[q] = d4[g];
     }
-    V[p] = (T)v;
-    if (B.want_delta) dV[p] = (T)dv;
+  } else {
+#pragma unroll
+    for (int q = 0; q < kPathsPerThread; ++q) {
+      const int64_t p = base + q * kPassThreads + threadIdx.x;
+      if (p >= B.n) break;
+      double v = (double)V[p], dv = B.want_delta ? (double)dV[p] : 0.0;
+      const double s1 = have_beta ? (double)S[(size_t)t * B.npad + p] : 0.0;      // spot at date t+1
+      const double s0 = ex_now ? (double)S[(size_t)(t - 1) * B.npad + p] : 0.0;  // spot at date t
+      lsm_path_update(B, C, beta, have_beta, ex_now, s1, s0, v, dv, mom);
+      V[p] = (T)v;
+      if (B.want_delta) dV[p] = (T)dv;
+    }
   }
   if (!ex_now) return;
   // block reduction of all moments with one barrier: warp shuffles, then one
