@@ -108,7 +108,7 @@ typedef struct of_mc_config {
   int32_t antithetic; /* 0/1 */
   int32_t precision; /* OF_PREC_* */
   int32_t control_variate; /* OF_CV_* */
-  int32_t reserved0;
+  int32_t tile_ilp; /* FP32 strip: samples in flight per thread (0 = default, 1 or 2) */
   double cv_expected; /* E[Y] of the control variate, undiscounted */
   double discount_factor;
   /* Test hook (the injection point PathGenerator::generate_from_normals,

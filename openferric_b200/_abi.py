@@ -66,7 +66,7 @@ class OfMcConfig(C.Structure):
         ("antithetic", C.c_int32),
         ("precision", C.c_int32),
         ("control_variate", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("tile_ilp", C.c_int32),
         ("cv_expected", C.c_double),
         ("discount_factor", C.c_double),
         ("injected_normals", C.POINTER(C.c_double)),

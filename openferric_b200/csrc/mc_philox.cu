@@ -113,6 +113,81 @@ __device__ __forceinline__ void simulate_terminal(const StepConsts& c, int32_t s
   }
 }
 
+// ILP independent samples advanced in the same loop by one thread: the
+// Philox rounds of the samples are separate dependency chains, so their
+// instructions interleave and fill the fixed-latency gaps of one chain.
+template <int MODEL, bool ANTI, int ILP>
+__device__ __forceinline__ void simulate_terminal_n(const StepConsts& c, int32_t steps, const uint64_t (&idx)[ILP],
+                                                    uint32_t stream, const of::PhiloxKeys& K, float (&ya)[ILP],
+                                                    float (&yb)[ILP]) {
+  if (ILP == 1) {
+    simulate_terminal<MODEL, ANTI>(c, steps, idx[0], stream, K, ya[0], yb[0]);
+    return;
+  }
+  uint32_t lo[ILP], hi[ILP];
+#pragma unroll
+  for (int l = 0; l < ILP; ++l) {
+    lo[l] = (uint32_t)idx[l];
+    hi[l] = (uint32_t)(idx[l] >> 32);
+  }
+  if (MODEL == OF_MODEL_GBM) {
+    float w[ILP];
+#pragma unroll
+    for (int l = 0; l < ILP; ++l) w[l] = 0.0f;
+    for (int32_t j = 0; j < steps; j += 4) {
+#pragma unroll
+      for (int l = 0; l < ILP; ++l) {
+        const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo[l], hi[l], stream), K);
+        w[l] += of::normal_from_u32(r.x);
+        if (j + 1 < steps) w[l] += of::normal_from_u32(r.y);
+        if (j + 2 < steps) w[l] += of::normal_from_u32(r.z);
+        if (j + 3 < steps) w[l] += of::normal_from_u32(r.w);
+      }
+    }
+    const float base = (float)steps * c.drift;
+#pragma unroll
+    for (int l = 0; l < ILP; ++l) {
+      ya[l] = fmaf(c.diff, w[l], base);
+      yb[l] = fmaf(-c.diff, w[l], base);
+    }
+  } else if (MODEL == OF_MODEL_HESTON_EULER) {
+    LegState a[ILP], b[ILP];
+#pragma unroll
+    for (int l = 0; l < ILP; ++l) a[l] = b[l] = LegState{0.0f, c.v0};
+    const int32_t pairs = steps >> 1;
+    for (int32_t q = 0; q < pairs; ++q) {
+#pragma unroll
+      for (int l = 0; l < ILP; ++l) {
+        const uint4 r = of::philox4x32_10(make_uint4((uint32_t)q, lo[l], hi[l], stream), K);
+        float z1 = of::normal_from_u32(r.x), z2 = of::normal_from_u32(r.y);
+        of::heston_euler_step(a[l], c, z1, z2);
+        if (ANTI) of::heston_euler_step(b[l], c, -z1, -z2);
+        z1 = of::normal_from_u32(r.z);
+        z2 = of::normal_from_u32(r.w);
+        of::heston_euler_step(a[l], c, z1, z2);
+        if (ANTI) of::heston_euler_step(b[l], c, -z1, -z2);
+      }
+    }
+    if (steps & 1) {
+#pragma unroll
+      for (int l = 0; l < ILP; ++l) {
+        const uint4 r = of::philox4x32_10(make_uint4((uint32_t)pairs, lo[l], hi[l], stream), K);
+        const float z1 = of::normal_from_u32(r.x), z2 = of::normal_from_u32(r.y);
+        of::heston_euler_step(a[l], c, z1, z2);
+        if (ANTI) of::heston_euler_step(b[l], c, -z1, -z2);
+      }
+    }
+#pragma unroll
+    for (int l = 0; l < ILP; ++l) {
+      ya[l] = a[l].y;
+      yb[l] = b[l].y;
+    }
+  } else {
+#pragma unroll
+    for (int l = 0; l < ILP; ++l) simulate_terminal<MODEL, ANTI>(c, steps, idx[l], stream, K, ya[l], yb[l]);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Strike strip: one shared path set, KPL strikes per lane.
 // ---------------------------------------------------------------------------
@@ -125,7 +200,7 @@ struct StripParams {
   const float* strikes;
 };
 
-template <int KPL, int MODEL, bool ANTI>
+template <int KPL, int MODEL, bool ANTI, int ILP = 1>
 __global__ void __launch_bounds__(256) strip_kernel(const __grid_constant__ StripParams P,
                                                     double* __restrict__ partials) {
   extern __shared__ double sh_strip[];  // [warps][n_strikes][2]
@@ -139,26 +214,37 @@ __global__ void __launch_bounds__(256) strip_kernel(const __grid_constant__ Stri
   }
   const bool call = P.option_type == OF_CALL;
   const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + warp * 32; base < P.samples; base += nthreads) {
-    const int64_t i = base + lane;
-    float sa = 0.0f, sb = 0.0f;
-    if (i < P.samples) {
-      float ya, yb;
-      simulate_terminal<MODEL, ANTI>(P.c, P.steps, (uint64_t)i, kStripStreamTag, P.keys, ya, yb);
-      sa = P.s0 * __expf(ya);
-      sb = P.s0 * __expf(yb);
-    }
-    const int64_t rem = P.samples - base;
-    const int nvalid = rem < 32 ? (int)rem : 32;
-    for (int j = 0; j < nvalid; ++j) {
-      const float st = __shfl_sync(of::kFullMask, sa, j);
-      const float sta = ANTI ? __shfl_sync(of::kFullMask, sb, j) : 0.0f;
+  // a warp round covers 32*ILP consecutive samples: lane + 32*l for l < ILP
+  for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + warp * 32) * ILP; base < P.samples;
+       base += nthreads * ILP) {
+    uint64_t idx[ILP];
+    float ya[ILP], yb[ILP], sa[ILP], sb[ILP];
 #pragma unroll
-      for (int q = 0; q < KPL; ++q) {
-        float x = fmaxf(call ? st - K[q] : K[q] - st, 0.0f);
-        if (ANTI) x = 0.5f * (x + fmaxf(call ? sta - K[q] : K[q] - sta, 0.0f));
-        s1[q].add(x);
-        s2[q].add(x * x);
+    for (int l = 0; l < ILP; ++l) {
+      idx[l] = (uint64_t)(base + lane + 32 * l);
+      ya[l] = yb[l] = 0.0f;
+    }
+    if (base + lane < P.samples)  // lanes past the end skip the paths; their shuffled values are unused
+      simulate_terminal_n<MODEL, ANTI, ILP>(P.c, P.steps, idx, kStripStreamTag, P.keys, ya, yb);
+#pragma unroll
+    for (int l = 0; l < ILP; ++l) {
+      sa[l] = P.s0 * __expf(ya[l]);
+      sb[l] = P.s0 * __expf(yb[l]);
+    }
+#pragma unroll
+    for (int l = 0; l < ILP; ++l) {
+      const int64_t rem = P.samples - (base + 32 * l);
+      const int nvalid = rem < 0 ? 0 : (rem < 32 ? (int)rem : 32);
+      for (int j = 0; j < nvalid; ++j) {
+        const float st = __shfl_sync(of::kFullMask, sa[l], j);
+        const float sta = ANTI ? __shfl_sync(of::kFullMask, sb[l], j) : 0.0f;
+#pragma unroll
+        for (int q = 0; q < KPL; ++q) {
+          float x = fmaxf(call ? st - K[q] : K[q] - st, 0.0f);
+          if (ANTI) x = 0.5f * (x + fmaxf(call ? sta - K[q] : K[q] - sta, 0.0f));
+          s1[q].add(x);
+          s2[q].add(x * x);
+        }
       }
     }
   }
@@ -181,12 +267,26 @@ __global__ void __launch_bounds__(256) strip_kernel(const __grid_constant__ Stri
 
 typedef void (*StripKernelFn)(StripParams, double*);
 
-template <int KPL>
+template <int KPL, int ILP = 1>
 StripKernelFn pick_strip(int model, bool anti) {
-  if (model == OF_MODEL_GBM) return anti ? strip_kernel<KPL, OF_MODEL_GBM, true> : strip_kernel<KPL, OF_MODEL_GBM, false>;
+  if (model == OF_MODEL_GBM)
+    return anti ? strip_kernel<KPL, OF_MODEL_GBM, true, ILP> : strip_kernel<KPL, OF_MODEL_GBM, false, ILP>;
   if (model == OF_MODEL_HESTON_EULER)
-    return anti ? strip_kernel<KPL, OF_MODEL_HESTON_EULER, true> : strip_kernel<KPL, OF_MODEL_HESTON_EULER, false>;
-  return anti ? strip_kernel<KPL, OF_MODEL_HESTON_QE, true> : strip_kernel<KPL, OF_MODEL_HESTON_QE, false>;
+    return anti ? strip_kernel<KPL, OF_MODEL_HESTON_EULER, true, ILP>
+                : strip_kernel<KPL, OF_MODEL_HESTON_EULER, false, ILP>;
+  return anti ? strip_kernel<KPL, OF_MODEL_HESTON_QE, true, ILP> : strip_kernel<KPL, OF_MODEL_HESTON_QE, false, ILP>;
+}
+
+// Kernel for KPL strikes per lane and ILP samples in flight per thread.
+StripKernelFn pick_strip_ilp(int kpl, int ilp, int model, bool anti) {
+  if (ilp == 2) {
+    if (kpl <= 1) return pick_strip<1, 2>(model, anti);
+    if (kpl <= 2) return pick_strip<2, 2>(model, anti);
+    return pick_strip<4, 2>(model, anti);
+  }
+  if (kpl <= 1) return pick_strip<1>(model, anti);
+  if (kpl <= 2) return pick_strip<2>(model, anti);
+  return pick_strip<4>(model, anti);
 }
 
 }  // namespace
@@ -269,12 +369,13 @@ static of_status strip_setup(of_ctx* ctx, const of_model* m, int32_t option_type
   P.s0 = (float)m->s0;
   P.keys = of::philox_keys(cfg->seed);
   const int kpl = (int)((n_strikes + 31) / 32);
-  const int kpl_t = kpl <= 1 ? 1 : (kpl <= 2 ? 2 : 4);
-  pl->fn = kpl_t == 1 ? pick_strip<1>(m->kind, P.antithetic) : kpl_t == 2 ? pick_strip<2>(m->kind, P.antithetic)
-                                                                           : pick_strip<4>(m->kind, P.antithetic);
+  if (cfg->tile_ilp < 0 || cfg->tile_ilp > 2)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "tile_ilp must be 0 (default), 1 or 2");
+  const int ilp = cfg->tile_ilp == 2 ? 2 : 1;
+  pl->fn = pick_strip_ilp(kpl, ilp, m->kind, P.antithetic);
   pl->smem = (size_t)(pl->block / 32) * n_strikes * 2 * sizeof(double);
   const int per_sm = of_blocks_per_sm((const void*)pl->fn, pl->block, pl->smem);
-  const int64_t want = (pl->samples + pl->block - 1) / pl->block;
+  const int64_t want = (pl->samples + (int64_t)pl->block * ilp - 1) / ((int64_t)pl->block * ilp);
   const int64_t cap = (int64_t)ctx->sm_count * per_sm;
   pl->grid = (int)std::max<int64_t>(1, std::min(want, cap));
   return OF_OK;

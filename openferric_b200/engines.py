@@ -513,7 +513,7 @@ class ArithmeticAsianMC:
 # ---------------------------------------------------------------------------
 def price_strike_strip(generator: PathGenerator, option_type: OptionType, strikes: Sequence[float], num_paths: int,
                        seed: int, discount_factor: float, antithetic: bool = False,
-                       device: int = 0) -> List[Tuple[float, float]]:
+                       device: int = 0, tile_ilp: int = 0) -> List[Tuple[float, float]]:
     """European (price, stderr) for every strike from one shared FP32 Philox
     path set (of_mc_strip)."""
     ctx = context(device)
@@ -524,7 +524,8 @@ def price_strike_strip(generator: PathGenerator, option_type: OptionType, strike
     for lo in range(0, len(ks), 128):
         chunk = ks[lo:lo + 128]
         cfg = A.OfMcConfig(num_paths=int(num_paths), seed=int(seed) & 0xFFFFFFFFFFFFFFFF, antithetic=int(antithetic),
-                           precision=A.OF_PREC_FP32_PHILOX, discount_factor=float(discount_factor))
+                           precision=A.OF_PREC_FP32_PHILOX, discount_factor=float(discount_factor),
+                           tile_ilp=int(tile_ilp))
         part = (A.OfMcResult * len(chunk))()
         with ctx.lock:
             ctx.check(ctx._L.of_mc_strip(ctx.handle, C.byref(model), option_type.value,
@@ -541,14 +542,15 @@ class StripPlan:
     `results` waits and returns (price, stderr) per strike."""
 
     def __init__(self, generator: PathGenerator, option_type: OptionType, strikes: Sequence[float], num_paths: int,
-                 seed: int, discount_factor: float, antithetic: bool = False, device: int = 0):
+                 seed: int, discount_factor: float, antithetic: bool = False, device: int = 0, tile_ilp: int = 0):
         self.ctx = context(device)
         self.n = len(strikes)
         self.path_steps = float(num_paths) * float(generator.steps)
         ks = np.ascontiguousarray(strikes, dtype=np.float64)
         model = generator.to_abi()
         cfg = A.OfMcConfig(num_paths=int(num_paths), seed=int(seed) & 0xFFFFFFFFFFFFFFFF, antithetic=int(antithetic),
-                           precision=A.OF_PREC_FP32_PHILOX, discount_factor=float(discount_factor))
+                           precision=A.OF_PREC_FP32_PHILOX, discount_factor=float(discount_factor),
+                           tile_ilp=int(tile_ilp))
         h = C.c_void_p()
         L = self.ctx._L
         with self.ctx.lock:

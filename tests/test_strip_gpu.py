@@ -86,3 +86,32 @@ def test_strip_rejects_bad_strikes():
     gen = GbmPathGenerator(Gbm(0.05, 0.2), 100.0, 1.0, 8)
     with pytest.raises(PricingError):
         price_strike_strip(gen, OptionType.Call, [100.0, -1.0], 1000, 3, 1.0)
+
+
+@pytest.mark.parametrize("scheme", ["euler", "qe"])
+@pytest.mark.parametrize("anti", [False, True])
+@pytest.mark.parametrize("n_paths", [1 << 16, 100_003])
+def test_strip_two_samples_in_flight_matches_one(scheme, anti, n_paths):
+    """tile_ilp=2 walks the same Philox counters in a different order, so the
+    prices agree with tile_ilp=1 up to the FP32 accumulation order; a ragged
+    path count exercises the partial last warp round."""
+    gen = HestonPathGenerator(HESTON, 100.0, 1.0, 63, scheme=scheme)
+    one = price_strike_strip(gen, OptionType.Call, STRIKES[:37], n_paths, 9, 0.97, antithetic=anti, tile_ilp=1)
+    two = price_strike_strip(gen, OptionType.Call, STRIKES[:37], n_paths, 9, 0.97, antithetic=anti, tile_ilp=2)
+    for (p1, s1), (p2, s2) in zip(one, two):
+        assert abs(p1 - p2) <= 2e-6 * max(1.0, abs(p1)), (p1, p2)
+        assert abs(s1 - s2) <= 2e-6 * max(1.0, s1), (s1, s2)
+
+
+def test_strip_gbm_two_samples_in_flight_matches_one():
+    gen = GbmPathGenerator(Gbm(0.05, 0.2), 100.0, 1.0, 30)
+    one = price_strike_strip(gen, OptionType.Put, STRIKES, 1 << 17, 4, 0.95, tile_ilp=1)
+    two = price_strike_strip(gen, OptionType.Put, STRIKES, 1 << 17, 4, 0.95, tile_ilp=2)
+    for (p1, _), (p2, _) in zip(one, two):
+        assert abs(p1 - p2) <= 2e-6 * max(1.0, abs(p1)), (p1, p2)
+
+
+def test_strip_rejects_bad_tile_ilp():
+    gen = GbmPathGenerator(Gbm(0.05, 0.2), 100.0, 1.0, 8)
+    with pytest.raises(PricingError):
+        price_strike_strip(gen, OptionType.Call, [100.0], 1000, 3, 1.0, tile_ilp=3)
