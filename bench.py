@@ -39,11 +39,18 @@ STRIKES = [80.0 + k for k in range(41)]
 PATHS, STEPS, SEED = 1 << 20, 256, 7
 PATH_STEPS = float(PATHS) * STEPS
 # Declared algorithmic work of one Heston Euler path-step in the FP32 kernel:
-# two inverse-normal draws (x, (1+x)(1-x), w - c, 8-term Horner, x*P: 24 flops
-# each) and the step (correlation 3, log-spot 6, variance 6, floors 2): 65 FP32
-# flops (FMA = 2) plus 3 SFU operations (2 lg2, 1 sqrt).
-FLOPS_PER_STEP = 65.0
-SFU_PER_STEP = 3.0
+# one Box-Muller pair (u1 2, -2 ln 2 scale 1, angle 3, r cos / r sin 2: 8
+# flops; lg2, sqrt, sin, cos on the MUFU unit) and the step (correlation 3,
+# log-spot 6, variance 5, floors 2: 16 flops; one sqrt): 24 FP32 flops
+# (FMA = 2) and 5 MUFU operations.  The Philox rounds (integer multiply and
+# xor, ~20 instructions per step) use neither pipe's budget in this count.
+FLOPS_PER_STEP = 24.0
+SFU_PER_STEP = 5.0
+# DRAM bytes (read + write) of one strip launch from an ncu capture of the
+# kernel at 2^18 paths; the kernel reads no input from HBM, so the figure
+# does not grow with the path count.
+STRIP_DRAM_BYTES = 21248
+STRIP_DRAM_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, strip_kernel at 2^18 paths (size-independent)"
 CONFIG = {"workload": "heston_euler_strike_strip", "paths": PATHS, "steps": STEPS, "strikes": 41,
           "strike_range": [80, 120], "kappa": 2.0, "theta": 0.04, "xi": 0.5, "rho": -0.7, "v0": 0.04, "s0": S0,
           "r": RATE, "q": 0.0, "T": T, "seed": SEED, "rng": "philox4x32-10", "path_dtype": "fp32",
@@ -227,7 +234,7 @@ def run_workload(args, local_rank):
                 "config": g}
     elif args.workload == "book":
         from openferric_b200.book import BookPlan, synthetic_book
-        plan = BookPlan(synthetic_book(), seed=20261203)
+        plan = BookPlan(synthetic_book(args.book_options), seed=20261203)
         info = plan.info()
         for _ in range(max(1, args.warmup)):
             plan.launch()
@@ -244,14 +251,15 @@ def run_workload(args, local_rank):
         plan.close()
         line = {"metric": "path-steps/s", "value": info["path_steps"] / (ms / 1e3), "unit": "path-steps/s",
                 "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic", "ms_per_step": ms,
-                "config": {"workload": "batched_book_4096", "tiles": info["tiles"], "block": info["block"],
+                "config": {"workload": f"batched_book_{args.book_options}", "tiles": info["tiles"],
+                           "block": info["block"],
                            "paths_per_thread": info["paths_per_thread"], "path_steps": info["path_steps"],
-                           "options_per_s": 4096 / (ms / 1e3), "cuda_graph": True}}
+                           "options_per_s": args.book_options / (ms / 1e3), "cuda_graph": True}}
     else:  # lsm
         from openferric_b200.lsm import LongstaffSchwartzEngine
         rng = np.random.default_rng(20261203)
         items = []
-        for i in range(256):
+        for i in range(args.contracts):
             vol, T = (0.2, 0.4)[i % 2], (1.0, 2.0)[(i // 2) % 2]
             m = of.Market.builder().spot(rng.uniform(30.0, 50.0)).rate(0.06).flat_vol(vol).build()
             items.append((of.VanillaOption.american_put(40.0, T), m))
@@ -264,9 +272,10 @@ def run_workload(args, local_rank):
             eng.price_batch(sub, with_delta=True)
             total_ms += eng.last_kernel_ms
             alg_bytes += len(sub) * float(args.paths) * int(50 * T) * 16.0
-        line = {"metric": "LSM contracts/s (price + delta)", "value": 256 / (total_ms / 1e3), "unit": "contracts/s",
+        line = {"metric": "LSM contracts/s (price + delta)", "value": args.contracts / (total_ms / 1e3),
+                "unit": "contracts/s",
                 "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic", "ms_per_step": total_ms,
-                "config": {"workload": "lsm_american_put_256", "paths": args.paths, "dates_per_year": 50,
+                "config": {"workload": f"lsm_american_put_{args.contracts}", "paths": args.paths, "dates_per_year": 50,
                            "basis": "1,x,x^2,x^3 (x=S/K), Cholesky", "algorithmic_bytes": alg_bytes,
                            "algorithmic_GBps": alg_bytes / (total_ms / 1e3) / 1e9}}
     print(json.dumps(line), flush=True)
@@ -284,6 +293,10 @@ def main():
                     help="strip is the benchmark line; the others are single-GPU lines for configurations 3-5")
     ap.add_argument("--paths", type=int, default=PATHS,
                     help="paths per strip (profiling a smaller case; the benchmark workload is 2^20)")
+    ap.add_argument("--book-options", type=int, default=4096,
+                    help="book workload: number of options (4096 in the benchmark; fewer for a profiler capture)")
+    ap.add_argument("--contracts", type=int, default=256,
+                    help="LSM workload: number of American puts (256 in the benchmark; fewer for a profiler capture)")
     args = ap.parse_args()
     global PATH_STEPS
     PATH_STEPS = float(args.paths) * STEPS
@@ -316,6 +329,7 @@ def main():
     for _ in range(max(3, args.warmup)):
         plan.launch()
     prices = plan.results()
+    peaks = ctx.device_peaks()  # MUFU and FP32 denominators, measured on this GPU before the timed region
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -359,18 +373,26 @@ def main():
     value = world * PATH_STEPS * args.steps / (total_ms / 1e3)
     per_gpu = PATH_STEPS / (ms_per_step / 1e3)
     sm_max = clk.get("sm_max_mhz") or 1965.0
-    peak_fp32 = 148 * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s, derived from the SM clock
-    achieved = per_gpu * FLOPS_PER_STEP / 1e12
-    sfu_peak = 148 * 16 * sm_max * 1e6
+    sfu_peak, fp32_peak = peaks["sfu_ops_per_s"], peaks["fp32_flops_per_s"]
+    sfu_frac = per_gpu * SFU_PER_STEP / sfu_peak
+    fp32_frac = per_gpu * FLOPS_PER_STEP / fp32_peak
+    probe_src = "measured in this run by of_measure_device_peaks"
+    fp32_line = {"achieved": per_gpu * FLOPS_PER_STEP / 1e12, "peak": fp32_peak / 1e12, "unit": "TFLOP/s",
+                 "frac": fp32_frac, "per_step": FLOPS_PER_STEP,
+                 "peak_source": f"{probe_src} (FP32 FMA chains); derived nominal "
+                                f"{148 * 128 * 2 * sm_max * 1e6 / 1e12:.1f} TFLOP/s at {sm_max:.0f} MHz"}
+    sfu_line = {"achieved": per_gpu * SFU_PER_STEP / 1e12, "peak": sfu_peak / 1e12, "unit": "TOP/s",
+                "frac": sfu_frac, "per_step": SFU_PER_STEP,
+                "peak_source": f"{probe_src} (MUFU lg2/sqrt/sin/cos chains); derived nominal "
+                               f"{148 * 16 * sm_max * 1e6 / 1e12:.2f} TOP/s at 16/clk/SM"}
+    bound, main_line, other_name, other_line = (
+        ("sfu", sfu_line, "fp32", fp32_line) if sfu_frac >= fp32_frac else ("fp32", fp32_line, "sfu", sfu_line))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": dict(CONFIG, parallelism=f"replicas{world}"),
-        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
-                     "frac": achieved / peak_fp32, "traffic": None,
-                     "peak_source": f"derived: 148 SM x 128 FP32 lanes x 2 x {sm_max:.0f} MHz (no FP32 figure in "
-                                    f"MEASURED_PEAKS.json)",
-                     "sfu_frac": per_gpu * SFU_PER_STEP / sfu_peak},
+        "roofline": dict(main_line, bound=bound, traffic=STRIP_DRAM_BYTES, traffic_source=STRIP_DRAM_SOURCE,
+                         **{other_name: other_line}),
         "e2e": {"value": world * PATH_STEPS * args.steps / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": 41 * 4, "d2h_bytes_per_step": 41 * 2 * 8},
         "gpu_launches": 2 * args.steps,

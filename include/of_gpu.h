@@ -142,6 +142,22 @@ of_status of_ctx_get_stream(of_ctx* ctx, void** cuda_stream);
 int of_abi_version(void);
 int of_device_sm_count(of_ctx* ctx);
 
+/* Throughput of this GPU's FP32 pipe and special-function unit (MUFU),
+ * measured by two short probe kernels on the context's stream: the
+ * denominators of a compute-bound roofline at the clocks of the moment.  No
+ * counterpart in the reference.
+ *   sfu_ops_per_s: MUFU results per second for the mix that the FP32 Philox
+ *     kernels issue (lg2, sqrt, sin, cos), 8 independent chains per thread;
+ *   fp32_flops_per_s: FP32 FMA throughput, 2 flops per FMA, 8 independent
+ *     chains per thread;
+ *   probe_ms: device time of the two probes together. */
+typedef struct {
+  double sfu_ops_per_s;
+  double fp32_flops_per_s;
+  double probe_ms;
+} of_device_peaks;
+of_status of_measure_device_peaks(of_ctx* ctx, of_device_peaks* out);
+
 /* ---- generic Monte Carlo run -------------------------------------------- */
 /* Replaces mc::MonteCarloEngine::run (src/mc/simulation.rs:182-348) with a
  * built-in payoff in place of the Rust closure; the caller (the Rust

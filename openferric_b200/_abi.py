@@ -229,3 +229,11 @@ class OfMcResult(C.Structure):
         ("sum_y2", C.c_double),
         ("kernel_ms", C.c_double),
     ]
+
+
+class OfDevicePeaks(C.Structure):
+    _fields_ = [
+        ("sfu_ops_per_s", C.c_double),
+        ("fp32_flops_per_s", C.c_double),
+        ("probe_ms", C.c_double),
+    ]

@@ -23,6 +23,7 @@ EXPORTED = [
     "of_book_plan_create", "of_book_plan_launch", "of_book_plan_results", "of_book_plan_info",
     "of_book_plan_destroy", "of_mc_european_pathwise_aad", "of_heston_price_delta_aad", "of_mc_greek_estimators",
     "of_lsm_price", "of_xoshiro_jump", "of_heston_price_adjoint", "of_mc_european_gpu", "of_mc_strip_noalloc",
+    "of_measure_device_peaks",
 ]
 
 
@@ -87,6 +88,8 @@ def _declare(L):
     L.of_mc_strip_noalloc.argtypes = [vp, P(A.OfModel), C.c_int32, P(C.c_double), C.c_int64, P(A.OfMcConfig),
                                       P(A.OfMcResult), C.c_char_p, C.c_size_t]
     L.of_mc_strip_noalloc.restype = C.c_int
+    L.of_measure_device_peaks.argtypes = [vp, P(A.OfDevicePeaks)]
+    L.of_measure_device_peaks.restype = C.c_int
     for name in ["of_ctx_create", "of_ctx_set_stream", "of_ctx_get_stream", "of_mc_run", "of_mc_strip",
                  "of_strip_plan_create", "of_strip_plan_launch", "of_strip_plan_results", "of_mc_price_book",
                  "of_book_plan_create", "of_book_plan_launch", "of_book_plan_results", "of_book_plan_info"]:
@@ -154,6 +157,14 @@ class Context:
 
     def set_stream(self, ptr: int):
         self.check(self._L.of_ctx_set_stream(self.handle, C.c_void_p(ptr or None)))
+
+    def device_peaks(self) -> dict:
+        """MUFU and FP32 FMA throughput of this GPU, measured by probe kernels."""
+        out = A.OfDevicePeaks()
+        with self.lock:
+            self.check(self._L.of_measure_device_peaks(self.handle, C.byref(out)))
+        return {"sfu_ops_per_s": out.sfu_ops_per_s, "fp32_flops_per_s": out.fp32_flops_per_s,
+                "probe_ms": out.probe_ms}
 
     def close(self):
         if getattr(self, "handle", None) and self.handle.value:

@@ -15,8 +15,9 @@
 //
 // Kernel 1 (forward): one thread per path; (v, y) checkpointed every 32 steps
 // to HBM, time-major ckpt[segment][path]; the payoff gradient of each path.
-// Kernel 2 (backward): each warp owns a contiguous range of paths, queues the
-// in-the-money ones in shared memory (ballot), and sweeps them 32 at a time:
+// Kernel 2 (backward): each warp scans 128-path ranges (grid stride), queues
+// the in-the-money paths in shared memory (ballot; the queue carries over
+// between ranges), and sweeps them 32 at a time:
 // per segment (last first) the 32 steps are recomputed from the checkpoint
 // into shared memory (v, e^y), each step's Philox draws are regenerated from
 // its counter, and the adjoints (y_bar, v_bar) and parameter adjoints are
@@ -38,7 +39,7 @@ constexpr int kSeg = 32;                          // checkpoint interval
 constexpr int kMaxSegments = 64;
 constexpr int kBwdThreads = 128;
 constexpr int kBwdWarps = kBwdThreads / 32;
-constexpr int kRangePerWarp = 32 * 16;  // paths whose in-the-money subset one warp sweeps
+constexpr int kRangePerWarp = 32 * 4;  // paths one warp scans for in-the-money paths per grid-stride turn
 constexpr float kLn2 = 0.69314718055994531f;
 
 __device__ __forceinline__ float sqrt_approx(float x) {
@@ -315,9 +316,9 @@ __global__ void __launch_bounds__(kBwdThreads) adjoint_backward(const __grid_con
   for (int k = 0; k < 14; ++k) acc[k] = 0.0;
   const int64_t nranges = (c.paths + kRangePerWarp - 1) / kRangePerWarp;
   const int64_t gwarps = (int64_t)gridDim.x * kBwdWarps;
+  int qn = 0;  // queued in-the-money paths; the queue carries over from one range to the next
   for (int64_t rg = (int64_t)blockIdx.x * kBwdWarps + warp; rg < nranges; rg += gwarps) {
     const int64_t r0 = rg * kRangePerWarp;
-    int qn = 0;
     for (int chunk = 0; chunk < kRangePerWarp; chunk += 32) {
       const int64_t i = r0 + chunk + lane;
       const bool itm = i < c.paths && c.grad[i] != 0.0f;
@@ -333,9 +334,9 @@ __global__ void __launch_bounds__(kBwdThreads) adjoint_backward(const __grid_con
         __syncwarp();
       }
     }
-    if (lane < qn) sweep_path(c, queue[warp][lane], seg_v + threadIdx.x, seg_s + threadIdx.x, acc);
-    __syncwarp();
   }
+  if (lane < qn) sweep_path(c, queue[warp][lane], seg_v + threadIdx.x, seg_s + threadIdx.x, acc);
+  __syncwarp();
   // block reduction of the 14 sums (fixed order)
 #pragma unroll
   for (int k = 0; k < 14; ++k) {

@@ -2,7 +2,10 @@
 //
 // Generator: Philox4x32-10, counter {draw block, sample lo, sample hi, stream},
 // key = the 64-bit seed; one call yields 4 draws (4 GBM steps or 2 Heston
-// steps).  Paths live in registers (one path per thread at a time), payoff
+// steps).  GBM and Heston Euler turn each draw pair into two normals by
+// Box-Muller; Heston QE keeps the inverse CDF, which its variance step
+// needs (the same uniform drives the exponential branch and, through
+// Phi^-1, the quadratic one).  Paths live in registers (one path per thread at a time), payoff
 // sums are compensated FP32 per thread and FP64 from the warp level up.
 // Compiled with -use_fast_math: sqrt/exp/log/div map to single MUFU
 // operations; the few places that need more accuracy say so.
@@ -67,10 +70,11 @@ __device__ __forceinline__ void simulate_terminal(const StepConsts& c, int32_t s
     float wa = 0.0f;  // sum of normals; y_T = steps*drift + diff*sum
     for (int32_t j = 0; j < steps; j += 4) {
       const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo, hi, stream), K);
-      wa += of::normal_from_u32(r.x);
-      if (j + 1 < steps) wa += of::normal_from_u32(r.y);
-      if (j + 2 < steps) wa += of::normal_from_u32(r.z);
-      if (j + 3 < steps) wa += of::normal_from_u32(r.w);
+      const float2 p = of::normal_pair_from_u32(r.x, r.y), q = of::normal_pair_from_u32(r.z, r.w);
+      wa += p.x;
+      if (j + 1 < steps) wa += p.y;
+      if (j + 2 < steps) wa += q.x;
+      if (j + 3 < steps) wa += q.y;
     }
     const float base = (float)steps * c.drift;
     ya = fmaf(c.diff, wa, base);
@@ -79,19 +83,18 @@ __device__ __forceinline__ void simulate_terminal(const StepConsts& c, int32_t s
     const int32_t pairs = steps >> 1;  // full Philox calls; an odd last step below
     for (int32_t q = 0; q < pairs; ++q) {
       const uint4 r = of::philox4x32_10(make_uint4((uint32_t)q, lo, hi, stream), K);
-      float z1 = of::normal_from_u32(r.x), z2 = of::normal_from_u32(r.y);
-      of::heston_euler_step(a, c, z1, z2);
-      if (ANTI) of::heston_euler_step(b, c, -z1, -z2);
-      z1 = of::normal_from_u32(r.z);
-      z2 = of::normal_from_u32(r.w);
-      of::heston_euler_step(a, c, z1, z2);
-      if (ANTI) of::heston_euler_step(b, c, -z1, -z2);
+      float2 z = of::normal_pair_from_u32(r.x, r.y);
+      of::heston_euler_step(a, c, z.x, z.y);
+      if (ANTI) of::heston_euler_step(b, c, -z.x, -z.y);
+      z = of::normal_pair_from_u32(r.z, r.w);
+      of::heston_euler_step(a, c, z.x, z.y);
+      if (ANTI) of::heston_euler_step(b, c, -z.x, -z.y);
     }
     if (steps & 1) {
       const uint4 r = of::philox4x32_10(make_uint4((uint32_t)pairs, lo, hi, stream), K);
-      const float z1 = of::normal_from_u32(r.x), z2 = of::normal_from_u32(r.y);
-      of::heston_euler_step(a, c, z1, z2);
-      if (ANTI) of::heston_euler_step(b, c, -z1, -z2);
+      const float2 z = of::normal_pair_from_u32(r.x, r.y);
+      of::heston_euler_step(a, c, z.x, z.y);
+      if (ANTI) of::heston_euler_step(b, c, -z.x, -z.y);
     }
     ya = a.y;
     yb = b.y;
@@ -138,10 +141,11 @@ __device__ __forceinline__ void simulate_terminal_n(const StepConsts& c, int32_t
 #pragma unroll
       for (int l = 0; l < ILP; ++l) {
         const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo[l], hi[l], stream), K);
-        w[l] += of::normal_from_u32(r.x);
-        if (j + 1 < steps) w[l] += of::normal_from_u32(r.y);
-        if (j + 2 < steps) w[l] += of::normal_from_u32(r.z);
-        if (j + 3 < steps) w[l] += of::normal_from_u32(r.w);
+        const float2 p = of::normal_pair_from_u32(r.x, r.y), q = of::normal_pair_from_u32(r.z, r.w);
+        w[l] += p.x;
+        if (j + 1 < steps) w[l] += p.y;
+        if (j + 2 < steps) w[l] += q.x;
+        if (j + 3 < steps) w[l] += q.y;
       }
     }
     const float base = (float)steps * c.drift;
@@ -159,22 +163,21 @@ __device__ __forceinline__ void simulate_terminal_n(const StepConsts& c, int32_t
 #pragma unroll
       for (int l = 0; l < ILP; ++l) {
         const uint4 r = of::philox4x32_10(make_uint4((uint32_t)q, lo[l], hi[l], stream), K);
-        float z1 = of::normal_from_u32(r.x), z2 = of::normal_from_u32(r.y);
-        of::heston_euler_step(a[l], c, z1, z2);
-        if (ANTI) of::heston_euler_step(b[l], c, -z1, -z2);
-        z1 = of::normal_from_u32(r.z);
-        z2 = of::normal_from_u32(r.w);
-        of::heston_euler_step(a[l], c, z1, z2);
-        if (ANTI) of::heston_euler_step(b[l], c, -z1, -z2);
+        float2 z = of::normal_pair_from_u32(r.x, r.y);
+        of::heston_euler_step(a[l], c, z.x, z.y);
+        if (ANTI) of::heston_euler_step(b[l], c, -z.x, -z.y);
+        z = of::normal_pair_from_u32(r.z, r.w);
+        of::heston_euler_step(a[l], c, z.x, z.y);
+        if (ANTI) of::heston_euler_step(b[l], c, -z.x, -z.y);
       }
     }
     if (steps & 1) {
 #pragma unroll
       for (int l = 0; l < ILP; ++l) {
         const uint4 r = of::philox4x32_10(make_uint4((uint32_t)pairs, lo[l], hi[l], stream), K);
-        const float z1 = of::normal_from_u32(r.x), z2 = of::normal_from_u32(r.y);
-        of::heston_euler_step(a[l], c, z1, z2);
-        if (ANTI) of::heston_euler_step(b[l], c, -z1, -z2);
+        const float2 z = of::normal_pair_from_u32(r.x, r.y);
+        of::heston_euler_step(a[l], c, z.x, z.y);
+        if (ANTI) of::heston_euler_step(b[l], c, -z.x, -z.y);
       }
     }
 #pragma unroll
@@ -597,15 +600,22 @@ __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, const 
   for (int32_t j = 0; j < o.steps; j += SPC) {
     const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j / SPC), lo, hi, o.stream), K);
     const uint32_t rr[4] = {r.x, r.y, r.z, r.w};
+    // Box-Muller normals of the two draw pairs (GBM and Heston Euler)
+    float2 p01 = make_float2(0.0f, 0.0f), p23 = make_float2(0.0f, 0.0f);
+    if (MODEL != OF_MODEL_HESTON_QE) {
+      p01 = of::normal_pair_from_u32(r.x, r.y);
+      p23 = of::normal_pair_from_u32(r.z, r.w);
+    }
 #pragma unroll
     for (int q = 0; q < SPC; ++q) {
       if (j + q >= o.steps) break;
       if (MODEL == OF_MODEL_GBM) {
-        const float z = of::normal_from_u32(rr[q]);
+        const float z = q == 0 ? p01.x : q == 1 ? p01.y : q == 2 ? p23.x : p23.y;
         a.y = fmaf(c.diff, z, a.y + c.drift);
         if (anti) b.y = fmaf(-c.diff, z, b.y + c.drift);
       } else if (MODEL == OF_MODEL_HESTON_EULER) {
-        const float z1 = of::normal_from_u32(rr[2 * q]), z2 = of::normal_from_u32(rr[2 * q + 1]);
+        const float2 z = q == 0 ? p01 : p23;
+        const float z1 = z.x, z2 = z.y;
         of::heston_euler_step(a, c, z1, z2);
         if (anti) of::heston_euler_step(b, c, -z1, -z2);
       } else {
@@ -628,7 +638,9 @@ __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, const 
   }
 }
 
-__global__ void __launch_bounds__(256) book_kernel(const __grid_constant__ BookParams P) {
+// Three 256-thread blocks per SM: ptxas's own choice without the hint is 64
+// registers with spills in the step loop.
+__global__ void __launch_bounds__(256, 3) book_kernel(const __grid_constant__ BookParams P) {
   __shared__ int tile_sh;
   __shared__ double red_sh[5 * 8];
   for (;;) {
@@ -1103,5 +1115,92 @@ extern "C" of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* m, i
     of_mc_finish(sums, P.samples, OF_CV_NONE, 0.0, cfg->discount_factor, &results[k]);
     results[k].kernel_ms = 0.0;
   }
+  return OF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Device peak probes (of_measure_device_peaks)
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kProbeChains = 8;
+constexpr int kProbeBlock = 256;
+
+// kProbeChains independent chains per thread.  One link is five MUFU
+// operations (lg2, sqrt, sin, cos, sqrt) and a few FP32 adds that keep the
+// value bounded: lg2(x + 1.5) in (0.58, 1.81), sqrt(. + 0.5) in (1.04, 1.52),
+// sin in (0.86, 1), cos in (0.54, 0.65), sqrt(. + 0.25) in (0.89, 0.95).
+__global__ void __launch_bounds__(kProbeBlock) sfu_probe_kernel(int iters, float* sink) {
+  float a[kProbeChains];
+#pragma unroll
+  for (int k = 0; k < kProbeChains; ++k) a[k] = 0.5f + 0.01f * k + 1e-7f * threadIdx.x;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < kProbeChains; ++k) {
+      float x = __log2f(a[k] + 1.5f);
+      x = sqrtf(x + 0.5f);
+      x = __sinf(x);
+      x = __cosf(x);
+      a[k] = sqrtf(x + 0.25f);
+    }
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int k = 0; k < kProbeChains; ++k) s += a[k];
+  if (s < 0.0f) sink[blockIdx.x] = s;  // never taken (s > 7); keeps the chains live
+}
+
+// kProbeChains independent FMA chains per thread converging to 1.
+__global__ void __launch_bounds__(kProbeBlock) fma_probe_kernel(int iters, float* sink) {
+  float a[kProbeChains];
+#pragma unroll
+  for (int k = 0; k < kProbeChains; ++k) a[k] = 0.5f + 0.01f * k + 1e-7f * threadIdx.x;
+#pragma unroll 16
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < kProbeChains; ++k) a[k] = fmaf(a[k], 0.99993896484375f, 6.103515625e-5f);
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int k = 0; k < kProbeChains; ++k) s += a[k];
+  if (s < 0.0f) sink[blockIdx.x] = s;  // never taken; keeps the chains live
+}
+
+}  // namespace
+
+extern "C" of_status of_measure_device_peaks(of_ctx* ctx, of_device_peaks* out) {
+  if (!ctx || !out) return OF_ERR_INVALID_INPUT;
+  OF_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const int per_sm_s = of_blocks_per_sm((const void*)sfu_probe_kernel, kProbeBlock, 0);
+  const int per_sm_f = of_blocks_per_sm((const void*)fma_probe_kernel, kProbeBlock, 0);
+  const int grid_s = ctx->sm_count * std::max(per_sm_s, 1), grid_f = ctx->sm_count * std::max(per_sm_f, 1);
+  void* sink = nullptr;
+  OF_TRY(of_scratch(ctx, SLOT_MISC, (size_t)std::max(grid_s, grid_f) * sizeof(float), &sink));
+  const int it_s = 2048, it_f = 65536;
+  // warm-up (clocks up), then the best of three timed launches of each probe
+  sfu_probe_kernel<<<grid_s, kProbeBlock, 0, ctx->stream>>>(it_s / 8, (float*)sink);
+  fma_probe_kernel<<<grid_f, kProbeBlock, 0, ctx->stream>>>(it_f / 8, (float*)sink);
+  OF_CUDA_TRY(ctx, cudaGetLastError());
+  float best_s = 1e30f, best_f = 1e30f;
+  for (int rep = 0; rep < 3; ++rep) {
+    float ms = 0.0f;
+    OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+    sfu_probe_kernel<<<grid_s, kProbeBlock, 0, ctx->stream>>>(it_s, (float*)sink);
+    OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+    OF_CUDA_TRY(ctx, cudaEventSynchronize(ctx->ev_stop));
+    OF_CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+    best_s = std::min(best_s, ms);
+    OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+    fma_probe_kernel<<<grid_f, kProbeBlock, 0, ctx->stream>>>(it_f, (float*)sink);
+    OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+    OF_CUDA_TRY(ctx, cudaEventSynchronize(ctx->ev_stop));
+    OF_CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+    best_f = std::min(best_f, ms);
+  }
+  OF_CUDA_TRY(ctx, cudaGetLastError());
+  const double threads_s = (double)grid_s * kProbeBlock, threads_f = (double)grid_f * kProbeBlock;
+  out->sfu_ops_per_s = threads_s * it_s * kProbeChains * 5.0 / (best_s * 1e-3);
+  out->fp32_flops_per_s = threads_f * (double)it_f * kProbeChains * 2.0 / (best_f * 1e-3);
+  out->probe_ms = (double)best_s + (double)best_f;
   return OF_OK;
 }

@@ -2,23 +2,120 @@
 from __future__ import annotations
 
 from dataclasses import dataclass, field
-from typing import Callable, Optional
+import math
+from typing import Callable, Optional, Sequence
 
 from .core import PricingError
 
 
-class VolSource:
-    """market::VolSource (src/market/market.rs:179-198): a flat vol or a surface
-    callable `vol(strike, expiry)`."""
+class SampledVolSurface:
+    """market::SampledVolSurface (src/market/market.rs:52-175): vols on a
+    strictly increasing strike x expiry grid, looked up bilinearly
+    (strike first, then expiry), flat outside the grid."""
 
-    def __init__(self, flat: Optional[float] = None, surface: Optional[Callable[[float, float], float]] = None):
+    # The grids MarketBuilder samples a non-parametric surface onto
+    # (market.rs:93-102): strikes are spot times these multipliers.
+    DEFAULT_MONEYNESS = (0.5, 0.6, 0.7, 0.8, 0.9, 0.95, 1.0, 1.05, 1.1, 1.15, 1.2, 1.3, 1.4, 1.5, 1.7, 1.9, 2.1)
+    DEFAULT_EXPIRIES = (1.0 / 52.0, 1.0 / 12.0, 0.25, 0.5, 1.0, 2.0, 3.0, 5.0, 10.0)
+
+    def __init__(self, strikes: Sequence[float], expiries: Sequence[float], vols: Sequence[Sequence[float]]):
+        self.strikes = [float(k) for k in strikes]
+        self.expiries = [float(t) for t in expiries]
+        self.vols = [[float(v) for v in row] for row in vols]
+
+    @staticmethod
+    def new(strikes, expiries, vols) -> "SampledVolSurface":
+        """SampledVolSurface::new (market.rs:62-91), same messages (raised as InvalidInput)."""
+        if len(strikes) < 2 or len(expiries) < 2:
+            raise PricingError.InvalidInput("sampled surface requires >= 2 strikes and >= 2 expiries")
+        if any(b <= a for a, b in zip(strikes, strikes[1:])):
+            raise PricingError.InvalidInput("sampled surface strikes must be strictly increasing")
+        if any(b <= a for a, b in zip(expiries, expiries[1:])):
+            raise PricingError.InvalidInput("sampled surface expiries must be strictly increasing")
+        if len(vols) != len(expiries):
+            raise PricingError.InvalidInput("sampled surface row count must match expiries")
+        if any(len(row) != len(strikes) for row in vols):
+            raise PricingError.InvalidInput("sampled surface each row must match strike count")
+        if any((not math.isfinite(v)) or v <= 0.0 for row in vols for v in row):
+            raise PricingError.InvalidInput("sampled surface vols must be finite and > 0")
+        return SampledVolSurface(strikes, expiries, vols)
+
+    @staticmethod
+    def from_surface(surface: Callable[[float, float], float], spot: float) -> "SampledVolSurface":
+        """SampledVolSurface::from_surface (market.rs:127-146)."""
+        spot = max(spot, 1.0e-8)
+        strikes = [max(spot * m, 1.0e-8) for m in SampledVolSurface.DEFAULT_MONEYNESS]
+        rows = []
+        for t in SampledVolSurface.DEFAULT_EXPIRIES:
+            row = []
+            for k in strikes:
+                v = float(surface(k, t))
+                row.append(max(v, 1.0e-8) if math.isfinite(v) else 1.0e-8)
+            rows.append(row)
+        return SampledVolSurface(strikes, list(SampledVolSurface.DEFAULT_EXPIRIES), rows)
+
+    @staticmethod
+    def _locate(grid, x):
+        if x <= grid[0]:
+            return 0, 0, 0.0
+        last = len(grid) - 1
+        if x >= grid[last]:
+            return last, last, 0.0
+        lo = 0
+        for i in range(last):
+            if grid[i] <= x <= grid[i + 1]:
+                lo = i
+                break
+        return lo, lo + 1, (x - grid[lo]) / (grid[lo + 1] - grid[lo])
+
+    def vol(self, strike: float, expiry: float) -> float:
+        e0, e1, ew = self._locate(self.expiries, max(expiry, self.expiries[0]))
+        s0, s1, sw = self._locate(self.strikes, max(strike, self.strikes[0]))
+        v = self.vols
+        if e0 == e1 and s0 == s1:
+            return v[e0][s0]
+        if e0 == e1:
+            return v[e0][s0] + (v[e0][s1] - v[e0][s0]) * sw
+        if s0 == s1:
+            return v[e0][s0] + (v[e1][s0] - v[e0][s0]) * ew
+        a = v[e0][s0] + (v[e0][s1] - v[e0][s0]) * sw
+        b = v[e1][s0] + (v[e1][s1] - v[e1][s0]) * sw
+        return a + (b - a) * ew
+
+    def grid(self):
+        """(strikes, expiries, vols[expiry][strike]) as float64 arrays."""
+        import numpy as np
+        return (np.asarray(self.strikes, dtype=np.float64), np.asarray(self.expiries, dtype=np.float64),
+                np.asarray(self.vols, dtype=np.float64))
+
+
+class VolSource:
+    """market::VolSource (src/market/market.rs:179-198): a flat vol, or a
+    sampled surface (MarketBuilder samples a callable surface onto the
+    default grid, as the reference does for non-parametric surfaces)."""
+
+    def __init__(self, flat: Optional[float] = None, sampled: Optional[SampledVolSurface] = None,
+                 surface: Optional[Callable[[float, float], float]] = None):
         self.flat = flat
+        self.sampled = sampled
         self.surface = surface
 
     def vol(self, strike: float, expiry: float) -> float:
+        if self.sampled is not None:
+            return self.sampled.vol(strike, expiry)
         if self.surface is not None:
             return float(self.surface(strike, expiry))
         return float(self.flat)
+
+    def grid(self):
+        """The source as a sampled grid (a flat vol is a 1 x 1 grid)."""
+        import numpy as np
+        if self.sampled is not None:
+            return self.sampled.grid()
+        if self.surface is not None:
+            raise PricingError.InvalidInput("an unsampled vol surface has no grid")
+        one = np.ones(1, dtype=np.float64)
+        return one, one, np.full((1, 1), float(self.flat))
 
 
 @dataclass
@@ -78,7 +175,9 @@ class MarketBuilder:
         self._surface = None
         return self
 
-    def vol_surface(self, surface: Callable[[float, float], float]) -> "MarketBuilder":
+    def vol_surface(self, surface) -> "MarketBuilder":
+        """A SampledVolSurface, or a callable vol(strike, expiry) that build()
+        samples onto the default grid (market.rs:385-391)."""
         self._surface = surface
         self._flat = None
         return self
@@ -93,7 +192,10 @@ class MarketBuilder:
         if self._spot <= 0.0:
             raise PricingError.InvalidInput("market spot must be > 0")
         if self._surface is not None:
-            vol = VolSource(surface=self._surface)
+            if isinstance(self._surface, SampledVolSurface):
+                vol = VolSource(sampled=self._surface)
+            else:
+                vol = VolSource(sampled=SampledVolSurface.from_surface(self._surface, self._spot))
         else:
             if self._flat is None:
                 raise PricingError.InvalidInput("either market flat_vol or vol_surface is required")

@@ -1045,6 +1045,242 @@ int orc_lsm_price(int option_type, double strike, double expiry, int exercise, c
 }
 
 /* ------------------------------------------------------------------------ */
+/* Bermudan LSM with the exercise boundary                                  */
+/* ------------------------------------------------------------------------ */
+
+/* SampledVolSurface::locate_bounds, src/market/market.rs:104-125 */
+static void sampled_locate(const double* g, int64_t n, double x, int64_t* lo, int64_t* hi, double* w) {
+  if (x <= g[0]) {
+    *lo = *hi = 0;
+    *w = 0.0;
+    return;
+  }
+  if (x >= g[n - 1]) {
+    *lo = *hi = n - 1;
+    *w = 0.0;
+    return;
+  }
+  int64_t l = 0;
+  for (int64_t i = 0; i < n - 1; ++i)
+    if (x >= g[i] && x <= g[i + 1]) {
+      l = i;
+      break;
+    }
+  *lo = l;
+  *hi = l + 1;
+  *w = (x - g[l]) / (g[l + 1] - g[l]);
+}
+
+/* SampledVolSurface::vol (bilinear), src/market/market.rs:149-174; vols is
+ * row-major [expiry][strike]. */
+double orc_sampled_vol(const double* strikes, int64_t nk, const double* expiries, int64_t nt, const double* vols,
+                       double strike, double expiry) {
+  int64_t e0, e1, s0, s1;
+  double ew, sw;
+  sampled_locate(expiries, nt, expiry > expiries[0] ? expiry : expiries[0], &e0, &e1, &ew);
+  sampled_locate(strikes, nk, strike > strikes[0] ? strike : strikes[0], &s0, &s1, &sw);
+  if (e0 == e1 && s0 == s1) return vols[e0 * nk + s0];
+  if (e0 == e1) {
+    const double v0 = vols[e0 * nk + s0], v1 = vols[e0 * nk + s1];
+    return v0 + (v1 - v0) * sw;
+  }
+  if (s0 == s1) {
+    const double v0 = vols[e0 * nk + s0], v1 = vols[e1 * nk + s0];
+    return v0 + (v1 - v0) * ew;
+  }
+  const double v00 = vols[e0 * nk + s0], v01 = vols[e0 * nk + s1];
+  const double v10 = vols[e1 * nk + s0], v11 = vols[e1 * nk + s1];
+  const double v0 = v00 + (v01 - v00) * sw;
+  const double v1 = v10 + (v11 - v10) * sw;
+  return v0 + (v1 - v0) * ew;
+}
+
+/* LongstaffSchwartzEngine::price_bermudan_with_boundary restated
+ * (src/engines/lsm/longstaff_schwartz.rs:294-417, paths :190-283). */
+int orc_lsm_bermudan(int option_type, double expiry, const double* sched_t, const double* sched_k, int64_t n_sched,
+                     int dynamics, double spot, double rate, double q, double vol, const double* lv_strikes,
+                     int64_t lv_nk, const double* lv_expiries, int64_t lv_nt, const double* lv_vols, double kappa,
+                     double theta, double xi, double rho, double v0, int64_t num_paths, int64_t num_steps,
+                     uint64_t seed, int degree, const double* normals, double* out2, double* boundary,
+                     int64_t* n_boundary) {
+  if (num_steps < 2 || num_paths < 3 || n_sched < 1) return OF_ERR_INVALID_INPUT;
+  if (degree != 2 && degree != 3) return OF_ERR_INVALID_INPUT;
+  const int64_t M = num_steps;
+  const double dt = expiry / (double)M;
+  const double sqrt_dt = sqrt(dt);
+  const double drift_rn = rate - q;
+  const double terminal_strike = sched_k[n_sched - 1];
+  const int64_t stride = (M + 1 + 7) & ~(int64_t)7;
+  const int draws = dynamics == 2 ? 2 : 1;
+  double* paths = (double*)malloc(sizeof(double) * (size_t)(num_paths * stride));
+  double* values = (double*)malloc(sizeof(double) * (size_t)num_paths);
+  int64_t* itm = (int64_t*)malloc(sizeof(int64_t) * (size_t)num_paths);
+  int64_t* sched_of_step = (int64_t*)malloc(sizeof(int64_t) * (size_t)(M + 1));
+  if (!paths || !values || !itm || !sched_of_step) {
+    free(paths);
+    free(values);
+    free(itm);
+    free(sched_of_step);
+    return OF_ERR_ALLOC;
+  }
+  orc_xoshiro rng;
+  orc_xoshiro_seed(&rng, seed);
+  for (int64_t pi = 0; pi < num_paths; ++pi) {
+    double* row = paths + pi * stride;
+    const double* z = normals ? normals + pi * M * draws : NULL;
+    row[0] = spot;
+    double s = spot, v = v0;
+    for (int64_t ti = 1; ti <= M; ++ti) {
+      const double z1 = z ? z[(ti - 1) * draws] : draw_normal(&rng);
+      if (dynamics == 0) {
+        const double drift = (drift_rn - 0.5 * vol * vol) * dt;
+        const double step_vol = vol * sqrt_dt;
+        row[ti] = row[ti - 1] * exp(fma(step_vol, z1, drift));
+      } else if (dynamics == 1) {
+        const double t = (double)ti * dt > 1.0e-8 ? (double)ti * dt : 1.0e-8;
+        const double sigma =
+            orc_sampled_vol(lv_strikes, lv_nk, lv_expiries, lv_nt, lv_vols, s > 1.0e-8 ? s : 1.0e-8, t);
+        const double drift = (drift_rn - 0.5 * sigma * sigma) * dt;
+        s *= exp(drift + sigma * sqrt_dt * z1);
+        row[ti] = s > 1.0e-12 ? s : 1.0e-12;
+        s = row[ti];
+      } else {
+        const double z2 = z ? z[(ti - 1) * draws + 1] : draw_normal(&rng);
+        /* Heston::step_euler, src/models/stochastic.rs:56-71 (mu = r - q) */
+        const double v_pos = v > 0.0 ? v : 0.0;
+        const double zs = rho * z1 + sqrt(1.0 - rho * rho) * z2;
+        double v_next = v + kappa * (theta - v_pos) * dt + xi * sqrt(v_pos) * sqrt_dt * z1;
+        v_next = v_next > 0.0 ? v_next : 0.0;
+        const double s_next = s * exp((drift_rn - 0.5 * v_pos) * dt + sqrt(v_pos) * sqrt_dt * zs);
+        s = s_next > 1.0e-12 ? s_next : 1.0e-12;
+        v = v_next > 0.0 ? v_next : 0.0;
+        row[ti] = s;
+      }
+    }
+  }
+  const double disc = exp(-rate * dt);
+  for (int64_t i = 0; i <= M; ++i) sched_of_step[i] = -1;
+  for (int64_t d = 0; d < n_sched; ++d) {
+    double idx = round((sched_t[d] / expiry) * (double)M);
+    int64_t i = isnan(idx) || idx < 1.0 ? 1 : (idx > (double)M ? M : (int64_t)idx);
+    sched_of_step[i] = d;
+  }
+  int64_t terminal_itm = 0;
+  for (int64_t pi = 0; pi < num_paths; ++pi) {
+    values[pi] = vanilla_payoff(option_type, paths[pi * stride + M], terminal_strike);
+    if (values[pi] > 0.0) ++terminal_itm;
+  }
+  /* boundary records, filled last date first then reversed */
+  int64_t nb = 0;
+  double* rec = boundary + 5 * nb++;
+  rec[0] = expiry;
+  rec[1] = terminal_strike;
+  rec[2] = terminal_strike;
+  rec[3] = (double)terminal_itm;
+  rec[4] = (double)terminal_itm;
+  for (int64_t ti = M - 1; ti >= 1; --ti) {
+    for (int64_t pi = 0; pi < num_paths; ++pi) values[pi] *= disc;
+    const int64_t d = sched_of_step[ti];
+    if (d < 0) continue;
+    const double strike = sched_k[d];
+    int64_t n_itm = 0;
+    for (int64_t pi = 0; pi < num_paths; ++pi)
+      if (vanilla_payoff(option_type, paths[pi * stride + ti], strike) > 0.0) itm[n_itm++] = pi;
+    rec = boundary + 5 * nb++;
+    rec[0] = sched_t[d];
+    rec[1] = strike;
+    rec[2] = NAN;
+    rec[3] = (double)n_itm;
+    rec[4] = 0.0;
+    if (n_itm < 3) continue;
+    double beta[4] = {0, 0, 0, 0};
+    const double inv_k = 1.0 / strike;
+    if (degree == 2) {
+      double s1 = 0, s_s = 0, s_s2 = 0, s_s3 = 0, s_s4 = 0, s_y = 0, s_sy = 0, s_s2y = 0;
+      for (int64_t k = 0; k < n_itm; ++k) {
+        const double s = paths[itm[k] * stride + ti];
+        const double s2 = s * s;
+        const double y = values[itm[k]];
+        s1 += 1.0;
+        s_s += s;
+        s_s2 += s2;
+        s_s3 += s2 * s;
+        s_s4 += s2 * s2;
+        s_y += y;
+        s_sy += s * y;
+        s_s2y += s2 * y;
+      }
+      double a[3][3] = {{s1, s_s, s_s2}, {s_s, s_s2, s_s3}, {s_s2, s_s3, s_s4}};
+      double b[3] = {s_y, s_sy, s_s2y};
+      double x[3];
+      if (lu_solve3(a, b, x)) {
+        beta[0] = x[0];
+        beta[1] = x[1];
+        beta[2] = x[2];
+      }
+    } else {
+      double m[7] = {0, 0, 0, 0, 0, 0, 0}, r[4] = {0, 0, 0, 0};
+      for (int64_t k = 0; k < n_itm; ++k) {
+        const double x = paths[itm[k] * stride + ti] * inv_k;
+        const double y = values[itm[k]];
+        double p = 1.0;
+        for (int e = 0; e < 7; ++e) {
+          m[e] += p;
+          if (e < 4) r[e] += p * y;
+          p *= x;
+        }
+      }
+      double a[4][4];
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) a[i][j] = m[i + j];
+      double x4[4];
+      if (chol_solve4(a, r, x4))
+        for (int i = 0; i < 4; ++i) beta[i] = x4[i];
+    }
+    int64_t n_ex = 0;
+    double bnd = NAN;
+    for (int64_t k = 0; k < n_itm; ++k) {
+      const double s = paths[itm[k] * stride + ti];
+      const double cont = degree == 2 ? beta[0] + beta[1] * s + beta[2] * s * s
+                                      : beta[0] + (s * inv_k) * (beta[1] + (s * inv_k) * (beta[2] + (s * inv_k) * beta[3]));
+      const double ex = vanilla_payoff(option_type, s, strike);
+      if (ex > cont) {
+        values[itm[k]] = ex;
+        /* boundary_from_exercised, :178-188: put max, call min */
+        if (n_ex == 0 || (option_type == OF_PUT ? s > bnd : s < bnd)) bnd = s;
+        ++n_ex;
+      }
+    }
+    rec[2] = bnd;
+    rec[4] = (double)n_ex;
+  }
+  double sum = 0.0, sum_sq = 0.0;
+  for (int64_t pi = 0; pi < num_paths; ++pi) {
+    const double v = values[pi] * disc;
+    sum += v;
+    sum_sq += v * v;
+  }
+  const double n = (double)num_paths;
+  const double mean = sum / n;
+  const double var = num_paths > 1 ? (sum_sq - sum * sum / n) / (n - 1.0) : 0.0;
+  out2[0] = mean;
+  out2[1] = sqrt(var / n);
+  /* chronological order */
+  for (int64_t i = 0, j = nb - 1; i < j; ++i, --j)
+    for (int f = 0; f < 5; ++f) {
+      const double t = boundary[5 * i + f];
+      boundary[5 * i + f] = boundary[5 * j + f];
+      boundary[5 * j + f] = t;
+    }
+  *n_boundary = nb;
+  free(paths);
+  free(values);
+  free(itm);
+  free(sched_of_step);
+  return OF_OK;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Reference WGSL shader math (src/engines/gpu/mc_shader.wgsl, gpu_mc.rs)    */
 /* ------------------------------------------------------------------------ */
 

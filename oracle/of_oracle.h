@@ -93,6 +93,27 @@ int orc_lsm_price(int option_type, double strike, double expiry, int exercise, c
                   double spot, double rate, double q, double vol, int64_t num_paths, int64_t num_steps,
                   uint64_t seed, int degree, const double* normals, double* out2);
 
+/* SampledVolSurface::vol (src/market/market.rs:104-174): bilinear lookup on a
+ * strictly increasing strike x expiry grid, vols row-major [expiry][strike]. */
+double orc_sampled_vol(const double* strikes, int64_t nk, const double* expiries, int64_t nt, const double* vols,
+                       double strike, double expiry);
+
+/* LongstaffSchwartzEngine::price_bermudan_with_boundary restated
+ * (src/engines/lsm/longstaff_schwartz.rs:294-417; path simulation :190-283).
+ * Schedule: n_sched (time, strike) pairs, BermudanOption::effective_schedule.
+ * dynamics: 0 GBM (vol), 1 local-vol Euler on the sampled grid lv_*,
+ * 2 Heston Euler (kappa..v0, drift r - q).  normals: NULL draws the single
+ * sequential xoshiro stream (1 draw per step, 2 for Heston: z1 then z2),
+ * else [path][step][draw].  out2 = {price, stderr}; boundary receives
+ * n_sched + 1 records at most of {time, strike, boundary_spot (NaN = none),
+ * itm_paths, exercised_paths}, chronological; *n_boundary = records. */
+int orc_lsm_bermudan(int option_type, double expiry, const double* sched_t, const double* sched_k, int64_t n_sched,
+                     int dynamics, double spot, double rate, double q, double vol, const double* lv_strikes,
+                     int64_t lv_nk, const double* lv_expiries, int64_t lv_nt, const double* lv_vols, double kappa,
+                     double theta, double xi, double rho, double v0, int64_t num_paths, int64_t num_steps,
+                     uint64_t seed, int degree, const double* normals, double* out2, double* boundary,
+                     int64_t* n_boundary);
+
 /* Reference WGSL kernel math (src/engines/gpu/mc_shader.wgsl:28-142) in C
  * float arithmetic.  Returns the per-workgroup sums the shader writes. */
 int orc_wgsl_european(double spot, double strike, double rate, double vol, double expiry, uint32_t num_paths,

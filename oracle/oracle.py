@@ -76,6 +76,11 @@ def lib():
         L.orc_lsm_price.restype = C.c_int
         L.orc_lsm_price.argtypes = [C.c_int, D, D, C.c_int, PD, I64, D, D, D, D, I64, I64, C.c_uint64, C.c_int,
                                     PD, PD]
+        L.orc_sampled_vol.restype = D
+        L.orc_sampled_vol.argtypes = [PD, I64, PD, I64, PD, D, D]
+        L.orc_lsm_bermudan.restype = C.c_int
+        L.orc_lsm_bermudan.argtypes = ([C.c_int, D, PD, PD, I64, C.c_int, D, D, D, D, PD, I64, PD, I64, PD] + [D] * 5 +
+                                       [I64, I64, C.c_uint64, C.c_int, PD, PD, PD, C.POINTER(I64)])
         L.orc_wgsl_european.restype = C.c_int
         L.orc_wgsl_european.argtypes = [D, D, D, D, D, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, PD, PD]
         L.orc_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
@@ -213,6 +218,43 @@ def lsm_price(option_type, strike, expiry, exercise, spot, rate, q, vol, num_pat
     if st != 0:
         raise RuntimeError(f"orc_lsm_price status {st}")
     return float(out[0]), float(out[1])
+
+
+def sampled_vol(strikes, expiries, vols, strike, expiry):
+    k = np.ascontiguousarray(strikes, dtype=np.float64)
+    t = np.ascontiguousarray(expiries, dtype=np.float64)
+    v = np.ascontiguousarray(vols, dtype=np.float64)
+    return lib().orc_sampled_vol(_ptr(k), len(k), _ptr(t), len(t), _ptr(v), strike, expiry)
+
+
+def lsm_bermudan(option_type, expiry, schedule, spot, rate, q, num_paths, num_steps, seed, dynamics=0, vol=0.0,
+                 lv=None, heston=None, degree=2, normals=None):
+    """Bermudan LSM with the exercise boundary; schedule = [(t, K), ...];
+    lv = (strikes, expiries, vols[expiry][strike]); heston = (kappa, theta, xi, rho, v0).
+    Returns (price, stderr, [(time, strike, boundary or None, itm, exercised), ...])."""
+    ts = np.ascontiguousarray([a for a, _ in schedule], dtype=np.float64)
+    ks = np.ascontiguousarray([b for _, b in schedule], dtype=np.float64)
+    lk = lt = lvv = None
+    if lv is not None:
+        lk = np.ascontiguousarray(lv[0], dtype=np.float64)
+        lt = np.ascontiguousarray(lv[1], dtype=np.float64)
+        lvv = np.ascontiguousarray(lv[2], dtype=np.float64)
+    h = heston or (0.0, 0.0, 0.0, 0.0, 0.0)
+    z = None if normals is None else np.ascontiguousarray(normals, dtype=np.float64)
+    out = np.zeros(2)
+    bnd = np.zeros(5 * (len(schedule) + 1))
+    nb = I64()
+    st = lib().orc_lsm_bermudan(option_type, expiry, _ptr(ts), _ptr(ks), len(ts), dynamics, spot, rate, q, vol,
+                                _ptr(lk), 0 if lk is None else len(lk), _ptr(lt), 0 if lt is None else len(lt),
+                                _ptr(lvv), *h, num_paths, num_steps, seed, degree, _ptr(z), _ptr(out), _ptr(bnd),
+                                C.byref(nb))
+    if st != 0:
+        raise RuntimeError(f"orc_lsm_bermudan status {st}")
+    recs = []
+    for i in range(nb.value):
+        t, k, b, itm, ex = bnd[5 * i:5 * i + 5]
+        recs.append((float(t), float(k), None if np.isnan(b) else float(b), int(itm), int(ex)))
+    return float(out[0]), float(out[1]), recs
 
 
 def wgsl_european(spot, strike, rate, vol, expiry, num_paths, num_steps, seed, is_call=True):

@@ -7,6 +7,7 @@ Reads (once, in a container where the openferric source tree is mounted):
   tests/fixtures/heston_expected_put_call.csv
   tests/fixtures/asian_arithmetic_cases4.csv
   tests/fang_oosterlee_heston.rs         Fang-Oosterlee (2008) parameter set and values
+  tests/bermudan_quantlib.rs             QuantLib FD Bermudan cases and the LSM engine settings
 The fixtures are committed so that the GPU tests need no access to the
 reference tree.
 
@@ -98,6 +99,32 @@ def fang_oosterlee(ref):
     return {"source": "tests/fang_oosterlee_heston.rs (Fang-Oosterlee 2008)", "params": consts, "values": vals}
 
 
+def bermudan_quantlib(ref):
+    src = open(os.path.join(ref, "tests/bermudan_quantlib.rs")).read()
+    grids = {}
+    for name, body in re.findall(r"const (D\w+): &\[f64\] = &\[(.*?)\];", src, re.S):
+        grids[name] = [float(x.replace("_", "")) for x in re.findall(r"[0-9][0-9_.eE]*", body)]
+    fn = src[src.index("fn quantlib_reference_cases"):]
+    fn = fn[:fn.index("\n}\n")]
+    cases = []
+    for m in re.finditer(r"QlBermudanCase\s*\{(.*?)\}", fn, re.S):
+        f = dict(re.findall(r"(\w+):\s*([^,]+),", m.group(1)))
+        cases.append({"option_type": "Put" if "Put" in f["option_type"] else "Call",
+                      "spot": float(f["spot"].replace("_", "")), "strike": float(f["strike"].replace("_", "")),
+                      "rate": float(f["rate"].replace("_", "")), "dividend": float(f["dividend"].replace("_", "")),
+                      "vol": float(f["vol"].replace("_", "")), "expiry": float(f["expiry"].replace("_", "")),
+                      "dates": grids[f["dates"].strip()],
+                      "quantlib_fd_price": float(f["quantlib_fd_price"].replace("_", ""))})
+    test = src[src.index("fn bermudan_lsm_matches_quantlib_fd_within_half_percent_on_reference_puts"):]
+    mm = re.search(r"LongstaffSchwartzEngine::new\(([0-9_]+),\s*([0-9_]+),\s*([0-9_]+)\)", test)
+    tol = re.search(r"err <= ([0-9.]+)", test)
+    return {"source": "tests/bermudan_quantlib.rs (QuantLib 1.41 FdBlackScholesVanillaEngine(2000, 400) Bermudan "
+                      "prices; LSM put check)",
+            "lsm_engine": {"num_paths": int(mm.group(1).replace("_", "")), "num_steps": int(mm.group(2).replace("_", "")),
+                           "seed": int(mm.group(3).replace("_", ""))},
+            "rel_tolerance": float(tol.group(1)), "cases": cases}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -107,6 +134,7 @@ def main():
         "heston_lewis.json": heston_lewis(a.reference),
         "asian_cases4.json": asian_cases4(a.reference),
         "fang_oosterlee.json": fang_oosterlee(a.reference),
+        "bermudan_quantlib.json": bermudan_quantlib(a.reference),
     }
     for name, data in fixtures.items():
         with open(os.path.join(HERE, name), "w") as f:

@@ -45,6 +45,9 @@ STRUCTS = {
     "of_lsm_contract": A.OfLsmContract,
     "of_lsm_config": A.OfLsmConfig,
     "of_lsm_result": A.OfLsmResult,
+    "of_heston_adjoint_params": A.OfHestonAdjointParams,
+    "of_adjoint_result": A.OfAdjointResult,
+    "of_device_peaks": A.OfDevicePeaks,
 }
 
 

@@ -274,3 +274,13 @@ def test_qe_has_no_fp64_reference_mode():
     gen = HestonPathGenerator(Heston(0.03, 2.0, 0.04, 0.5, -0.7, 0.04), 100.0, 1.0, 8, scheme="qe")
     with pytest.raises(PricingError):
         MonteCarloEngine(100, 1).run(gen, VanillaOption.european_call(100, 1), 1.0)
+
+
+def test_device_peak_probes_are_plausible():
+    """The roofline denominators: MUFU results/s and FP32 flops/s of a B200
+    (148 SMs, <= 2.1 GHz: nominal 16 MUFU and 256 FP32 flops per clock per SM)."""
+    from openferric_b200._lib import context
+    p = context(0).device_peaks()
+    assert 1e12 < p["sfu_ops_per_s"] < 148 * 16 * 2.1e9 * 1.05
+    assert 2e13 < p["fp32_flops_per_s"] < 148 * 256 * 2.1e9 * 1.05
+    assert p["probe_ms"] > 0.0

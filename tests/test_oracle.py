@@ -353,6 +353,87 @@ def test_lsm_european_exercise_is_discounted_payoff(orc):
     assert abs(p - bs) < 3 * s + 1e-3
 
 
+# ---- Bermudan LSM (tests/bermudan_quantlib.rs:73-389) ----------------------------
+def _schedule(c):
+    s = [(t, c["strike"]) for t in c["dates"]]
+    if c["expiry"] - s[-1][0] > 1e-12:
+        s.append((c["expiry"], c["strike"]))
+    return s
+
+
+def test_bermudan_oracle_matches_quantlib_fd_puts(orc):
+    """The reference's own check: LSM(450000 paths, 120 steps, seed 7) within
+    0.5 % of the QuantLib FD price on every put case, with a populated boundary."""
+    g = load_golden("bermudan_quantlib.json")
+    e = g["lsm_engine"]
+    puts = [c for c in g["cases"] if c["option_type"] == "Put"]
+    assert len(puts) == 5
+    for c in puts:
+        p, se, recs = orc.lsm_bermudan(OF_PUT, c["expiry"], _schedule(c), c["spot"], c["rate"], c["dividend"],
+                                       e["num_paths"], e["num_steps"], e["seed"], dynamics=0, vol=c["vol"])
+        assert abs(p - c["quantlib_fd_price"]) / c["quantlib_fd_price"] <= g["rel_tolerance"], (c, p, se)
+        assert any(r[2] is not None for r in recs)
+        # chronological, terminal last: (expiry, K, K, itm, itm)
+        assert [r[0] for r in recs] == sorted(r[0] for r in recs)
+        assert recs[-1][0] == c["expiry"] and recs[-1][2] == c["strike"] and recs[-1][3] == recs[-1][4]
+        for t, k, b, itm, ex in recs[:-1]:
+            assert ex <= itm
+            if b is not None:
+                assert b < k  # a put is exercised below the strike
+
+
+def test_bermudan_oracle_step_down_strike_is_cheaper(orc):
+    dates = [0.25, 0.5, 0.75, 1.0]
+    step = orc.lsm_bermudan(OF_PUT, 1.0, list(zip(dates, [100.0, 97.5, 95.0, 92.5])), 100.0, 0.03, 0.0, 60000, 100,
+                            42, vol=0.25)
+    const = orc.lsm_bermudan(OF_PUT, 1.0, [(t, 100.0) for t in dates], 100.0, 0.03, 0.0, 60000, 100, 42, vol=0.25)
+    assert step[0] < const[0]
+    assert [r[1] for r in step[2]] == [100.0, 97.5, 95.0, 92.5]
+
+
+def test_bermudan_oracle_local_vol_and_heston_dynamics(orc):
+    """bermudan_quantlib.rs:268-335 at reduced path counts: finite positive
+    prices and a populated boundary under both dynamics; a flat local-vol grid
+    and a zero vol-of-vol Heston reproduce the GBM price on the same draws'
+    distribution within a few SE."""
+    from openferric_b200.market import Market
+    sched = [(t, 100.0) for t in (0.2, 0.4, 0.6, 0.8, 1.0)]
+
+    def smile(k, t):
+        return max(0.18 + 0.08 * abs(k / 100.0 - 1.0) + 0.03 * math.sqrt(max(t, 1e-6)), 0.05)
+
+    m = Market.builder().spot(100).rate(0.02).dividend_yield(0.01).vol_surface(smile).build()
+    lv = m.vol.grid()
+    p, se, recs = orc.lsm_bermudan(OF_PUT, 1.0, sched, 100.0, 0.02, 0.01, 20000, 90, 123, dynamics=1, lv=lv)
+    assert math.isfinite(p) and p > 0 and any(r[2] is not None for r in recs)
+    p, se, recs = orc.lsm_bermudan(OF_PUT, 1.0, sched, 100.0, 0.02, 0.01, 20000, 100, 321, dynamics=2,
+                                   heston=(2.0, 0.04, 0.6, -0.5, 0.04))
+    assert math.isfinite(p) and p > 0 and any(r[2] is not None for r in recs)
+    flat = (np.ones(1), np.ones(1), np.full((1, 1), 0.2))
+    g = orc.lsm_bermudan(OF_PUT, 1.0, sched, 100.0, 0.02, 0.01, 40000, 50, 5, dynamics=0, vol=0.2)
+    l = orc.lsm_bermudan(OF_PUT, 1.0, sched, 100.0, 0.02, 0.01, 40000, 50, 5, dynamics=1, lv=flat)
+    h = orc.lsm_bermudan(OF_PUT, 1.0, sched, 100.0, 0.02, 0.01, 40000, 50, 6, dynamics=2,
+                         heston=(1.0, 0.04, 0.0, 0.0, 0.04))
+    assert abs(g[0] - l[0]) < 1e-9  # same single stream, same GBM arithmetic up to the 1e-12 floor
+    assert abs(g[0] - h[0]) < 4 * math.hypot(g[1], h[1])
+
+
+def test_sampled_vol_matches_python_mirror(orc):
+    from openferric_b200.market import Market
+
+    def smile(k, t):
+        return 0.2 + 0.1 * (k / 100.0 - 1.0) ** 2 + 0.02 * t
+
+    m = Market.builder().spot(100).vol_surface(smile).build()
+    K, T, V = m.vol.grid()
+    rng = np.random.default_rng(3)
+    for k, t in zip(rng.uniform(10, 300, 500), rng.uniform(0, 15, 500)):
+        assert orc.sampled_vol(K, T, V, k, t) == m.vol_for(k, t)
+    for k in K:  # grid points take the lower interval with weight 1, as the linear scan does
+        for t in T:
+            assert orc.sampled_vol(K, T, V, k, t) == m.vol_for(k, t)
+
+
 # ---- mc_aad.rs:344-480, mc_greeks.rs:344-419 ------------------------------------
 def test_pathwise_aad_recovers_bs_greeks(orc):
     g = orc.gbm_pathwise_aad(OF_CALL, 100.0, 100.0, 0.03, 0.01, 0.2, 1.0, 120000, 64, 42, True)
