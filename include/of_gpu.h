@@ -296,6 +296,55 @@ typedef struct of_lsm_result {
 of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* contracts, int64_t n,
                        const of_lsm_config* cfg, of_lsm_result* results);
 
+/* ---- Bermudan LSM with the exercise boundary ----------------------------- */
+/* LsmDynamics (src/engines/lsm/longstaff_schwartz.rs:24-39) */
+enum { OF_LSM_GBM = 0, OF_LSM_LOCAL_VOL = 1, OF_LSM_HESTON_EULER = 2 };
+
+typedef struct of_bermudan_contract {
+  int32_t option_type; /* OF_CALL / OF_PUT */
+  int32_t dynamics;    /* OF_LSM_* */
+  double spot, rate, dividend_yield;
+  double vol;          /* GBM: market.vol_for(terminal strike, expiry) */
+  double expiry;
+  int64_t num_steps;
+  /* BermudanOption::effective_schedule (src/instruments/bermudan.rs:82-101):
+   * strictly increasing times in (0, expiry] and their strikes */
+  const double* schedule_times;
+  const double* schedule_strikes;
+  int64_t n_schedule;
+  /* OF_LSM_LOCAL_VOL: the market's sampled surface (SampledVolSurface,
+   * src/market/market.rs:52-175), strictly increasing grids, vols row-major
+   * [expiry][strike]; a flat vol is a 1 x 1 grid */
+  const double* lv_strikes;
+  int64_t lv_n_strikes;
+  const double* lv_expiries;
+  int64_t lv_n_expiries;
+  const double* lv_vols;
+  /* OF_LSM_HESTON_EULER (with_heston_dynamics, :95-112; drift r - q) */
+  double kappa, theta, xi, rho, v0;
+} of_bermudan_contract;
+
+/* ExerciseBoundaryPoint (longstaff_schwartz.rs:42-55) */
+typedef struct of_boundary_point {
+  double time, strike;
+  double boundary_spot;  /* NaN when no path exercised (has_boundary = 0) */
+  int32_t has_boundary;
+  int32_t reserved0;
+  int64_t itm_paths, exercised_paths;
+} of_boundary_point;
+
+/* LongstaffSchwartzEngine::price_bermudan_with_boundary
+ * (src/engines/lsm/longstaff_schwartz.rs:294-417): price, stderr and the
+ * exercise boundary (largest exercised spot of a put, smallest of a call)
+ * at every scheduled step before expiry plus the terminal point, in
+ * chronological order.  FP64 reference mode draws the reference's single
+ * xoshiro256++ stream (1 normal per step, 2 for Heston: z1 then z2).
+ * `boundary` receives min(capacity, *n_boundary) points; *n_boundary is the
+ * full count (at most n_schedule + 1).  want_delta is rejected for local vol. */
+of_status of_lsm_bermudan(of_ctx* ctx, const of_bermudan_contract* contract, const of_lsm_config* cfg,
+                          of_lsm_result* result, of_boundary_point* boundary, int64_t capacity,
+                          int64_t* n_boundary);
+
 /* xoshiro256++ jump-ahead: the state of the stream seeded with `seed`
  * (Xoshiro256PlusPlus::seed_from_u64, src/math/fast_rng.rs:36-48) after
  * `draws` calls of next_u64, computed on the device by GF(2) matrix powers.

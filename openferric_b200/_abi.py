@@ -237,3 +237,44 @@ class OfDevicePeaks(C.Structure):
         ("fp32_flops_per_s", C.c_double),
         ("probe_ms", C.c_double),
     ]
+
+
+OF_LSM_GBM, OF_LSM_LOCAL_VOL, OF_LSM_HESTON_EULER = 0, 1, 2
+
+
+class OfBermudanContract(C.Structure):
+    _fields_ = [
+        ("option_type", C.c_int32),
+        ("dynamics", C.c_int32),
+        ("spot", C.c_double),
+        ("rate", C.c_double),
+        ("dividend_yield", C.c_double),
+        ("vol", C.c_double),
+        ("expiry", C.c_double),
+        ("num_steps", C.c_int64),
+        ("schedule_times", C.POINTER(C.c_double)),
+        ("schedule_strikes", C.POINTER(C.c_double)),
+        ("n_schedule", C.c_int64),
+        ("lv_strikes", C.POINTER(C.c_double)),
+        ("lv_n_strikes", C.c_int64),
+        ("lv_expiries", C.POINTER(C.c_double)),
+        ("lv_n_expiries", C.c_int64),
+        ("lv_vols", C.POINTER(C.c_double)),
+        ("kappa", C.c_double),
+        ("theta", C.c_double),
+        ("xi", C.c_double),
+        ("rho", C.c_double),
+        ("v0", C.c_double),
+    ]
+
+
+class OfBoundaryPoint(C.Structure):
+    _fields_ = [
+        ("time", C.c_double),
+        ("strike", C.c_double),
+        ("boundary_spot", C.c_double),
+        ("has_boundary", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("itm_paths", C.c_int64),
+        ("exercised_paths", C.c_int64),
+    ]

@@ -29,6 +29,7 @@
 
 #include "of_device.cuh"
 #include "of_internal.h"
+#include "path_fp32.cuh"
 
 namespace {
 
@@ -131,16 +132,38 @@ __global__ void jump_test_kernel(uint64_t seed, const uint64_t* draws, int64_t n
 // ---------------------------------------------------------------------------
 // Contract constants
 // ---------------------------------------------------------------------------
+enum : int32_t { DYN_GBM = 0, DYN_LOCAL_VOL = 1, DYN_HESTON = 2 };
+
 struct LsmC {
   int32_t put;
   int32_t steps;
-  double spot, strike, inv_strike, drift, step_vol, disc, inv_spot;
-  float fdrift, fstep_vol, fspot;
+  int32_t dynamics;
+  int32_t lv_nk;             // local vol: strikes in the sampled grid
+  double spot, strike, inv_strike, drift, step_vol, disc, inv_spot;  // strike = terminal strike
+  // local-vol and Heston Euler (longstaff_schwartz.rs:218-281), FP64
+  double mu, dt, sqrt_dt, kappa, theta, xi, rho, v0;
+  const double* lv_k;        // [lv_nk] strikes of the sampled surface
+  const double* lv_v;        // [n_expiries][lv_nk] vols
+  const float* lv_kf;        // FP32 copies for the Philox mode
+  const float* lv_vf;
+  float fdrift, fstep_vol, fspot, fmudt, fsqrt_dt, fdt, fy_floor;
+  of::StepConsts hc;         // FP32 Heston Euler constants
+};
+
+// Per simulation step: the strike of an exercise date there (the terminal
+// strike elsewhere) and the local-vol expiry bracket of the step's end time
+// t = max(ti dt, 1e-8) (path-independent, so computed once on the host).
+struct LsmStep {
+  double strike, inv_strike;
+  int32_t e0, e1;
+  double ew;
+  float fstrike, finv_strike, few, pad;
 };
 
 struct LsmBatch {
   const LsmC* c;             // [nc]
   const uint8_t* can_ex;     // [nc][steps+1]
+  const LsmStep* st;         // [nc][steps+1]
   int32_t nc, steps;
   int64_t n, npad;           // paths, padded path stride
   void* S;                   // [nc][steps][npad] (T)
@@ -155,10 +178,15 @@ struct LsmBatch {
   int32_t blocks;            // blocks per contract
   int32_t degree;
   int32_t want_delta;
+  int32_t track;             // exercise-boundary statistics wanted
+  unsigned long long* ex_count;  // [nc][steps+1] paths exercised at each date
+  unsigned long long* ex_bits;   // [nc][steps+1] bits of the max (put) / min (call) exercised spot
+  double* itm_count;             // [nc][steps+1] in-the-money paths at each regression date
+  unsigned long long* term_itm;  // [nc] paths in the money at expiry
   uint64_t seed;
   of::PhiloxKeys keys;
   uint32_t contract_base;
-  const double* inj;         // [nc][n][steps] or null
+  const double* inj;         // [nc][n][steps][draws] or null
   const uint64_t* jump;      // jump tables
   int32_t chunk;             // paths per thread in the reference generator
 };
@@ -169,33 +197,102 @@ __device__ __forceinline__ T intrinsic_v(bool put, T s, T k) {
   return v > T(0) ? v : T(0);
 }
 
-// FP64 reference generator: chunk of consecutive paths per thread.
+// SampledVolSurface::vol (src/market/market.rs:104-174) with the expiry
+// bracket of the step precomputed: locate the strike by the same first-match
+// linear scan (a grid point takes the lower interval with weight 1), then
+// interpolate in strike, then in expiry.
+template <typename T>
+__device__ __forceinline__ T lsm_local_vol(const T* __restrict__ g, const T* __restrict__ v, int nk, int e0, int e1,
+                                           T ew, T strike) {
+  const T x = strike > __ldg(g) ? strike : __ldg(g);
+  int s0 = 0, s1 = 0;
+  T sw = T(0);
+  if (x >= __ldg(g + nk - 1)) {
+    s0 = s1 = nk - 1;
+  } else if (x > __ldg(g)) {
+    int lo = 0;
+    for (int i = 0; i < nk - 1; ++i)
+      if (x >= __ldg(g + i) && x <= __ldg(g + i + 1)) {
+        lo = i;
+        break;
+      }
+    s0 = lo;
+    s1 = lo + 1;
+    sw = (x - __ldg(g + lo)) / (__ldg(g + lo + 1) - __ldg(g + lo));
+  }
+  const T* r0 = v + (size_t)e0 * nk;
+  const T* r1 = v + (size_t)e1 * nk;
+  if (e0 == e1 && s0 == s1) return __ldg(r0 + s0);
+  if (e0 == e1) return __ldg(r0 + s0) + (__ldg(r0 + s1) - __ldg(r0 + s0)) * sw;
+  if (s0 == s1) return __ldg(r0 + s0) + (__ldg(r1 + s0) - __ldg(r0 + s0)) * ew;
+  const T a = __ldg(r0 + s0) + (__ldg(r0 + s1) - __ldg(r0 + s0)) * sw;
+  const T b = __ldg(r1 + s0) + (__ldg(r1 + s1) - __ldg(r1 + s0)) * sw;
+  return a + (b - a) * ew;
+}
+
+// Terminal cash flow of a path and, when boundary statistics are wanted,
+// the count of in-the-money paths at expiry (one atomic per thread that has any).
+__device__ __forceinline__ int terminal_value(const LsmC& C, double k_T, double s, double& v, double& dv) {
+  v = intrinsic_v<double>(C.put, s, k_T);
+  dv = v > 0.0 ? (C.put ? -s * C.inv_spot : s * C.inv_spot) : 0.0;
+  return v > 0.0 ? 1 : 0;
+}
+
+// FP64 reference generator: chunk of consecutive paths per thread.  The
+// single xoshiro256++ stream feeds path after path; 1 draw per step (GBM,
+// local vol) or 2 (Heston: z1 then z2), longstaff_schwartz.rs:190-283.
 __global__ void __launch_bounds__(128) lsm_gen_ref(LsmBatch B) {
   const int c = blockIdx.y;
   const LsmC C = B.c[c];
   const int64_t chunk0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * B.chunk;
   if (chunk0 >= B.n) return;
+  const int draws = C.dynamics == DYN_HESTON ? 2 : 1;
+  const LsmStep* st = B.st + (size_t)c * (B.steps + 1);
   double* S = (double*)B.S + (size_t)c * B.steps * B.npad;
   double* V = (double*)B.V + (size_t)c * B.npad;
   double* dV = (double*)B.dV + (size_t)c * B.npad;
   of::Xoshiro256pp rng;
   if (!B.inj) {
     rng.seed(B.seed);
-    xoshiro_jump(rng, (uint64_t)chunk0 * (uint64_t)B.steps, B.jump);
+    xoshiro_jump(rng, (uint64_t)chunk0 * (uint64_t)B.steps * (uint64_t)draws, B.jump);
   }
+  const double k_T = st[B.steps].strike;
+  const double rho_c = sqrt(1.0 - C.rho * C.rho);
+  int itm = 0;
   const int64_t end = chunk0 + B.chunk < B.n ? chunk0 + B.chunk : B.n;
   for (int64_t p = chunk0; p < end; ++p) {
-    double s = C.spot;
-    const double* z = B.inj ? B.inj + ((size_t)c * B.n + p) * B.steps : nullptr;
+    double s = C.spot, var = C.v0;
+    const double* z = B.inj ? B.inj + ((size_t)c * B.n + p) * B.steps * draws : nullptr;
     for (int t = 1; t <= B.steps; ++t) {
-      const double zz = z ? z[t - 1] : of::acklam_inv_cdf(rng.next_f64());
-      s = s * exp(fma(C.step_vol, zz, C.drift));  // longstaff_schwartz.rs:507
+      const double z1 = z ? z[(size_t)(t - 1) * draws] : of::acklam_inv_cdf(rng.next_f64());
+      if (C.dynamics == DYN_GBM) {
+        s = s * exp(fma(C.step_vol, z1, C.drift));  // longstaff_schwartz.rs:213-214
+      } else if (C.dynamics == DYN_LOCAL_VOL) {
+        // :223-235: sigma at the step's end time and the previous spot
+        const double sigma = lsm_local_vol<double>(C.lv_k, C.lv_v, C.lv_nk, st[t].e0, st[t].e1, st[t].ew,
+                                                   s > 1.0e-8 ? s : 1.0e-8);
+        const double drift = (C.mu - 0.5 * sigma * sigma) * C.dt;
+        s *= exp(drift + sigma * C.sqrt_dt * z1);
+        s = s > 1.0e-12 ? s : 1.0e-12;
+      } else {
+        // Heston::step_euler (src/models/stochastic.rs:56-71), :259-275
+        const double z2 = z ? z[(size_t)(t - 1) * draws + 1] : of::acklam_inv_cdf(rng.next_f64());
+        const double v_pos = var > 0.0 ? var : 0.0;
+        const double zs = C.rho * z1 + rho_c * z2;
+        double v_next = var + C.kappa * (C.theta - v_pos) * C.dt + C.xi * sqrt(v_pos) * C.sqrt_dt * z1;
+        v_next = v_next > 0.0 ? v_next : 0.0;
+        const double s_next = s * exp((C.mu - 0.5 * v_pos) * C.dt + sqrt(v_pos) * C.sqrt_dt * zs);
+        s = s_next > 1.0e-12 ? s_next : 1.0e-12;
+        var = v_next;
+      }
       S[(size_t)(t - 1) * B.npad + p] = s;
     }
-    const double v = intrinsic_v<double>(C.put, s, C.strike);
+    double v, dv;
+    itm += terminal_value(C, k_T, s, v, dv);
     V[p] = v;
-    dV[p] = v > 0.0 ? (C.put ? -s * C.inv_spot : s * C.inv_spot) : 0.0;
+    dV[p] = dv;
   }
+  if (B.track && itm) atomicAdd(B.term_itm + c, (unsigned long long)itm);
 }
 
 // FP32 Philox generator: 4 consecutive paths per thread, float4 stores.
@@ -203,37 +300,67 @@ __global__ void __launch_bounds__(256) lsm_gen_philox(const __grid_constant__ Ls
   const int c = blockIdx.y;
   const LsmC C = B.c[c];
   const int64_t p0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
-  if (p0 >= B.npad) return;
-  float* S = (float*)B.S + (size_t)c * B.steps * B.npad;
-  float y[4] = {0.f, 0.f, 0.f, 0.f};
-  uint4 r[4];
+  const bool live = p0 < B.npad;  // the grid's last block may reach past the padded path count
+  const LsmStep* st = B.st + (size_t)c * (B.steps + 1);
   const uint32_t cid = B.contract_base + (uint32_t)c;
-  for (int t = 0; t < B.steps; ++t) {
-    if ((t & 3) == 0) {
+  int itm = 0;
+  if (live) {
+    float* S = (float*)B.S + (size_t)c * B.steps * B.npad;
+    of::LegState L[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        r[q] = of::philox4x32_10(make_uint4((uint32_t)(t >> 2), (uint32_t)(p0 + q), cid, kLsmStreamTag), B.keys);
+    for (int q = 0; q < 4; ++q) L[q] = of::LegState{0.0f, C.hc.v0};
+    float s[4] = {C.fspot, C.fspot, C.fspot, C.fspot};
+    uint4 r[4];
+    for (int t = 0; t < B.steps; ++t) {
+      // draw t of a path: counter block t/4, word t%4; Heston draws (z1, z2)
+      // of step t: words 2(t%2), 2(t%2)+1 of counter block t/2
+      const bool refill = C.dynamics == DYN_HESTON ? (t & 1) == 0 : (t & 3) == 0;
+      if (refill) {
+        const uint32_t blk = C.dynamics == DYN_HESTON ? (uint32_t)(t >> 1) : (uint32_t)(t >> 2);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          r[q] = of::philox4x32_10(make_uint4(blk, (uint32_t)(p0 + q), cid, kLsmStreamTag), B.keys);
+      }
+      float4 out;
+      float* o = &out.x;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (C.dynamics == DYN_HESTON) {
+          const float z1 = of::normal_from_u32((t & 1) ? r[q].z : r[q].x);
+          const float z2 = of::normal_from_u32((t & 1) ? r[q].w : r[q].y);
+          of::heston_euler_step(L[q], C.hc, z1, z2);
+        } else {
+          const uint32_t bits = (t & 3) == 0 ? r[q].x : (t & 3) == 1 ? r[q].y : (t & 3) == 2 ? r[q].z : r[q].w;
+          const float z = of::normal_from_u32(bits);
+          if (C.dynamics == DYN_GBM) {
+            L[q].y = fmaf(C.fstep_vol, z, L[q].y + C.fdrift);
+          } else {
+            const LsmStep& e = st[t + 1];
+            const float sig = lsm_local_vol<float>(C.lv_kf, C.lv_vf, C.lv_nk, e.e0, e.e1, e.few,
+                                                   s[q] > 1.0e-8f ? s[q] : 1.0e-8f);
+            const float y = fmaf(sig * C.fsqrt_dt, z, fmaf(-0.5f * sig * sig, C.fdt, L[q].y + C.fmudt));
+            L[q].y = y > C.fy_floor ? y : C.fy_floor;
+          }
+        }
+        s[q] = C.fspot * __expf(L[q].y);
+        o[q] = s[q];
+      }
+      *reinterpret_cast<float4*>(S + (size_t)t * B.npad + p0) = out;
     }
-    float4 out;
-    float* o = &out.x;
-#pragma unroll
+    float* V = (float*)B.V + (size_t)c * B.npad;
+    float* dV = (float*)B.dV + (size_t)c * B.npad;
+    const float fk = st[B.steps].fstrike, finv = (float)C.inv_spot;
     for (int q = 0; q < 4; ++q) {
-      const uint32_t bits = (t & 3) == 0 ? r[q].x : (t & 3) == 1 ? r[q].y : (t & 3) == 2 ? r[q].z : r[q].w;
-      const float z = of::normal_from_u32(bits);
-      y[q] = fmaf(C.fstep_vol, z, y[q] + C.fdrift);
-      o[q] = C.fspot * __expf(y[q]);
+      const float v = intrinsic_v<float>(C.put, s[q], fk);
+      const bool in = p0 + q < B.n;
+      V[p0 + q] = in ? v : 0.0f;
+      dV[p0 + q] = (in && v > 0.0f) ? (C.put ? -s[q] * finv : s[q] * finv) : 0.0f;
+      itm += (in && v > 0.0f) ? 1 : 0;
     }
-    *reinterpret_cast<float4*>(S + (size_t)t * B.npad + p0) = out;
   }
-  float* V = (float*)B.V + (size_t)c * B.npad;
-  float* dV = (float*)B.dV + (size_t)c * B.npad;
-  const float* last = S + (size_t)(B.steps - 1) * B.npad + p0;
-  const float fk = (float)C.strike, finv = (float)C.inv_spot;
-  for (int q = 0; q < 4; ++q) {
-    const float s = last[q];
-    const float v = intrinsic_v<float>(C.put, s, fk);
-    V[p0 + q] = (p0 + q < B.n) ? v : 0.0f;
-    dV[p0 + q] = (p0 + q < B.n && v > 0.0f) ? (C.put ? -s * finv : s * finv) : 0.0f;
+  if (B.track) {
+    itm = __reduce_add_sync(of::kFullMask, itm);
+    if ((threadIdx.x & 31) == 0 && itm) atomicAdd(B.term_itm + c, (unsigned long long)itm);
   }
 }
 
@@ -347,25 +474,52 @@ __device__ void last_block_reduce(const LsmBatch& B, int c, int nm, double* mome
     int32_t* ok = B.beta_ok + (size_t)buf * B.nc + c;
     solve_beta(B.degree, moments_sh, beta, ok);
     if (*ok) B.regress_count[c] += 1;
+    if (B.track) B.itm_count[(size_t)c * (B.steps + 1) + t_pass] = moments_sh[0];
+  }
+}
+
+// Exercise statistics of one date, reduced over the warp and added with one
+// atomic per warp: the count, and the largest (put) or smallest (call)
+// exercised spot.  Positive doubles order like their bit patterns; a lane
+// that exercised nothing passes 0 (put) or +inf (call).  Called by all 32
+// lanes of the warp.
+__device__ __forceinline__ void record_exercise(const LsmBatch& B, int c, int date, bool put, unsigned cnt,
+                                                double ext) {
+  cnt = __reduce_add_sync(of::kFullMask, cnt);
+  unsigned long long bits = (unsigned long long)__double_as_longlong(ext);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(of::kFullMask, bits, o);
+    bits = put ? (other > bits ? other : bits) : (other < bits ? other : bits);
+  }
+  if ((threadIdx.x & 31) == 0 && cnt) {
+    const size_t k = (size_t)c * (B.steps + 1) + date;
+    atomicAdd(B.ex_count + k, (unsigned long long)cnt);
+    if (put) atomicMax(B.ex_bits + k, bits);
+    else atomicMin(B.ex_bits + k, bits);
   }
 }
 
 // One path of a pass: exercise at date t+1 (spot s1) with the betas of that
 // date, discount one step, and the in-the-money basis moments at date t
 // (spot s0, longstaff_schwartz.rs:543-601).
-__device__ __forceinline__ void lsm_path_update(const LsmBatch& B, const LsmC& C, const double* beta, bool have_beta,
-                                                bool ex_now, double s1, double s0, double& v, double& dv,
-                                                double* mom) {
+// k1/ik1: strike and its inverse at date t+1, k0/ik0 at date t.  Returns
+// whether the path exercised at t+1.
+__device__ __forceinline__ bool lsm_path_update(const LsmBatch& B, const LsmC& C, const double* beta, bool have_beta,
+                                                bool ex_now, double k1, double ik1, double k0, double ik0, double s1,
+                                                double s0, double& v, double& dv, double* mom) {
+  bool exercised = false;
   if (have_beta) {
-    const double ex = intrinsic_v<double>(C.put, s1, C.strike);
-    if (ex > 0.0 && ex > continuation(B.degree, beta, s1, C.inv_strike)) {
+    const double ex = intrinsic_v<double>(C.put, s1, k1);
+    if (ex > 0.0 && ex > continuation(B.degree, beta, s1, ik1)) {
       v = ex;
       dv = C.put ? -s1 * C.inv_spot : s1 * C.inv_spot;
+      exercised = true;
     }
   }
   v *= C.disc;
   dv *= C.disc;
-  if (ex_now && intrinsic_v<double>(C.put, s0, C.strike) > 0.0) {
+  if (ex_now && intrinsic_v<double>(C.put, s0, k0) > 0.0) {
     if (B.degree == 2) {
       const double s2 = s0 * s0;
       mom[0] += 1.0;
@@ -377,7 +531,7 @@ __device__ __forceinline__ void lsm_path_update(const LsmBatch& B, const LsmC& C
       mom[6] += s0 * v;
       mom[7] += s2 * v;
     } else {
-      const double x = s0 * C.inv_strike;
+      const double x = s0 * ik0;
       double pw = 1.0;
 #pragma unroll
       for (int e = 0; e < 7; ++e) {
@@ -387,6 +541,7 @@ __device__ __forceinline__ void lsm_path_update(const LsmBatch& B, const LsmC& C
       }
     }
   }
+  return exercised;
 }
 
 // One exercise date t (1 <= t <= steps-1): exercise(t+1), discount, moments(t).
@@ -407,6 +562,10 @@ __global__ void __launch_bounds__(kPassThreads) lsm_pass(LsmBatch B, int t) {
   double beta[4] = {0, 0, 0, 0};
   if (have_beta)
     for (int k = 0; k < 4; ++k) beta[k] = B.betas[((size_t)nb * B.nc + c) * 4 + k];
+  const LsmStep* st = B.st + (size_t)c * (B.steps + 1);
+  const double k1 = st[t + 1].strike, ik1 = st[t + 1].inv_strike, k0 = st[t].strike, ik0 = st[t].inv_strike;
+  unsigned n_ex = 0;
+  double ext = C.put ? 0.0 : __longlong_as_double(0x7FF0000000000000LL);
   const int nm = B.degree == 2 ? 8 : 11;
   double mom[kMaxMoments];
 #pragma unroll
@@ -440,7 +599,10 @@ __global__ void __launch_bounds__(kPassThreads) lsm_pass(LsmBatch B, int t) {
       for (int e = 0; e < 4; ++e) {
         if (p0 + e >= B.n) continue;  // padding
         double v = vv[e], dv = dd[e];
-        lsm_path_update(B, C, beta, have_beta, ex_now, s1[e], s0[e], v, dv, mom);
+        if (lsm_path_update(B, C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1[e], s0[e], v, dv, mom)) {
+          ++n_ex;
+          ext = C.put ? fmax(ext, (double)s1[e]) : fmin(ext, (double)s1[e]);
+        }
         vv[e] = (float)v;
         dd[e] = (float)dv;
       }
@@ -456,11 +618,15 @@ __global__ void __launch_bounds__(kPassThreads) lsm_pass(LsmBatch B, int t) {
       double v = (double)V[p], dv = B.want_delta ? (double)dV[p] : 0.0;
       const double s1 = have_beta ? (double)S[(size_t)t * B.npad + p] : 0.0;      // spot at date t+1
       const double s0 = ex_now ? (double)S[(size_t)(t - 1) * B.npad + p] : 0.0;  // spot at date t
-      lsm_path_update(B, C, beta, have_beta, ex_now, s1, s0, v, dv, mom);
+      if (lsm_path_update(B, C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1, s0, v, dv, mom)) {
+        ++n_ex;
+        ext = C.put ? fmax(ext, s1) : fmin(ext, s1);
+      }
       V[p] = (T)v;
       if (B.want_delta) dV[p] = (T)dv;
     }
   }
+  if (B.track && have_beta) record_exercise(B, c, t + 1, C.put, n_ex, ext);  // block-uniform condition
   if (!ex_now) return;
   // block reduction of all moments with one barrier: warp shuffles, then one
   // thread per moment sums the warps in a fixed order -> partials
@@ -511,6 +677,9 @@ __global__ void __launch_bounds__(kPassThreads) lsm_final(LsmBatch B) {
   if (have_beta)
     for (int k = 0; k < 4; ++k) beta[k] = B.betas[((size_t)nb * B.nc + c) * 4 + k];
   double acc[3] = {0, 0, 0};
+  const LsmStep& st1 = B.st[(size_t)c * (B.steps + 1) + 1];
+  unsigned n_ex = 0;
+  double ext = C.put ? 0.0 : __longlong_as_double(0x7FF0000000000000LL);
   const int64_t base = (int64_t)blockIdx.x * kPathsPerBlock;
   for (int q = 0; q < kPathsPerThread; ++q) {
     const int64_t p = base + q * kPassThreads + threadIdx.x;
@@ -518,10 +687,12 @@ __global__ void __launch_bounds__(kPassThreads) lsm_final(LsmBatch B) {
     double v = (double)V[p], dv = B.want_delta ? (double)dV[p] : 0.0;
     if (have_beta) {
       const double s1 = (double)S[p];  // spot at date 1
-      const double ex = intrinsic_v<double>(C.put, s1, C.strike);
-      if (ex > 0.0 && ex > continuation(B.degree, beta, s1, C.inv_strike)) {
+      const double ex = intrinsic_v<double>(C.put, s1, st1.strike);
+      if (ex > 0.0 && ex > continuation(B.degree, beta, s1, st1.inv_strike)) {
         v = ex;
         dv = C.put ? -s1 * C.inv_spot : s1 * C.inv_spot;
+        ++n_ex;
+        ext = C.put ? fmax(ext, s1) : fmin(ext, s1);
       }
     }
     v *= C.disc;
@@ -530,6 +701,7 @@ __global__ void __launch_bounds__(kPassThreads) lsm_final(LsmBatch B) {
     acc[1] += v * v;
     acc[2] += dv;
   }
+  if (B.track && have_beta) record_exercise(B, c, 1, C.put, n_ex, ext);  // block-uniform condition
   double* part = B.partials + ((size_t)c * B.blocks + blockIdx.x) * kMaxMoments;
   for (int k = 0; k < 3; ++k) {
     double w = of::warp_sum(acc[k]);
@@ -628,6 +800,249 @@ extern "C" of_status of_xoshiro_jump(of_ctx* ctx, uint64_t seed, const uint64_t*
   return OF_OK;
 }
 
+namespace {
+
+// Host description of one contract of a batch.
+struct LsmHost {
+  LsmC C{};                              // device grid pointers are set by lsm_run_batch
+  std::vector<uint8_t> can;              // [steps+1] exercise allowed at step t
+  std::vector<LsmStep> st;               // [steps+1]
+  std::vector<double> lv_k, lv_t, lv_v;  // sampled local-vol grid (local-vol dynamics only)
+};
+
+// Exercise-boundary statistics of one contract, [steps+1] entries each.
+struct LsmTrack {
+  std::vector<unsigned long long> ex_count, ex_bits;
+  std::vector<double> itm;
+  unsigned long long term_itm = 0;
+};
+
+// SampledVolSurface::locate_bounds (src/market/market.rs:104-125).
+void locate_bounds(const std::vector<double>& g, double x, int32_t* lo, int32_t* hi, double* w) {
+  const int n = (int)g.size();
+  if (x <= g[0]) {
+    *lo = *hi = 0;
+    *w = 0.0;
+    return;
+  }
+  if (x >= g[(size_t)n - 1]) {
+    *lo = *hi = n - 1;
+    *w = 0.0;
+    return;
+  }
+  int l = 0;
+  for (int i = 0; i < n - 1; ++i)
+    if (x >= g[(size_t)i] && x <= g[(size_t)i + 1]) {
+      l = i;
+      break;
+    }
+  *lo = l;
+  *hi = l + 1;
+  *w = (x - g[(size_t)l]) / (g[(size_t)l + 1] - g[(size_t)l]);
+}
+
+// Per-step strikes and local-vol expiry brackets of a contract.
+void fill_steps(LsmHost& h, int64_t steps, double expiry, const double* strike_of_step) {
+  h.st.assign((size_t)steps + 1, LsmStep{});
+  const double dt = expiry / (double)steps;
+  for (int64_t t = 0; t <= steps; ++t) {
+    LsmStep& s = h.st[(size_t)t];
+    s.strike = strike_of_step[t];
+    s.inv_strike = 1.0 / s.strike;
+    s.fstrike = (float)s.strike;
+    s.finv_strike = (float)s.inv_strike;
+    if (!h.lv_t.empty()) {
+      const double te = (double)t * dt > 1.0e-8 ? (double)t * dt : 1.0e-8;  // longstaff_schwartz.rs:224
+      locate_bounds(h.lv_t, te > h.lv_t[0] ? te : h.lv_t[0], &s.e0, &s.e1, &s.ew);
+      s.few = (float)s.ew;
+    }
+  }
+}
+
+// Generation, the backward passes and the final reduction for contracts that
+// share a step count; results[c] = {price, stderr, delta}.
+of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, const of_lsm_config* cfg,
+                        const uint64_t* jump, uint32_t contract_base, const double* inj_host, int draws,
+                        std::vector<LsmTrack>* track, std::vector<double>& results, std::vector<int32_t>& regs,
+                        float* ms_out) {
+  const bool fp64 = cfg->precision == OF_PREC_FP64_REFERENCE;
+  const int64_t N = cfg->num_paths;
+  const size_t esz = fp64 ? sizeof(double) : sizeof(float);
+  const int64_t npad = (N + kPathsPerBlock - 1) / kPathsPerBlock * kPathsPerBlock;
+  const int blocks = (int)(npad / kPathsPerBlock);
+  const int nc = (int)hs.size();
+  const size_t per = (size_t)steps * npad * esz;
+  const size_t ns = (size_t)nc * (size_t)(steps + 1);
+  // device buffers: path store, cash flows, and one auxiliary block
+  void *dS = nullptr, *dV = nullptr, *dAux = nullptr, *dInj = nullptr;
+  OF_TRY(of_scratch(ctx, SLOT_LSM_PATHS, (size_t)nc * per, &dS));
+  OF_TRY(of_scratch(ctx, SLOT_LSM_VALUES, (size_t)nc * npad * esz * 2, &dV));
+  size_t off = 0;
+  auto take = [&off](size_t bytes) {
+    const size_t o = off;
+    off = (off + bytes + 255) & ~(size_t)255;
+    return o;
+  };
+  const size_t o_part = take((size_t)nc * blocks * kMaxMoments * sizeof(double));
+  const size_t o_beta = take((size_t)nc * 8 * sizeof(double));
+  const size_t o_res = take((size_t)nc * 3 * sizeof(double));
+  const size_t o_c = take((size_t)nc * sizeof(LsmC));
+  const size_t o_ok = take((size_t)nc * 2 * sizeof(int32_t));
+  const size_t o_reg = take((size_t)nc * sizeof(int32_t));
+  const size_t o_cnt = take((size_t)nc * sizeof(uint32_t));
+  const size_t o_can = take(ns);
+  const size_t o_st = take(ns * sizeof(LsmStep));
+  const size_t o_exc = take(ns * sizeof(unsigned long long));
+  const size_t o_exb = take(ns * sizeof(unsigned long long));
+  const size_t o_itm = take(ns * sizeof(double));
+  const size_t o_term = take((size_t)nc * sizeof(unsigned long long));
+  std::vector<size_t> o_lv((size_t)nc * 4, 0);
+  for (int c = 0; c < nc; ++c) {
+    const size_t nk = hs[(size_t)c].lv_k.size(), nv = hs[(size_t)c].lv_v.size();
+    if (!nk) continue;
+    o_lv[(size_t)c * 4 + 0] = take(nk * sizeof(double));
+    o_lv[(size_t)c * 4 + 1] = take(nv * sizeof(double));
+    o_lv[(size_t)c * 4 + 2] = take(nk * sizeof(float));
+    o_lv[(size_t)c * 4 + 3] = take(nv * sizeof(float));
+  }
+  OF_TRY(of_scratch(ctx, SLOT_LSM_AUX, off, &dAux));
+  char* a = (char*)dAux;
+  LsmBatch B{};
+  B.partials = (double*)(a + o_part);
+  B.betas = (double*)(a + o_beta);
+  B.results = (double*)(a + o_res);
+  LsmC* dC = (LsmC*)(a + o_c);
+  B.beta_ok = (int32_t*)(a + o_ok);
+  B.regress_count = (int32_t*)(a + o_reg);
+  B.counters = (uint32_t*)(a + o_cnt);
+  uint8_t* dCan = (uint8_t*)(a + o_can);
+  LsmStep* dSt = (LsmStep*)(a + o_st);
+  B.ex_count = (unsigned long long*)(a + o_exc);
+  B.ex_bits = (unsigned long long*)(a + o_exb);
+  B.itm_count = (double*)(a + o_itm);
+  B.term_itm = (unsigned long long*)(a + o_term);
+  // host images of the tables (the device pointers of the grids go into LsmC)
+  std::vector<LsmC> hc((size_t)nc);
+  std::vector<uint8_t> can(ns);
+  std::vector<LsmStep> st(ns);
+  std::vector<std::vector<float>> lvf((size_t)nc * 2);
+  for (int c = 0; c < nc; ++c) {
+    LsmHost& h = hs[(size_t)c];
+    LsmC C = h.C;
+    std::copy(h.can.begin(), h.can.end(), can.begin() + (size_t)c * (steps + 1));
+    std::copy(h.st.begin(), h.st.end(), st.begin() + (size_t)c * (steps + 1));
+    if (!h.lv_k.empty()) {
+      C.lv_k = (const double*)(a + o_lv[(size_t)c * 4 + 0]);
+      C.lv_v = (const double*)(a + o_lv[(size_t)c * 4 + 1]);
+      C.lv_kf = (const float*)(a + o_lv[(size_t)c * 4 + 2]);
+      C.lv_vf = (const float*)(a + o_lv[(size_t)c * 4 + 3]);
+      C.lv_nk = (int32_t)h.lv_k.size();
+      lvf[(size_t)c * 2].assign(h.lv_k.begin(), h.lv_k.end());
+      lvf[(size_t)c * 2 + 1].assign(h.lv_v.begin(), h.lv_v.end());
+      OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)C.lv_k, h.lv_k.data(), h.lv_k.size() * sizeof(double),
+                                       cudaMemcpyHostToDevice, ctx->stream));
+      OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)C.lv_v, h.lv_v.data(), h.lv_v.size() * sizeof(double),
+                                       cudaMemcpyHostToDevice, ctx->stream));
+      OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)C.lv_kf, lvf[(size_t)c * 2].data(), h.lv_k.size() * sizeof(float),
+                                       cudaMemcpyHostToDevice, ctx->stream));
+      OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)C.lv_vf, lvf[(size_t)c * 2 + 1].data(), h.lv_v.size() * sizeof(float),
+                                       cudaMemcpyHostToDevice, ctx->stream));
+    }
+    hc[(size_t)c] = C;
+  }
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(dC, hc.data(), hc.size() * sizeof(LsmC), cudaMemcpyHostToDevice, ctx->stream));
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(dCan, can.data(), ns, cudaMemcpyHostToDevice, ctx->stream));
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(dSt, st.data(), ns * sizeof(LsmStep), cudaMemcpyHostToDevice, ctx->stream));
+  OF_CUDA_TRY(ctx, cudaMemsetAsync(B.beta_ok, 0, (size_t)nc * 2 * sizeof(int32_t), ctx->stream));
+  OF_CUDA_TRY(ctx, cudaMemsetAsync(B.regress_count, 0, (size_t)nc * sizeof(int32_t), ctx->stream));
+  OF_CUDA_TRY(ctx, cudaMemsetAsync(B.counters, 0, (size_t)nc * sizeof(uint32_t), ctx->stream));
+  std::vector<unsigned long long> bits0(track ? ns : 0);
+  if (track) {
+    for (int c = 0; c < nc; ++c)  // identity of max (put) / min (call) over positive doubles
+      std::fill(bits0.begin() + (size_t)c * (steps + 1), bits0.begin() + (size_t)(c + 1) * (steps + 1),
+                hs[(size_t)c].C.put ? 0ULL : 0x7FF0000000000000ULL);
+    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.ex_count, 0, ns * sizeof(unsigned long long), ctx->stream));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(B.ex_bits, bits0.data(), ns * sizeof(unsigned long long),
+                                     cudaMemcpyHostToDevice, ctx->stream));
+    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.itm_count, 0, ns * sizeof(double), ctx->stream));
+    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.term_itm, 0, (size_t)nc * sizeof(unsigned long long), ctx->stream));
+  }
+  if (inj_host) {
+    const size_t cnt = (size_t)N * steps * draws;
+    OF_TRY(of_scratch(ctx, SLOT_INJECT, cnt * sizeof(double), &dInj));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(dInj, inj_host, cnt * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  B.c = dC;
+  B.can_ex = dCan;
+  B.st = dSt;
+  B.nc = nc;
+  B.steps = (int32_t)steps;
+  B.n = N;
+  B.npad = npad;
+  B.S = dS;
+  B.V = dV;
+  B.dV = (char*)dV + (size_t)nc * npad * esz;
+  B.blocks = blocks;
+  B.degree = cfg->basis_degree;
+  B.want_delta = cfg->want_delta;
+  B.track = track ? 1 : 0;
+  B.seed = cfg->seed;
+  B.keys = of::philox_keys(cfg->seed);
+  B.contract_base = contract_base;
+  B.inj = (const double*)dInj;
+  B.jump = jump;
+  B.chunk = 8;
+  if (!fp64) OF_CUDA_TRY(ctx, cudaMemsetAsync(dV, 0, (size_t)nc * npad * esz * 2, ctx->stream));
+  OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+  if (fp64) {
+    const int64_t chunks = (N + B.chunk - 1) / B.chunk;
+    lsm_gen_ref<<<dim3((unsigned)((chunks + 127) / 128), nc), 128, 0, ctx->stream>>>(B);
+  } else {
+    const int64_t quads = npad / 4;
+    lsm_gen_philox<<<dim3((unsigned)((quads + 255) / 256), nc), 256, 0, ctx->stream>>>(B);
+  }
+  OF_CUDA_TRY(ctx, cudaGetLastError());
+  const dim3 grid((unsigned)blocks, nc);
+  for (int t = (int)steps - 1; t >= 1; --t) {
+    if (fp64) lsm_pass<double><<<grid, kPassThreads, 0, ctx->stream>>>(B, t);
+    else lsm_pass<float><<<grid, kPassThreads, 0, ctx->stream>>>(B, t);
+  }
+  if (fp64) lsm_final<double><<<grid, kPassThreads, 0, ctx->stream>>>(B);
+  else lsm_final<float><<<grid, kPassThreads, 0, ctx->stream>>>(B);
+  OF_CUDA_TRY(ctx, cudaGetLastError());
+  OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+  results.assign((size_t)nc * 3, 0.0);
+  regs.assign((size_t)nc, 0);
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(results.data(), B.results, results.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(regs.data(), B.regress_count, regs.size() * sizeof(int32_t),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  std::vector<unsigned long long> hcnt(track ? ns : 0), hbits(track ? ns : 0), hterm(track ? (size_t)nc : 0);
+  std::vector<double> hitm(track ? ns : 0);
+  if (track) {
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(hcnt.data(), B.ex_count, ns * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(hbits.data(), B.ex_bits, ns * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(hitm.data(), B.itm_count, ns * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(hterm.data(), B.term_itm, (size_t)nc * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  OF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  OF_CUDA_TRY(ctx, cudaEventElapsedTime(ms_out, ctx->ev_start, ctx->ev_stop));
+  if (track) {
+    track->assign((size_t)nc, LsmTrack{});
+    for (int c = 0; c < nc; ++c) {
+      LsmTrack& tr = (*track)[(size_t)c];
+      const size_t b = (size_t)c * (steps + 1), e = b + (size_t)steps + 1;
+      tr.ex_count.assign(hcnt.begin() + b, hcnt.begin() + e);
+      tr.ex_bits.assign(hbits.begin() + b, hbits.begin() + e);
+      tr.itm.assign(hitm.begin() + b, hitm.begin() + e);
+      tr.term_itm = hterm[(size_t)c];
+    }
+  }
+  return OF_OK;
+}
+
+}  // namespace
+
 extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_t n, const of_lsm_config* cfg,
                                   of_lsm_result* res) {
   if (!ctx || !ks || !cfg || !res || n <= 0) return OF_ERR_INVALID_INPUT;
@@ -685,11 +1100,15 @@ extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_
            ks[order[pos]].expiry != 0.0)
       batch.push_back(order[pos++]);
     const int nc = (int)batch.size();
-    std::vector<LsmC> hc((size_t)nc);
-    std::vector<uint8_t> can((size_t)nc * (steps + 1), 0);
+    std::vector<LsmHost> hs((size_t)nc);
     for (int c = 0; c < nc; ++c) {
       const of_lsm_contract& k = ks[batch[(size_t)c]];
-      LsmC& C = hc[(size_t)c];
+      LsmHost& h = hs[(size_t)c];
+      h.can.assign((size_t)steps + 1, 0);
+      const std::vector<double> kk((size_t)steps + 1, k.strike);
+      fill_steps(h, steps, k.expiry, kk.data());
+      LsmC& C = h.C;
+      C.dynamics = DYN_GBM;
       const double dt = k.expiry / (double)steps;
       C.put = k.option_type == OF_PUT;
       C.steps = (int32_t)steps;
@@ -703,7 +1122,7 @@ extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_
       C.fdrift = (float)C.drift;
       C.fstep_vol = (float)C.step_vol;
       C.fspot = (float)k.spot;
-      uint8_t* ce = can.data() + (size_t)c * (steps + 1);
+      uint8_t* ce = h.can.data();
       if (k.exercise == OF_EXERCISE_EUROPEAN) {
         ce[steps] = 1;
       } else if (k.exercise == OF_EXERCISE_AMERICAN) {
@@ -717,89 +1136,12 @@ extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_
         ce[steps] = 1;
       }
     }
-    // device buffers
-    void *dS = nullptr, *dV = nullptr, *dAux = nullptr, *dInj = nullptr;
-    OF_TRY(of_scratch(ctx, SLOT_LSM_PATHS, (size_t)nc * per, &dS));
-    OF_TRY(of_scratch(ctx, SLOT_LSM_VALUES, (size_t)nc * npad * esz * 2, &dV));
-    const size_t part_bytes = (size_t)nc * blocks * kMaxMoments * sizeof(double);
-    const size_t aux_bytes = part_bytes + (size_t)nc * (sizeof(LsmC) + 2 * 4 * sizeof(double) + 3 * sizeof(double) +
-                                                        2 * sizeof(int32_t) + sizeof(int32_t) + sizeof(uint32_t)) +
-                             can.size() + 1024;
-    OF_TRY(of_scratch(ctx, SLOT_LSM_AUX, aux_bytes, &dAux));
-    char* a = (char*)dAux;
-    LsmBatch B{};
-    B.partials = (double*)a;
-    a += part_bytes;
-    B.betas = (double*)a;
-    a += (size_t)nc * 8 * sizeof(double);
-    B.results = (double*)a;
-    a += (size_t)nc * 3 * sizeof(double);
-    LsmC* dC = (LsmC*)a;
-    a += (size_t)nc * sizeof(LsmC);
-    B.beta_ok = (int32_t*)a;
-    a += (size_t)nc * 2 * sizeof(int32_t);
-    B.regress_count = (int32_t*)a;
-    a += (size_t)nc * sizeof(int32_t);
-    B.counters = (uint32_t*)a;
-    a += (size_t)nc * sizeof(uint32_t);
-    uint8_t* dCan = (uint8_t*)a;
-    OF_CUDA_TRY(ctx, cudaMemcpyAsync(dC, hc.data(), hc.size() * sizeof(LsmC), cudaMemcpyHostToDevice, ctx->stream));
-    OF_CUDA_TRY(ctx, cudaMemcpyAsync(dCan, can.data(), can.size(), cudaMemcpyHostToDevice, ctx->stream));
-    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.beta_ok, 0, (size_t)nc * 4 * sizeof(int32_t), ctx->stream));
-    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.regress_count, 0, (size_t)nc * sizeof(int32_t), ctx->stream));
-    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.counters, 0, (size_t)nc * sizeof(uint32_t), ctx->stream));
-    if (cfg->injected_normals) {
-      const size_t cnt = (size_t)N * steps;
-      OF_TRY(of_scratch(ctx, SLOT_INJECT, cnt * sizeof(double), &dInj));
-      OF_CUDA_TRY(ctx, cudaMemcpyAsync(dInj, cfg->injected_normals + inj_off[(size_t)batch[0]], cnt * sizeof(double),
-                                       cudaMemcpyHostToDevice, ctx->stream));
-    }
-    B.c = dC;
-    B.can_ex = dCan;
-    B.nc = nc;
-    B.steps = (int32_t)steps;
-    B.n = N;
-    B.npad = npad;
-    B.S = dS;
-    B.V = dV;
-    B.dV = (char*)dV + (size_t)nc * npad * esz;
-    B.blocks = blocks;
-    B.degree = cfg->basis_degree;
-    B.want_delta = cfg->want_delta;
-    B.seed = cfg->seed;
-    B.keys = of::philox_keys(cfg->seed);
-    B.contract_base = (uint32_t)batch[0];
-    B.inj = (const double*)dInj;
-    B.jump = jump;
-    B.chunk = 8;
-    if (!fp64) OF_CUDA_TRY(ctx, cudaMemsetAsync(dV, 0, (size_t)nc * npad * esz * 2, ctx->stream));
-    OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
-    if (fp64) {
-      const int64_t chunks = (N + B.chunk - 1) / B.chunk;
-      lsm_gen_ref<<<dim3((unsigned)((chunks + 127) / 128), nc), 128, 0, ctx->stream>>>(B);
-    } else {
-      const int64_t quads = npad / 4;
-      lsm_gen_philox<<<dim3((unsigned)((quads + 255) / 256), nc), 256, 0, ctx->stream>>>(B);
-    }
-    OF_CUDA_TRY(ctx, cudaGetLastError());
-    const dim3 grid((unsigned)blocks, nc);
-    for (int t = (int)steps - 1; t >= 1; --t) {
-      if (fp64) lsm_pass<double><<<grid, kPassThreads, 0, ctx->stream>>>(B, t);
-      else lsm_pass<float><<<grid, kPassThreads, 0, ctx->stream>>>(B, t);
-    }
-    if (fp64) lsm_final<double><<<grid, kPassThreads, 0, ctx->stream>>>(B);
-    else lsm_final<float><<<grid, kPassThreads, 0, ctx->stream>>>(B);
-    OF_CUDA_TRY(ctx, cudaGetLastError());
-    OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
-    std::vector<double> hres((size_t)nc * 3);
-    std::vector<int32_t> hreg((size_t)nc);
-    OF_CUDA_TRY(ctx, cudaMemcpyAsync(hres.data(), B.results, hres.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                                     ctx->stream));
-    OF_CUDA_TRY(ctx, cudaMemcpyAsync(hreg.data(), B.regress_count, hreg.size() * sizeof(int32_t),
-                                     cudaMemcpyDeviceToHost, ctx->stream));
-    OF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    std::vector<double> hres;
+    std::vector<int32_t> hreg;
     float ms = 0.0f;
-    OF_CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+    OF_TRY(lsm_run_batch(ctx, hs, steps, cfg, jump, (uint32_t)batch[0],
+                         cfg->injected_normals ? cfg->injected_normals + inj_off[(size_t)batch[0]] : nullptr, 1,
+                         nullptr, hres, hreg, &ms));
     total_ms += ms;
     for (int c = 0; c < nc; ++c) {
       of_lsm_result& r = res[batch[(size_t)c]];
@@ -810,5 +1152,180 @@ extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_
     }
   }
   for (int64_t i = 0; i < n; ++i) res[i].kernel_ms = total_ms;
+  return OF_OK;
+}
+
+static bool strictly_increasing(const double* g, int64_t n) {
+  for (int64_t i = 1; i < n; ++i)
+    if (!(g[i] > g[i - 1])) return false;
+  return true;
+}
+
+extern "C" of_status of_lsm_bermudan(of_ctx* ctx, const of_bermudan_contract* k, const of_lsm_config* cfg,
+                                     of_lsm_result* result, of_boundary_point* boundary, int64_t capacity,
+                                     int64_t* n_boundary) {
+  if (!ctx || !k || !cfg || !result || !n_boundary || (capacity > 0 && !boundary)) return OF_ERR_INVALID_INPUT;
+  if (cfg->basis_degree != 2 && cfg->basis_degree != 3)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "basis_degree must be 2 or 3");
+  const bool fp64 = cfg->precision == OF_PREC_FP64_REFERENCE;
+  if (!fp64 && cfg->precision != OF_PREC_FP32_PHILOX)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown precision %d", cfg->precision);
+  if (cfg->injected_normals && !fp64)
+    return of_fail(ctx, OF_ERR_UNSUPPORTED, "injected normals are a FP64 reference-mode test hook");
+  // BermudanOption::validate (src/instruments/bermudan.rs:104-150) and the
+  // engine's own checks (longstaff_schwartz.rs:302-313, 198-204, 226-231, 256-260)
+  if (k->option_type != OF_CALL && k->option_type != OF_PUT)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown option type %d", k->option_type);
+  if (!(k->expiry > 0.0) || !std::isfinite(k->expiry))
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "bermudan expiry must be finite and > 0");
+  if (k->n_schedule <= 0 || !k->schedule_times || !k->schedule_strikes)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "bermudan exercise_dates cannot be empty");
+  for (int64_t d = 0; d < k->n_schedule; ++d) {
+    const double t = k->schedule_times[d], K = k->schedule_strikes[d];
+    if (!std::isfinite(t) || t <= 0.0 || t > k->expiry)
+      return of_fail(ctx, OF_ERR_INVALID_INPUT, "bermudan exercise_dates must be finite and in (0, expiry]");
+    if (!std::isfinite(K) || K <= 0.0)
+      return of_fail(ctx, OF_ERR_INVALID_INPUT, "bermudan strike_schedule entries must be finite and > 0");
+  }
+  if (!strictly_increasing(k->schedule_times, k->n_schedule))
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "bermudan exercise_dates must be strictly increasing");
+  if (k->num_steps < 2) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_steps must be >= 2 for Longstaff-Schwartz");
+  if (k->num_steps > (1 << 20)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_steps too large");
+  if (cfg->num_paths < 3) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_paths must be >= 3 for Longstaff-Schwartz");
+  if (!(k->spot > 0.0)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "market spot must be > 0");
+  if (k->dynamics == OF_LSM_GBM) {
+    if (!std::isfinite(k->vol) || k->vol <= 0.0)
+      return of_fail(ctx, OF_ERR_INVALID_INPUT, "market volatility must be finite and > 0");
+  } else if (k->dynamics == OF_LSM_LOCAL_VOL) {
+    if (k->lv_n_strikes < 1 || k->lv_n_expiries < 1 || !k->lv_strikes || !k->lv_expiries || !k->lv_vols ||
+        !strictly_increasing(k->lv_strikes, k->lv_n_strikes) || !strictly_increasing(k->lv_expiries, k->lv_n_expiries))
+      return of_fail(ctx, OF_ERR_INVALID_INPUT, "local volatility grid must be non-empty and strictly increasing");
+    for (int64_t i = 0; i < k->lv_n_strikes * k->lv_n_expiries; ++i)
+      if (!std::isfinite(k->lv_vols[i]) || k->lv_vols[i] <= 0.0)
+        return of_fail(ctx, OF_ERR_INVALID_INPUT, "local volatility surface returned non-positive value");
+    if (cfg->want_delta)
+      return of_fail(ctx, OF_ERR_UNSUPPORTED, "pathwise delta is not defined for local-vol dynamics");
+  } else if (k->dynamics == OF_LSM_HESTON_EULER) {
+    if (!(k->kappa > 0.0 && k->theta >= 0.0 && k->xi >= 0.0 && k->v0 >= 0.0 && k->rho > -1.0 && k->rho < 1.0))
+      return of_fail(ctx, OF_ERR_INVALID_INPUT, "invalid Heston parameters for Bermudan LSM dynamics");
+  } else {
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown LSM dynamics %d", k->dynamics);
+  }
+  const int64_t steps = k->num_steps, N = cfg->num_paths;
+  const int draws = k->dynamics == OF_LSM_HESTON_EULER ? 2 : 1;
+  if (cfg->injected_normals && cfg->n_injected < N * steps * draws)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "injected normals: need %lld values, got %lld",
+                   (long long)(N * steps * draws), (long long)cfg->n_injected);
+  if ((double)N * (double)steps * (fp64 ? 8.0 : 4.0) > (double)((size_t)48 << 30))
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "path store of %lld x %lld exceeds 48 GB", (long long)N,
+                   (long long)steps);
+  OF_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  std::memset(result, 0, sizeof(*result));
+  *n_boundary = 0;
+  const uint64_t* jump = nullptr;
+  if (fp64 && !cfg->injected_normals) OF_TRY(upload_jump_tables(ctx, &jump));
+
+  // schedule -> steps (longstaff_schwartz.rs:329-335): the later date wins a shared step
+  std::vector<int64_t> date_of_step((size_t)steps + 1, -1);
+  for (int64_t d = 0; d < k->n_schedule; ++d) {
+    const double idx = std::round((k->schedule_times[d] / k->expiry) * (double)steps);
+    const int64_t i = (std::isnan(idx) || idx < 1.0) ? 1 : (idx > (double)steps ? steps : (int64_t)idx);
+    date_of_step[(size_t)i] = d;
+  }
+  const double k_T = k->schedule_strikes[k->n_schedule - 1];
+  std::vector<LsmHost> hs(1);
+  LsmHost& h = hs[0];
+  h.can.assign((size_t)steps + 1, 0);
+  std::vector<double> kk((size_t)steps + 1, k_T);
+  for (int64_t t = 1; t < steps; ++t)
+    if (date_of_step[(size_t)t] >= 0) {
+      h.can[(size_t)t] = 1;
+      kk[(size_t)t] = k->schedule_strikes[date_of_step[(size_t)t]];
+    }
+  h.can[(size_t)steps] = 1;
+  if (k->dynamics == OF_LSM_LOCAL_VOL) {
+    h.lv_k.assign(k->lv_strikes, k->lv_strikes + k->lv_n_strikes);
+    h.lv_t.assign(k->lv_expiries, k->lv_expiries + k->lv_n_expiries);
+    h.lv_v.assign(k->lv_vols, k->lv_vols + k->lv_n_strikes * k->lv_n_expiries);
+  }
+  fill_steps(h, steps, k->expiry, kk.data());
+  LsmC& C = h.C;
+  const double dt = k->expiry / (double)steps, sqdt = std::sqrt(dt);
+  const double mu = k->rate - k->dividend_yield;
+  C.put = k->option_type == OF_PUT;
+  C.steps = (int32_t)steps;
+  C.dynamics = k->dynamics == OF_LSM_GBM ? DYN_GBM : (k->dynamics == OF_LSM_LOCAL_VOL ? DYN_LOCAL_VOL : DYN_HESTON);
+  C.spot = k->spot;
+  C.strike = k_T;
+  C.inv_strike = 1.0 / k_T;
+  C.inv_spot = 1.0 / k->spot;
+  C.drift = (mu - 0.5 * k->vol * k->vol) * dt;  // longstaff_schwartz.rs:205
+  C.step_vol = k->vol * sqdt;
+  C.disc = std::exp(-k->rate * dt);
+  C.mu = mu;
+  C.dt = dt;
+  C.sqrt_dt = sqdt;
+  C.kappa = k->kappa;
+  C.theta = k->theta;
+  C.xi = k->xi;
+  C.rho = k->rho;
+  C.v0 = k->v0;
+  C.fdrift = (float)C.drift;
+  C.fstep_vol = (float)C.step_vol;
+  C.fspot = (float)k->spot;
+  C.fmudt = (float)(mu * dt);
+  C.fsqrt_dt = (float)sqdt;
+  C.fdt = (float)dt;
+  C.fy_floor = (float)std::log(1e-12 / k->spot);
+  C.hc.mudt = (float)(mu * dt);
+  C.hc.half_dt = (float)(0.5 * dt);
+  C.hc.sqdt = (float)sqdt;
+  C.hc.kdt = (float)(k->kappa * dt);
+  C.hc.kdt_theta = (float)(k->kappa * k->theta * dt);
+  C.hc.one_m_kdt = (float)(1.0 - k->kappa * dt);
+  C.hc.xi_sqdt = (float)(k->xi * sqdt);
+  C.hc.rho = (float)k->rho;
+  C.hc.rho_c = (float)std::sqrt(1.0 - k->rho * k->rho);
+  C.hc.v0 = (float)k->v0;
+  C.hc.y_floor = C.fy_floor;
+
+  std::vector<double> hres;
+  std::vector<int32_t> hreg;
+  std::vector<LsmTrack> tr;
+  float ms = 0.0f;
+  OF_TRY(lsm_run_batch(ctx, hs, steps, cfg, jump, 0u, cfg->injected_normals, draws, &tr, hres, hreg, &ms));
+  result->price = hres[0];
+  result->stderr_ = hres[1];
+  result->delta = cfg->want_delta ? hres[2] : 0.0;
+  result->regressions = hreg[0];
+  result->kernel_ms = ms;
+
+  // boundary points, chronological (longstaff_schwartz.rs:337-412): every
+  // scheduled step before expiry, then the terminal point
+  std::vector<of_boundary_point> pts;
+  for (int64_t t = 1; t < steps; ++t) {
+    const int64_t d = date_of_step[(size_t)t];
+    if (d < 0) continue;
+    of_boundary_point p{};
+    p.time = k->schedule_times[d];
+    p.strike = k->schedule_strikes[d];
+    p.itm_paths = (int64_t)tr[0].itm[(size_t)t];
+    p.exercised_paths = p.itm_paths >= 3 ? (int64_t)tr[0].ex_count[(size_t)t] : 0;
+    p.has_boundary = p.exercised_paths > 0 ? 1 : 0;
+    double b;
+    const unsigned long long bits = tr[0].ex_bits[(size_t)t];
+    std::memcpy(&b, &bits, sizeof(b));
+    p.boundary_spot = p.has_boundary ? b : std::nan("");
+    pts.push_back(p);
+  }
+  of_boundary_point term{};
+  term.time = k->expiry;
+  term.strike = k_T;
+  term.boundary_spot = k_T;
+  term.has_boundary = 1;
+  term.itm_paths = term.exercised_paths = (int64_t)tr[0].term_itm;
+  pts.push_back(term);
+  *n_boundary = (int64_t)pts.size();
+  for (int64_t i = 0; i < (int64_t)pts.size() && i < capacity; ++i) boundary[i] = pts[(size_t)i];
   return OF_OK;
 }
