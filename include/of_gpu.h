@@ -76,6 +76,16 @@ enum {
  *   compensated FP32 per-thread sums, FP64 cross-thread reduction. */
 enum { OF_PREC_FP64_REFERENCE = 0, OF_PREC_FP32_PHILOX = 1 };
 
+/* DividendKind / DividendEvent (src/market/dividends.rs:16-92) */
+enum { OF_DIV_CASH = 0, OF_DIV_PROPORTIONAL = 1 };
+
+typedef struct of_dividend_event {
+  double time;    /* ex-dividend time in years, > 0 */
+  int32_t kind;   /* OF_DIV_CASH: S+ = max(S- - amount, 0); OF_DIV_PROPORTIONAL: S+ = S- (1 - amount) */
+  int32_t reserved0;
+  double amount;  /* cash amount >= 0, or ratio in [0, 1) */
+} of_dividend_event;
+
 typedef struct of_model {
   int32_t kind; /* OF_MODEL_* */
   int32_t reserved0;
@@ -85,6 +95,12 @@ typedef struct of_model {
   double maturity; /* simulation horizon in years */
   int64_t steps;
   double kappa, theta, xi, rho, v0; /* Heston parameters */
+  /* GBM only: a discrete dividend schedule with strictly increasing times
+   * (DiscreteDividendGbmPathGenerator, src/engines/monte_carlo/mc_engine.rs:
+   * 123-175): after step j every event with time <= maturity + 1e-12 and
+   * time <= (j+1) dt + 1e-12 not yet applied jumps the spot.  NULL / 0 = none. */
+  const of_dividend_event* dividends;
+  int64_t n_dividends;
 } of_model;
 
 typedef struct of_payoff {

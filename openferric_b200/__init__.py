@@ -12,13 +12,14 @@ from .engines import (ArithmeticAsianMC, ControlVariate, ControlVariateKind, Fas
                       Heston, HestonPathGenerator, MonteCarloEngine, MonteCarloPricingEngine, Precision,
                       VarianceReduction, price_strike_strip)
 from .instruments import AsianOption, BarrierOption, BermudanOption, VanillaOption, daily_fixings
-from .market import Market, MarketBuilder, SampledVolSurface
+from .market import DividendEvent, DividendKind, DividendSchedule, Market, MarketBuilder, SampledVolSurface
 
 __all__ = [
     "GpuUnavailable", "OfGpuError", "context", "AsianSpec", "Averaging", "BarrierDirection", "BarrierSpec",
     "BarrierStyle", "Diagnostics", "ExerciseStyle", "Greeks", "OptionType", "PricingError", "PricingResult",
     "StrikeType", "ArithmeticAsianMC", "ControlVariate", "ControlVariateKind", "FastRngKind", "Gbm",
     "GbmPathGenerator", "Heston", "HestonPathGenerator", "MonteCarloEngine", "MonteCarloPricingEngine", "Precision",
-    "VarianceReduction", "price_strike_strip", "SampledVolSurface", "AsianOption", "BarrierOption", "BermudanOption", "VanillaOption",
+    "VarianceReduction", "price_strike_strip", "SampledVolSurface", "DividendEvent", "DividendKind",
+    "DividendSchedule", "AsianOption", "BarrierOption", "BermudanOption", "VanillaOption",
     "daily_fixings", "Market", "MarketBuilder",
 ]

@@ -25,6 +25,18 @@ OF_CV_NONE, OF_CV_VANILLA_TERMINAL, OF_CV_GEOMETRIC_ASIAN, OF_CV_TERMINAL_SPOT =
 OF_PREC_FP64_REFERENCE, OF_PREC_FP32_PHILOX = 0, 1
 
 
+OF_DIV_CASH, OF_DIV_PROPORTIONAL = 0, 1
+
+
+class OfDividendEvent(C.Structure):
+    _fields_ = [
+        ("time", C.c_double),
+        ("kind", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("amount", C.c_double),
+    ]
+
+
 class OfModel(C.Structure):
     _fields_ = [
         ("kind", C.c_int32),
@@ -39,6 +51,8 @@ class OfModel(C.Structure):
         ("xi", C.c_double),
         ("rho", C.c_double),
         ("v0", C.c_double),
+        ("dividends", C.POINTER(OfDividendEvent)),
+        ("n_dividends", C.c_int64),
     ]
 
 

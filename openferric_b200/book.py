@@ -50,9 +50,11 @@ class BookPlan:
             inst, m = e.instrument, e.market
             inst.validate()
             vol = m.vol_for(max(reference_strike(inst, m.spot), 1e-12), inst.expiry)
-            gen = GbmPathGenerator(Gbm(m.rate - m.dividend_yield, vol), m.spot, inst.expiry, e.num_steps)
+            gen = GbmPathGenerator(Gbm(m.rate - m.dividend_yield, vol), m.spot, inst.expiry, e.num_steps,
+                                   m.dividend_schedule if m.has_discrete_dividends() else None)
             payoff, keep = _payoff_abi(inst)
             self._keep.append(keep)
+            self._keep.append(gen)  # holds the dividend array the model points to
             self._vols.append(vol)
             cv = instrument_control_variate(inst, m, vol) \
                 if e.variance_reduction is VarianceReduction.ControlVariate else None

@@ -350,6 +350,8 @@ static of_status strip_setup(of_ctx* ctx, const of_model* m, int32_t option_type
   dummy.strike = 1.0;
   OF_TRY(of_validate_mc(ctx, m, &dummy, cfg));
   OF_TRY(validate_fp32_model(ctx, m));
+  if (m->n_dividends > 0)  // the strip keeps only the sum of the normals of a GBM path
+    return of_fail(ctx, OF_ERR_UNSUPPORTED, "the strike strip takes no discrete dividends (price them as a book)");
   if (n_strikes <= 0 || !strikes) return of_fail(ctx, OF_ERR_INVALID_INPUT, "strip needs at least one strike");
   if (n_strikes > 128) return of_fail(ctx, OF_ERR_UNSUPPORTED, "strip supports at most 128 strikes per call");
   for (int64_t k = 0; k < n_strikes; ++k)
@@ -507,6 +509,15 @@ struct BookOpt {
   int32_t obs_offset;  // into the shared weight array, -1 when unused
   float s0, strike, barrier_y, rebate, inv_nobs;
   uint32_t stream;
+  int32_t div_offset, n_div;  // discrete dividend triggers (GBM), in the shared table
+};
+
+// A dividend trigger in log-spot form: after step `step`, a cash dividend
+// sets y = log(max(e^y - a, 0)) with a = D/S0; a proportional one adds
+// a = log(1 - p).
+struct BookDiv {
+  int32_t step, kind;
+  float a, pad;
 };
 
 struct BookTile {
@@ -521,6 +532,7 @@ struct BookParams {
   const BookOpt* opts;
   const BookTile* tiles;
   const float* obs_w;
+  const BookDiv* divs;
   int32_t n_tiles;
   int32_t ppt;  // samples per thread per tile (tile = block * ppt samples)
   of::PhiloxKeys keys;
@@ -585,9 +597,14 @@ __device__ __forceinline__ void book_payoff(const BookOpt& o, const PathObs& ob,
 }
 
 // One sample (and its antithetic twin) of option o; returns (x, y).
+// DividendEvent::apply_jump (src/market/dividends.rs:76-83) on the log-spot.
+__device__ __forceinline__ float book_dividend(const BookDiv& d, float y) {
+  return d.kind == OF_DIV_CASH ? __logf(fmaxf(__expf(y) - d.a, 0.0f)) : y + d.a;
+}
+
 template <int MODEL>
 __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, const of::PhiloxKeys& K, const float* obs_w,
-                                            float& x, float& cvy) {
+                                            const BookDiv* divs, float& x, float& cvy) {
   const bool anti = o.flags & BF_ANTI;
   const StepConsts& c = o.c;
   LegState a{0.0f, c.v0}, b{0.0f, c.v0};
@@ -595,6 +612,7 @@ __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, const 
   book_observe(o, oa, 0.0f, 0, obs_w);
   if (anti) book_observe(o, obb, 0.0f, 0, obs_w);
   const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
+  int32_t ev = 0;  // next dividend trigger (GBM)
   const bool observe_each = (o.payoff != OF_PAYOFF_VANILLA) || (o.flags & (BF_NEED_ARITH | BF_NEED_GEO));
   constexpr int SPC = MODEL == OF_MODEL_GBM ? 4 : 2;  // steps per Philox call
   for (int32_t j = 0; j < o.steps; j += SPC) {
@@ -613,6 +631,11 @@ __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, const 
         const float z = q == 0 ? p01.x : q == 1 ? p01.y : q == 2 ? p23.x : p23.y;
         a.y = fmaf(c.diff, z, a.y + c.drift);
         if (anti) b.y = fmaf(-c.diff, z, b.y + c.drift);
+        for (; ev < o.n_div && divs[o.div_offset + ev].step == j + q; ++ev) {  // mc_engine.rs:157-167
+          const BookDiv d = divs[o.div_offset + ev];
+          a.y = book_dividend(d, a.y);
+          if (anti) b.y = book_dividend(d, b.y);
+        }
       } else if (MODEL == OF_MODEL_HESTON_EULER) {
         const float2 z = q == 0 ? p01 : p23;
         const float z1 = z.x, z2 = z.y;
@@ -656,9 +679,10 @@ __global__ void __launch_bounds__(256, 3) book_kernel(const __grid_constant__ Bo
       if (local >= tile.count) break;
       const uint64_t i = (uint64_t)(tile.first + local);
       float x, y;
-      if (o.model == OF_MODEL_GBM) book_sample<OF_MODEL_GBM>(o, i, P.keys, P.obs_w, x, y);
-      else if (o.model == OF_MODEL_HESTON_EULER) book_sample<OF_MODEL_HESTON_EULER>(o, i, P.keys, P.obs_w, x, y);
-      else book_sample<OF_MODEL_HESTON_QE>(o, i, P.keys, P.obs_w, x, y);
+      if (o.model == OF_MODEL_GBM) book_sample<OF_MODEL_GBM>(o, i, P.keys, P.obs_w, P.divs, x, y);
+      else if (o.model == OF_MODEL_HESTON_EULER)
+        book_sample<OF_MODEL_HESTON_EULER>(o, i, P.keys, P.obs_w, P.divs, x, y);
+      else book_sample<OF_MODEL_HESTON_QE>(o, i, P.keys, P.obs_w, P.divs, x, y);
       acc[0].add(x);
       acc[1].add(x * x);
       acc[2].add(y);
@@ -705,6 +729,7 @@ struct of_book_plan {
   BookOpt* d_opts = nullptr;
   BookTile* d_tiles = nullptr;
   float* d_obs = nullptr;
+  BookDiv* d_divs = nullptr;
   int* d_counter = nullptr;
   double* d_partials = nullptr;
   int32_t* d_begin = nullptr;
@@ -730,6 +755,7 @@ extern "C" void of_book_plan_destroy(of_book_plan* pl) {
   cudaFree(pl->d_opts);
   cudaFree(pl->d_tiles);
   cudaFree(pl->d_obs);
+  cudaFree(pl->d_divs);
   cudaFree(pl->d_counter);
   cudaFree(pl->d_partials);
   cudaFree(pl->d_begin);
@@ -761,6 +787,8 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
   };
   std::vector<BookOpt> opts((size_t)n);
   std::vector<float> obs;
+  std::vector<BookDiv> divs;
+  std::vector<of_div_trigger> trig;
   pl->samples.resize((size_t)n);
   pl->cv_kind.resize((size_t)n);
   pl->cv_expected.resize((size_t)n);
@@ -800,6 +828,16 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
     if (!(b.payoff.barrier_level > 0.0)) d.barrier_y = b.payoff.barrier_direction == OF_BARRIER_UP ? INFINITY : -INFINITY;
     d.stream = (uint32_t)o;
     d.obs_offset = -1;
+    st = of_dividend_triggers(ctx, &b.model, trig);
+    if (st != OF_OK) {
+      ctx->last_error = "book entry " + std::to_string(o) + ": " + ctx->last_error;
+      return fail(st);
+    }
+    d.div_offset = (int32_t)divs.size();
+    d.n_div = (int32_t)trig.size();
+    for (const of_div_trigger& t : trig)
+      divs.push_back(BookDiv{t.step, t.kind,
+                             (float)(t.kind == OF_DIV_CASH ? t.amount / b.model.s0 : std::log1p(-t.amount)), 0.0f});
     int32_t f = 0;
     if (b.antithetic) f |= BF_ANTI;
     if (b.payoff.barrier_direction == OF_BARRIER_UP) f |= BF_UP;
@@ -863,6 +901,7 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
   if (cudaMalloc(&pl->d_opts, opts.size() * sizeof(BookOpt)) != cudaSuccess ||
       cudaMalloc(&pl->d_tiles, nt * sizeof(BookTile)) != cudaSuccess ||
       cudaMalloc(&pl->d_obs, std::max<size_t>(1, obs.size()) * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&pl->d_divs, std::max<size_t>(1, divs.size()) * sizeof(BookDiv)) != cudaSuccess ||
       cudaMalloc(&pl->d_counter, sizeof(int)) != cudaSuccess ||
       cudaMalloc(&pl->d_partials, nt * 5 * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&pl->d_begin, begin.size() * sizeof(int32_t)) != cudaSuccess ||
@@ -872,12 +911,15 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
   if (cudaMemcpy(pl->d_opts, opts.data(), opts.size() * sizeof(BookOpt), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(pl->d_tiles, sorted.data(), nt * sizeof(BookTile), cudaMemcpyHostToDevice) != cudaSuccess ||
       (!obs.empty() && cudaMemcpy(pl->d_obs, obs.data(), obs.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) ||
+      (!divs.empty() &&
+       cudaMemcpy(pl->d_divs, divs.data(), divs.size() * sizeof(BookDiv), cudaMemcpyHostToDevice) != cudaSuccess) ||
       cudaMemcpy(pl->d_begin, begin.data(), begin.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(of_fail(ctx, OF_ERR_CUDA, "book upload failed"));
   BookParams& P = pl->P;
   P.opts = pl->d_opts;
   P.tiles = pl->d_tiles;
   P.obs_w = pl->d_obs;
+  P.divs = pl->d_divs;
   P.n_tiles = (int32_t)nt;
   P.ppt = pl->ppt;
   P.keys = of::philox_keys(cfg->seed);
@@ -1033,6 +1075,8 @@ extern "C" of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* m, i
   } else {
     return noalloc_msg(err, err_len, "unknown model kind %d", m->kind), OF_ERR_INVALID_INPUT;
   }
+  if (m->n_dividends > 0)
+    return noalloc_msg(err, err_len, "the strike strip takes no discrete dividends"), OF_ERR_UNSUPPORTED;
   if (option_type != OF_CALL && option_type != OF_PUT)
     return noalloc_msg(err, err_len, "unknown option type %d", option_type), OF_ERR_INVALID_INPUT;
   if (cfg->control_variate != OF_CV_NONE || cfg->injected_normals)

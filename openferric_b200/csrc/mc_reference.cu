@@ -31,6 +31,8 @@ struct RefParams {
   double mu, dt, sqrt_dt, kappa, theta, xi, rho, rho_c, v0;  // Heston (stochastic.rs:56-71)
   const double* obs_w;  // [steps+1] observation counts
   const double* inj;    // injected normals or nullptr
+  const of_div_trigger* div;  // GBM discrete dividends by trigger step, or nullptr
+  int32_t n_div;
 };
 
 struct Leg {
@@ -108,6 +110,15 @@ __device__ __forceinline__ double leg_cv(const Leg& L, const RefParams& P) {
   }
 }
 
+// DividendEvent::apply_jump (src/market/dividends.rs:76-83).
+__device__ __forceinline__ double dividend_jump(const of_div_trigger& e, double s) {
+  if (e.kind == OF_DIV_CASH) {
+    const double x = s - e.amount;
+    return x > 0.0 ? x : 0.0;
+  }
+  return s * (1.0 - e.amount);
+}
+
 __global__ void __launch_bounds__(128) mc_ref_kernel(RefParams P, double* __restrict__ partials) {
   __shared__ double sh[5 * 4];
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -121,6 +132,7 @@ __global__ void __launch_bounds__(128) mc_ref_kernel(RefParams P, double* __rest
     Leg a, b;
     leg_init(a, P);
     if (P.antithetic) leg_init(b, P);
+    int32_t ev = 0;  // next dividend trigger
     for (int64_t j = 0; j < P.steps; ++j) {
       double z1, z2 = 0.0;
       if (inj) {
@@ -133,6 +145,10 @@ __global__ void __launch_bounds__(128) mc_ref_kernel(RefParams P, double* __rest
       if (!heston) {
         a.s *= exp(fma(P.diffusion, z1, P.drift));  // simulation.rs:67-71
         if (P.antithetic) b.s *= exp(fma(P.diffusion, -z1, P.drift));
+        for (; ev < P.n_div && P.div[ev].step == j; ++ev) {  // mc_engine.rs:157-167
+          a.s = dividend_jump(P.div[ev], a.s);
+          if (P.antithetic) b.s = dividend_jump(P.div[ev], b.s);
+        }
       } else {
         heston_step(a, P, z1, z2);
         if (P.antithetic) heston_step(b, P, -z1, -z2);
@@ -167,6 +183,42 @@ static int64_t obs_index(double t, double maturity, int64_t len) {
   return i < len - 1 ? i : len - 1;
 }
 
+of_status of_dividend_triggers(of_ctx* ctx, const of_model* m, std::vector<of_div_trigger>& out) {
+  out.clear();
+  if (m->n_dividends <= 0) return OF_OK;
+  if (!m->dividends) return of_fail(ctx, OF_ERR_INVALID_INPUT, "dividends is null");
+  if (m->kind != OF_MODEL_GBM)
+    return of_fail(ctx, OF_ERR_UNSUPPORTED, "discrete dividends apply to GBM paths only");
+  double prev = 0.0;
+  for (int64_t e = 0; e < m->n_dividends; ++e) {
+    const of_dividend_event& d = m->dividends[e];
+    if (!std::isfinite(d.time) || d.time <= 0.0)
+      return of_fail(ctx, OF_ERR_INVALID_INPUT, "dividend event time must be finite and > 0");
+    if (d.kind == OF_DIV_CASH) {
+      if (!std::isfinite(d.amount) || d.amount < 0.0)
+        return of_fail(ctx, OF_ERR_INVALID_INPUT, "cash dividend amount must be finite and >= 0");
+    } else if (d.kind == OF_DIV_PROPORTIONAL) {
+      if (!std::isfinite(d.amount) || d.amount < 0.0 || d.amount >= 1.0)
+        return of_fail(ctx, OF_ERR_INVALID_INPUT, "proportional dividend ratio must be finite and in [0, 1)");
+    } else {
+      return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown dividend kind %d", d.kind);
+    }
+    if (d.time <= prev) return of_fail(ctx, OF_ERR_INVALID_INPUT, "dividend event times must be strictly increasing");
+    prev = d.time;
+  }
+  const double dt = m->maturity / (double)m->steps;
+  int64_t ev = 0;
+  for (int64_t j = 0; j < m->steps && ev < m->n_dividends; ++j) {
+    const double t = (double)(j + 1) * dt;
+    while (ev < m->n_dividends && m->dividends[ev].time <= m->maturity + 1.0e-12 &&
+           m->dividends[ev].time <= t + 1.0e-12) {
+      out.push_back(of_div_trigger{(int32_t)j, m->dividends[ev].kind, m->dividends[ev].amount});
+      ++ev;
+    }
+  }
+  return OF_OK;
+}
+
 of_status of_validate_mc(of_ctx* ctx, const of_model* m, const of_payoff* p, const of_mc_config* c) {
   if (!m || !p || !c) return of_fail(ctx, OF_ERR_INVALID_INPUT, "null argument");
   if (c->num_paths <= 0) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_paths must be > 0");
@@ -185,6 +237,10 @@ of_status of_validate_mc(of_ctx* ctx, const of_model* m, const of_payoff* p, con
       return of_fail(ctx, OF_ERR_INVALID_INPUT, "invalid Heston parameters");
   } else {
     return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown model kind %d", m->kind);
+  }
+  if (m->n_dividends > 0) {
+    std::vector<of_div_trigger> trig;
+    OF_TRY(of_dividend_triggers(ctx, m, trig));
   }
   if (p->option_type != OF_CALL && p->option_type != OF_PUT)
     return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown option type %d", p->option_type);
@@ -272,6 +328,17 @@ extern "C" of_status of_mc_run(of_ctx* ctx, const of_model* m, const of_payoff* 
     OF_CUDA_TRY(ctx, cudaMemcpyAsync(d_obs, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   }
   P.obs_w = (const double*)d_obs;
+
+  std::vector<of_div_trigger> trig;
+  OF_TRY(of_dividend_triggers(ctx, m, trig));
+  if (!trig.empty()) {
+    void* d_div = nullptr;
+    OF_TRY(of_scratch(ctx, SLOT_DIVIDENDS, trig.size() * sizeof(of_div_trigger), &d_div));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(d_div, trig.data(), trig.size() * sizeof(of_div_trigger),
+                                     cudaMemcpyHostToDevice, ctx->stream));
+    P.div = (const of_div_trigger*)d_div;
+    P.n_div = (int32_t)trig.size();
+  }
 
   const int streams = m->kind == OF_MODEL_GBM ? 1 : 2;
   if (c->injected_normals) {

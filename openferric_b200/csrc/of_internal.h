@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 #include "../../include/of_gpu.h"
 
@@ -21,7 +22,7 @@ enum OfSlot {
   SLOT_STRIKES = 4,    // strike strip
   SLOT_BOOK = 5,       // batched-book option table
   SLOT_TILES = 6,      // batched-book tile table
-  SLOT_BOOK_OBS = 7,   // unused
+  SLOT_DIVIDENDS = 7,  // discrete dividend triggers
   SLOT_LSM_PATHS = 8,  // LSM path store (time-major)
   SLOT_LSM_VALUES = 9, // LSM cash flows
   SLOT_LSM_AUX = 10,   // LSM betas / counters
@@ -82,3 +83,17 @@ void of_mc_finish(const double sums[5], int64_t count, int32_t cv_kind, double c
 
 // Blocks per SM the occupancy calculator allows for `kernel` at `block` threads.
 int of_blocks_per_sm(const void* kernel, int block, size_t smem);
+
+// A discrete dividend of a GBM model resolved to the simulation step after
+// which it applies (0-based step j: the jump follows the move to t = (j+1) dt).
+struct of_div_trigger {
+  int32_t step;
+  int32_t kind;   // OF_DIV_CASH / OF_DIV_PROPORTIONAL
+  double amount;  // cash amount or ratio
+};
+
+// Validates m->dividends (DividendSchedule::validate, src/market/dividends.rs:
+// 131-144) and resolves them with the loop of DiscreteDividendGbmPathGenerator
+// (src/engines/monte_carlo/mc_engine.rs:157-167): events that never trigger
+// before maturity are dropped.  Non-GBM models with dividends are rejected.
+of_status of_dividend_triggers(of_ctx* ctx, const of_model* m, std::vector<of_div_trigger>& out);

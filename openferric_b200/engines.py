@@ -84,17 +84,28 @@ class Heston:
 
 @dataclass
 class GbmPathGenerator:
+    """GbmPathGenerator (simulation.rs:39-78); with a dividend schedule it is
+    DiscreteDividendGbmPathGenerator (mc_engine.rs:123-175)."""
+
     model: Gbm
     s0: float
     maturity: float
     steps: int
+    dividends: Optional[object] = None  # market.DividendSchedule
 
     def num_normal_streams(self) -> int:
         return 1
 
     def to_abi(self) -> A.OfModel:
-        return A.OfModel(kind=A.OF_MODEL_GBM, s0=self.s0, mu=self.model.mu, sigma=self.model.sigma,
-                         maturity=self.maturity, steps=int(self.steps))
+        """The model struct; a dividend array stays referenced by this generator."""
+        m = A.OfModel(kind=A.OF_MODEL_GBM, s0=self.s0, mu=self.model.mu, sigma=self.model.sigma,
+                      maturity=self.maturity, steps=int(self.steps))
+        arr = self.dividends.to_abi() if self.dividends is not None else None
+        if arr is not None:
+            self._abi_dividends = arr
+            m.dividends = C.cast(arr, C.POINTER(A.OfDividendEvent))
+            m.n_dividends = len(arr)
+        return m
 
 
 @dataclass
@@ -366,13 +377,12 @@ class MonteCarloPricingEngine:
             raise PricingError.InvalidInput("instrument maturity must be >= 0")
         if maturity == 0.0:
             return None, PricingResult(price=payoff_from_path(instrument, [market.spot]), stderr=0.0)
-        if market.has_discrete_dividends():
-            raise PricingError.InvalidInput("discrete dividend schedules are not supported by the GPU engine")
         ref_k = max(reference_strike(instrument, market.spot), 1e-12)
         vol = market.vol_for(ref_k, maturity)
         if vol <= 0.0:
             raise PricingError.InvalidInput("market volatility must be > 0")
-        gen = GbmPathGenerator(Gbm(market.rate - market.dividend_yield, vol), market.spot, maturity, self.num_steps)
+        gen = GbmPathGenerator(Gbm(market.rate - market.dividend_yield, vol), market.spot, maturity, self.num_steps,
+                               market.dividend_schedule if market.has_discrete_dividends() else None)
         anti = self.variance_reduction is VarianceReduction.Antithetic
         cv = instrument_control_variate(instrument, market, vol) \
             if self.variance_reduction is VarianceReduction.ControlVariate else None
@@ -415,6 +425,7 @@ class MonteCarloPricingEngine:
             gen, anti, cv, df, vol = setup
             payoff, k = _payoff_abi(inst)
             keep.append(k)
+            keep.append(gen)  # holds the dividend array the model points to
             e = A.OfBookEntry(model=gen.to_abi(), payoff=payoff, num_paths=self.num_paths, antithetic=int(anti),
                               discount_factor=df)
             if cv is not None:
@@ -490,11 +501,10 @@ class ArithmeticAsianMC:
         vol = market.vol_for(instrument.strike, maturity)
         if vol <= 0.0 or not math.isfinite(vol):
             raise PricingError.InvalidInput("market volatility must be finite and > 0")
-        if market.has_discrete_dividends():
-            raise PricingError.InvalidInput("discrete dividend schedules are not supported by the GPU engine")
-        gen = GbmPathGenerator(Gbm(market.rate - market.dividend_yield, vol), market.spot, maturity, self.steps)
+        gen = GbmPathGenerator(Gbm(market.rate - market.dividend_yield, vol), market.spot, maturity, self.steps,
+                               market.dividend_schedule if market.has_discrete_dividends() else None)
         eng = MonteCarloEngine(self.paths, self.seed, self.device).with_antithetic(True).with_precision(self.precision)
-        if self.control_variate:
+        if self.control_variate and not market.has_discrete_dividends():  # mc_engine.rs:791
             expected_disc = geometric_asian_discrete_fixed(instrument.option_type, market.spot, instrument.strike,
                                                            market.rate, market.dividend_yield, vol,
                                                            instrument.asian.observation_times)

@@ -118,30 +118,151 @@ class VolSource:
         return one, one, np.full((1, 1), float(self.flat))
 
 
+class DividendKind:
+    """DividendKind (src/market/dividends.rs:16-43)."""
+
+    CASH = 0
+    PROPORTIONAL = 1
+
+
+@dataclass(frozen=True)
+class DividendEvent:
+    """DividendEvent (src/market/dividends.rs:45-92): a cash amount or a
+    proportional ratio at an ex-dividend time (years)."""
+
+    time: float
+    kind: int
+    amount: float
+
+    @staticmethod
+    def cash(time: float, amount: float) -> "DividendEvent":
+        e = DividendEvent(float(time), DividendKind.CASH, float(amount))
+        e.validate()
+        return e
+
+    @staticmethod
+    def proportional(time: float, ratio: float) -> "DividendEvent":
+        e = DividendEvent(float(time), DividendKind.PROPORTIONAL, float(ratio))
+        e.validate()
+        return e
+
+    def apply_jump(self, pre_div_spot: float) -> float:
+        if self.kind == DividendKind.CASH:
+            return max(pre_div_spot - self.amount, 0.0)
+        return pre_div_spot * (1.0 - self.amount)
+
+    def validate(self) -> None:
+        if not math.isfinite(self.time) or self.time <= 0.0:
+            raise PricingError.InvalidInput("dividend event time must be finite and > 0")
+        if self.kind == DividendKind.CASH:
+            if not math.isfinite(self.amount) or self.amount < 0.0:
+                raise PricingError.InvalidInput("cash dividend amount must be finite and >= 0")
+        elif not math.isfinite(self.amount) or not 0.0 <= self.amount < 1.0:
+            raise PricingError.InvalidInput("proportional dividend ratio must be finite and in [0, 1)")
+
+
+class DividendSchedule:
+    """DividendSchedule (src/market/dividends.rs:93-228): events sorted by
+    time, strictly increasing."""
+
+    def __init__(self, events=()):
+        self._events = tuple(sorted(events, key=lambda e: e.time))
+
+    @staticmethod
+    def new(events) -> "DividendSchedule":
+        s = DividendSchedule(events)
+        s.validate()
+        return s
+
+    @staticmethod
+    def empty() -> "DividendSchedule":
+        return DividendSchedule(())
+
+    def is_empty(self) -> bool:
+        return not self._events
+
+    def events(self):
+        return self._events
+
+    def events_until(self, maturity: float):
+        return [e for e in self._events if e.time <= maturity]
+
+    def validate(self) -> None:
+        prev = 0.0
+        for e in self._events:
+            e.validate()
+            if e.time <= prev:
+                raise PricingError.InvalidInput("dividend event times must be strictly increasing")
+            prev = e.time
+
+    def forward_price(self, spot: float, rate: float, q: float, maturity: float) -> float:
+        """Forward with deterministic jumps (dividends.rs:145-184)."""
+        if maturity <= 0.0:
+            return spot
+        if not math.isfinite(spot) or spot <= 0.0:
+            return 0.0
+        carry = rate - q
+        fwd = spot * math.exp(carry * maturity)
+        for e in self.events_until(maturity):
+            if e.kind == DividendKind.CASH:
+                fwd -= e.amount * math.exp(carry * (maturity - e.time))
+            else:
+                fwd *= 1.0 - e.amount
+        return max(fwd, 0.0)
+
+    def prepaid_forward_spot(self, spot: float, rate: float, q: float, maturity: float) -> float:
+        return self.forward_price(spot, rate, q, maturity) * math.exp(-rate * maturity)
+
+    def escrowed_spot_adjustment(self, spot: float, rate: float, maturity: float) -> float:
+        return self.prepaid_forward_spot(spot, rate, 0.0, maturity)
+
+    def effective_dividend_yield(self, spot: float, rate: float, q: float, maturity: float) -> float:
+        """dividends.rs:203-218."""
+        if maturity <= 0.0 or spot <= 0.0:
+            return q
+        ratio = max(self.forward_price(spot, rate, q, maturity) / spot, 1.0e-16)
+        return rate - math.log(ratio) / maturity
+
+    def apply_jumps_until(self, spot: float, time: float) -> float:
+        for e in self.events_until(time):
+            spot = e.apply_jump(spot)
+        return spot
+
+    def to_abi(self):
+        """The events as an of_dividend_event array (None when empty)."""
+        from . import _abi as A
+        if not self._events:
+            return None
+        return (A.OfDividendEvent * len(self._events))(
+            *[A.OfDividendEvent(time=e.time, kind=e.kind, amount=e.amount) for e in self._events])
+
+
 @dataclass
 class Market:
-    """market::Market (src/market/market.rs:201-302).  Discrete dividend
-    schedules are not supported by the GPU engines (an empty schedule is the
-    only accepted value)."""
+    """market::Market (src/market/market.rs:201-302)."""
 
     spot: float
     rate: float
     dividend_yield: float
     vol: VolSource
     reference_date: Optional[str] = None
-    dividend_schedule: tuple = field(default_factory=tuple)
+    dividend_schedule: "DividendSchedule" = field(default_factory=lambda: DividendSchedule.empty())
 
     @staticmethod
     def builder() -> "MarketBuilder":
         return MarketBuilder()
 
     def has_discrete_dividends(self) -> bool:
-        return len(self.dividend_schedule) > 0
+        return not self.dividend_schedule.is_empty()
+
+    def forward_price(self, maturity: float) -> float:
+        return self.dividend_schedule.forward_price(self.spot, self.rate, self.dividend_yield, maturity)
+
+    def prepaid_forward_spot(self, maturity: float) -> float:
+        return self.dividend_schedule.prepaid_forward_spot(self.spot, self.rate, self.dividend_yield, maturity)
 
     def effective_dividend_yield(self, maturity: float) -> float:
-        # With no discrete schedule the effective yield is the continuous one
-        # (market/dividends.rs effective_dividend_yield).
-        return self.dividend_yield
+        return self.dividend_schedule.effective_dividend_yield(self.spot, self.rate, self.dividend_yield, maturity)
 
     def vol_for(self, strike: float, expiry: float) -> float:
         return self.vol.vol(strike, expiry)
@@ -157,6 +278,12 @@ class MarketBuilder:
         self._flat = None
         self._surface = None
         self._ref = None
+        self._divs = None
+
+    def dividend_schedule(self, schedule: DividendSchedule) -> "MarketBuilder":
+        """Sets a deterministic discrete dividend schedule (market.rs:340-343)."""
+        self._divs = schedule
+        return self
 
     def spot(self, spot: float) -> "MarketBuilder":
         self._spot = float(spot)
@@ -202,5 +329,7 @@ class MarketBuilder:
             if self._flat <= 0.0:
                 raise PricingError.InvalidInput("market flat_vol must be > 0")
             vol = VolSource(flat=self._flat)
+        sched = self._divs if self._divs is not None else DividendSchedule.empty()
+        sched.validate()
         return Market(spot=self._spot, rate=self._rate or 0.0, dividend_yield=self._q or 0.0, vol=vol,
-                      reference_date=self._ref)
+                      reference_date=self._ref, dividend_schedule=sched)

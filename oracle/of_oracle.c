@@ -331,8 +331,25 @@ void orc_generate_path(const of_model* m, const double* z1, const double* z2, do
     const double sqrt_dt = sqrt(dt);
     const double drift = (m->mu - 0.5 * m->sigma * m->sigma) * dt;
     const double diffusion = m->sigma * sqrt_dt;
+    int64_t ev = 0;
     for (int64_t j = 0; j < m->steps; ++j) {
       s *= exp(fma(diffusion, z1[j], drift));
+      if (m->n_dividends > 0) {
+        /* DiscreteDividendGbmPathGenerator::generate_into, mc_engine.rs:146-170;
+         * DividendEvent::apply_jump, market/dividends.rs:76-83 */
+        const double t = (double)(j + 1) * dt;
+        while (ev < m->n_dividends && m->dividends[ev].time <= m->maturity + 1.0e-12 &&
+               m->dividends[ev].time <= t + 1.0e-12) {
+          const of_dividend_event* e = &m->dividends[ev];
+          if (e->kind == OF_DIV_CASH) {
+            const double x = s - e->amount;
+            s = x > 0.0 ? x : 0.0;
+          } else {
+            s = s * (1.0 - e->amount);
+          }
+          ++ev;
+        }
+      }
       path[j + 1] = s;
     }
   } else {

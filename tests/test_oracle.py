@@ -15,7 +15,7 @@ from scipy.special import ndtr
 from conftest import load_golden
 from openferric_b200._abi import (OF_AVG_ARITHMETIC, OF_AVG_GEOMETRIC, OF_CALL, OF_CV_GEOMETRIC_ASIAN, OF_CV_NONE,
                                   OF_CV_TERMINAL_SPOT, OF_CV_VANILLA_TERMINAL, OF_MODEL_GBM, OF_PAYOFF_ASIAN,
-                                  OF_PAYOFF_VANILLA, OF_PUT, OfMcConfig, OfModel, OfPayoff)
+                                  OF_PAYOFF_BARRIER, OF_PAYOFF_VANILLA, OF_PUT, OfMcConfig, OfModel, OfPayoff)
 
 M64 = (1 << 64) - 1
 
@@ -186,6 +186,40 @@ def test_mc_call_within_two_stderr_of_bs(orc):
                    OfMcConfig(num_paths=60000, seed=42, antithetic=1, discount_factor=math.exp(-0.05)), threads=8)
     bs = orc.bs_price(OF_CALL, 100, 100, 0.05, 0, 0.2, 1.0)
     assert abs(r.price - bs) <= 2.0 * r.stderr_ + 2e-2
+
+
+def test_dividend_paths_reproduce_the_schedule_forward(orc):
+    """DiscreteDividendGbmPathGenerator (mc_engine.rs:123-175): the mean
+    terminal spot is DividendSchedule::forward_price (dividends.rs:145-184)."""
+    from openferric_b200 import DividendEvent, DividendSchedule
+    from openferric_b200.engines import Gbm, GbmPathGenerator
+    sched = DividendSchedule.new([DividendEvent.cash(0.25, 1.5), DividendEvent.proportional(0.5, 0.02),
+                                  DividendEvent.cash(0.75, 2.0), DividendEvent.cash(1.5, 9.0)])
+    gen = GbmPathGenerator(Gbm(0.04, 0.25), 100.0, 1.0, 64, sched)
+    r = orc.mc_run(gen.to_abi(), OfPayoff(kind=OF_PAYOFF_VANILLA, option_type=OF_CALL, strike=1e-9),
+                   OfMcConfig(num_paths=200000, seed=3, discount_factor=1.0), threads=8)
+    fwd = sched.forward_price(100.0, 0.04, 0.0, 1.0)
+    assert abs(r.price - fwd) <= 4.0 * r.stderr_
+    # a path with a tiny vol lands on the deterministic jump sequence
+    gen0 = GbmPathGenerator(Gbm(0.0, 1e-9), 100.0, 1.0, 8, sched)
+    path = orc.generate_path(gen0.to_abi(), np.zeros(8))
+    assert path[2] == pytest.approx(98.5, abs=1e-6)            # cash 1.5 after t = 0.25
+    assert path[4] == pytest.approx(98.5 * 0.98, abs=1e-6)     # 2 % at t = 0.5
+    assert path[6] == pytest.approx(98.5 * 0.98 - 2.0, abs=1e-6)
+    assert path[8] == path[6]                                    # the t = 1.5 event is past maturity
+
+
+def test_dividend_barrier_knock_in(orc):
+    """dividend_modelling_issue58.rs:57-112 on the oracle: ~10 with the jump, ~0 without."""
+    from openferric_b200 import DividendEvent, DividendSchedule
+    from openferric_b200.engines import Gbm, GbmPathGenerator
+    pay = OfPayoff(kind=OF_PAYOFF_BARRIER, option_type=OF_PUT, strike=100.0, barrier_direction=1, barrier_style=0,
+                   barrier_level=95.0, rebate=0.0, expiry=1.0)
+    cfg = OfMcConfig(num_paths=20000, seed=42, antithetic=1, discount_factor=1.0)
+    with_div = GbmPathGenerator(Gbm(0.0, 1e-8), 100.0, 1.0, 252, DividendSchedule.new([DividendEvent.cash(0.5, 10.0)]))
+    no_div = GbmPathGenerator(Gbm(0.0, 1e-8), 100.0, 1.0, 252)
+    assert orc.mc_run(no_div.to_abi(), pay, cfg, threads=4).price <= 1e-3
+    assert abs(orc.mc_run(with_div.to_abi(), pay, cfg, threads=4).price - 10.0) <= 1e-3
 
 
 def test_control_variate_not_worse(orc):
