@@ -312,6 +312,29 @@ typedef struct of_lsm_result {
 of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* contracts, int64_t n,
                        const of_lsm_config* cfg, of_lsm_result* results);
 
+/* ---- Sobol quasi-Monte Carlo --------------------------------------------- */
+typedef struct of_qmc_params {
+  int32_t option_type; /* OF_CALL / OF_PUT */
+  int32_t precision;   /* FP64_REFERENCE: the reference's arithmetic on its point set;
+                          FP32_PHILOX: FP32 paths on the same Sobol points */
+  double spot, strike, rate;
+  double dividend_yield; /* market.effective_dividend_yield(expiry) */
+  double vol;            /* market.vol_for(strike, expiry) */
+  double expiry;
+  int64_t num_paths;     /* Sobol points 1..num_paths, at most 2^40 */
+  int64_t num_steps;     /* one Sobol dimension per step, at most 21201 */
+  uint64_t seed;
+} of_qmc_params;
+
+/* mc_european_qmc_with_seed (src/engines/monte_carlo/mc_qmc.rs:39-150) for a
+ * European vanilla under GBM on the reference's SobolSequence
+ * (src/math/sobol.rs: canonical dimension 0, hashed direction numbers and an
+ * XOR scrambler per further dimension).  The reference's NaN results
+ * (no paths, no steps, vol <= 0) are OF_ERR_INVALID_INPUT here; expiry <= 0
+ * is the caller's intrinsic shortcut.  `out` gets price, stderr_, samples,
+ * sum_x, sum_x2 and kernel_ms. */
+of_status of_mc_european_qmc(of_ctx* ctx, const of_qmc_params* params, of_mc_result* out);
+
 /* ---- Bermudan LSM with the exercise boundary ----------------------------- */
 /* LsmDynamics (src/engines/lsm/longstaff_schwartz.rs:24-39) */
 enum { OF_LSM_GBM = 0, OF_LSM_LOCAL_VOL = 1, OF_LSM_HESTON_EULER = 2 };

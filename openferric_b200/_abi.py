@@ -292,3 +292,19 @@ class OfBoundaryPoint(C.Structure):
         ("itm_paths", C.c_int64),
         ("exercised_paths", C.c_int64),
     ]
+
+
+class OfQmcParams(C.Structure):
+    _fields_ = [
+        ("option_type", C.c_int32),
+        ("precision", C.c_int32),
+        ("spot", C.c_double),
+        ("strike", C.c_double),
+        ("rate", C.c_double),
+        ("dividend_yield", C.c_double),
+        ("vol", C.c_double),
+        ("expiry", C.c_double),
+        ("num_paths", C.c_int64),
+        ("num_steps", C.c_int64),
+        ("seed", C.c_uint64),
+    ]

@@ -30,6 +30,7 @@ UNIT_FLAGS = {
     "mc_reference.cu": ["--fmad=false"],
     "greeks_reference.cu": ["--fmad=false"],
     "lsm.cu": ["--fmad=false"],
+    "qmc.cu": ["--fmad=false"],
     "mc_philox.cu": ["-use_fast_math"],
     # explicit fmaf only, so the forward pass and the backward-sweep recompute
     # are bit-identical; MUFU approximations are written as intrinsics

@@ -1062,6 +1062,124 @@ int orc_lsm_price(int option_type, double strike, double expiry, int exercise, c
 }
 
 /* ------------------------------------------------------------------------ */
+/* Sobol QMC (src/math/sobol.rs, src/engines/monte_carlo/mc_qmc.rs)          */
+/* ------------------------------------------------------------------------ */
+
+/* splitmix64 of sobol.rs:121-126 (a pure function of x) */
+static inline uint64_t sobol_mix(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+
+/* build_direction_numbers (sobol.rs:99-119) and the scrambler of
+ * SobolSequence::new (:27-45) for dimension `dim`: v[64], *scr. */
+void orc_sobol_dimension(uint64_t dim, uint64_t seed, uint64_t* v, uint64_t* scr) {
+  for (int j = 0; j < 64; ++j) {
+    if (dim == 0) {
+      v[j] = 1ULL << (63 - j);
+    } else {
+      const uint64_t hash = sobol_mix(seed ^ ((dim + 1) << 40) ^ (uint64_t)j);
+      const uint64_t mask = j == 63 ? ~0ULL : (1ULL << (j + 1)) - 1;
+      v[j] = ((hash | 1ULL) & mask) << (63 - j);
+    }
+  }
+  *scr = sobol_mix(seed ^ ((dim + 1) << 32));
+}
+
+/* Points first..first+count-1 (1-based index, as next_into produces them:
+ * x ^= v[ctz(index)], u = fma((double)(x ^ scr), 2^-64, 2^-65)), row-major
+ * [point][dim]. */
+int orc_sobol_points(int64_t dims, uint64_t seed, int64_t count, double* out) {
+  if (dims < 1 || dims > 21201 || count < 0) return OF_ERR_INVALID_INPUT;
+  uint64_t* v = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(64 * dims));
+  uint64_t* scr = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)dims);
+  uint64_t* x = (uint64_t*)calloc((size_t)dims, sizeof(uint64_t));
+  if (!v || !scr || !x) {
+    free(v);
+    free(scr);
+    free(x);
+    return OF_ERR_ALLOC;
+  }
+  for (int64_t d = 0; d < dims; ++d) orc_sobol_dimension((uint64_t)d, seed, v + 64 * d, scr + d);
+  const double inv = 1.0 / 18446744073709551616.0, half = 0.5 * inv;
+  for (int64_t n = 1; n <= count; ++n) {
+    const int c = __builtin_ctzll((uint64_t)n);
+    for (int64_t d = 0; d < dims; ++d) {
+      x[d] ^= v[64 * d + c];
+      out[(n - 1) * dims + d] = fma((double)(x[d] ^ scr[d]), inv, half);
+    }
+  }
+  free(v);
+  free(scr);
+  free(x);
+  return OF_OK;
+}
+
+/* mc_european_qmc_with_seed (mc_qmc.rs:39-150); q = effective dividend
+ * yield.  out[0] = price, out[1] = stderr (NaN/NaN for the reference's
+ * invalid-input results, which carry no stderr). */
+int orc_mc_european_qmc(int option_type, double spot, double strike, double rate, double q, double vol,
+                        double expiry, int64_t n_paths, int64_t n_steps, uint64_t seed, double* out2) {
+  if (n_paths <= 0 || n_steps <= 0 || !(vol > 0.0) || !isfinite(vol)) {
+    if (n_paths > 0 && n_steps > 0 && expiry <= 0.0) {
+      out2[0] = vanilla_payoff(option_type, spot, strike);
+      out2[1] = 0.0;
+      return OF_OK;
+    }
+    out2[0] = NAN;
+    out2[1] = NAN;
+    return OF_OK;
+  }
+  if (expiry <= 0.0) {
+    out2[0] = vanilla_payoff(option_type, spot, strike);
+    out2[1] = 0.0;
+    return OF_OK;
+  }
+  if (n_steps > 21201) return OF_ERR_INVALID_INPUT;
+  const double dt = expiry / (double)n_steps;
+  const double dt_drift = (rate - q - 0.5 * vol * vol) * dt;
+  const double dt_vol = vol * sqrt(dt);
+  const double discount = exp(-rate * expiry);
+  uint64_t* v = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(64 * n_steps));
+  uint64_t* scr = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n_steps);
+  uint64_t* x = (uint64_t*)calloc((size_t)n_steps, sizeof(uint64_t));
+  if (!v || !scr || !x) {
+    free(v);
+    free(scr);
+    free(x);
+    return OF_ERR_ALLOC;
+  }
+  for (int64_t d = 0; d < n_steps; ++d) orc_sobol_dimension((uint64_t)d, seed, v + 64 * d, scr + d);
+  const double inv = 1.0 / 18446744073709551616.0, half = 0.5 * inv;
+  double sum = 0.0, sum_sq = 0.0;
+  for (int64_t n = 1; n <= n_paths; ++n) {
+    const int c = __builtin_ctzll((uint64_t)n);
+    double s = spot;
+    for (int64_t d = 0; d < n_steps; ++d) {
+      x[d] ^= v[64 * d + c];
+      const double u = fma((double)(x[d] ^ scr[d]), inv, half);
+      const double z = orc_acklam_inv_cdf(orc_uniform_open01(u));
+      s *= exp(fma(dt_vol, z, dt_drift));
+    }
+    const double px = vanilla_payoff(option_type, s, strike);
+    sum += px;
+    sum_sq += px * px;
+  }
+  const double nn = (double)n_paths;
+  const double mean = sum / nn;
+  double var = n_paths > 1 ? (sum_sq - sum * sum / nn) / (nn - 1.0) : 0.0;
+  var = var > 0.0 ? var : 0.0;
+  out2[0] = discount * mean;
+  out2[1] = discount * sqrt(var / nn);
+  free(v);
+  free(scr);
+  free(x);
+  return OF_OK;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Bermudan LSM with the exercise boundary                                  */
 /* ------------------------------------------------------------------------ */
 

@@ -93,6 +93,17 @@ int orc_lsm_price(int option_type, double strike, double expiry, int exercise, c
                   double spot, double rate, double q, double vol, int64_t num_paths, int64_t num_steps,
                   uint64_t seed, int degree, const double* normals, double* out2);
 
+/* SobolSequence (src/math/sobol.rs:16-126): direction numbers and scrambler
+ * of one dimension; points 1..count in next_into order, row-major [point][dim]. */
+void orc_sobol_dimension(uint64_t dim, uint64_t seed, uint64_t* v64, uint64_t* scrambler);
+int orc_sobol_points(int64_t dims, uint64_t seed, int64_t count, double* out);
+
+/* mc_european_qmc_with_seed (src/engines/monte_carlo/mc_qmc.rs:39-150) for a
+ * European vanilla; q is market.effective_dividend_yield(expiry).
+ * out2 = {price, stderr}; NaN, NaN where the reference returns NaN without a stderr. */
+int orc_mc_european_qmc(int option_type, double spot, double strike, double rate, double q, double vol,
+                        double expiry, int64_t n_paths, int64_t n_steps, uint64_t seed, double* out2);
+
 /* SampledVolSurface::vol (src/market/market.rs:104-174): bilinear lookup on a
  * strictly increasing strike x expiry grid, vols row-major [expiry][strike]. */
 double orc_sampled_vol(const double* strikes, int64_t nk, const double* expiries, int64_t nt, const double* vols,

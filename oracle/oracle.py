@@ -76,6 +76,12 @@ def lib():
         L.orc_lsm_price.restype = C.c_int
         L.orc_lsm_price.argtypes = [C.c_int, D, D, C.c_int, PD, I64, D, D, D, D, I64, I64, C.c_uint64, C.c_int,
                                     PD, PD]
+        L.orc_sobol_dimension.restype = None
+        L.orc_sobol_dimension.argtypes = [C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.orc_sobol_points.restype = C.c_int
+        L.orc_sobol_points.argtypes = [I64, C.c_uint64, I64, PD]
+        L.orc_mc_european_qmc.restype = C.c_int
+        L.orc_mc_european_qmc.argtypes = [C.c_int, D, D, D, D, D, D, I64, I64, C.c_uint64, PD]
         L.orc_sampled_vol.restype = D
         L.orc_sampled_vol.argtypes = [PD, I64, PD, I64, PD, D, D]
         L.orc_lsm_bermudan.restype = C.c_int
@@ -217,6 +223,30 @@ def lsm_price(option_type, strike, expiry, exercise, spot, rate, q, vol, num_pat
                              rate, q, vol, num_paths, num_steps, seed, degree, _ptr(z), _ptr(out))
     if st != 0:
         raise RuntimeError(f"orc_lsm_price status {st}")
+    return float(out[0]), float(out[1])
+
+
+def sobol_points(dims, seed, count):
+    out = np.zeros((count, dims))
+    st = lib().orc_sobol_points(dims, seed & ((1 << 64) - 1), count, _ptr(out))
+    if st != 0:
+        raise RuntimeError(f"orc_sobol_points status {st}")
+    return out
+
+
+def sobol_dimension(dim, seed):
+    v = (C.c_uint64 * 64)()
+    s = C.c_uint64()
+    lib().orc_sobol_dimension(dim, seed & ((1 << 64) - 1), v, C.byref(s))
+    return list(v), s.value
+
+
+def mc_european_qmc(option_type, spot, strike, rate, q, vol, expiry, n_paths, n_steps, seed=0):
+    out = np.zeros(2)
+    st = lib().orc_mc_european_qmc(option_type, spot, strike, rate, q, vol, expiry, n_paths, n_steps,
+                                   seed & ((1 << 64) - 1), _ptr(out))
+    if st != 0:
+        raise RuntimeError(f"orc_mc_european_qmc status {st}")
     return float(out[0]), float(out[1])
 
 

@@ -50,6 +50,8 @@ STRUCTS = {
     "of_device_peaks": A.OfDevicePeaks,
     "of_bermudan_contract": A.OfBermudanContract,
     "of_boundary_point": A.OfBoundaryPoint,
+    "of_qmc_params": A.OfQmcParams,
+    "of_dividend_event": A.OfDividendEvent,
 }
 
 

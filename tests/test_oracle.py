@@ -387,6 +387,58 @@ def test_lsm_european_exercise_is_discounted_payoff(orc):
     assert abs(p - bs) < 3 * s + 1e-3
 
 
+# ---- Sobol QMC (src/math/sobol.rs:128-188, mc_qmc.rs:152-199) --------------------
+def test_sobol_points_unit_interval_and_reproducible(orc):
+    p = orc.sobol_points(8, 42, 1000)
+    assert p.min() >= 0.0 and p.max() < 1.0
+    assert np.array_equal(orc.sobol_points(5, 99, 100), orc.sobol_points(5, 99, 100))
+
+
+def test_sobol_first_dimension_is_van_der_corput_and_beats_prng_mean(orc):
+    n = 1000
+    p = orc.sobol_points(1, 7, n)[:, 0]
+    sobol_mean = p.mean()
+    rng = orc.Xoshiro(7)
+    prng_mean = sum(rng.next_f64() for _ in range(n)) / n
+    assert abs(sobol_mean - 0.5) <= abs(prng_mean - 0.5)
+    v, scr = orc.sobol_dimension(0, 7)
+    assert v == [1 << (63 - j) for j in range(64)]
+    # point n of dimension 0 = gray(n) bit-reversed, XOR the scrambler
+    for n in (1, 2, 3, 17, 1000):
+        g = n ^ (n >> 1)
+        x = 0
+        for j in range(64):
+            if (g >> j) & 1:
+                x ^= v[j]
+        assert p[n - 1] == fma(float(x ^ scr), 2.0 ** -64, 2.0 ** -65)
+
+
+def test_sobol_direction_numbers_are_odd_and_bounded(orc):
+    for dim in (1, 5, 200):
+        v, _ = orc.sobol_dimension(dim, 123)
+        for j, vj in enumerate(v):
+            m = vj >> (63 - j)
+            assert m & 1 and m < (1 << (j + 1))
+
+
+def test_qmc_known_answers(orc):
+    """mc_qmc.rs:178-198: 10k points (1 step, seed 11) within 0.1 % of BS;
+    :160-176: at 50k the QMC stderr is no worse than 1.2 x the PRNG one."""
+    bs = orc.bs_price(OF_CALL, 100, 100, 0.05, 0, 0.2, 1.0)
+    p, _ = orc.mc_european_qmc(OF_CALL, 100.0, 100.0, 0.05, 0.0, 0.2, 1.0, 10000, 1, 11)
+    assert abs(p - bs) / bs <= 0.001
+    _, qse = orc.mc_european_qmc(OF_CALL, 100.0, 100.0, 0.05, 0.0, 0.2, 1.0, 50000, 1, 7)
+    r = orc.mc_run(_gbm(1), OfPayoff(kind=OF_PAYOFF_VANILLA, option_type=OF_CALL, strike=100.0),
+                   OfMcConfig(num_paths=50000, seed=7, discount_factor=math.exp(-0.05)), threads=8)
+    assert qse < 1.2 * r.stderr_
+
+
+def test_qmc_reference_edge_results(orc):
+    assert all(math.isnan(x) for x in orc.mc_european_qmc(OF_CALL, 100, 100, 0.05, 0, 0.2, 1.0, 0, 10, 1))
+    assert orc.mc_european_qmc(OF_PUT, 90, 100, 0.05, 0, 0.2, 0.0, 100, 10, 1) == (10.0, 0.0)
+    assert all(math.isnan(x) for x in orc.mc_european_qmc(OF_CALL, 100, 100, 0.05, 0, -0.2, 1.0, 100, 10, 1))
+
+
 # ---- Bermudan LSM (tests/bermudan_quantlib.rs:73-389) ----------------------------
 def _schedule(c):
     s = [(t, c["strike"]) for t in c["dates"]]
