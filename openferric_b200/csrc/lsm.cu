@@ -35,7 +35,7 @@ namespace {
 
 constexpr uint32_t kLsmStreamTag = 0x4C534D31u;  // "LSM1"
 constexpr int kPassThreads = 256;
-constexpr int kPathsPerThread = 8;
+constexpr int kPathsPerThread = 4;
 constexpr int kPathsPerBlock = kPassThreads * kPathsPerThread;
 constexpr int kMaxMoments = 12;  // degree 3: x^0..x^6 (7) + y x^0..x^3 (4) ; degree 2: 8
 
@@ -452,22 +452,20 @@ __device__ void solve_beta(int degree, const double* m, double* beta, int32_t* o
 }
 
 // Fixed-order reduction of the per-block partials of one contract by the
-// block that finished last; thread 0 then solves for the betas.
-__device__ void last_block_reduce(const LsmBatch& B, int c, int nm, double* moments_sh, double* red_sh,
+// block that finished last: warp w sums moments w, w + 8, ... with its lanes
+// striding over the blocks' rows and a shuffle tree (one barrier in all);
+// thread 0 then solves for the betas.
+__device__ void last_block_reduce(const LsmBatch& B, int c, int nm, int nblk, double* moments_sh, double* red_sh,
                                   int t_pass) {
   const double* part = B.partials + (size_t)c * B.blocks * kMaxMoments;
-  for (int k = 0; k < nm; ++k) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = warp; k < nm; k += nw) {
     double acc = 0.0;
-    for (int b = threadIdx.x; b < B.blocks; b += blockDim.x) acc += part[(size_t)b * kMaxMoments + k];
-    red_sh[threadIdx.x] = acc;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-      if ((int)threadIdx.x < s) red_sh[threadIdx.x] += red_sh[threadIdx.x + s];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) moments_sh[k] = red_sh[0];
-    __syncthreads();
+    for (int b = lane; b < nblk; b += 32) acc += __ldcg(part + (size_t)b * kMaxMoments + k);
+    acc = of::warp_sum(acc);
+    if (lane == 0) moments_sh[k] = acc;
   }
+  __syncthreads();
   if (threadIdx.x == 0) {
     const int buf = t_pass & 1;
     double* beta = B.betas + ((size_t)buf * B.nc + c) * 4;
@@ -505,13 +503,14 @@ __device__ __forceinline__ void record_exercise(const LsmBatch& B, int c, int da
 // (spot s0, longstaff_schwartz.rs:543-601).
 // k1/ik1: strike and its inverse at date t+1, k0/ik0 at date t.  Returns
 // whether the path exercised at t+1.
-__device__ __forceinline__ bool lsm_path_update(const LsmBatch& B, const LsmC& C, const double* beta, bool have_beta,
-                                                bool ex_now, double k1, double ik1, double k0, double ik0, double s1,
-                                                double s0, double& v, double& dv, double* mom) {
+template <int DEG>
+__device__ __forceinline__ bool lsm_path_update(const LsmC& C, const double* beta, bool have_beta, bool ex_now,
+                                                double k1, double ik1, double k0, double ik0, double s1, double s0,
+                                                double& v, double& dv, double* mom) {
   bool exercised = false;
   if (have_beta) {
     const double ex = intrinsic_v<double>(C.put, s1, k1);
-    if (ex > 0.0 && ex > continuation(B.degree, beta, s1, ik1)) {
+    if (ex > 0.0 && ex > continuation(DEG, beta, s1, ik1)) {
       v = ex;
       dv = C.put ? -s1 * C.inv_spot : s1 * C.inv_spot;
       exercised = true;
@@ -520,7 +519,7 @@ __device__ __forceinline__ bool lsm_path_update(const LsmBatch& B, const LsmC& C
   v *= C.disc;
   dv *= C.disc;
   if (ex_now && intrinsic_v<double>(C.put, s0, k0) > 0.0) {
-    if (B.degree == 2) {
+    if (DEG == 2) {
       const double s2 = s0 * s0;
       mom[0] += 1.0;
       mom[1] += s0;
@@ -545,8 +544,11 @@ __device__ __forceinline__ bool lsm_path_update(const LsmBatch& B, const LsmC& C
 }
 
 // One exercise date t (1 <= t <= steps-1): exercise(t+1), discount, moments(t).
-template <typename T>
-__global__ void __launch_bounds__(kPassThreads) lsm_pass(LsmBatch B, int t) {
+// A block walks the contract's chunks of kPathsPerBlock paths with a grid
+// stride and reduces its moments once at the end; DEG (the basis degree) is a
+// template parameter so that the moment count is known at compile time.
+template <typename T, int DEG>
+__global__ void __launch_bounds__(kPassThreads, 3) lsm_pass(LsmBatch B, int t) {
   __shared__ double red_sh[kPassThreads];
   __shared__ double mom_sh[kMaxMoments];
   __shared__ bool is_last;
@@ -566,64 +568,55 @@ __global__ void __launch_bounds__(kPassThreads) lsm_pass(LsmBatch B, int t) {
   const double k1 = st[t + 1].strike, ik1 = st[t + 1].inv_strike, k0 = st[t].strike, ik0 = st[t].inv_strike;
   unsigned n_ex = 0;
   double ext = C.put ? 0.0 : __longlong_as_double(0x7FF0000000000000LL);
-  const int nm = B.degree == 2 ? 8 : 11;
-  double mom[kMaxMoments];
+  constexpr int nm = DEG == 2 ? 8 : 11;
+  double mom[nm];
 #pragma unroll
-  for (int k = 0; k < kMaxMoments; ++k) mom[k] = 0.0;
-  const int64_t base = (int64_t)blockIdx.x * kPathsPerBlock;
-  if constexpr (sizeof(T) == 4) {
-    // FP32 store: 4 groups of 4 consecutive paths per thread; every float4
-    // load of the pass is issued before any of them is used.
-    constexpr int G = kPathsPerThread / 4;
-    const float4* S1 = reinterpret_cast<const float4*>(S + (size_t)t * B.npad);
-    const float4* S0 = reinterpret_cast<const float4*>(S + (size_t)(t - 1) * B.npad);
-    float4* V4 = reinterpret_cast<float4*>(V);
-    float4* D4 = reinterpret_cast<float4*>(dV);
-    float4 v4[G], d4[G], a4[G], b4[G];
-#pragma unroll
-    for (int g = 0; g < G; ++g) {
-      const int64_t q = base / 4 + g * kPassThreads + threadIdx.x;
-      v4[g] = V4[q];
-      d4[g] = B.want_delta ? D4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
-      a4[g] = have_beta ? S1[q] : make_float4(0.f, 0.f, 0.f, 0.f);
-      b4[g] = ex_now ? S0[q] : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-#pragma unroll
-    for (int g = 0; g < G; ++g) {
-      const int64_t p0 = base + ((int64_t)g * kPassThreads + threadIdx.x) * 4;
-      float* vv = &v4[g].x;
-      float* dd = &d4[g].x;
-      const float* s1 = &a4[g].x;
-      const float* s0 = &b4[g].x;
+  for (int k = 0; k < nm; ++k) mom[k] = 0.0;
+  for (int64_t chunk = blockIdx.x; chunk < B.blocks; chunk += gridDim.x) {
+    const int64_t base = chunk * kPathsPerBlock;
+    if constexpr (sizeof(T) == 4) {
+      // FP32 store: 4 consecutive paths per thread; the four float4 loads are
+      // issued before any of them is used
+      const int64_t q = base / 4 + threadIdx.x;
+      float4 v4 = reinterpret_cast<const float4*>(V)[q];
+      float4 d4 = B.want_delta ? reinterpret_cast<const float4*>(dV)[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 a4 = have_beta ? reinterpret_cast<const float4*>(S + (size_t)t * B.npad)[q]
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 b4 = ex_now ? reinterpret_cast<const float4*>(S + (size_t)(t - 1) * B.npad)[q]
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
+      const int64_t p0 = base + (int64_t)threadIdx.x * 4;
+      float* vv = &v4.x;
+      float* dd = &d4.x;
+      const float* s1 = &a4.x;
+      const float* s0 = &b4.x;
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         if (p0 + e >= B.n) continue;  // padding
         double v = vv[e], dv = dd[e];
-        if (lsm_path_update(B, C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1[e], s0[e], v, dv, mom)) {
+        if (lsm_path_update<DEG>(C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1[e], s0[e], v, dv, mom)) {
           ++n_ex;
           ext = C.put ? fmax(ext, (double)s1[e]) : fmin(ext, (double)s1[e]);
         }
         vv[e] = (float)v;
         dd[e] = (float)dv;
       }
-      const int64_t q = base / 4 + g * kPassThreads + threadIdx.x;
-      V4[q] = v4[g];
-      if (B.want_delta) D4[q] = d4[g];
-    }
-  } else {
+      reinterpret_cast<float4*>(V)[q] = v4;
+      if (B.want_delta) reinterpret_cast<float4*>(dV)[q] = d4;
+    } else {
 #pragma unroll
-    for (int q = 0; q < kPathsPerThread; ++q) {
-      const int64_t p = base + q * kPassThreads + threadIdx.x;
-      if (p >= B.n) break;
-      double v = (double)V[p], dv = B.want_delta ? (double)dV[p] : 0.0;
-      const double s1 = have_beta ? (double)S[(size_t)t * B.npad + p] : 0.0;      // spot at date t+1
-      const double s0 = ex_now ? (double)S[(size_t)(t - 1) * B.npad + p] : 0.0;  // spot at date t
-      if (lsm_path_update(B, C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1, s0, v, dv, mom)) {
-        ++n_ex;
-        ext = C.put ? fmax(ext, s1) : fmin(ext, s1);
+      for (int q = 0; q < kPathsPerThread; ++q) {
+        const int64_t p = base + q * kPassThreads + threadIdx.x;
+        if (p >= B.n) break;
+        double v = (double)V[p], dv = B.want_delta ? (double)dV[p] : 0.0;
+        const double s1 = have_beta ? (double)S[(size_t)t * B.npad + p] : 0.0;      // spot at date t+1
+        const double s0 = ex_now ? (double)S[(size_t)(t - 1) * B.npad + p] : 0.0;  // spot at date t
+        if (lsm_path_update<DEG>(C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1, s0, v, dv, mom)) {
+          ++n_ex;
+          ext = C.put ? fmax(ext, s1) : fmin(ext, s1);
+        }
+        V[p] = (T)v;
+        if (B.want_delta) dV[p] = (T)dv;
       }
-      V[p] = (T)v;
-      if (B.want_delta) dV[p] = (T)dv;
     }
   }
   if (B.track && have_beta) record_exercise(B, c, t + 1, C.put, n_ex, ext);  // block-uniform condition
@@ -632,11 +625,9 @@ __global__ void __launch_bounds__(kPassThreads) lsm_pass(LsmBatch B, int t) {
   // thread per moment sums the warps in a fixed order -> partials
   double* part = B.partials + ((size_t)c * B.blocks + blockIdx.x) * kMaxMoments;
 #pragma unroll
-  for (int k = 0; k < kMaxMoments; ++k) {
-    if (k < nm) {
-      const double w = of::warp_sum(mom[k]);
-      if ((threadIdx.x & 31) == 0) red_sh[(threadIdx.x >> 5) * kMaxMoments + k] = w;
-    }
+  for (int k = 0; k < nm; ++k) {
+    const double w = of::warp_sum(mom[k]);
+    if ((threadIdx.x & 31) == 0) red_sh[(threadIdx.x >> 5) * kMaxMoments + k] = w;
   }
   __syncthreads();
   if ((int)threadIdx.x < nm) {
@@ -648,12 +639,12 @@ __global__ void __launch_bounds__(kPassThreads) lsm_pass(LsmBatch B, int t) {
   __syncthreads();
   if (threadIdx.x == 0) {
     const uint32_t done = atomicAdd(B.counters + c, 1u);
-    is_last = done == (uint32_t)B.blocks - 1;
+    is_last = done == gridDim.x - 1;
   }
   __syncthreads();
   if (is_last) {
     __threadfence();
-    last_block_reduce(B, c, nm, mom_sh, red_sh, t);
+    last_block_reduce(B, c, nm, (int)gridDim.x, mom_sh, red_sh, t);
     if (threadIdx.x == 0) B.counters[c] = 0;
   }
 }
@@ -1003,10 +994,29 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
   }
   OF_CUDA_TRY(ctx, cudaGetLastError());
   const dim3 grid((unsigned)blocks, nc);
-  for (int t = (int)steps - 1; t >= 1; --t) {
-    if (fp64) lsm_pass<double><<<grid, kPassThreads, 0, ctx->stream>>>(B, t);
-    else lsm_pass<float><<<grid, kPassThreads, 0, ctx->stream>>>(B, t);
+  // The passes: one wave of resident blocks over the whole batch, each block
+  // striding over its contract's chunks.
+  void (*pass)(LsmBatch, int) = fp64 ? (B.degree == 2 ? lsm_pass<double, 2> : lsm_pass<double, 3>)
+                                     : (B.degree == 2 ? lsm_pass<float, 2> : lsm_pass<float, 3>);
+  const int bps = std::max(1, of_blocks_per_sm((const void*)pass, kPassThreads, 0));
+  const int64_t wave = (int64_t)ctx->sm_count * bps;
+  // Blocks per contract: floor(k wave / nc) fills exactly k waves up to the
+  // rounding; take the smallest k whose waves are at least 95% occupied (a
+  // grid a few blocks over a wave would run those blocks as a second wave).
+  int64_t pass_blocks = 1;
+  double best = 0.0;
+  for (int k = 1; k <= 8; ++k) {
+    const int64_t bpc = std::max<int64_t>(1, std::min<int64_t>(blocks, k * wave / nc));
+    const int64_t total = bpc * nc, waves = (total + wave - 1) / wave;
+    const double fill = (double)total / (double)(waves * wave);
+    if (fill > best + 1e-9) {
+      best = fill;
+      pass_blocks = bpc;
+    }
+    if (fill >= 0.95 || bpc == blocks) break;
   }
+  const dim3 pgrid((unsigned)pass_blocks, nc);
+  for (int t = (int)steps - 1; t >= 1; --t) pass<<<pgrid, kPassThreads, 0, ctx->stream>>>(B, t);
   if (fp64) lsm_final<double><<<grid, kPassThreads, 0, ctx->stream>>>(B);
   else lsm_final<float><<<grid, kPassThreads, 0, ctx->stream>>>(B);
   OF_CUDA_TRY(ctx, cudaGetLastError());
