@@ -310,6 +310,7 @@ def main():
     import torch
     import openferric_b200 as of
     from openferric_b200.engines import StripPlan
+    from openferric_b200.replicas import max_over_ranks, replica_seed
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -321,7 +322,7 @@ def main():
     ctx = of.context(local_rank)
     gen = of.HestonPathGenerator(of.Heston(**HESTON), S0, T, STEPS)
     df = math.exp(-RATE * T)
-    seed = SEED + rank
+    seed = replica_seed(SEED, rank)  # independent replica per GPU
     plan = StripPlan(gen, of.OptionType.Call, STRIKES, args.paths, seed, df)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", local_rank))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
@@ -347,10 +348,8 @@ def main():
         torch.cuda.synchronize()
     kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = sum(kernel_ms)
+    total_ms = max_over_ranks(total_ms, device=torch.device("cuda", local_rank))
     if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{local_rank}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
     prices = plan.results()
     clk = clocks.summary()
@@ -364,10 +363,7 @@ def main():
     for _ in range(args.steps):
         e2e_prices = of.price_strike_strip(gen, of.OptionType.Call, STRIKES, args.paths, seed, df)
     e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{local_rank}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, device=torch.device("cuda", local_rank))
 
     ms_per_step = total_ms / args.steps
     value = world * PATH_STEPS * args.steps / (total_ms / 1e3)

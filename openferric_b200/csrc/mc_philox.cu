@@ -204,7 +204,7 @@ struct StripParams {
 };
 
 template <int KPL, int MODEL, bool ANTI, int ILP = 1>
-__global__ void __launch_bounds__(256) strip_kernel(const __grid_constant__ StripParams P,
+__global__ void __launch_bounds__(256, 5) strip_kernel(const __grid_constant__ StripParams P,
                                                     double* __restrict__ partials) {
   extern __shared__ double sh_strip[];  // [warps][n_strikes][2]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
