@@ -602,7 +602,9 @@ __device__ __forceinline__ float book_dividend(const BookDiv& d, float y) {
   return d.kind == OF_DIV_CASH ? __logf(fmaxf(__expf(y) - d.a, 0.0f)) : y + d.a;
 }
 
-template <int MODEL>
+// DIVS: the option has discrete dividends (GBM only); without them the step
+// loop carries no trigger check.
+template <int MODEL, bool DIVS = false>
 __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, const of::PhiloxKeys& K, const float* obs_w,
                                             const BookDiv* divs, float& x, float& cvy) {
   const bool anti = o.flags & BF_ANTI;
@@ -631,7 +633,7 @@ __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, const 
         const float z = q == 0 ? p01.x : q == 1 ? p01.y : q == 2 ? p23.x : p23.y;
         a.y = fmaf(c.diff, z, a.y + c.drift);
         if (anti) b.y = fmaf(-c.diff, z, b.y + c.drift);
-        for (; ev < o.n_div && divs[o.div_offset + ev].step == j + q; ++ev) {  // mc_engine.rs:157-167
+        for (; DIVS && ev < o.n_div && divs[o.div_offset + ev].step == j + q; ++ev) {  // mc_engine.rs:157-167
           const BookDiv d = divs[o.div_offset + ev];
           a.y = book_dividend(d, a.y);
           if (anti) b.y = book_dividend(d, b.y);
@@ -679,7 +681,10 @@ __global__ void __launch_bounds__(256, 3) book_kernel(const __grid_constant__ Bo
       if (local >= tile.count) break;
       const uint64_t i = (uint64_t)(tile.first + local);
       float x, y;
-      if (o.model == OF_MODEL_GBM) book_sample<OF_MODEL_GBM>(o, i, P.keys, P.obs_w, P.divs, x, y);
+      if (o.model == OF_MODEL_GBM) {
+        if (o.n_div) book_sample<OF_MODEL_GBM, true>(o, i, P.keys, P.obs_w, P.divs, x, y);
+        else book_sample<OF_MODEL_GBM, false>(o, i, P.keys, P.obs_w, P.divs, x, y);
+      }
       else if (o.model == OF_MODEL_HESTON_EULER)
         book_sample<OF_MODEL_HESTON_EULER>(o, i, P.keys, P.obs_w, P.divs, x, y);
       else book_sample<OF_MODEL_HESTON_QE>(o, i, P.keys, P.obs_w, P.divs, x, y);
