@@ -4,8 +4,10 @@
 // (src/engines/lsm/longstaff_schwartz.rs:421-618) for a batch of contracts.
 //
 // Layout: S[contract][step-1][path] (time-major: a date's column is one
-// contiguous, coalesced read), cash flows V[contract][path] and their pathwise
-// spot derivatives dV.  One kernel per exercise date does
+// contiguous, coalesced read), cash flows V[contract][path] and, for the
+// pathwise delta, the step tau[contract][path] at which each path's cash flow
+// is paid (written only when a path exercises; the final kernel derives
+// dV = +-S_tau disc^tau / S0 from V and tau).  One kernel per exercise date does
 //   exercise(t+1) with the betas of the previous pass -> discount -> FP64
 //   in-the-money basis moments at t -> block partials,
 // and the last block of each contract (last-block-done counter, no spin)
@@ -168,7 +170,7 @@ struct LsmBatch {
   int64_t n, npad;           // paths, padded path stride
   void* S;                   // [nc][steps][npad] (T)
   void* V;                   // [nc][npad]
-  void* dV;                  // [nc][npad]
+  int32_t* tau;             // [nc][npad] step of each path's cash flow (delta only)
   double* partials;          // [nc][blocks][kMaxMoments]
   double* betas;             // [2][nc][4] + valid flag in [2][nc] (separate)
   int32_t* beta_ok;          // [2][nc]
@@ -250,7 +252,7 @@ __global__ void __launch_bounds__(128) lsm_gen_ref(LsmBatch B) {
   const LsmStep* st = B.st + (size_t)c * (B.steps + 1);
   double* S = (double*)B.S + (size_t)c * B.steps * B.npad;
   double* V = (double*)B.V + (size_t)c * B.npad;
-  double* dV = (double*)B.dV + (size_t)c * B.npad;
+  int32_t* tau = B.tau + (size_t)c * B.npad;
   of::Xoshiro256pp rng;
   if (!B.inj) {
     rng.seed(B.seed);
@@ -290,7 +292,7 @@ __global__ void __launch_bounds__(128) lsm_gen_ref(LsmBatch B) {
     double v, dv;
     itm += terminal_value(C, k_T, s, v, dv);
     V[p] = v;
-    dV[p] = dv;
+    if (B.want_delta) tau[p] = B.steps;
   }
   if (B.track && itm) atomicAdd(B.term_itm + c, (unsigned long long)itm);
 }
@@ -348,15 +350,14 @@ __global__ void __launch_bounds__(256) lsm_gen_philox(const __grid_constant__ Ls
       *reinterpret_cast<float4*>(S + (size_t)t * B.npad + p0) = out;
     }
     float* V = (float*)B.V + (size_t)c * B.npad;
-    float* dV = (float*)B.dV + (size_t)c * B.npad;
-    const float fk = st[B.steps].fstrike, finv = (float)C.inv_spot;
+    const float fk = st[B.steps].fstrike;
     for (int q = 0; q < 4; ++q) {
       const float v = intrinsic_v<float>(C.put, s[q], fk);
       const bool in = p0 + q < B.n;
       V[p0 + q] = in ? v : 0.0f;
-      dV[p0 + q] = (in && v > 0.0f) ? (C.put ? -s[q] * finv : s[q] * finv) : 0.0f;
       itm += (in && v > 0.0f) ? 1 : 0;
     }
+    if (B.want_delta) *reinterpret_cast<int4*>(B.tau + (size_t)c * B.npad + p0) = make_int4(B.steps, B.steps, B.steps, B.steps);
   }
   if (B.track) {
     itm = __reduce_add_sync(of::kFullMask, itm);
@@ -506,18 +507,16 @@ __device__ __forceinline__ void record_exercise(const LsmBatch& B, int c, int da
 template <int DEG>
 __device__ __forceinline__ bool lsm_path_update(const LsmC& C, const double* beta, bool have_beta, bool ex_now,
                                                 double k1, double ik1, double k0, double ik0, double s1, double s0,
-                                                double& v, double& dv, double* mom) {
+                                                double& v, double* mom) {
   bool exercised = false;
   if (have_beta) {
     const double ex = intrinsic_v<double>(C.put, s1, k1);
     if (ex > 0.0 && ex > continuation(DEG, beta, s1, ik1)) {
       v = ex;
-      dv = C.put ? -s1 * C.inv_spot : s1 * C.inv_spot;
       exercised = true;
     }
   }
   v *= C.disc;
-  dv *= C.disc;
   if (ex_now && intrinsic_v<double>(C.put, s0, k0) > 0.0) {
     if (DEG == 2) {
       const double s2 = s0 * s0;
@@ -556,7 +555,7 @@ __global__ void __launch_bounds__(kPassThreads, 3) lsm_pass(LsmBatch B, int t) {
   const LsmC C = B.c[c];
   const T* S = (const T*)B.S + (size_t)c * B.steps * B.npad;
   T* V = (T*)B.V + (size_t)c * B.npad;
-  T* dV = (T*)B.dV + (size_t)c * B.npad;
+  int32_t* tau = B.tau + (size_t)c * B.npad;
   const bool ex_next = (t + 1 < B.steps) && B.can_ex[(size_t)c * (B.steps + 1) + t + 1];
   const bool ex_now = B.can_ex[(size_t)c * (B.steps + 1) + t];
   const int nb = (t + 1) & 1;  // betas of date t+1 were written by the previous pass
@@ -579,43 +578,40 @@ __global__ void __launch_bounds__(kPassThreads, 3) lsm_pass(LsmBatch B, int t) {
       // issued before any of them is used
       const int64_t q = base / 4 + threadIdx.x;
       float4 v4 = reinterpret_cast<const float4*>(V)[q];
-      float4 d4 = B.want_delta ? reinterpret_cast<const float4*>(dV)[q] : make_float4(0.f, 0.f, 0.f, 0.f);
       const float4 a4 = have_beta ? reinterpret_cast<const float4*>(S + (size_t)t * B.npad)[q]
                                   : make_float4(0.f, 0.f, 0.f, 0.f);
       const float4 b4 = ex_now ? reinterpret_cast<const float4*>(S + (size_t)(t - 1) * B.npad)[q]
                                : make_float4(0.f, 0.f, 0.f, 0.f);
       const int64_t p0 = base + (int64_t)threadIdx.x * 4;
       float* vv = &v4.x;
-      float* dd = &d4.x;
       const float* s1 = &a4.x;
       const float* s0 = &b4.x;
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         if (p0 + e >= B.n) continue;  // padding
-        double v = vv[e], dv = dd[e];
-        if (lsm_path_update<DEG>(C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1[e], s0[e], v, dv, mom)) {
+        double v = vv[e];
+        if (lsm_path_update<DEG>(C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1[e], s0[e], v, mom)) {
           ++n_ex;
           ext = C.put ? fmax(ext, (double)s1[e]) : fmin(ext, (double)s1[e]);
+          if (B.want_delta) tau[p0 + e] = t + 1;  // the cash flow now comes at date t+1
         }
         vv[e] = (float)v;
-        dd[e] = (float)dv;
       }
       reinterpret_cast<float4*>(V)[q] = v4;
-      if (B.want_delta) reinterpret_cast<float4*>(dV)[q] = d4;
     } else {
 #pragma unroll
       for (int q = 0; q < kPathsPerThread; ++q) {
         const int64_t p = base + q * kPassThreads + threadIdx.x;
         if (p >= B.n) break;
-        double v = (double)V[p], dv = B.want_delta ? (double)dV[p] : 0.0;
+        double v = (double)V[p];
         const double s1 = have_beta ? (double)S[(size_t)t * B.npad + p] : 0.0;      // spot at date t+1
         const double s0 = ex_now ? (double)S[(size_t)(t - 1) * B.npad + p] : 0.0;  // spot at date t
-        if (lsm_path_update<DEG>(C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1, s0, v, dv, mom)) {
+        if (lsm_path_update<DEG>(C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1, s0, v, mom)) {
           ++n_ex;
           ext = C.put ? fmax(ext, s1) : fmin(ext, s1);
+          if (B.want_delta) tau[p] = t + 1;  // the cash flow now comes at date t+1
         }
         V[p] = (T)v;
-        if (B.want_delta) dV[p] = (T)dv;
       }
     }
   }
@@ -660,7 +656,8 @@ __global__ void __launch_bounds__(kPassThreads) lsm_final(LsmBatch B) {
   const LsmC C = B.c[c];
   const T* S = (const T*)B.S + (size_t)c * B.steps * B.npad;
   const T* V = (const T*)B.V + (size_t)c * B.npad;
-  const T* dV = (const T*)B.dV + (size_t)c * B.npad;
+  const int32_t* tau = B.tau + (size_t)c * B.npad;
+  const LsmStep* st = B.st + (size_t)c * (B.steps + 1);
   const bool ex1 = (1 < B.steps) && B.can_ex[(size_t)c * (B.steps + 1) + 1];
   const int nb = 1 & 1;
   const bool have_beta = ex1 && B.beta_ok[(size_t)nb * B.nc + c];
@@ -675,19 +672,28 @@ __global__ void __launch_bounds__(kPassThreads) lsm_final(LsmBatch B) {
   for (int q = 0; q < kPathsPerThread; ++q) {
     const int64_t p = base + q * kPassThreads + threadIdx.x;
     if (p >= B.n) break;
-    double v = (double)V[p], dv = B.want_delta ? (double)dV[p] : 0.0;
+    double v = (double)V[p];
+    int tp = B.want_delta ? tau[p] : 0;
     if (have_beta) {
       const double s1 = (double)S[p];  // spot at date 1
       const double ex = intrinsic_v<double>(C.put, s1, st1.strike);
       if (ex > 0.0 && ex > continuation(B.degree, beta, s1, st1.inv_strike)) {
         v = ex;
-        dv = C.put ? -s1 * C.inv_spot : s1 * C.inv_spot;
+        tp = 1;
         ++n_ex;
         ext = C.put ? fmax(ext, s1) : fmin(ext, s1);
       }
     }
     v *= C.disc;
-    dv *= C.disc;
+    // Pathwise delta under the fitted policy: the cash flow E paid at step tp
+    // is now v = E disc^tp with S_tp = K_tp -/+ E, so dv = +-S_tp disc^tp / S0
+    // = +-(K_tp disc^tp -/+ v) / S0 (put / call); no cash flow, no delta.
+    double dv = 0.0;
+    if (B.want_delta && v > 0.0) {
+      const double D = pow(C.disc, (double)tp);
+      const double K = st[tp].strike;
+      dv = C.put ? -(K * D - v) * C.inv_spot : (K * D + v) * C.inv_spot;
+    }
     acc[0] += v;
     acc[1] += v * v;
     acc[2] += dv;
@@ -865,9 +871,9 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
   const size_t per = (size_t)steps * npad * esz;
   const size_t ns = (size_t)nc * (size_t)(steps + 1);
   // device buffers: path store, cash flows, and one auxiliary block
-  void *dS = nullptr, *dV = nullptr, *dAux = nullptr, *dInj = nullptr;
+  void *dS = nullptr, *dVal = nullptr, *dAux = nullptr, *dInj = nullptr;
   OF_TRY(of_scratch(ctx, SLOT_LSM_PATHS, (size_t)nc * per, &dS));
-  OF_TRY(of_scratch(ctx, SLOT_LSM_VALUES, (size_t)nc * npad * esz * 2, &dV));
+  OF_TRY(of_scratch(ctx, SLOT_LSM_VALUES, (size_t)nc * npad * (esz + sizeof(int32_t)), &dVal));
   size_t off = 0;
   auto take = [&off](size_t bytes) {
     const size_t o = off;
@@ -971,8 +977,8 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
   B.n = N;
   B.npad = npad;
   B.S = dS;
-  B.V = dV;
-  B.dV = (char*)dV + (size_t)nc * npad * esz;
+  B.V = dVal;
+  B.tau = (int32_t*)((char*)dVal + (size_t)nc * npad * esz);
   B.blocks = blocks;
   B.degree = cfg->basis_degree;
   B.want_delta = cfg->want_delta;
@@ -983,7 +989,6 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
   B.inj = (const double*)dInj;
   B.jump = jump;
   B.chunk = 8;
-  if (!fp64) OF_CUDA_TRY(ctx, cudaMemsetAsync(dV, 0, (size_t)nc * npad * esz * 2, ctx->stream));
   OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
   if (fp64) {
     const int64_t chunks = (N + B.chunk - 1) / B.chunk;
