@@ -241,6 +241,29 @@ of_status of_book_plan_info(of_book_plan* plan, int32_t* block, int32_t* paths_p
                             int64_t* n_tiles, double* path_steps);
 void of_book_plan_destroy(of_book_plan* plan);
 
+/* ---- tile-shape autotuner ----------------------------------------------- */
+/* The reference has no counterpart (its GPU engine uses one fixed launch
+ * shape: WORKGROUP_SIZE 256 and one path per invocation,
+ * src/engines/gpu/gpu_mc.rs:19,207).  One candidate tile shape and
+ * its measured time. */
+typedef struct of_tune_candidate {
+  int32_t block;            /* book: threads per block; strip: written as 0 */
+  int32_t paths_per_thread; /* book: samples per thread per tile; strip: samples in flight per thread (1 or 2) */
+  double ms;                /* out: median device milliseconds of the timed replays */
+} of_tune_candidate;
+
+/* Builds a strip plan for each candidate (cfg->tile_ilp replaced by the
+ * candidate's paths_per_thread), replays it once untimed and `reps` times
+ * between CUDA events on the context stream, fills each candidate's ms and
+ * writes the index of the fastest to *best. */
+of_status of_autotune_strip(of_ctx* ctx, const of_model* model, int32_t option_type,
+                            const double* strikes, int64_t n_strikes, const of_mc_config* cfg,
+                            of_tune_candidate* candidates, int32_t n_candidates, int32_t reps, int32_t* best);
+/* The same for the persistent book kernel over (block, paths_per_thread);
+ * each candidate's plan is a CUDA graph whatever cfg->use_graph says. */
+of_status of_autotune_book(of_ctx* ctx, const of_book_entry* entries, int64_t n, const of_book_config* cfg,
+                           of_tune_candidate* candidates, int32_t n_candidates, int32_t reps, int32_t* best);
+
 /* ---- Monte Carlo Greeks on the reference streams (FP64) ----------------- */
 typedef struct of_greeks_params {
   int32_t option_type; /* OF_CALL / OF_PUT */

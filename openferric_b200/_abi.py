@@ -110,6 +110,14 @@ class OfBookConfig(C.Structure):
     ]
 
 
+class OfTuneCandidate(C.Structure):
+    _fields_ = [
+        ("block", C.c_int32),
+        ("paths_per_thread", C.c_int32),
+        ("ms", C.c_double),
+    ]
+
+
 class OfGreeksParams(C.Structure):
     _fields_ = [
         ("option_type", C.c_int32),

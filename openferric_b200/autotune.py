@@ -2,20 +2,25 @@
 
 `tune_strip` times the strike-strip kernel for each candidate number of
 samples in flight per thread (ILP); `tune_book` times the persistent book
-kernel for candidate (threads per block, samples per thread per tile).  Each
-candidate is a prepared plan (CUDA graph) replayed a few times on the
-engine's stream and timed with CUDA events; the fastest wins.  Results are
+kernel for candidate (threads per block, samples per thread per tile).  The
+timing is native (of_autotune_strip / of_autotune_book): each candidate is a
+prepared plan (CUDA graph) replayed a few times on the engine's stream and
+timed with CUDA events; the fastest wins.  Results are
 cached per device name and workload signature in a JSON file
 (OF_AUTOTUNE_CACHE, default ~/.cache/openferric_b200/autotune.json) and
 reused by `best_strip_ilp` / `best_book_tile` without re-timing.
 """
 from __future__ import annotations
 
+import ctypes as C
 import json
 import os
 import threading
-from typing import Dict, List, Optional, Sequence, Tuple
+from typing import Dict, Optional, Sequence, Tuple
 
+import numpy as np
+
+from . import _abi as A
 from ._lib import context
 
 _LOCK = threading.Lock()
@@ -48,20 +53,11 @@ def _device_name(device: int) -> str:
     return torch.cuda.get_device_name(device)
 
 
-def _time_launches(ctx, launch, reps: int) -> float:
-    """Median milliseconds of `reps` launches on the engine's stream (CUDA events)."""
-    import statistics
-    import torch
-    stream = torch.cuda.ExternalStream(ctx.stream_ptr())
-    launch()
-    stream.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
-    for s, e in ev:
-        s.record(stream)
-        launch()
-        e.record(stream)
-    stream.synchronize()
-    return statistics.median(s.elapsed_time(e) for s, e in ev)
+def _candidates(shapes: Sequence[Tuple[int, int]]):
+    arr = (A.OfTuneCandidate * len(shapes))()
+    for i, (block, ppt) in enumerate(shapes):
+        arr[i].block, arr[i].paths_per_thread = int(block), int(ppt)
+    return arr
 
 
 def _strip_key(device: int, generator, n_strikes: int, antithetic: bool) -> str:
@@ -74,16 +70,19 @@ def tune_strip(generator, strikes: Sequence[float], num_paths: int, antithetic: 
                candidates: Sequence[int] = (1, 2), reps: int = 5) -> Tuple[int, Dict[int, float]]:
     """Times the strip for each ILP candidate; stores and returns the best."""
     from .core import OptionType
-    from .engines import StripPlan
     ctx = context(device)
-    times = {}
-    for ilp in candidates:
-        plan = StripPlan(generator, OptionType.Call, strikes, num_paths, 1, 1.0, antithetic, device, tile_ilp=ilp)
-        try:
-            times[ilp] = _time_launches(ctx, plan.launch, reps)
-        finally:
-            plan.close()
-    best = min(times, key=times.get)
+    ks = np.ascontiguousarray(strikes, dtype=np.float64)
+    model = generator.to_abi()
+    cfg = A.OfMcConfig(num_paths=int(num_paths), seed=1, antithetic=int(antithetic),
+                       precision=A.OF_PREC_FP32_PHILOX, discount_factor=1.0)
+    cands = _candidates([(0, ilp) for ilp in candidates])
+    best_i = C.c_int32()
+    with ctx.lock:
+        ctx.check(ctx._L.of_autotune_strip(ctx.handle, C.byref(model), OptionType.Call.value,
+                                           ks.ctypes.data_as(C.POINTER(C.c_double)), len(ks), C.byref(cfg),
+                                           cands, len(cands), int(reps), C.byref(best_i)))
+    times = {c.paths_per_thread: c.ms for c in cands}
+    best = cands[best_i.value].paths_per_thread
     with _LOCK:
         table = _load()
         table[_strip_key(device, generator, len(strikes), antithetic)] = {
@@ -102,16 +101,17 @@ def tune_book(entries, seed: int = 1, device: int = 0,
               candidates: Sequence[Tuple[int, int]] = ((256, 4), (256, 2), (256, 8), (128, 4), (128, 8)),
               reps: int = 3) -> Tuple[Tuple[int, int], Dict[str, float]]:
     """Times the persistent book kernel for each (block, paths_per_thread)."""
-    from .book import BookPlan
+    from .book import book_entries_abi
     ctx = context(device)
-    times = {}
-    for block, ppt in candidates:
-        plan = BookPlan(entries, seed, block=block, paths_per_thread=ppt, use_graph=True, device=device)
-        try:
-            times[(block, ppt)] = _time_launches(ctx, plan.launch, reps)
-        finally:
-            plan.close()
-    best = min(times, key=times.get)
+    arr, _keep, _ = book_entries_abi(entries)
+    cfg = A.OfBookConfig(seed=int(seed) & 0xFFFFFFFFFFFFFFFF, use_graph=1)
+    cands = _candidates(candidates)
+    best_i = C.c_int32()
+    with ctx.lock:
+        ctx.check(ctx._L.of_autotune_book(ctx.handle, arr, len(arr), C.byref(cfg), cands, len(cands), int(reps),
+                                          C.byref(best_i)))
+    times = {(c.block, c.paths_per_thread): c.ms for c in cands}
+    best = (cands[best_i.value].block, cands[best_i.value].paths_per_thread)
     key = f"book|{_device_name(device)}|n={len(entries)}"
     with _LOCK:
         table = _load()

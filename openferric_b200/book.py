@@ -36,6 +36,32 @@ class BookEntry:
     variance_reduction: VarianceReduction = VarianceReduction.None_
 
 
+def book_entries_abi(entries: Sequence[BookEntry]):
+    """The of_book_entry array of a book, the objects its pointers refer to
+    (keep them alive while the array is in use) and each entry's volatility."""
+    arr = (A.OfBookEntry * len(entries))()
+    keep, vols = [], []
+    for k, e in enumerate(entries):
+        inst, m = e.instrument, e.market
+        inst.validate()
+        vol = m.vol_for(max(reference_strike(inst, m.spot), 1e-12), inst.expiry)
+        gen = GbmPathGenerator(Gbm(m.rate - m.dividend_yield, vol), m.spot, inst.expiry, e.num_steps,
+                               m.dividend_schedule if m.has_discrete_dividends() else None)
+        payoff, held = _payoff_abi(inst)
+        keep.append(held)
+        keep.append(gen)  # holds the dividend array the model points to
+        vols.append(vol)
+        cv = instrument_control_variate(inst, m, vol) \
+            if e.variance_reduction is VarianceReduction.ControlVariate else None
+        arr[k] = A.OfBookEntry(model=gen.to_abi(), payoff=payoff, num_paths=int(e.num_paths),
+                               antithetic=int(e.variance_reduction is VarianceReduction.Antithetic),
+                               discount_factor=math.exp(-m.rate * inst.expiry))
+        if cv is not None:
+            arr[k].control_variate = cv.kind.value
+            arr[k].cv_expected = cv.expected
+    return arr, keep, vols
+
+
 class BookPlan:
     """Device tables + CUDA graph for a book; launch() replays without a host sync."""
 
@@ -43,27 +69,7 @@ class BookPlan:
                  use_graph: bool = True, device: int = 0):
         self.ctx = context(device)
         self.n = len(entries)
-        self._keep = []
-        self._vols = []
-        arr = (A.OfBookEntry * self.n)()
-        for k, e in enumerate(entries):
-            inst, m = e.instrument, e.market
-            inst.validate()
-            vol = m.vol_for(max(reference_strike(inst, m.spot), 1e-12), inst.expiry)
-            gen = GbmPathGenerator(Gbm(m.rate - m.dividend_yield, vol), m.spot, inst.expiry, e.num_steps,
-                                   m.dividend_schedule if m.has_discrete_dividends() else None)
-            payoff, keep = _payoff_abi(inst)
-            self._keep.append(keep)
-            self._keep.append(gen)  # holds the dividend array the model points to
-            self._vols.append(vol)
-            cv = instrument_control_variate(inst, m, vol) \
-                if e.variance_reduction is VarianceReduction.ControlVariate else None
-            arr[k] = A.OfBookEntry(model=gen.to_abi(), payoff=payoff, num_paths=int(e.num_paths),
-                                   antithetic=int(e.variance_reduction is VarianceReduction.Antithetic),
-                                   discount_factor=math.exp(-m.rate * inst.expiry))
-            if cv is not None:
-                arr[k].control_variate = cv.kind.value
-                arr[k].cv_expected = cv.expected
+        arr, self._keep, self._vols = book_entries_abi(entries)
         cfg = A.OfBookConfig(seed=int(seed) & 0xFFFFFFFFFFFFFFFF, block=block, paths_per_thread=paths_per_thread,
                              use_graph=int(use_graph))
         h = C.c_void_p()

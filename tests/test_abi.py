@@ -48,6 +48,7 @@ STRUCTS = {
     "of_heston_adjoint_params": A.OfHestonAdjointParams,
     "of_adjoint_result": A.OfAdjointResult,
     "of_device_peaks": A.OfDevicePeaks,
+    "of_tune_candidate": A.OfTuneCandidate,
     "of_bermudan_contract": A.OfBermudanContract,
     "of_boundary_point": A.OfBoundaryPoint,
     "of_qmc_params": A.OfQmcParams,

@@ -43,3 +43,17 @@ def test_tune_book_caches_winner(tmp_path, monkeypatch):
     res = plan.results()
     plan.close()
     assert all(math.isfinite(r.price) for r in res)
+
+
+def test_native_autotune_rejects_bad_candidates(tmp_path, monkeypatch):
+    monkeypatch.setenv("OF_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    from openferric_b200 import PricingError
+    gen = HestonPathGenerator(HESTON, 100.0, 1.0, 8)
+    with pytest.raises(PricingError, match="1 or 2"):
+        autotune.tune_strip(gen, [100.0], 1 << 12, candidates=(1, 3))
+    with pytest.raises(PricingError, match="reps"):
+        autotune.tune_strip(gen, [100.0], 1 << 12, reps=0)
+    book = synthetic_book(4, seed=3, min_log2_paths=10, max_log2_paths=11)
+    with pytest.raises(PricingError, match="multiple of 32"):
+        autotune.tune_book(book, candidates=((512, 4),))
+    assert not (tmp_path / "tune.json").exists()  # nothing cached from a refused call
