@@ -5,9 +5,11 @@
 //
 // Layout: S[contract][step-1][path] (time-major: a date's column is one
 // contiguous, coalesced read), cash flows V[contract][path] and, for the
-// pathwise delta, the step tau[contract][path] at which each path's cash flow
-// is paid (written only when a path exercises; the final kernel derives
-// dV = +-S_tau disc^tau / S0 from V and tau).  One kernel per exercise date does
+// pathwise delta, the step tau at which each path's cash flow is paid: in FP64
+// mode an array tau[contract][path] written when a path exercises, in FP32
+// mode one dense row of exercise flags per date (a bit per path) from which
+// the final kernel takes the first flagged date.  The final kernel derives
+// dV = +-S_tau disc^tau / S0 from V and tau.  One kernel per exercise date does
 //   exercise(t+1) with the betas of the previous pass -> discount -> FP64
 //   in-the-money basis moments at t -> block partials,
 // and the last block of each contract (last-block-done counter, no spin)
@@ -31,6 +33,7 @@
 
 #include "of_device.cuh"
 #include "of_internal.h"
+#include "bulk_copy.cuh"
 #include "path_fp32.cuh"
 
 namespace {
@@ -170,7 +173,9 @@ struct LsmBatch {
   int64_t n, npad;           // paths, padded path stride
   void* S;                   // [nc][steps][npad] (T)
   void* V;                   // [nc][npad]
-  int32_t* tau;             // [nc][npad] step of each path's cash flow (delta only)
+  int32_t* tau;             // [nc][npad] step of each path's cash flow (FP64 mode, delta only)
+  uint32_t* exflags;        // [nc][steps+1][npad/32] FP32 mode, delta only: per date, word 4g+e
+                            // bit L = path 4(32g+L)+e exercised at that date
   double* partials;          // [nc][blocks][kMaxMoments]
   double* betas;             // [2][nc][4] + valid flag in [2][nc] (separate)
   int32_t* beta_ok;          // [2][nc]
@@ -184,6 +189,8 @@ struct LsmBatch {
   unsigned long long* ex_count;  // [nc][steps+1] paths exercised at each date
   unsigned long long* ex_bits;   // [nc][steps+1] bits of the max (put) / min (call) exercised spot
   double* itm_count;             // [nc][steps+1] in-the-money paths at each regression date
+  const double* disc_pow;        // [nc][steps+1] disc^k by repeated multiplication, as V is discounted
+  uint32_t* status;              // nonzero: a pass gave up waiting for its bulk copies
   unsigned long long* term_itm;  // [nc] paths in the money at expiry
   uint64_t seed;
   of::PhiloxKeys keys;
@@ -297,67 +304,80 @@ __global__ void __launch_bounds__(128) lsm_gen_ref(LsmBatch B) {
   if (B.track && itm) atomicAdd(B.term_itm + c, (unsigned long long)itm);
 }
 
-// FP32 Philox generator: 4 consecutive paths per thread, float4 stores.
-__global__ void __launch_bounds__(256) lsm_gen_philox(const __grid_constant__ LsmBatch B) {
+// FP32 Philox generator: 4 consecutive paths per thread, float4 stores.  The
+// dynamics are a template parameter and the time loop walks whole counter
+// blocks, so each step reads its Philox word without a select: draw t of a
+// path is word t%4 of counter block t/4; Heston's (z1, z2) of step t are words
+// 2(t%2), 2(t%2)+1 of counter block t/2.  A batch holds one dynamics kind.
+template <int DYN>
+__global__ void __launch_bounds__(256, DYN == DYN_GBM ? 4 : 2) lsm_gen_philox(const __grid_constant__ LsmBatch B) {
+  constexpr int kStepsPerBlock = DYN == DYN_HESTON ? 2 : 4;
   const int c = blockIdx.y;
-  const LsmC C = B.c[c];
+  const LsmC& C = B.c[c];
   const int64_t p0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
   const bool live = p0 < B.npad;  // the grid's last block may reach past the padded path count
   const LsmStep* st = B.st + (size_t)c * (B.steps + 1);
   const uint32_t cid = B.contract_base + (uint32_t)c;
+  const bool put = C.put != 0;
+  const float fspot = C.fspot;
   int itm = 0;
   if (live) {
-    float* S = (float*)B.S + (size_t)c * B.steps * B.npad;
+    // padding paths (p >= n) store a spot that is out of the money at every date
+    const float pad = put ? __int_as_float(0x7F800000) : 0.0f;
+    bool in[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) in[q] = p0 + q < B.n;
+    float* S = (float*)B.S + (size_t)c * B.steps * B.npad + p0;
     of::LegState L[4];
+    float s[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) L[q] = of::LegState{0.0f, C.hc.v0};
-    float s[4] = {C.fspot, C.fspot, C.fspot, C.fspot};
-    uint4 r[4];
-    for (int t = 0; t < B.steps; ++t) {
-      // draw t of a path: counter block t/4, word t%4; Heston draws (z1, z2)
-      // of step t: words 2(t%2), 2(t%2)+1 of counter block t/2
-      const bool refill = C.dynamics == DYN_HESTON ? (t & 1) == 0 : (t & 3) == 0;
-      if (refill) {
-        const uint32_t blk = C.dynamics == DYN_HESTON ? (uint32_t)(t >> 1) : (uint32_t)(t >> 2);
+    for (int q = 0; q < 4; ++q) {
+      L[q] = of::LegState{0.0f, DYN == DYN_HESTON ? C.hc.v0 : 0.0f};
+      s[q] = fspot;
+    }
+    for (int tb = 0; tb < B.steps; tb += kStepsPerBlock) {
+      const uint32_t blk = (uint32_t)(tb / kStepsPerBlock);
+      uint4 r[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-          r[q] = of::philox4x32_10(make_uint4(blk, (uint32_t)(p0 + q), cid, kLsmStreamTag), B.keys);
-      }
-      float4 out;
-      float* o = &out.x;
+      for (int q = 0; q < 4; ++q)
+        r[q] = of::philox4x32_10(make_uint4(blk, (uint32_t)(p0 + q), cid, kLsmStreamTag), B.keys);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (C.dynamics == DYN_HESTON) {
-          const float z1 = of::normal_from_u32((t & 1) ? r[q].z : r[q].x);
-          const float z2 = of::normal_from_u32((t & 1) ? r[q].w : r[q].y);
-          of::heston_euler_step(L[q], C.hc, z1, z2);
-        } else {
-          const uint32_t bits = (t & 3) == 0 ? r[q].x : (t & 3) == 1 ? r[q].y : (t & 3) == 2 ? r[q].z : r[q].w;
-          const float z = of::normal_from_u32(bits);
-          if (C.dynamics == DYN_GBM) {
-            L[q].y = fmaf(C.fstep_vol, z, L[q].y + C.fdrift);
+      for (int k = 0; k < kStepsPerBlock; ++k) {
+        const int t = tb + k;
+        if (t >= B.steps) break;
+        float4 out;
+        float* o = &out.x;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint32_t* w = &r[q].x;
+          if (DYN == DYN_HESTON) {
+            of::heston_euler_step(L[q], C.hc, of::normal_from_u32(w[2 * k]), of::normal_from_u32(w[2 * k + 1]));
+          } else if (DYN == DYN_GBM) {
+            L[q].y = fmaf(C.fstep_vol, of::normal_from_u32(w[k]), L[q].y + C.fdrift);
           } else {
+            const float z = of::normal_from_u32(w[k]);
             const LsmStep& e = st[t + 1];
             const float sig = lsm_local_vol<float>(C.lv_kf, C.lv_vf, C.lv_nk, e.e0, e.e1, e.few,
                                                    s[q] > 1.0e-8f ? s[q] : 1.0e-8f);
             const float y = fmaf(sig * C.fsqrt_dt, z, fmaf(-0.5f * sig * sig, C.fdt, L[q].y + C.fmudt));
             L[q].y = y > C.fy_floor ? y : C.fy_floor;
           }
+          s[q] = fspot * __expf(L[q].y);
+          o[q] = in[q] ? s[q] : pad;
         }
-        s[q] = C.fspot * __expf(L[q].y);
-        o[q] = s[q];
+        *reinterpret_cast<float4*>(S + (size_t)t * B.npad) = out;
       }
-      *reinterpret_cast<float4*>(S + (size_t)t * B.npad + p0) = out;
     }
-    float* V = (float*)B.V + (size_t)c * B.npad;
     const float fk = st[B.steps].fstrike;
+    float4 v4;
+    float* vv = &v4.x;
+#pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const float v = intrinsic_v<float>(C.put, s[q], fk);
-      const bool in = p0 + q < B.n;
-      V[p0 + q] = in ? v : 0.0f;
-      itm += (in && v > 0.0f) ? 1 : 0;
+      const float v = intrinsic_v<float>(put, s[q], fk);
+      vv[q] = in[q] ? v : 0.0f;
+      itm += (in[q] && v > 0.0f) ? 1 : 0;
     }
-    if (B.want_delta) *reinterpret_cast<int4*>(B.tau + (size_t)c * B.npad + p0) = make_int4(B.steps, B.steps, B.steps, B.steps);
+    *reinterpret_cast<float4*>((float*)B.V + (size_t)c * B.npad + p0) = v4;
   }
   if (B.track) {
     itm = __reduce_add_sync(of::kFullMask, itm);
@@ -499,6 +519,40 @@ __device__ __forceinline__ void record_exercise(const LsmBatch& B, int c, int da
   }
 }
 
+// The end of a pass: the block's moments are reduced with one barrier (warp
+// shuffles, then one thread per moment sums the warps in a fixed order) into
+// its partials; the block that finishes last reduces every block's partials
+// and solves for the betas of date t.
+template <int NM>
+__device__ __forceinline__ void block_moments(const LsmBatch& B, int c, int t, const double* mom, double* red_sh,
+                                              double* mom_sh) {
+  __shared__ bool is_last;
+  double* part = B.partials + ((size_t)c * B.blocks + blockIdx.x) * kMaxMoments;
+#pragma unroll
+  for (int k = 0; k < NM; ++k) {
+    const double w = of::warp_sum(mom[k]);
+    if ((threadIdx.x & 31) == 0) red_sh[(threadIdx.x >> 5) * kMaxMoments + k] = w;
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < NM) {
+    double acc = 0.0;
+    for (int i = 0; i < kPassThreads / 32; ++i) acc += red_sh[i * kMaxMoments + threadIdx.x];
+    part[threadIdx.x] = acc;
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t done = atomicAdd(B.counters + c, 1u);
+    is_last = done == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (is_last) {
+    __threadfence();
+    last_block_reduce(B, c, NM, (int)gridDim.x, mom_sh, red_sh, t);
+    if (threadIdx.x == 0) B.counters[c] = 0;
+  }
+}
+
 // One path of a pass: exercise at date t+1 (spot s1) with the betas of that
 // date, discount one step, and the in-the-money basis moments at date t
 // (spot s0, longstaff_schwartz.rs:543-601).
@@ -542,15 +596,16 @@ __device__ __forceinline__ bool lsm_path_update(const LsmC& C, const double* bet
   return exercised;
 }
 
-// One exercise date t (1 <= t <= steps-1): exercise(t+1), discount, moments(t).
-// A block walks the contract's chunks of kPathsPerBlock paths with a grid
-// stride and reduces its moments once at the end; DEG (the basis degree) is a
-// template parameter so that the moment count is known at compile time.
+// One exercise date t (1 <= t <= steps-1) of the FP64 reference mode:
+// exercise(t+1), discount, moments(t), all in FP64 with the reference's
+// operation order (no contraction).  A block walks the contract's chunks of
+// kPathsPerBlock paths with a grid stride and reduces its moments once at the
+// end; DEG (the basis degree) is a template parameter so that the moment count
+// is known at compile time.
 template <typename T, int DEG>
 __global__ void __launch_bounds__(kPassThreads, 3) lsm_pass(LsmBatch B, int t) {
   __shared__ double red_sh[kPassThreads];
   __shared__ double mom_sh[kMaxMoments];
-  __shared__ bool is_last;
   const int c = blockIdx.y;
   const LsmC C = B.c[c];
   const T* S = (const T*)B.S + (size_t)c * B.steps * B.npad;
@@ -573,75 +628,269 @@ __global__ void __launch_bounds__(kPassThreads, 3) lsm_pass(LsmBatch B, int t) {
   for (int k = 0; k < nm; ++k) mom[k] = 0.0;
   for (int64_t chunk = blockIdx.x; chunk < B.blocks; chunk += gridDim.x) {
     const int64_t base = chunk * kPathsPerBlock;
-    if constexpr (sizeof(T) == 4) {
-      // FP32 store: 4 consecutive paths per thread; the four float4 loads are
-      // issued before any of them is used
-      const int64_t q = base / 4 + threadIdx.x;
-      float4 v4 = reinterpret_cast<const float4*>(V)[q];
-      const float4 a4 = have_beta ? reinterpret_cast<const float4*>(S + (size_t)t * B.npad)[q]
-                                  : make_float4(0.f, 0.f, 0.f, 0.f);
-      const float4 b4 = ex_now ? reinterpret_cast<const float4*>(S + (size_t)(t - 1) * B.npad)[q]
-                               : make_float4(0.f, 0.f, 0.f, 0.f);
-      const int64_t p0 = base + (int64_t)threadIdx.x * 4;
-      float* vv = &v4.x;
-      const float* s1 = &a4.x;
-      const float* s0 = &b4.x;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        if (p0 + e >= B.n) continue;  // padding
-        double v = vv[e];
-        if (lsm_path_update<DEG>(C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1[e], s0[e], v, mom)) {
-          ++n_ex;
-          ext = C.put ? fmax(ext, (double)s1[e]) : fmin(ext, (double)s1[e]);
-          if (B.want_delta) tau[p0 + e] = t + 1;  // the cash flow now comes at date t+1
-        }
-        vv[e] = (float)v;
+    for (int q = 0; q < kPathsPerThread; ++q) {
+      const int64_t p = base + q * kPassThreads + threadIdx.x;
+      if (p >= B.n) break;
+      double v = (double)V[p];
+      const double s1 = have_beta ? (double)S[(size_t)t * B.npad + p] : 0.0;      // spot at date t+1
+      const double s0 = ex_now ? (double)S[(size_t)(t - 1) * B.npad + p] : 0.0;  // spot at date t
+      if (lsm_path_update<DEG>(C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1, s0, v, mom)) {
+        ++n_ex;
+        ext = C.put ? fmax(ext, s1) : fmin(ext, s1);
+        if (B.want_delta) tau[p] = t + 1;  // the cash flow now comes at date t+1
       }
-      reinterpret_cast<float4*>(V)[q] = v4;
-    } else {
-#pragma unroll
-      for (int q = 0; q < kPathsPerThread; ++q) {
-        const int64_t p = base + q * kPassThreads + threadIdx.x;
-        if (p >= B.n) break;
-        double v = (double)V[p];
-        const double s1 = have_beta ? (double)S[(size_t)t * B.npad + p] : 0.0;      // spot at date t+1
-        const double s0 = ex_now ? (double)S[(size_t)(t - 1) * B.npad + p] : 0.0;  // spot at date t
-        if (lsm_path_update<DEG>(C, beta, have_beta, ex_now, k1, ik1, k0, ik0, s1, s0, v, mom)) {
-          ++n_ex;
-          ext = C.put ? fmax(ext, s1) : fmin(ext, s1);
-          if (B.want_delta) tau[p] = t + 1;  // the cash flow now comes at date t+1
-        }
-        V[p] = (T)v;
-      }
+      V[p] = (T)v;
     }
   }
   if (B.track && have_beta) record_exercise(B, c, t + 1, C.put, n_ex, ext);  // block-uniform condition
   if (!ex_now) return;
-  // block reduction of all moments with one barrier: warp shuffles, then one
-  // thread per moment sums the warps in a fixed order -> partials
-  double* part = B.partials + ((size_t)c * B.blocks + blockIdx.x) * kMaxMoments;
+  block_moments<nm>(B, c, t, mom, red_sh, mom_sh);
+}
+
+// FP32 path store, FP32 arithmetic for everything but the regression moments:
+// the exercise decision (continuation with FP32 betas, explicit fmaf), the
+// one-step discount (v*d with d split into two floats, so the rounding of d
+// does not compound over the dates) and the in-the-money test.  The moments
+// stay FP64 (one fma per cross moment, the count as an integer).  No per-path
+// bounds test: the generator stores an out-of-the-money spot (+inf for a put,
+// 0 for a call) and V = 0 for the padding paths p >= n, so they never exercise
+// and never enter the moments.  For the pathwise delta each pass writes one
+// dense row of exercise flags (a bit per path, warp ballots) for its date
+// instead of scattered per-path payment steps: a scattered 4-byte store
+// leaves a partly written sector that the L2 fills from DRAM, which cost a
+// quarter of the pass's traffic.  The final kernel takes each path's payment
+// step as the first date whose flag is set.
+struct F32Pass {
+  bool have_beta, ex_now, want_delta;
+  float b0, b1, b2, b3, k1, ik1, k0, ik0, dh, dl;
+};
+
+// One quad (four consecutive paths) of an FP32 pass; returns the paths that
+// exercised at date t+1 as a 4-bit mask.
+template <int DEG, bool PUT>
+__device__ __forceinline__ unsigned f32_quad(const F32Pass& P, float4& v4, const float4& a4, const float4& p4,
+                                             double* mom, unsigned& n_ex, unsigned& n_itm, float& ext) {
+  float* vv = &v4.x;
+  const float* s1 = &a4.x;
+  const float* s0 = &p4.x;
+  unsigned exm = 0;
 #pragma unroll
-  for (int k = 0; k < nm; ++k) {
-    const double w = of::warp_sum(mom[k]);
-    if ((threadIdx.x & 31) == 0) red_sh[(threadIdx.x >> 5) * kMaxMoments + k] = w;
+  for (int e = 0; e < 4; ++e) {
+    float v = vv[e];
+    if (P.have_beta) {
+      const float ex = PUT ? P.k1 - s1[e] : s1[e] - P.k1;
+      const float x1 = DEG == 3 ? s1[e] * P.ik1 : s1[e];
+      const float cont = DEG == 3 ? fmaf(x1, fmaf(x1, fmaf(x1, P.b3, P.b2), P.b1), P.b0)
+                                  : fmaf(x1, fmaf(x1, P.b2, P.b1), P.b0);
+      if (ex > 0.0f && ex > cont) {
+        v = ex;
+        ++n_ex;
+        ext = PUT ? fmaxf(ext, s1[e]) : fminf(ext, s1[e]);
+        exm |= 1u << e;
+      }
+    }
+    v = fmaf(v, P.dh, v * P.dl);
+    vv[e] = v;
+    if (P.ex_now && (PUT ? P.k0 - s0[e] : s0[e] - P.k0) > 0.0f) {
+      ++n_itm;
+      const double x = DEG == 3 ? (double)(s0[e] * P.ik0) : (double)s0[e];
+      const double y = (double)v;
+      const double x2 = x * x, x3 = x2 * x;
+      if (DEG == 2) {
+        mom[1] += x;
+        mom[2] += x2;
+        mom[3] += x3;
+        mom[4] += x2 * x2;
+        mom[5] += y;
+        mom[6] = fma(x, y, mom[6]);
+        mom[7] = fma(x2, y, mom[7]);
+      } else {
+        const double x4 = x2 * x2;
+        mom[1] += x;
+        mom[2] += x2;
+        mom[3] += x3;
+        mom[4] += x4;
+        mom[5] += x4 * x;
+        mom[6] += x3 * x3;
+        mom[7] += y;
+        mom[8] = fma(x, y, mom[8]);
+        mom[9] = fma(x2, y, mom[9]);
+        mom[10] = fma(x3, y, mom[10]);
+      }
+    }
   }
-  __syncthreads();
-  if ((int)threadIdx.x < nm) {
-    double acc = 0.0;
-    for (int i = 0; i < kPassThreads / 32; ++i) acc += red_sh[i * kMaxMoments + threadIdx.x];
-    part[threadIdx.x] = acc;
-    __threadfence();
+  return exm;
+}
+
+constexpr int kStages = 3;                                     // ring depth of the FP32 pass
+constexpr uint32_t kChunkBytes = kPathsPerBlock * sizeof(float);  // one array's share of a chunk
+constexpr uint64_t kWaitLimitNs = 1000000000ull;               // a bulk copy lands in microseconds
+
+// The FP32 pass streams its three inputs through shared memory: chunk j of
+// the block (1024 paths, grid-stride over the contract) has its V, S(t+1) and
+// S(t) segments (4 KB each, only the ones the date needs) copied by
+// cp.async.bulk into ring stage j % kStages, completed on that stage's
+// mbarrier.  Thread 0 keeps kStages chunks in flight; one barrier per chunk
+// both publishes the landed stage and frees the one consumed before it.  The
+// new cash flows go straight to global memory.  A copy that has not landed
+// after kWaitLimitNs sets B.status, and the block drains its outstanding
+// copies (bounded the same way) and returns without its moments.
+template <int DEG, bool PUT>
+__device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, float* ring, uint64_t* full,
+                                                  double* red_sh, double* mom_sh) {
+  constexpr int nm = DEG == 2 ? 8 : 11;
+  const int c = blockIdx.y;
+  const float* S = (const float*)B.S + (size_t)c * B.steps * B.npad;
+  const float* gS1 = S + (size_t)t * B.npad;        // spot at date t+1
+  const float* gS0 = S + (size_t)(t - 1) * B.npad;  // spot at date t
+  float* gV = (float*)B.V + (size_t)c * B.npad;
+  uint32_t* flags = B.exflags + ((size_t)c * (B.steps + 1) + (t + 1)) * (B.npad / 32);  // date t+1
+  const uint8_t* can = B.can_ex + (size_t)c * (B.steps + 1);
+  F32Pass P;
+  P.ex_now = can[t];
+  const int nb = (t + 1) & 1;  // betas of date t+1 were written by the previous pass
+  P.have_beta = (t + 1 < B.steps) && can[t + 1] && B.beta_ok[(size_t)nb * B.nc + c];
+  P.b0 = P.b1 = P.b2 = P.b3 = 0.0f;
+  if (P.have_beta) {
+    const double* bp = B.betas + ((size_t)nb * B.nc + c) * 4;
+    P.b0 = (float)bp[0];
+    P.b1 = (float)bp[1];
+    P.b2 = (float)bp[2];
+    P.b3 = (float)bp[3];
   }
-  __syncthreads();
+  const LsmStep* st = B.st + (size_t)c * (B.steps + 1);
+  P.k1 = st[t + 1].fstrike;
+  P.ik1 = st[t + 1].finv_strike;
+  P.k0 = st[t].fstrike;
+  P.ik0 = st[t].finv_strike;
+  const double disc = B.c[c].disc;
+  P.dh = (float)disc;
+  P.dl = (float)(disc - (double)P.dh);
+  P.want_delta = B.want_delta != 0;
+  const int n_chunks = (B.blocks - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const uint32_t bytes = kChunkBytes * (1u + (P.have_beta ? 1u : 0u) + (P.ex_now ? 1u : 0u));
+  // stage layout: [S(t+1) | S(t) | V], kPathsPerBlock floats each
+  auto issue = [&](int j) {
+    const int s = j % kStages;
+    const int64_t off = ((int64_t)blockIdx.x + (int64_t)j * gridDim.x) * kPathsPerBlock;
+    float* dst = ring + (size_t)s * 3 * kPathsPerBlock;
+    const uint32_t bar = of::smem_u32(full + s);
+    of::mbar_arrive_expect_tx(bar, bytes);
+    if (P.have_beta) of::bulk_load(of::smem_u32(dst), gS1 + off, kChunkBytes, bar);
+    if (P.ex_now) of::bulk_load(of::smem_u32(dst + kPathsPerBlock), gS0 + off, kChunkBytes, bar);
+    of::bulk_load(of::smem_u32(dst + 2 * kPathsPerBlock), gV + off, kChunkBytes, bar);
+  };
   if (threadIdx.x == 0) {
-    const uint32_t done = atomicAdd(B.counters + c, 1u);
-    is_last = done == gridDim.x - 1;
+    for (int s = 0; s < kStages; ++s) of::mbar_init(of::smem_u32(full + s), 1);
+    of::mbar_fence_init();
   }
   __syncthreads();
-  if (is_last) {
-    __threadfence();
-    last_block_reduce(B, c, nm, (int)gridDim.x, mom_sh, red_sh, t);
-    if (threadIdx.x == 0) B.counters[c] = 0;
+  if (threadIdx.x == 0)
+    for (int j = 0; j < kStages && j < n_chunks; ++j) issue(j);
+  unsigned n_ex = 0, n_itm = 0;
+  float ext = PUT ? 0.0f : __int_as_float(0x7F800000);
+  double mom[nm];
+#pragma unroll
+  for (int k = 0; k < nm; ++k) mom[k] = 0.0;
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  int i = 0;
+  for (; i < n_chunks; ++i) {
+    const int s = i % kStages;
+    const bool landed = of::mbar_wait(of::smem_u32(full + s), (uint32_t)(i / kStages) & 1u, kWaitLimitNs);
+    // every thread has finished chunk i-1, so its stage can be refilled
+    if (!__syncthreads_and(landed)) break;
+    if (threadIdx.x == 0 && i >= 1 && i - 1 + kStages < n_chunks) issue(i - 1 + kStages);
+    const float* src = ring + (size_t)s * 3 * kPathsPerBlock;
+    const float4 a4 = P.have_beta ? reinterpret_cast<const float4*>(src)[threadIdx.x] : zero;
+    const float4 p4 = P.ex_now ? reinterpret_cast<const float4*>(src + kPathsPerBlock)[threadIdx.x] : zero;
+    float4 v4 = reinterpret_cast<const float4*>(src + 2 * kPathsPerBlock)[threadIdx.x];
+    const int64_t q = ((int64_t)blockIdx.x + (int64_t)i * gridDim.x) * kPassThreads + threadIdx.x;
+    const unsigned exm = f32_quad<DEG, PUT>(P, v4, a4, p4, mom, n_ex, n_itm, ext);
+    reinterpret_cast<float4*>(gV)[q] = v4;
+    if (P.want_delta) {
+      // word 4g+e of the date's flag row: bit L = path 4(32g+L)+e exercised,
+      // for the warp's 32 quads 32g .. 32g+31
+      const unsigned lane = threadIdx.x & 31u;
+      uint32_t word = 0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const uint32_t m = __ballot_sync(of::kFullMask, (exm >> e) & 1u);
+        if (lane == (unsigned)e) word = m;
+      }
+      if (lane < 4) flags[(q >> 5) * 4 + lane] = word;
+    }
+  }
+  if (i < n_chunks) {  // a copy did not land: record it, drain what is in flight, give up
+    if (threadIdx.x == 0) {
+      atomicOr(B.status, 1u);
+      // issued so far: chunks 0 .. kStages-1, then chunk k-1+kStages at each completed iteration k >= 1
+      const int issued = i >= 1 ? i - 2 + kStages : kStages - 1;
+      const int last = issued < n_chunks - 1 ? issued : n_chunks - 1;
+      for (int j = i; j <= last; ++j)
+        of::mbar_wait(of::smem_u32(full + j % kStages), (uint32_t)(j / kStages) & 1u, kWaitLimitNs);
+    }
+    __syncthreads();
+    return;
+  }
+  if (B.track && P.have_beta) record_exercise(B, c, t + 1, PUT, n_ex, (double)ext);  // block-uniform condition
+  if (!P.ex_now) return;
+  mom[0] = (double)n_itm;
+  block_moments<nm>(B, c, t, mom, red_sh, mom_sh);
+}
+
+template <int DEG>
+__global__ void __launch_bounds__(kPassThreads, 4) lsm_pass_f32(const __grid_constant__ LsmBatch B, int t) {
+  __shared__ __align__(128) float ring[kStages * 3 * kPathsPerBlock];
+  __shared__ __align__(8) uint64_t full[kStages];
+  __shared__ double red_sh[kPassThreads];
+  __shared__ double mom_sh[kMaxMoments];
+  if (B.c[blockIdx.y].put) lsm_pass_f32_body<DEG, true>(B, t, ring, full, red_sh, mom_sh);
+  else lsm_pass_f32_body<DEG, false>(B, t, ring, full, red_sh, mom_sh);
+}
+
+// 32 x 32 bit transpose across a warp: lane i holds row i on entry and column
+// i on exit (bit j of the result = bit i of lane j's row).  Recursive block
+// swap with one shuffle per level (the transpose32 recurrence of Hacker's
+// Delight, 2nd ed., section 7-3, with the rows spread over the lanes).
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, unsigned lane) {
+  uint32_t m = 0x0000FFFFu;
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1, m ^= m << s) {
+    const uint32_t y = __shfl_xor_sync(of::kFullMask, x, s);
+    x = (lane & (unsigned)s) ? ((x & ~m) | ((y & ~m) >> s)) : ((x & m) | ((y & m) << s));
+  }
+  return x;
+}
+
+// Payment steps of the calling lane's quad q (FP32 mode): the first date in
+// [2, steps-1] whose exercise flag is set, else `steps` (paid at expiry).  The
+// lanes of a warp hold quads 32g .. 32g+31, i.e. the 16 bytes 4g .. 4g+3 of
+// each flag row.  Lane j loads those 16 bytes of row d0+j, so one load covers
+// 32 dates; a bit transpose per word then gives lane L, for each of its four
+// paths, the dates of the 32 at which it was flagged, and the first is a
+// find-first-set.  Stops when every path of the warp has its date.  All 32
+// lanes call it.
+__device__ __forceinline__ void first_exercise_dates(const LsmBatch& B, int c, int64_t q, int tp[4]) {
+  const size_t row4 = (size_t)(B.npad / 128);  // uint4 per flag row
+  const uint4* col = reinterpret_cast<const uint4*>(B.exflags) + (size_t)c * (B.steps + 1) * row4 + (size_t)(q >> 5);
+  const unsigned lane = threadIdx.x & 31u;  // == q & 31
+  unsigned todo = 0xFu;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) tp[e] = B.steps;
+  for (int d0 = 2; d0 < B.steps; d0 += 32) {
+    if (!__any_sync(of::kFullMask, todo != 0u)) break;
+    const int d = d0 + (int)lane;
+    const uint4 w = d < B.steps ? __ldg(col + (size_t)d * row4) : make_uint4(0u, 0u, 0u, 0u);
+    const uint32_t words[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const uint32_t dates = warp_transpose32(words[e], lane);  // bit j: path e flagged at date d0+j
+      if (((todo >> e) & 1u) && dates) {
+        tp[e] = d0 + __ffs((int)dates) - 1;
+        todo &= ~(1u << e);
+      }
+    }
   }
 }
 
@@ -656,7 +905,6 @@ __global__ void __launch_bounds__(kPassThreads) lsm_final(LsmBatch B) {
   const LsmC C = B.c[c];
   const T* S = (const T*)B.S + (size_t)c * B.steps * B.npad;
   const T* V = (const T*)B.V + (size_t)c * B.npad;
-  const int32_t* tau = B.tau + (size_t)c * B.npad;
   const LsmStep* st = B.st + (size_t)c * (B.steps + 1);
   const bool ex1 = (1 < B.steps) && B.can_ex[(size_t)c * (B.steps + 1) + 1];
   const int nb = 1 & 1;
@@ -668,14 +916,10 @@ __global__ void __launch_bounds__(kPassThreads) lsm_final(LsmBatch B) {
   const LsmStep& st1 = B.st[(size_t)c * (B.steps + 1) + 1];
   unsigned n_ex = 0;
   double ext = C.put ? 0.0 : __longlong_as_double(0x7FF0000000000000LL);
-  const int64_t base = (int64_t)blockIdx.x * kPathsPerBlock;
-  for (int q = 0; q < kPathsPerThread; ++q) {
-    const int64_t p = base + q * kPassThreads + threadIdx.x;
-    if (p >= B.n) break;
-    double v = (double)V[p];
-    int tp = B.want_delta ? tau[p] : 0;
+  // v: the path's cash flow discounted to date 1; s1: its spot at date 1;
+  // tp: the step its cash flow is paid at
+  auto path_final = [&](double v, double s1, int tp) {
     if (have_beta) {
-      const double s1 = (double)S[p];  // spot at date 1
       const double ex = intrinsic_v<double>(C.put, s1, st1.strike);
       if (ex > 0.0 && ex > continuation(B.degree, beta, s1, st1.inv_strike)) {
         v = ex;
@@ -690,13 +934,34 @@ __global__ void __launch_bounds__(kPassThreads) lsm_final(LsmBatch B) {
     // = +-(K_tp disc^tp -/+ v) / S0 (put / call); no cash flow, no delta.
     double dv = 0.0;
     if (B.want_delta && v > 0.0) {
-      const double D = pow(C.disc, (double)tp);
+      const double D = B.disc_pow[(size_t)c * (B.steps + 1) + tp];
       const double K = st[tp].strike;
       dv = C.put ? -(K * D - v) * C.inv_spot : (K * D + v) * C.inv_spot;
     }
     acc[0] += v;
     acc[1] += v * v;
     acc[2] += dv;
+  };
+  if constexpr (sizeof(T) == 4) {
+    // FP32 store: four consecutive paths per thread (padding paths carry
+    // V = 0 and an out-of-the-money spot); payment steps from the flag rows
+    const int64_t q = (int64_t)blockIdx.x * kPassThreads + threadIdx.x;
+    const float4 v4 = reinterpret_cast<const float4*>(V)[q];
+    const float4 s4 = have_beta ? reinterpret_cast<const float4*>(S)[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+    int tp[4] = {0, 0, 0, 0};
+    if (B.want_delta) first_exercise_dates(B, c, q, tp);
+    path_final(v4.x, s4.x, tp[0]);
+    path_final(v4.y, s4.y, tp[1]);
+    path_final(v4.z, s4.z, tp[2]);
+    path_final(v4.w, s4.w, tp[3]);
+  } else {
+    const int32_t* tau = B.tau + (size_t)c * B.npad;
+    const int64_t base = (int64_t)blockIdx.x * kPathsPerBlock;
+    for (int q = 0; q < kPathsPerThread; ++q) {
+      const int64_t p = base + q * kPassThreads + threadIdx.x;
+      if (p >= B.n) break;
+      path_final((double)V[p], have_beta ? (double)S[p] : 0.0, B.want_delta ? tau[p] : 0);
+    }
   }
   if (B.track && have_beta) record_exercise(B, c, 1, C.put, n_ex, ext);  // block-uniform condition
   double* part = B.partials + ((size_t)c * B.blocks + blockIdx.x) * kMaxMoments;
@@ -873,7 +1138,11 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
   // device buffers: path store, cash flows, and one auxiliary block
   void *dS = nullptr, *dVal = nullptr, *dAux = nullptr, *dInj = nullptr;
   OF_TRY(of_scratch(ctx, SLOT_LSM_PATHS, (size_t)nc * per, &dS));
-  OF_TRY(of_scratch(ctx, SLOT_LSM_VALUES, (size_t)nc * npad * (esz + sizeof(int32_t)), &dVal));
+  // after the cash flows: payment steps (FP64 mode) or the per-date exercise
+  // flag rows (FP32 mode), for the delta
+  const size_t aux_values = fp64 ? (size_t)nc * npad * sizeof(int32_t)
+                                 : (size_t)nc * (size_t)(steps + 1) * (size_t)(npad / 32) * sizeof(uint32_t);
+  OF_TRY(of_scratch(ctx, SLOT_LSM_VALUES, (size_t)nc * npad * esz + aux_values, &dVal));
   size_t off = 0;
   auto take = [&off](size_t bytes) {
     const size_t o = off;
@@ -893,6 +1162,8 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
   const size_t o_exb = take(ns * sizeof(unsigned long long));
   const size_t o_itm = take(ns * sizeof(double));
   const size_t o_term = take((size_t)nc * sizeof(unsigned long long));
+  const size_t o_dpow = take(ns * sizeof(double));
+  const size_t o_status = take(sizeof(uint32_t));
   std::vector<size_t> o_lv((size_t)nc * 4, 0);
   for (int c = 0; c < nc; ++c) {
     const size_t nk = hs[(size_t)c].lv_k.size(), nv = hs[(size_t)c].lv_v.size();
@@ -918,16 +1189,23 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
   B.ex_bits = (unsigned long long*)(a + o_exb);
   B.itm_count = (double*)(a + o_itm);
   B.term_itm = (unsigned long long*)(a + o_term);
+  double* dDpow = (double*)(a + o_dpow);
+  B.disc_pow = dDpow;
+  B.status = (uint32_t*)(a + o_status);
   // host images of the tables (the device pointers of the grids go into LsmC)
   std::vector<LsmC> hc((size_t)nc);
   std::vector<uint8_t> can(ns);
   std::vector<LsmStep> st(ns);
+  std::vector<double> dpow(ns);
   std::vector<std::vector<float>> lvf((size_t)nc * 2);
   for (int c = 0; c < nc; ++c) {
     LsmHost& h = hs[(size_t)c];
     LsmC C = h.C;
     std::copy(h.can.begin(), h.can.end(), can.begin() + (size_t)c * (steps + 1));
     std::copy(h.st.begin(), h.st.end(), st.begin() + (size_t)c * (steps + 1));
+    double* dp = dpow.data() + (size_t)c * (steps + 1);
+    dp[0] = 1.0;
+    for (int64_t k = 1; k <= steps; ++k) dp[k] = dp[k - 1] * h.C.disc;
     if (!h.lv_k.empty()) {
       C.lv_k = (const double*)(a + o_lv[(size_t)c * 4 + 0]);
       C.lv_v = (const double*)(a + o_lv[(size_t)c * 4 + 1]);
@@ -950,9 +1228,11 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
   OF_CUDA_TRY(ctx, cudaMemcpyAsync(dC, hc.data(), hc.size() * sizeof(LsmC), cudaMemcpyHostToDevice, ctx->stream));
   OF_CUDA_TRY(ctx, cudaMemcpyAsync(dCan, can.data(), ns, cudaMemcpyHostToDevice, ctx->stream));
   OF_CUDA_TRY(ctx, cudaMemcpyAsync(dSt, st.data(), ns * sizeof(LsmStep), cudaMemcpyHostToDevice, ctx->stream));
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(dDpow, dpow.data(), ns * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   OF_CUDA_TRY(ctx, cudaMemsetAsync(B.beta_ok, 0, (size_t)nc * 2 * sizeof(int32_t), ctx->stream));
   OF_CUDA_TRY(ctx, cudaMemsetAsync(B.regress_count, 0, (size_t)nc * sizeof(int32_t), ctx->stream));
   OF_CUDA_TRY(ctx, cudaMemsetAsync(B.counters, 0, (size_t)nc * sizeof(uint32_t), ctx->stream));
+  OF_CUDA_TRY(ctx, cudaMemsetAsync(B.status, 0, sizeof(uint32_t), ctx->stream));
   std::vector<unsigned long long> bits0(track ? ns : 0);
   if (track) {
     for (int c = 0; c < nc; ++c)  // identity of max (put) / min (call) over positive doubles
@@ -978,7 +1258,8 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
   B.npad = npad;
   B.S = dS;
   B.V = dVal;
-  B.tau = (int32_t*)((char*)dVal + (size_t)nc * npad * esz);
+  B.tau = fp64 ? (int32_t*)((char*)dVal + (size_t)nc * npad * esz) : nullptr;
+  B.exflags = fp64 ? nullptr : (uint32_t*)((char*)dVal + (size_t)nc * npad * esz);
   B.blocks = blocks;
   B.degree = cfg->basis_degree;
   B.want_delta = cfg->want_delta;
@@ -995,14 +1276,19 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
     lsm_gen_ref<<<dim3((unsigned)((chunks + 127) / 128), nc), 128, 0, ctx->stream>>>(B);
   } else {
     const int64_t quads = npad / 4;
-    lsm_gen_philox<<<dim3((unsigned)((quads + 255) / 256), nc), 256, 0, ctx->stream>>>(B);
+    const int dyn = hs[0].C.dynamics;
+    for (const LsmHost& h : hs)
+      if (h.C.dynamics != dyn) return of_fail(ctx, OF_ERR_INVALID_INPUT, "an LSM batch mixes path dynamics");
+    void (*gen)(LsmBatch) = dyn == DYN_HESTON ? lsm_gen_philox<DYN_HESTON>
+                            : dyn == DYN_LOCAL_VOL ? lsm_gen_philox<DYN_LOCAL_VOL> : lsm_gen_philox<DYN_GBM>;
+    gen<<<dim3((unsigned)((quads + 255) / 256), nc), 256, 0, ctx->stream>>>(B);
   }
   OF_CUDA_TRY(ctx, cudaGetLastError());
   const dim3 grid((unsigned)blocks, nc);
   // The passes: one wave of resident blocks over the whole batch, each block
   // striding over its contract's chunks.
   void (*pass)(LsmBatch, int) = fp64 ? (B.degree == 2 ? lsm_pass<double, 2> : lsm_pass<double, 3>)
-                                     : (B.degree == 2 ? lsm_pass<float, 2> : lsm_pass<float, 3>);
+                                     : (B.degree == 2 ? lsm_pass_f32<2> : lsm_pass_f32<3>);
   const int bps = std::max(1, of_blocks_per_sm((const void*)pass, kPassThreads, 0));
   const int64_t wave = (int64_t)ctx->sm_count * bps;
   // Blocks per contract: floor(k wave / nc) fills exactly k waves up to the
@@ -1032,6 +1318,8 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
                                    ctx->stream));
   OF_CUDA_TRY(ctx, cudaMemcpyAsync(regs.data(), B.regress_count, regs.size() * sizeof(int32_t),
                                    cudaMemcpyDeviceToHost, ctx->stream));
+  uint32_t status = 0;
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(&status, B.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
   std::vector<unsigned long long> hcnt(track ? ns : 0), hbits(track ? ns : 0), hterm(track ? (size_t)nc : 0);
   std::vector<double> hitm(track ? ns : 0);
   if (track) {
@@ -1042,6 +1330,7 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
   }
   OF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   OF_CUDA_TRY(ctx, cudaEventElapsedTime(ms_out, ctx->ev_start, ctx->ev_stop));
+  if (status) return of_fail(ctx, OF_ERR_TIMEOUT, "LSM pass: a bulk copy into shared memory did not complete in time");
   if (track) {
     track->assign((size_t)nc, LsmTrack{});
     for (int c = 0; c < nc; ++c) {
@@ -1084,7 +1373,6 @@ extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_
 
   const size_t esz = fp64 ? sizeof(double) : sizeof(float);
   const int64_t npad = (N + kPathsPerBlock - 1) / kPathsPerBlock * kPathsPerBlock;
-  const int blocks = (int)(npad / kPathsPerBlock);
   // Contracts sharing a step count go through the date loop together, in
   // batches bounded by a path-store budget.
   const size_t budget = (size_t)24 << 30;

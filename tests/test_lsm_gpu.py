@@ -115,6 +115,24 @@ def test_fp32_and_fp64_modes_agree_statistically(orc):
     assert abs(a.price - b.price) <= 4 * math.hypot(a.stderr, b.stderr) + 0.01
 
 
+def test_fp32_flag_row_delta_agrees_with_fp64_payment_steps():
+    """The FP32 mode takes each path's payment step from per-date exercise
+    flag rows, the FP64 mode from a per-path array: on independent draws the
+    two deltas agree statistically, for a put and a call, with padding paths
+    (n not a multiple of the 1024-path chunk) and a batch of two contracts."""
+    n = (1 << 18) + 333
+    items = [(VanillaOption.american_put(40.0, 1.0), Market.builder().spot(38.0).rate(0.06).flat_vol(0.3).build()),
+             (VanillaOption.american_call(40.0, 1.0),
+              Market.builder().spot(42.0).rate(0.03).dividend_yield(0.08).flat_vol(0.3).build())]
+    d32 = LongstaffSchwartzEngine(n, 50, 3).with_precision(Precision.Fp32Philox).price_batch(items, with_delta=True)
+    d64 = LongstaffSchwartzEngine(n, 50, 4).price_batch(items, with_delta=True)
+    for a, b in zip(d32, d64):
+        # delta per path is bounded by S_tau/S0 (~1.5); its SE at n paths is below 2e-3
+        assert abs(a.greeks.delta - b.greeks.delta) < 0.01, (a.greeks.delta, b.greeks.delta)
+        assert abs(a.price - b.price) <= 4 * math.hypot(a.stderr, b.stderr) + 0.01
+    assert d32[0].greeks.delta < -0.3 and d32[1].greeks.delta > 0.3
+
+
 def test_lsm_validation_messages():
     m = Market.builder().spot(40.0).rate(0.06).flat_vol(0.2).build()
     with pytest.raises(PricingError, match="num_steps must be >= 2 for Longstaff-Schwartz"):
