@@ -29,7 +29,9 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNIT_FLAGS = {
     "mc_reference.cu": ["--fmad=false"],
     "greeks_reference.cu": ["--fmad=false"],
-    "lsm.cu": ["--fmad=false"],
+    # FP64 mode: no contraction.  The single-precision flags (flush to zero,
+    # approximate sqrt and divide) touch only the FP32 Philox mode.
+    "lsm.cu": ["--fmad=false", "-ftz=true", "-prec-sqrt=false", "-prec-div=false"],
     "qmc.cu": ["--fmad=false"],
     "mc_philox.cu": ["-use_fast_math"],
     # explicit fmaf only, so the forward pass and the backward-sweep recompute

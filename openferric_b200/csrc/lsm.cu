@@ -24,7 +24,9 @@
 // matrix powers of the (linear) xoshiro state transition.
 // FP32 Philox mode: counter-based normals, FP32 path store.
 //
-// Compiled with --fmad=false; FP32 code uses explicit fmaf.
+// Compiled with --fmad=false (FP32 code uses explicit fmaf) and with the
+// single-precision-only flags -ftz=true -prec-sqrt=false -prec-div=false,
+// which leave the FP64 reference mode untouched.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -306,9 +308,11 @@ __global__ void __launch_bounds__(128) lsm_gen_ref(LsmBatch B) {
 
 // FP32 Philox generator: 4 consecutive paths per thread, float4 stores.  The
 // dynamics are a template parameter and the time loop walks whole counter
-// blocks, so each step reads its Philox word without a select: draw t of a
-// path is word t%4 of counter block t/4; Heston's (z1, z2) of step t are words
-// 2(t%2), 2(t%2)+1 of counter block t/2.  A batch holds one dynamics kind.
+// blocks, so each step reads its Philox words without a select.  Normals come
+// in Box-Muller pairs: GBM and local vol take steps t, t+1 (t even) from words
+// (0,1) or (2,3) of counter block t/4; Heston's (z1, z2) of step t are the pair
+// of words 2(t%2), 2(t%2)+1 of counter block t/2.  A batch holds one dynamics
+// kind.
 template <int DYN>
 __global__ void __launch_bounds__(256, DYN == DYN_GBM ? 4 : 2) lsm_gen_philox(const __grid_constant__ LsmBatch B) {
   constexpr int kStepsPerBlock = DYN == DYN_HESTON ? 2 : 4;
@@ -341,6 +345,7 @@ __global__ void __launch_bounds__(256, DYN == DYN_GBM ? 4 : 2) lsm_gen_philox(co
 #pragma unroll
       for (int q = 0; q < 4; ++q)
         r[q] = of::philox4x32_10(make_uint4(blk, (uint32_t)(p0 + q), cid, kLsmStreamTag), B.keys);
+      float2 zp[4];  // Box-Muller pair of words (0,1) or (2,3) of the counter block
 #pragma unroll
       for (int k = 0; k < kStepsPerBlock; ++k) {
         const int t = tb + k;
@@ -351,16 +356,20 @@ __global__ void __launch_bounds__(256, DYN == DYN_GBM ? 4 : 2) lsm_gen_philox(co
         for (int q = 0; q < 4; ++q) {
           const uint32_t* w = &r[q].x;
           if (DYN == DYN_HESTON) {
-            of::heston_euler_step(L[q], C.hc, of::normal_from_u32(w[2 * k]), of::normal_from_u32(w[2 * k + 1]));
-          } else if (DYN == DYN_GBM) {
-            L[q].y = fmaf(C.fstep_vol, of::normal_from_u32(w[k]), L[q].y + C.fdrift);
+            const float2 z = of::normal_pair_from_u32(w[2 * k], w[2 * k + 1]);
+            of::heston_euler_step(L[q], C.hc, z.x, z.y);
           } else {
-            const float z = of::normal_from_u32(w[k]);
-            const LsmStep& e = st[t + 1];
-            const float sig = lsm_local_vol<float>(C.lv_kf, C.lv_vf, C.lv_nk, e.e0, e.e1, e.few,
-                                                   s[q] > 1.0e-8f ? s[q] : 1.0e-8f);
-            const float y = fmaf(sig * C.fsqrt_dt, z, fmaf(-0.5f * sig * sig, C.fdt, L[q].y + C.fmudt));
-            L[q].y = y > C.fy_floor ? y : C.fy_floor;
+            if ((k & 1) == 0) zp[q] = of::normal_pair_from_u32(w[k], w[k + 1]);
+            const float z = (k & 1) ? zp[q].y : zp[q].x;
+            if (DYN == DYN_GBM) {
+              L[q].y = fmaf(C.fstep_vol, z, L[q].y + C.fdrift);
+            } else {
+              const LsmStep& e = st[t + 1];
+              const float sig = lsm_local_vol<float>(C.lv_kf, C.lv_vf, C.lv_nk, e.e0, e.e1, e.few,
+                                                     s[q] > 1.0e-8f ? s[q] : 1.0e-8f);
+              const float y = fmaf(sig * C.fsqrt_dt, z, fmaf(-0.5f * sig * sig, C.fdt, L[q].y + C.fmudt));
+              L[q].y = y > C.fy_floor ? y : C.fy_floor;
+            }
           }
           s[q] = fspot * __expf(L[q].y);
           o[q] = in[q] ? s[q] : pad;
