@@ -510,7 +510,15 @@ struct BookOpt {
   float s0, strike, barrier_y, rebate, inv_nobs;
   uint32_t stream;
   int32_t div_offset, n_div;  // discrete dividend triggers (GBM), in the shared table
+  int32_t kind;               // BK_*: which step loop the option needs
 };
+
+// Step loops of the book.  GBM options without dividends and without a
+// geometric-average control variate get a loop that carries only what their
+// payoff reads: nothing per step (vanilla, terminal-only Asian), the barrier
+// test, or the daily-fixing arithmetic sum.  Everything else takes the
+// general loop.
+enum : int32_t { BK_GENERIC = 0, BK_TERMINAL = 1, BK_BARRIER = 2, BK_ASIAN_DAILY = 3 };
 
 // A dividend trigger in log-spot form: after step `step`, a cash dividend
 // sets y = log(max(e^y - a, 0)) with a = D/S0; a proportional one adds
@@ -663,6 +671,94 @@ __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, const 
   }
 }
 
+// The GBM step loop of one sample (and its antithetic twin) for the option
+// kinds BK_TERMINAL, BK_BARRIER and BK_ASIAN_DAILY: the same draws, steps and
+// observations as book_sample<OF_MODEL_GBM, false>, with the option's payoff
+// and flags resolved at compile time instead of tested every step.  Whole
+// Philox counter blocks (four steps) run without a bounds test; the last,
+// partial block follows.
+template <int KIND, bool ANTI>
+__device__ __forceinline__ void book_sample_gbm(const BookOpt& o, uint64_t i, const of::PhiloxKeys& K, float& x,
+                                                float& cvy) {
+  const float drift = o.c.drift, diff = o.c.diff;
+  // barrier test as sg*y >= sg*b: sg = +1 for an up barrier, -1 for a down one
+  const float sg = (o.flags & BF_UP) ? 1.0f : -1.0f, sgb = sg * o.barrier_y;
+  float ya = 0.0f, yb = 0.0f;
+  PathObs oa{0.0f, 0.0f, 0.0f, false}, ob{0.0f, 0.0f, 0.0f, false};
+  if (KIND == BK_BARRIER) oa.hit = ob.hit = 0.0f >= sgb;  // the scan includes path[0]
+  auto add_fixing = [](PathObs& p, float y) {  // Kahan sum of the daily fixings S/S0
+    const float yk = __expf(y) - p.arith_comp;
+    const float t = p.arith_sum + yk;
+    p.arith_comp = (t - p.arith_sum) - yk;
+    p.arith_sum = t;
+  };
+  auto step = [&](float z) {
+    ya = fmaf(diff, z, ya + drift);
+    if (ANTI) yb = fmaf(-diff, z, yb + drift);
+    if (KIND == BK_BARRIER) {
+      oa.hit |= sg * ya >= sgb;
+      if (ANTI) ob.hit |= sg * yb >= sgb;
+    } else if (KIND == BK_ASIAN_DAILY) {
+      add_fixing(oa, ya);
+      if (ANTI) add_fixing(ob, yb);
+    }
+  };
+  const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
+  const int32_t full = o.steps & ~3;
+  for (int32_t j = 0; j < full; j += 4) {
+    const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo, hi, o.stream), K);
+    const float2 p01 = of::normal_pair_from_u32(r.x, r.y), p23 = of::normal_pair_from_u32(r.z, r.w);
+    step(p01.x);
+    step(p01.y);
+    step(p23.x);
+    step(p23.y);
+  }
+  if (full < o.steps) {
+    const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(full >> 2), lo, hi, o.stream), K);
+    const float2 p01 = of::normal_pair_from_u32(r.x, r.y), p23 = of::normal_pair_from_u32(r.z, r.w);
+    step(p01.x);
+    if (full + 1 < o.steps) step(p01.y);
+    if (full + 2 < o.steps) step(p23.x);
+  }
+  book_payoff(o, oa, ya, x, cvy);
+  if (ANTI) {
+    float xb, yb2;
+    book_payoff(o, ob, yb, xb, yb2);
+    x = 0.5f * (x + xb);
+    cvy = 0.5f * (cvy + yb2);
+  }
+}
+
+// One sample of option o: the specialised GBM loop when the option has one,
+// the general loop otherwise.
+__device__ __forceinline__ void book_dispatch(const BookOpt& o, uint64_t i, const BookParams& P, float& x, float& y) {
+  const bool anti = o.flags & BF_ANTI;
+  switch (o.kind) {
+    case BK_TERMINAL:
+      if (anti) book_sample_gbm<BK_TERMINAL, true>(o, i, P.keys, x, y);
+      else book_sample_gbm<BK_TERMINAL, false>(o, i, P.keys, x, y);
+      return;
+    case BK_BARRIER:
+      if (anti) book_sample_gbm<BK_BARRIER, true>(o, i, P.keys, x, y);
+      else book_sample_gbm<BK_BARRIER, false>(o, i, P.keys, x, y);
+      return;
+    case BK_ASIAN_DAILY:
+      if (anti) book_sample_gbm<BK_ASIAN_DAILY, true>(o, i, P.keys, x, y);
+      else book_sample_gbm<BK_ASIAN_DAILY, false>(o, i, P.keys, x, y);
+      return;
+    default:
+      break;
+  }
+  if (o.model == OF_MODEL_GBM) {
+    if (o.n_div) book_sample<OF_MODEL_GBM, true>(o, i, P.keys, P.obs_w, P.divs, x, y);
+    else book_sample<OF_MODEL_GBM, false>(o, i, P.keys, P.obs_w, P.divs, x, y);
+  } else if (o.model == OF_MODEL_HESTON_EULER) {
+    book_sample<OF_MODEL_HESTON_EULER>(o, i, P.keys, P.obs_w, P.divs, x, y);
+  } else {
+    book_sample<OF_MODEL_HESTON_QE>(o, i, P.keys, P.obs_w, P.divs, x, y);
+  }
+}
+
 // Three 256-thread blocks per SM: ptxas's own choice without the hint is 64
 // registers with spills in the step loop.
 __global__ void __launch_bounds__(256, 3) book_kernel(const __grid_constant__ BookParams P) {
@@ -681,13 +777,7 @@ __global__ void __launch_bounds__(256, 3) book_kernel(const __grid_constant__ Bo
       if (local >= tile.count) break;
       const uint64_t i = (uint64_t)(tile.first + local);
       float x, y;
-      if (o.model == OF_MODEL_GBM) {
-        if (o.n_div) book_sample<OF_MODEL_GBM, true>(o, i, P.keys, P.obs_w, P.divs, x, y);
-        else book_sample<OF_MODEL_GBM, false>(o, i, P.keys, P.obs_w, P.divs, x, y);
-      }
-      else if (o.model == OF_MODEL_HESTON_EULER)
-        book_sample<OF_MODEL_HESTON_EULER>(o, i, P.keys, P.obs_w, P.divs, x, y);
-      else book_sample<OF_MODEL_HESTON_QE>(o, i, P.keys, P.obs_w, P.divs, x, y);
+      book_dispatch(o, i, P, x, y);
       acc[0].add(x);
       acc[1].add(x * x);
       acc[2].add(y);
@@ -876,6 +966,12 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
     if (need_geo) f |= BF_NEED_GEO;
     if (asian && !need_arith && !need_geo) f |= BF_TERMINAL_ONLY;
     d.flags = f;
+    d.kind = BK_GENERIC;
+    if (d.model == OF_MODEL_GBM && d.n_div == 0 && !need_geo) {
+      if (b.payoff.kind == OF_PAYOFF_VANILLA || (f & BF_TERMINAL_ONLY)) d.kind = BK_TERMINAL;
+      else if (b.payoff.kind == OF_PAYOFF_BARRIER) d.kind = BK_BARRIER;
+      else if (need_arith && (f & BF_DAILY)) d.kind = BK_ASIAN_DAILY;
+    }
     const int64_t samples = b.antithetic ? (b.num_paths + 1) / 2 : b.num_paths;
     pl->samples[(size_t)o] = samples;
     pl->cv_kind[(size_t)o] = b.control_variate;
