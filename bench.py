@@ -255,6 +255,27 @@ def run_workload(args, local_rank):
                            "block": info["block"],
                            "paths_per_thread": info["paths_per_thread"], "path_steps": info["path_steps"],
                            "options_per_s": args.book_options / (ms / 1e3), "cuda_graph": True}}
+    elif args.workload == "book_se":
+        # options/s with every option priced to SE <= 1e-4 S0: pilot launch,
+        # then launches with the paths each option's pilot SE asks for
+        import time
+        from openferric_b200.book import price_book_to_stderr, synthetic_book
+        book = synthetic_book(4096)[:args.se_options]
+        price_book_to_stderr(book[:8], seed=1)  # warm-up (library load, clocks)
+        times, rounds = [], None
+        for k in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            res, rounds = price_book_to_stderr(book, seed=20261203 + 100 * k)
+            times.append(time.perf_counter() - t0)
+        s = statistics.median(times)
+        ok = sum(1 for e, r in zip(book, res) if r.stderr <= 1e-4 * e.market.spot)
+        ps = sum(r.path_steps for r in rounds)
+        line = {"metric": "options/s at SE<=1e-4*S0", "value": len(book) / s, "unit": "options/s", "n_gpus": 1,
+                "higher_is_better": True, "dtype": "f32", "data": "synthetic", "ms_per_step": s * 1e3,
+                "config": {"workload": f"batched_book_se_{len(book)}", "se_target": "1e-4*S0",
+                           "timing": "wall clock of the whole procedure (pilot + follow-up launches, host planning)",
+                           "options_meeting_target": ok, "path_steps": ps, "path_steps_per_s": ps / s,
+                           "rounds": [r.__dict__ for r in rounds]}}
     else:  # lsm
         from openferric_b200.lsm import LongstaffSchwartzEngine
         rng = np.random.default_rng(20261203)
@@ -289,8 +310,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-greeks", action="store_true", help="skip the adjoint vs FP64-bump comparison")
-    ap.add_argument("--workload", default="strip", choices=["strip", "adjoint", "book", "lsm"],
-                    help="strip is the benchmark line; the others are single-GPU lines for configurations 3-5")
+    ap.add_argument("--workload", default="strip", choices=["strip", "adjoint", "book", "book_se", "lsm"],
+                    help="strip is the benchmark line; the others are single-GPU lines for configurations 3-5 "
+                         "(book_se: the book's options priced to SE <= 1e-4 S0)")
+    ap.add_argument("--se-options", type=int, default=256,
+                    help="book_se workload: the first N options of the synthetic book")
     ap.add_argument("--paths", type=int, default=PATHS,
                     help="paths per strip (profiling a smaller case; the benchmark workload is 2^20)")
     ap.add_argument("--book-options", type=int, default=4096,

@@ -123,6 +123,71 @@ def price_book(entries: Sequence[BookEntry], seed: int, block: int = 0, paths_pe
         plan.close()
 
 
+@dataclass
+class StderrRound:
+    """One book launch of `price_book_to_stderr`: how many options it priced,
+    their total paths and path-steps, and how many met the target."""
+    options: int
+    paths: int
+    path_steps: float
+    converged: int
+
+
+def paths_for_stderr(paths: int, stderr: float, target: float, margin: float = 1.1, granule: int = 256) -> int:
+    """Paths that bring a standard error measured with `paths` down to
+    `target` (stderr scales as paths^-1/2), with a safety margin, rounded up to
+    a multiple of `granule`; never fewer than `paths`."""
+    if not (stderr > target):
+        return paths
+    need = paths * (stderr / target) ** 2 * margin
+    return max(paths, int(math.ceil(need / granule)) * granule)
+
+
+def price_book_to_stderr(entries: Sequence[BookEntry], seed: int, se_rel: float = 1e-4, pilot_paths: int = 8192,
+                         max_rounds: int = 4, device: int = 0):
+    """Prices every entry to a standard error of at most `se_rel` x its spot.
+
+    A pilot launch of the whole book with `pilot_paths` per option estimates
+    each option's standard error; every option above its target is priced
+    again, in one book launch, with the paths `paths_for_stderr` derives from
+    that estimate, and so on until all meet the target or `max_rounds`
+    launches have run.  Each round draws from its own seed (seed + round), and
+    an option's result is the one of its last round.  Returns the results and
+    the rounds."""
+    from dataclasses import replace
+    n = len(entries)
+    cur = [replace(e, num_paths=int(pilot_paths)) for e in entries]
+    results: List[Optional[PricingResult]] = [None] * n
+    pending = list(range(n))
+    rounds: List[StderrRound] = []
+    for r in range(max_rounds):
+        sub = [cur[i] for i in pending]
+        # samples per thread per tile: at most ~2^18 tiles (256 threads each) per launch
+        total = sum(e.num_paths for e in sub)
+        ppt = 4
+        while ppt < 256 and total > (256 * ppt) << 18:
+            ppt *= 2
+        plan = BookPlan(sub, seed + r, block=256, paths_per_thread=ppt, use_graph=False, device=device)
+        try:
+            plan.launch()
+            res = plan.results()
+        finally:
+            plan.close()
+        still = []
+        for i, pr in zip(pending, res):
+            results[i] = pr
+            target = se_rel * entries[i].market.spot
+            if pr.stderr > target:
+                cur[i] = replace(cur[i], num_paths=paths_for_stderr(cur[i].num_paths, pr.stderr, target))
+                still.append(i)
+        rounds.append(StderrRound(len(sub), sum(e.num_paths for e in sub),
+                                  float(sum(e.num_paths * e.num_steps for e in sub)), len(sub) - len(still)))
+        pending = still
+        if not pending:
+            break
+    return results, rounds
+
+
 def synthetic_book(n: int = 4096, seed: int = 20261203, steps_per_year: int = 252, min_log2_paths: int = 14,
                    max_log2_paths: int = 18, variance_reduction: VarianceReduction = VarianceReduction.None_
                    ) -> List[BookEntry]:

@@ -94,3 +94,38 @@ def test_full_book_plan_info():
     plan.close()
     assert info["path_steps"] == pytest.approx(sum(float(e.num_paths) * e.num_steps for e in book))
     assert info["tiles"] > 4096
+
+
+@pytest.mark.parametrize("vr", [VarianceReduction.None_, VarianceReduction.Antithetic])
+def test_specialised_step_loops_match_the_general_loop(vr):
+    """Vanilla, daily-fixing Asian and barrier options take step loops
+    specialised at compile time.  A 0 % proportional dividend (a jump that
+    adds log(1) = 0 to the log-spot) sends the same options through the
+    general loop, which must give the same numbers bit for bit: same draws,
+    same arithmetic."""
+    from dataclasses import replace
+    from openferric_b200 import Market
+    from openferric_b200.market import DividendEvent, DividendSchedule
+    book = synthetic_book(n=18, seed=4, min_log2_paths=11, max_log2_paths=12, variance_reduction=vr)
+    general = []
+    for e in book:
+        m = e.market
+        sched = DividendSchedule.new([DividendEvent.proportional(0.5 * e.instrument.expiry, 0.0)])
+        m2 = (Market.builder().spot(m.spot).rate(m.rate).dividend_yield(m.dividend_yield)
+              .flat_vol(m.vol_for(m.spot, e.instrument.expiry)).dividend_schedule(sched).build())
+        general.append(replace(e, market=m2))
+    a = price_book(book, seed=21)
+    b = price_book(general, seed=21)
+    for e, x, y in zip(book, a, b):
+        assert x.price == y.price and x.stderr == y.stderr, (e.instrument, x.price, y.price)
+
+
+def test_price_book_to_stderr_meets_the_target():
+    from openferric_b200.book import price_book_to_stderr
+    book = synthetic_book(n=12, seed=8, min_log2_paths=10, max_log2_paths=11)
+    res, rounds = price_book_to_stderr(book, seed=3, se_rel=2e-3, pilot_paths=2048)
+    for e, r in zip(book, res):
+        assert r.stderr <= 2e-3 * e.market.spot, (e.instrument, r.stderr)
+    assert rounds[0].options == len(book) and rounds[0].paths == 2048 * len(book)
+    assert sum(r.converged for r in rounds) == len(book)
+    assert all(later.options < earlier.options for earlier, later in zip(rounds, rounds[1:]))
