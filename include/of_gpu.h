@@ -413,6 +413,18 @@ of_status of_lsm_bermudan(of_ctx* ctx, const of_bermudan_contract* contract, con
  * Exposed for tests of the LSM reference stream. */
 of_status of_xoshiro_jump(of_ctx* ctx, uint64_t seed, const uint64_t* draws, int64_t n, uint64_t* states_out);
 
+/* Test of the bounded mbarrier wait the bulk-copy pipelines use (no
+ * reference counterpart).  One block initialises an mbarrier and waits up to
+ * `limit_us` microseconds for a phase:
+ *   arrive != 0: thread 0 arrives first, so the phase completes and the wait
+ *                succeeds;
+ *   arrive == 0: nothing arrives, so the wait runs out and gives up.
+ * *waited_ok receives 1 if the phase completed and 0 if the wait gave up;
+ * *elapsed_us receives the device time the wait took.  The kernel returns
+ * either way and the context stays usable. */
+of_status of_test_bounded_wait(of_ctx* ctx, int32_t arrive, uint32_t limit_us, int32_t* waited_ok,
+                               double* elapsed_us);
+
 /* ---- Heston pathwise adjoint (FP32, checkpointed) ------------------------ */
 typedef struct of_heston_adjoint_params {
   double spot, strike, rate, dividend_yield, expiry;
