@@ -347,7 +347,11 @@ def main():
     gen = of.HestonPathGenerator(of.Heston(**HESTON), S0, T, STEPS)
     df = math.exp(-RATE * T)
     seed = replica_seed(SEED, rank)  # independent replica per GPU
-    plan = StripPlan(gen, of.OptionType.Call, STRIKES, args.paths, seed, df)
+    # tile shape (samples in flight per thread) picked by the native autotuner
+    # on this GPU, before and outside the timed region
+    from openferric_b200 import autotune
+    tile_ilp, tune_ms = autotune.tune_strip(gen, STRIKES, args.paths, reps=5, device=local_rank)
+    plan = StripPlan(gen, of.OptionType.Call, STRIKES, args.paths, seed, df, tile_ilp=tile_ilp)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", local_rank))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
 
@@ -380,12 +384,12 @@ def main():
 
     # End to end through the public API (host wall clock, sync inside each call).
     for _ in range(2):
-        of.price_strike_strip(gen, of.OptionType.Call, STRIKES, args.paths, seed, df)
+        of.price_strike_strip(gen, of.OptionType.Call, STRIKES, args.paths, seed, df, tile_ilp=tile_ilp)
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        e2e_prices = of.price_strike_strip(gen, of.OptionType.Call, STRIKES, args.paths, seed, df)
+        e2e_prices = of.price_strike_strip(gen, of.OptionType.Call, STRIKES, args.paths, seed, df, tile_ilp=tile_ilp)
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s, device=torch.device("cuda", local_rank))
 
@@ -410,7 +414,8 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": dict(CONFIG, parallelism=f"replicas{world}"),
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": dict(CONFIG, parallelism=f"replicas{world}", tile_ilp=tile_ilp,
+                                                          tile_ilp_ms={str(k): v for k, v in tune_ms.items()}),
         "roofline": dict(main_line, bound=bound, traffic=STRIP_DRAM_BYTES, traffic_source=STRIP_DRAM_SOURCE,
                          **{other_name: other_line}),
         "e2e": {"value": world * PATH_STEPS * args.steps / e2e_s, "unit": UNIT,

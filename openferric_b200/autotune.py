@@ -39,13 +39,19 @@ def _load() -> Dict[str, dict]:
         return {}
 
 
-def _store(table: Dict[str, dict]) -> None:
+def _store(table: Dict[str, dict]) -> bool:
+    """Writes the table; False (and the tuning result still returned to the
+    caller) when the cache location is not writable."""
     path = cache_path()
-    os.makedirs(os.path.dirname(path), exist_ok=True)
-    tmp = path + ".tmp"
-    with open(tmp, "w") as f:
-        json.dump(table, f, indent=1, sort_keys=True)
-    os.replace(tmp, path)
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(table, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+        return True
+    except OSError:
+        return False
 
 
 def _device_name(device: int) -> str:

@@ -160,7 +160,9 @@ __device__ __forceinline__ float normal_from_u32(uint32_t r) {
 // u32 -> uniform in (0,1), the same grid as normal_from_u32: (k + 0.5) 2^-23.
 __device__ __forceinline__ float uniform_from_u32(uint32_t r) {
   const float f = __uint_as_float(0x3F800000u | (r >> 9));
-  return (f - 1.0f) + 5.9604644775390625e-8f;
+  // f - (1 - 2^-24) = (2k + 1) 2^-24: one exact subtraction (Sterbenz), the
+  // same value as (f - 1) + 2^-24
+  return f - 0.999999940395355224609375f;
 }
 
 // Two independent standard normals from two u32 draws, Box-Muller transform
