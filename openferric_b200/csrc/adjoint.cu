@@ -102,10 +102,14 @@ __device__ __forceinline__ float qe_vnext(const AdjC& c, float v, const QeDraw& 
   const float s2 = fmaf(v, c.c1, c.c2);
   const float inv_m = __fdividef(1.0f, m);
   const float psi = s2 * inv_m * inv_m;
-  if (psi <= c.sw_lo) return quad_branch(m, psi, d.ubits);
-  if (psi > c.sw_hi) return exp_branch(m, psi, d.u);
-  const float vq = quad_branch(m, psi, d.ubits);
-  const float ve = exp_branch(m, psi, d.u);
+  // each branch inlined once: quadratic below the band's top, exponential
+  // above its bottom, blended inside the band
+  const bool need_q = psi <= c.sw_hi, need_e = psi > c.sw_lo;
+  float vq = 0.0f, ve = 0.0f;
+  if (need_q) vq = quad_branch(m, psi, d.ubits);
+  if (need_e) ve = exp_branch(m, psi, d.u);
+  if (!need_e) return vq;
+  if (!need_q) return ve;
   const float s = (psi - c.sw_lo) * c.sw_inv_width;
   const float w = s * s * fmaf(-2.0f, s, 3.0f);
   return fmaf(w, ve - vq, vq);
@@ -162,20 +166,26 @@ __device__ __forceinline__ StepJac qe_jacobian(const AdjC& c, float v, float vn,
   const float s2 = fmaf(v, c.c1, c.c2);
   const float inv_m = __fdividef(1.0f, m);
   const float psi = s2 * inv_m * inv_m;
-  float A1, A2, vb;
-  if (psi <= c.sw_lo) {
-    quad_jac(m, psi, d.ubits, vb, A1, A2);
-  } else if (psi > c.sw_hi) {
-    exp_jac(m, psi, d.u, vb, A1, A2);
-  } else {
-    float vq, q1, q2, ve, e1, e2;
-    quad_jac(m, psi, d.ubits, vq, q1, q2);
-    exp_jac(m, psi, d.u, ve, e1, e2);
-    const float s = (psi - c.sw_lo) * c.sw_inv_width;
-    const float w = s * s * fmaf(-2.0f, s, 3.0f);
-    const float dw = 6.0f * s * (1.0f - s) * c.sw_inv_width;
-    A1 = fmaf(w, e1 - q1, q1);
-    A2 = fmaf(w, e2 - q2, q2) + (ve - vq) * dw;
+  float A1, A2;
+  {
+    // each branch inlined once, as in qe_vnext
+    const bool need_q = psi <= c.sw_hi, need_e = psi > c.sw_lo;
+    float vq = 0.0f, q1 = 0.0f, q2 = 0.0f, ve = 0.0f, e1 = 0.0f, e2 = 0.0f;
+    if (need_q) quad_jac(m, psi, d.ubits, vq, q1, q2);
+    if (need_e) exp_jac(m, psi, d.u, ve, e1, e2);
+    if (!need_e) {
+      A1 = q1;
+      A2 = q2;
+    } else if (!need_q) {
+      A1 = e1;
+      A2 = e2;
+    } else {
+      const float s = (psi - c.sw_lo) * c.sw_inv_width;
+      const float w = s * s * fmaf(-2.0f, s, 3.0f);
+      const float dw = 6.0f * s * (1.0f - s) * c.sw_inv_width;
+      A1 = fmaf(w, e1 - q1, q1);
+      A2 = fmaf(w, e2 - q2, q2) + (ve - vq) * dw;
+    }
   }
   const float im2 = inv_m * inv_m, tpm = 2.0f * psi * inv_m;
   const float m_v = c.e, m_t = 1.0f - c.e, m_k = (v - c.theta) * c.de_dk;
@@ -277,7 +287,10 @@ __device__ void sweep_path(const AdjC& c, int64_t i, float* sv, float* ss, doubl
     for (int k = (len - 1) & ~1; k >= 0; k -= 2) {
       const int j = j0 + k;
       const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 1), lo, hi, kAdjStreamTag), c.keys);
-#pragma unroll
+      // not unrolled: one copy of the step Jacobian keeps the kernel's code
+      // within the instruction cache (instruction-fetch stalls were the
+      // largest stall with two copies)
+#pragma unroll 1
       for (int o = 1; o >= 0; --o) {
         if (k + o < len) {
           ybar = fmaf(direct, ss[(k + o + 1) * kBwdThreads], ybar);  // y_{j+o+1} enters the average
