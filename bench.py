@@ -49,8 +49,9 @@ SFU_PER_STEP = 5.0
 # DRAM bytes (read + write) of one strip launch from an ncu capture of the
 # kernel at 2^18 paths; the kernel reads no input from HBM, so the figure
 # does not grow with the path count.
-STRIP_DRAM_BYTES = 21248
-STRIP_DRAM_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, strip_kernel at 2^18 paths (size-independent)"
+STRIP_DRAM_BYTES = 31488
+STRIP_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of strip_kernel<ILP=2> at 2^20 paths "
+                     "(the kernel reads no HBM input; the figure does not grow with paths)")
 CONFIG = {"workload": "heston_euler_strike_strip", "paths": PATHS, "steps": STEPS, "strikes": 41,
           "strike_range": [80, 120], "kappa": 2.0, "theta": 0.04, "xi": 0.5, "rho": -0.7, "v0": 0.04, "s0": S0,
           "r": RATE, "q": 0.0, "T": T, "seed": SEED, "rng": "philox4x32-10", "path_dtype": "fp32",
