@@ -1,6 +1,7 @@
 // bulk_copy.cuh - 1-D bulk asynchronous copies (global -> shared) completed on
-// an mbarrier, for sm_90+ (cp.async.bulk, PTX ISA 8.0).  CTA-local only: no
-// cluster multicast, and the sources are this GPU's own memory.
+// an mbarrier, for sm_90+ (cp.async.bulk, PTX ISA 8.0).  Each copy lands in
+// the issuing CTA's own shared memory, and the sources are this GPU's own
+// memory.
 //
 // Every wait is bounded: mbar_wait gives up after `limit_ns` of the global
 // timer and returns false, so a caller can record an error and return instead
