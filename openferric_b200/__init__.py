@@ -11,6 +11,7 @@ from .core import (AsianSpec, Averaging, BarrierDirection, BarrierSpec, BarrierS
 from .engines import (ArithmeticAsianMC, ControlVariate, ControlVariateKind, FastRngKind, Gbm, GbmPathGenerator,
                       Heston, HestonPathGenerator, MonteCarloEngine, MonteCarloPricingEngine, Precision,
                       VarianceReduction, price_strike_strip)
+from .gpu_mc_engine import GpuMcEngine
 from .instruments import AsianOption, BarrierOption, BermudanOption, VanillaOption, daily_fixings
 from .market import DividendEvent, DividendKind, DividendSchedule, Market, MarketBuilder, SampledVolSurface
 
@@ -21,5 +22,5 @@ __all__ = [
     "GbmPathGenerator", "Heston", "HestonPathGenerator", "MonteCarloEngine", "MonteCarloPricingEngine", "Precision",
     "VarianceReduction", "price_strike_strip", "SampledVolSurface", "DividendEvent", "DividendKind",
     "DividendSchedule", "AsianOption", "BarrierOption", "BermudanOption", "VanillaOption",
-    "daily_fixings", "Market", "MarketBuilder",
+    "daily_fixings", "Market", "MarketBuilder", "GpuMcEngine",
 ]
