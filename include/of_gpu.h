@@ -241,6 +241,42 @@ of_status of_book_plan_info(of_book_plan* plan, int32_t* block, int32_t* paths_p
                             int64_t* n_tiles, double* path_steps);
 void of_book_plan_destroy(of_book_plan* plan);
 
+/* ---- book priced to a standard-error target ----------------------------- */
+/* No single reference counterpart: the target is the one the batched-book
+ * metric is quoted at (every option at SE <= 1e-4 x spot), reached with
+ * MonteCarloPricingEngine::price's estimator (src/engines/monte_carlo/mc_engine.rs:875-975). */
+typedef struct of_stderr_target {
+  double se_rel;        /* each option's target: stderr <= se_rel x its model.s0 */
+  int64_t pilot_paths;  /* paths per option in the first launch */
+  int32_t max_rounds;   /* launches at most (1..64) */
+  int32_t reserved0;
+} of_stderr_target;
+
+/* One launch of of_book_price_to_stderr. */
+typedef struct of_stderr_round {
+  int64_t options;    /* options priced in this launch */
+  int64_t paths;      /* their total paths */
+  double path_steps;  /* their total path-steps */
+  int64_t converged;  /* of them, how many met their target */
+} of_stderr_round;
+
+/* A pilot launch prices every entry with target->pilot_paths paths
+ * (entries[i].num_paths is ignored).  Every option above its target is then
+ * priced again, all in one launch.  Its paths are scaled by
+ * (stderr / target)^2 x 1.1 and rounded up to 256.  This repeats until all
+ * meet the target or max_rounds launches have run.
+ * Round r draws with seed cfg->seed + r.  cfg->block and
+ * cfg->paths_per_thread of 0 choose a tile shape with at most ~2^18 tiles per
+ * launch; cfg->use_graph is ignored.
+ * Outputs:
+ *   results[i]   = option i's result from its last launch;
+ *   paths_out[i] = that launch's path count (optional);
+ *   rounds[r]    = round r's statistics (optional, capacity max_rounds);
+ *   *n_rounds    = the launches run. */
+of_status of_book_price_to_stderr(of_ctx* ctx, const of_book_entry* entries, int64_t n, const of_book_config* cfg,
+                                  const of_stderr_target* target, of_mc_result* results, int64_t* paths_out,
+                                  of_stderr_round* rounds, int32_t* n_rounds);
+
 /* ---- tile-shape autotuner ----------------------------------------------- */
 /* The reference has no counterpart (its GPU engine uses one fixed launch
  * shape: WORKGROUP_SIZE 256 and one path per invocation,

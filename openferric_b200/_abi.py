@@ -110,6 +110,24 @@ class OfBookConfig(C.Structure):
     ]
 
 
+class OfStderrTarget(C.Structure):
+    _fields_ = [
+        ("se_rel", C.c_double),
+        ("pilot_paths", C.c_int64),
+        ("max_rounds", C.c_int32),
+        ("reserved0", C.c_int32),
+    ]
+
+
+class OfStderrRound(C.Structure):
+    _fields_ = [
+        ("options", C.c_int64),
+        ("paths", C.c_int64),
+        ("path_steps", C.c_double),
+        ("converged", C.c_int64),
+    ]
+
+
 class OfTuneCandidate(C.Structure):
     _fields_ = [
         ("block", C.c_int32),

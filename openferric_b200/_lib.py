@@ -24,7 +24,7 @@ EXPORTED = [
     "of_book_plan_destroy", "of_mc_european_pathwise_aad", "of_heston_price_delta_aad", "of_mc_greek_estimators",
     "of_lsm_price", "of_xoshiro_jump", "of_heston_price_adjoint", "of_mc_european_gpu", "of_mc_strip_noalloc",
     "of_measure_device_peaks", "of_lsm_bermudan", "of_mc_european_qmc", "of_autotune_strip", "of_autotune_book",
-    "of_test_bounded_wait",
+    "of_test_bounded_wait", "of_book_price_to_stderr",
 ]
 
 
@@ -104,6 +104,9 @@ def _declare(L):
     L.of_autotune_book.restype = C.c_int
     L.of_test_bounded_wait.argtypes = [vp, C.c_int32, C.c_uint32, P(C.c_int32), P(C.c_double)]
     L.of_test_bounded_wait.restype = C.c_int
+    L.of_book_price_to_stderr.argtypes = [vp, P(A.OfBookEntry), C.c_int64, P(A.OfBookConfig), P(A.OfStderrTarget),
+                                          P(A.OfMcResult), P(C.c_int64), P(A.OfStderrRound), P(C.c_int32)]
+    L.of_book_price_to_stderr.restype = C.c_int
     for name in ["of_ctx_create", "of_ctx_set_stream", "of_ctx_get_stream", "of_mc_run", "of_mc_strip",
                  "of_strip_plan_create", "of_strip_plan_launch", "of_strip_plan_results", "of_mc_price_book",
                  "of_book_plan_create", "of_book_plan_launch", "of_book_plan_results", "of_book_plan_info"]:

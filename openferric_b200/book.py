@@ -136,7 +136,9 @@ class StderrRound:
 def paths_for_stderr(paths: int, stderr: float, target: float, margin: float = 1.1, granule: int = 256) -> int:
     """Paths that bring a standard error measured with `paths` down to
     `target` (stderr scales as paths^-1/2), with a safety margin, rounded up to
-    a multiple of `granule`; never fewer than `paths`."""
+    a multiple of `granule`; never fewer than `paths`.  The rule
+    of_book_price_to_stderr applies between rounds (margin 1.1, granule 256),
+    for planning a book's cost on the host."""
     if not (stderr > target):
         return paths
     need = paths * (stderr / target) ** 2 * margin
@@ -145,47 +147,37 @@ def paths_for_stderr(paths: int, stderr: float, target: float, margin: float = 1
 
 def price_book_to_stderr(entries: Sequence[BookEntry], seed: int, se_rel: float = 1e-4, pilot_paths: int = 8192,
                          max_rounds: int = 4, device: int = 0):
-    """Prices every entry to a standard error of at most `se_rel` x its spot.
+    """Prices every entry to a standard error of at most `se_rel` x its spot
+    (of_book_price_to_stderr).
 
     A pilot launch of the whole book with `pilot_paths` per option estimates
     each option's standard error; every option above its target is priced
     again, in one book launch, with the paths `paths_for_stderr` derives from
     that estimate, and so on until all meet the target or `max_rounds`
     launches have run.  Each round draws from its own seed (seed + round), and
-    an option's result is the one of its last round.  Returns the results and
-    the rounds."""
-    from dataclasses import replace
+    an option's result is the one of its last round (its diagnostics carry
+    that round's path count).  Returns the results and the rounds."""
+    ctx = context(device)
     n = len(entries)
-    cur = [replace(e, num_paths=int(pilot_paths)) for e in entries]
-    results: List[Optional[PricingResult]] = [None] * n
-    pending = list(range(n))
-    rounds: List[StderrRound] = []
-    for r in range(max_rounds):
-        sub = [cur[i] for i in pending]
-        # samples per thread per tile: at most ~2^18 tiles (256 threads each) per launch
-        total = sum(e.num_paths for e in sub)
-        ppt = 4
-        while ppt < 256 and total > (256 * ppt) << 18:
-            ppt *= 2
-        plan = BookPlan(sub, seed + r, block=256, paths_per_thread=ppt, use_graph=False, device=device)
-        try:
-            plan.launch()
-            res = plan.results()
-        finally:
-            plan.close()
-        still = []
-        for i, pr in zip(pending, res):
-            results[i] = pr
-            target = se_rel * entries[i].market.spot
-            if pr.stderr > target:
-                cur[i] = replace(cur[i], num_paths=paths_for_stderr(cur[i].num_paths, pr.stderr, target))
-                still.append(i)
-        rounds.append(StderrRound(len(sub), sum(e.num_paths for e in sub),
-                                  float(sum(e.num_paths * e.num_steps for e in sub)), len(sub) - len(still)))
-        pending = still
-        if not pending:
-            break
-    return results, rounds
+    arr, keep, vols = book_entries_abi(entries)
+    cfg = A.OfBookConfig(seed=int(seed) & 0xFFFFFFFFFFFFFFFF)
+    tgt = A.OfStderrTarget(se_rel=float(se_rel), pilot_paths=int(pilot_paths), max_rounds=int(max_rounds))
+    out = (A.OfMcResult * n)()
+    paths = (C.c_int64 * n)()
+    rounds = (A.OfStderrRound * max(1, int(max_rounds)))()
+    n_rounds = C.c_int32()
+    with ctx.lock:
+        ctx.check(ctx._L.of_book_price_to_stderr(ctx.handle, arr, n, C.byref(cfg), C.byref(tgt), out, paths, rounds,
+                                                 C.byref(n_rounds)))
+    del keep
+    results = []
+    for e, r, p, vol in zip(entries, out, paths, vols):
+        d = Diagnostics()
+        d.insert("num_paths", float(p))
+        d.insert("num_steps", float(e.num_steps))
+        d.insert("vol", vol)
+        results.append(PricingResult(price=r.price, stderr=r.stderr_, diagnostics=d))
+    return results, [StderrRound(rd.options, rd.paths, rd.path_steps, rd.converged) for rd in rounds[:n_rounds.value]]
 
 
 def synthetic_book(n: int = 4096, seed: int = 20261203, steps_per_year: int = 252, min_log2_paths: int = 14,

@@ -49,6 +49,8 @@ STRUCTS = {
     "of_adjoint_result": A.OfAdjointResult,
     "of_device_peaks": A.OfDevicePeaks,
     "of_tune_candidate": A.OfTuneCandidate,
+    "of_stderr_target": A.OfStderrTarget,
+    "of_stderr_round": A.OfStderrRound,
     "of_bermudan_contract": A.OfBermudanContract,
     "of_boundary_point": A.OfBoundaryPoint,
     "of_qmc_params": A.OfQmcParams,

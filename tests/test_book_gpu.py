@@ -129,3 +129,9 @@ def test_price_book_to_stderr_meets_the_target():
     assert rounds[0].options == len(book) and rounds[0].paths == 2048 * len(book)
     assert sum(r.converged for r in rounds) == len(book)
     assert all(later.options < earlier.options for earlier, later in zip(rounds, rounds[1:]))
+    for r in res:  # each result's path count: the pilot's, or a larger multiple of 256
+        p = int(r.diagnostics.get("num_paths"))
+        assert p >= 2048 and p % 256 == 0
+    from openferric_b200 import PricingError
+    with pytest.raises(PricingError, match="max_rounds"):
+        price_book_to_stderr(book, seed=3, max_rounds=0)
