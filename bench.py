@@ -46,9 +46,16 @@ PATH_STEPS = float(PATHS) * STEPS
 # xor, ~20 instructions per step) use neither pipe's budget in this count.
 FLOPS_PER_STEP = 24.0
 SFU_PER_STEP = 5.0
+# Issued thread instructions per path-step of the strip kernel, Philox
+# included, from ncu captures (smsp__inst_executed.sum x 32 / path-steps) of
+# the bench's kernel at 2^20 paths, by samples in flight per thread.  With the
+# sampled SM clock they give the issue fraction: warp instructions per second
+# over 148 SMs x 4 schedulers x 1 instruction per cycle.
+INSTR_PER_STEP = {1: 51.8, 2: 47.8}
+INSTR_SOURCE = "ncu smsp__inst_executed.sum of strip_kernel at 2^20 paths (profiles/strip_kernel_heston_euler_*)"
 # DRAM bytes (read + write) of one strip launch from an ncu capture of the
-# kernel at 2^18 paths; the kernel reads no input from HBM, so the figure
-# does not grow with the path count.
+# kernel; the kernel reads no input from HBM, so the figure does not grow
+# with the path count.
 STRIP_DRAM_BYTES = 31488
 STRIP_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of strip_kernel<ILP=2> at 2^20 paths "
                      "(the kernel reads no HBM input; the figure does not grow with paths)")
@@ -412,13 +419,22 @@ def main():
                                f"{148 * 16 * sm_max * 1e6 / 1e12:.2f} TOP/s at 16/clk/SM"}
     bound, main_line, other_name, other_line = (
         ("sfu", sfu_line, "fp32", fp32_line) if sfu_frac >= fp32_frac else ("fp32", fp32_line, "sfu", sfu_line))
+    # issue slots: Philox, conversions and control flow included
+    sm_run = clk.get("sm_mhz") or sm_max
+    ips = INSTR_PER_STEP.get(tile_ilp, INSTR_PER_STEP[1])
+    issue_peak = 148 * 4 * sm_run * 1e6
+    issue_line = {"achieved": per_gpu * ips / 32.0 / 1e12, "peak": issue_peak / 1e12, "unit": "T warp-inst/s",
+                  "frac": per_gpu * ips / 32.0 / issue_peak, "per_step": ips,
+                  "peak_source": f"148 SMs x 4 schedulers x 1 warp instruction per cycle at the sampled "
+                                 f"{sm_run:.0f} MHz",
+                  "per_step_source": INSTR_SOURCE}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": dict(CONFIG, parallelism=f"replicas{world}", tile_ilp=tile_ilp,
                                                           tile_ilp_ms={str(k): v for k, v in tune_ms.items()}),
         "roofline": dict(main_line, bound=bound, traffic=STRIP_DRAM_BYTES, traffic_source=STRIP_DRAM_SOURCE,
-                         **{other_name: other_line}),
+                         issue=issue_line, **{other_name: other_line}),
         "e2e": {"value": world * PATH_STEPS * args.steps / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": 41 * 4, "d2h_bytes_per_step": 41 * 2 * 8},
         "gpu_launches": 2 * args.steps,
