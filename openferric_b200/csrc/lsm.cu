@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -1130,170 +1131,267 @@ void fill_steps(LsmHost& h, int64_t steps, double expiry, const double* strike_o
   }
 }
 
-// Generation, the backward passes and the final reduction for contracts that
-// share a step count; results[c] = {price, stderr, delta}.
-of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, const of_lsm_config* cfg,
-                        const uint64_t* jump, uint32_t contract_base, const double* inj_host, int draws,
-                        std::vector<LsmTrack>* track, std::vector<double>& results, std::vector<int32_t>& regs,
-                        float* ms_out) {
+// Offsets of a run's tables in its auxiliary device block.
+struct DevOffsets {
+  size_t part = 0, beta = 0, res = 0, c = 0, ok = 0, reg = 0, cnt = 0, can = 0, st = 0, exc = 0, exb = 0, itm = 0,
+         term = 0, dpow = 0, status = 0;
+};
+
+// One batch of contracts sharing a step count, staged for an asynchronous
+// run on one of two device buffer sets: pinned host images of its tables
+// (uploaded when enqueued) and of its results (read back when enqueued, used
+// once the streams have drained).
+struct LsmRun {
+  std::vector<LsmHost> hs;
+  int64_t steps = 0;
+  uint32_t contract_base = 0;
+  const double* inj_host = nullptr;  // injected normals (FP64 test hook), or null
+  int draws = 1;
+  bool track = false;
+  std::vector<int64_t> index;  // the caller's contract of each batch slot (of_lsm_price)
+  LsmBatch B{};
+  DevOffsets dev;
+  void* d_inj = nullptr;
+  char* pin = nullptr;  // pinned staging, laid out by the o_* offsets
+  size_t o_hc = 0, o_can = 0, o_st = 0, o_dpow = 0, o_bits0 = 0, o_res = 0, o_reg = 0, o_status = 0, o_cnt = 0,
+         o_bits = 0, o_itm = 0, o_term = 0;
+  std::vector<size_t> o_lvh;  // [nc][4] staging offsets of the local-vol arrays
+  std::vector<size_t> o_lvd;  // [nc][4] their offsets in the auxiliary device block
+  size_t aux_bytes = 0, path_bytes = 0, value_bytes = 0;
+  cudaEvent_t gen_done = nullptr, done = nullptr;
+  LsmRun() = default;
+  LsmRun(const LsmRun&) = delete;
+  LsmRun& operator=(const LsmRun&) = delete;
+  ~LsmRun() {
+    if (pin) cudaFreeHost(pin);
+    if (gen_done) cudaEventDestroy(gen_done);
+    if (done) cudaEventDestroy(done);
+  }
+  int nc() const { return (int)hs.size(); }
+  size_t ns() const { return (size_t)nc() * (size_t)(steps + 1); }
+};
+
+// Sizes of a run's device buffers, the layout of its auxiliary block and the
+// scalar fields of its LsmBatch.
+void lsm_layout(LsmRun& r, const of_lsm_config* cfg) {
   const bool fp64 = cfg->precision == OF_PREC_FP64_REFERENCE;
   const int64_t N = cfg->num_paths;
   const size_t esz = fp64 ? sizeof(double) : sizeof(float);
   const int64_t npad = (N + kPathsPerBlock - 1) / kPathsPerBlock * kPathsPerBlock;
   const int blocks = (int)(npad / kPathsPerBlock);
-  const int nc = (int)hs.size();
-  const size_t per = (size_t)steps * npad * esz;
-  const size_t ns = (size_t)nc * (size_t)(steps + 1);
-  // device buffers: path store, cash flows, and one auxiliary block
-  void *dS = nullptr, *dVal = nullptr, *dAux = nullptr, *dInj = nullptr;
-  OF_TRY(of_scratch(ctx, SLOT_LSM_PATHS, (size_t)nc * per, &dS));
+  const int nc = r.nc();
+  const size_t ns = r.ns();
+  r.path_bytes = (size_t)nc * (size_t)r.steps * npad * esz;
   // after the cash flows: payment steps (FP64 mode) or the per-date exercise
   // flag rows (FP32 mode), for the delta
   const size_t aux_values = fp64 ? (size_t)nc * npad * sizeof(int32_t)
-                                 : (size_t)nc * (size_t)(steps + 1) * (size_t)(npad / 32) * sizeof(uint32_t);
-  OF_TRY(of_scratch(ctx, SLOT_LSM_VALUES, (size_t)nc * npad * esz + aux_values, &dVal));
+                                 : (size_t)nc * (size_t)(r.steps + 1) * (size_t)(npad / 32) * sizeof(uint32_t);
+  r.value_bytes = (size_t)nc * npad * esz + aux_values;
   size_t off = 0;
   auto take = [&off](size_t bytes) {
     const size_t o = off;
     off = (off + bytes + 255) & ~(size_t)255;
     return o;
   };
-  const size_t o_part = take((size_t)nc * blocks * kMaxMoments * sizeof(double));
-  const size_t o_beta = take((size_t)nc * 8 * sizeof(double));
-  const size_t o_res = take((size_t)nc * 3 * sizeof(double));
-  const size_t o_c = take((size_t)nc * sizeof(LsmC));
-  const size_t o_ok = take((size_t)nc * 2 * sizeof(int32_t));
-  const size_t o_reg = take((size_t)nc * sizeof(int32_t));
-  const size_t o_cnt = take((size_t)nc * sizeof(uint32_t));
-  const size_t o_can = take(ns);
-  const size_t o_st = take(ns * sizeof(LsmStep));
-  const size_t o_exc = take(ns * sizeof(unsigned long long));
-  const size_t o_exb = take(ns * sizeof(unsigned long long));
-  const size_t o_itm = take(ns * sizeof(double));
-  const size_t o_term = take((size_t)nc * sizeof(unsigned long long));
-  const size_t o_dpow = take(ns * sizeof(double));
-  const size_t o_status = take(sizeof(uint32_t));
-  std::vector<size_t> o_lv((size_t)nc * 4, 0);
+  DevOffsets& d = r.dev;
+  d.part = take((size_t)nc * blocks * kMaxMoments * sizeof(double));
+  d.beta = take((size_t)nc * 8 * sizeof(double));
+  d.res = take((size_t)nc * 3 * sizeof(double));
+  d.c = take((size_t)nc * sizeof(LsmC));
+  d.ok = take((size_t)nc * 2 * sizeof(int32_t));
+  d.reg = take((size_t)nc * sizeof(int32_t));
+  d.cnt = take((size_t)nc * sizeof(uint32_t));
+  d.can = take(ns);
+  d.st = take(ns * sizeof(LsmStep));
+  d.exc = take(ns * sizeof(unsigned long long));
+  d.exb = take(ns * sizeof(unsigned long long));
+  d.itm = take(ns * sizeof(double));
+  d.term = take((size_t)nc * sizeof(unsigned long long));
+  d.dpow = take(ns * sizeof(double));
+  d.status = take(sizeof(uint32_t));
+  r.o_lvd.assign((size_t)nc * 4, 0);
   for (int c = 0; c < nc; ++c) {
-    const size_t nk = hs[(size_t)c].lv_k.size(), nv = hs[(size_t)c].lv_v.size();
+    const size_t nk = r.hs[(size_t)c].lv_k.size(), nv = r.hs[(size_t)c].lv_v.size();
     if (!nk) continue;
-    o_lv[(size_t)c * 4 + 0] = take(nk * sizeof(double));
-    o_lv[(size_t)c * 4 + 1] = take(nv * sizeof(double));
-    o_lv[(size_t)c * 4 + 2] = take(nk * sizeof(float));
-    o_lv[(size_t)c * 4 + 3] = take(nv * sizeof(float));
+    r.o_lvd[(size_t)c * 4 + 0] = take(nk * sizeof(double));
+    r.o_lvd[(size_t)c * 4 + 1] = take(nv * sizeof(double));
+    r.o_lvd[(size_t)c * 4 + 2] = take(nk * sizeof(float));
+    r.o_lvd[(size_t)c * 4 + 3] = take(nv * sizeof(float));
   }
-  OF_TRY(of_scratch(ctx, SLOT_LSM_AUX, off, &dAux));
-  char* a = (char*)dAux;
-  LsmBatch B{};
-  B.partials = (double*)(a + o_part);
-  B.betas = (double*)(a + o_beta);
-  B.results = (double*)(a + o_res);
-  LsmC* dC = (LsmC*)(a + o_c);
-  B.beta_ok = (int32_t*)(a + o_ok);
-  B.regress_count = (int32_t*)(a + o_reg);
-  B.counters = (uint32_t*)(a + o_cnt);
-  uint8_t* dCan = (uint8_t*)(a + o_can);
-  LsmStep* dSt = (LsmStep*)(a + o_st);
-  B.ex_count = (unsigned long long*)(a + o_exc);
-  B.ex_bits = (unsigned long long*)(a + o_exb);
-  B.itm_count = (double*)(a + o_itm);
-  B.term_itm = (unsigned long long*)(a + o_term);
-  double* dDpow = (double*)(a + o_dpow);
-  B.disc_pow = dDpow;
-  B.status = (uint32_t*)(a + o_status);
-  // host images of the tables (the device pointers of the grids go into LsmC)
-  std::vector<LsmC> hc((size_t)nc);
-  std::vector<uint8_t> can(ns);
-  std::vector<LsmStep> st(ns);
-  std::vector<double> dpow(ns);
-  std::vector<std::vector<float>> lvf((size_t)nc * 2);
-  for (int c = 0; c < nc; ++c) {
-    LsmHost& h = hs[(size_t)c];
-    LsmC C = h.C;
-    std::copy(h.can.begin(), h.can.end(), can.begin() + (size_t)c * (steps + 1));
-    std::copy(h.st.begin(), h.st.end(), st.begin() + (size_t)c * (steps + 1));
-    double* dp = dpow.data() + (size_t)c * (steps + 1);
-    dp[0] = 1.0;
-    for (int64_t k = 1; k <= steps; ++k) dp[k] = dp[k - 1] * h.C.disc;
-    if (!h.lv_k.empty()) {
-      C.lv_k = (const double*)(a + o_lv[(size_t)c * 4 + 0]);
-      C.lv_v = (const double*)(a + o_lv[(size_t)c * 4 + 1]);
-      C.lv_kf = (const float*)(a + o_lv[(size_t)c * 4 + 2]);
-      C.lv_vf = (const float*)(a + o_lv[(size_t)c * 4 + 3]);
-      C.lv_nk = (int32_t)h.lv_k.size();
-      lvf[(size_t)c * 2].assign(h.lv_k.begin(), h.lv_k.end());
-      lvf[(size_t)c * 2 + 1].assign(h.lv_v.begin(), h.lv_v.end());
-      OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)C.lv_k, h.lv_k.data(), h.lv_k.size() * sizeof(double),
-                                       cudaMemcpyHostToDevice, ctx->stream));
-      OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)C.lv_v, h.lv_v.data(), h.lv_v.size() * sizeof(double),
-                                       cudaMemcpyHostToDevice, ctx->stream));
-      OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)C.lv_kf, lvf[(size_t)c * 2].data(), h.lv_k.size() * sizeof(float),
-                                       cudaMemcpyHostToDevice, ctx->stream));
-      OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)C.lv_vf, lvf[(size_t)c * 2 + 1].data(), h.lv_v.size() * sizeof(float),
-                                       cudaMemcpyHostToDevice, ctx->stream));
-    }
-    hc[(size_t)c] = C;
-  }
-  OF_CUDA_TRY(ctx, cudaMemcpyAsync(dC, hc.data(), hc.size() * sizeof(LsmC), cudaMemcpyHostToDevice, ctx->stream));
-  OF_CUDA_TRY(ctx, cudaMemcpyAsync(dCan, can.data(), ns, cudaMemcpyHostToDevice, ctx->stream));
-  OF_CUDA_TRY(ctx, cudaMemcpyAsync(dSt, st.data(), ns * sizeof(LsmStep), cudaMemcpyHostToDevice, ctx->stream));
-  OF_CUDA_TRY(ctx, cudaMemcpyAsync(dDpow, dpow.data(), ns * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  OF_CUDA_TRY(ctx, cudaMemsetAsync(B.beta_ok, 0, (size_t)nc * 2 * sizeof(int32_t), ctx->stream));
-  OF_CUDA_TRY(ctx, cudaMemsetAsync(B.regress_count, 0, (size_t)nc * sizeof(int32_t), ctx->stream));
-  OF_CUDA_TRY(ctx, cudaMemsetAsync(B.counters, 0, (size_t)nc * sizeof(uint32_t), ctx->stream));
-  OF_CUDA_TRY(ctx, cudaMemsetAsync(B.status, 0, sizeof(uint32_t), ctx->stream));
-  std::vector<unsigned long long> bits0(track ? ns : 0);
-  if (track) {
-    for (int c = 0; c < nc; ++c)  // identity of max (put) / min (call) over positive doubles
-      std::fill(bits0.begin() + (size_t)c * (steps + 1), bits0.begin() + (size_t)(c + 1) * (steps + 1),
-                hs[(size_t)c].C.put ? 0ULL : 0x7FF0000000000000ULL);
-    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.ex_count, 0, ns * sizeof(unsigned long long), ctx->stream));
-    OF_CUDA_TRY(ctx, cudaMemcpyAsync(B.ex_bits, bits0.data(), ns * sizeof(unsigned long long),
-                                     cudaMemcpyHostToDevice, ctx->stream));
-    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.itm_count, 0, ns * sizeof(double), ctx->stream));
-    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.term_itm, 0, (size_t)nc * sizeof(unsigned long long), ctx->stream));
-  }
-  if (inj_host) {
-    const size_t cnt = (size_t)N * steps * draws;
-    OF_TRY(of_scratch(ctx, SLOT_INJECT, cnt * sizeof(double), &dInj));
-    OF_CUDA_TRY(ctx, cudaMemcpyAsync(dInj, inj_host, cnt * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  }
-  B.c = dC;
-  B.can_ex = dCan;
-  B.st = dSt;
+  r.aux_bytes = off;
+  LsmBatch& B = r.B;
   B.nc = nc;
-  B.steps = (int32_t)steps;
+  B.steps = (int32_t)r.steps;
   B.n = N;
   B.npad = npad;
-  B.S = dS;
-  B.V = dVal;
-  B.tau = fp64 ? (int32_t*)((char*)dVal + (size_t)nc * npad * esz) : nullptr;
-  B.exflags = fp64 ? nullptr : (uint32_t*)((char*)dVal + (size_t)nc * npad * esz);
   B.blocks = blocks;
   B.degree = cfg->basis_degree;
   B.want_delta = cfg->want_delta;
-  B.track = track ? 1 : 0;
+  B.track = r.track ? 1 : 0;
   B.seed = cfg->seed;
   B.keys = of::philox_keys(cfg->seed);
-  B.contract_base = contract_base;
-  B.inj = (const double*)dInj;
-  B.jump = jump;
+  B.contract_base = r.contract_base;
   B.chunk = 8;
-  OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+}
+
+// Points a laid-out run at its device buffers, fills its pinned staging and
+// creates its events.
+of_status lsm_bind(of_ctx* ctx, LsmRun& r, const of_lsm_config* cfg, void* dS, void* dVal, void* dAux,
+                   const uint64_t* jump) {
+  const bool fp64 = cfg->precision == OF_PREC_FP64_REFERENCE;
+  const size_t esz = fp64 ? sizeof(double) : sizeof(float);
+  const int nc = r.nc();
+  const size_t ns = r.ns();
+  const int dyn = r.hs[0].C.dynamics;
+  for (const LsmHost& h : r.hs)
+    if (h.C.dynamics != dyn) return of_fail(ctx, OF_ERR_INVALID_INPUT, "an LSM batch mixes path dynamics");
+  LsmBatch& B = r.B;
+  char* a = (char*)dAux;
+  const DevOffsets& d = r.dev;
+  B.partials = (double*)(a + d.part);
+  B.betas = (double*)(a + d.beta);
+  B.results = (double*)(a + d.res);
+  B.c = (const LsmC*)(a + d.c);
+  B.beta_ok = (int32_t*)(a + d.ok);
+  B.regress_count = (int32_t*)(a + d.reg);
+  B.counters = (uint32_t*)(a + d.cnt);
+  B.can_ex = (const uint8_t*)(a + d.can);
+  B.st = (const LsmStep*)(a + d.st);
+  B.ex_count = (unsigned long long*)(a + d.exc);
+  B.ex_bits = (unsigned long long*)(a + d.exb);
+  B.itm_count = (double*)(a + d.itm);
+  B.term_itm = (unsigned long long*)(a + d.term);
+  B.disc_pow = (const double*)(a + d.dpow);
+  B.status = (uint32_t*)(a + d.status);
+  B.S = dS;
+  B.V = dVal;
+  B.tau = fp64 ? (int32_t*)((char*)dVal + (size_t)nc * B.npad * esz) : nullptr;
+  B.exflags = fp64 ? nullptr : (uint32_t*)((char*)dVal + (size_t)nc * B.npad * esz);
+  B.jump = jump;
+  size_t off = 0;
+  auto take = [&off](size_t bytes) {
+    const size_t o = off;
+    off = (off + bytes + 15) & ~(size_t)15;
+    return o;
+  };
+  r.o_hc = take((size_t)nc * sizeof(LsmC));
+  r.o_can = take(ns);
+  r.o_st = take(ns * sizeof(LsmStep));
+  r.o_dpow = take(ns * sizeof(double));
+  r.o_bits0 = take(r.track ? ns * sizeof(unsigned long long) : 0);
+  r.o_lvh.assign((size_t)nc * 4, 0);
+  for (int c = 0; c < nc; ++c) {
+    const size_t nk = r.hs[(size_t)c].lv_k.size(), nv = r.hs[(size_t)c].lv_v.size();
+    if (!nk) continue;
+    r.o_lvh[(size_t)c * 4 + 0] = take(nk * sizeof(double));
+    r.o_lvh[(size_t)c * 4 + 1] = take(nv * sizeof(double));
+    r.o_lvh[(size_t)c * 4 + 2] = take(nk * sizeof(float));
+    r.o_lvh[(size_t)c * 4 + 3] = take(nv * sizeof(float));
+  }
+  r.o_res = take((size_t)nc * 3 * sizeof(double));
+  r.o_reg = take((size_t)nc * sizeof(int32_t));
+  r.o_status = take(sizeof(uint32_t));
+  r.o_cnt = take(r.track ? ns * sizeof(unsigned long long) : 0);
+  r.o_bits = take(r.track ? ns * sizeof(unsigned long long) : 0);
+  r.o_itm = take(r.track ? ns * sizeof(double) : 0);
+  r.o_term = take(r.track ? (size_t)nc * sizeof(unsigned long long) : 0);
+  if (cudaMallocHost(&r.pin, off) != cudaSuccess) {
+    r.pin = nullptr;
+    return of_fail(ctx, OF_ERR_ALLOC, "LSM staging allocation failed");
+  }
+  LsmC* hc = (LsmC*)(r.pin + r.o_hc);
+  uint8_t* can = (uint8_t*)(r.pin + r.o_can);
+  LsmStep* st = (LsmStep*)(r.pin + r.o_st);
+  double* dpow = (double*)(r.pin + r.o_dpow);
+  for (int c = 0; c < nc; ++c) {
+    const LsmHost& h = r.hs[(size_t)c];
+    LsmC C = h.C;
+    std::copy(h.can.begin(), h.can.end(), can + (size_t)c * (r.steps + 1));
+    std::copy(h.st.begin(), h.st.end(), st + (size_t)c * (r.steps + 1));
+    double* dp = dpow + (size_t)c * (r.steps + 1);
+    dp[0] = 1.0;
+    for (int64_t k = 1; k <= r.steps; ++k) dp[k] = dp[k - 1] * h.C.disc;
+    if (!h.lv_k.empty()) {
+      C.lv_k = (const double*)(a + r.o_lvd[(size_t)c * 4 + 0]);
+      C.lv_v = (const double*)(a + r.o_lvd[(size_t)c * 4 + 1]);
+      C.lv_kf = (const float*)(a + r.o_lvd[(size_t)c * 4 + 2]);
+      C.lv_vf = (const float*)(a + r.o_lvd[(size_t)c * 4 + 3]);
+      C.lv_nk = (int32_t)h.lv_k.size();
+      std::copy(h.lv_k.begin(), h.lv_k.end(), (double*)(r.pin + r.o_lvh[(size_t)c * 4 + 0]));
+      std::copy(h.lv_v.begin(), h.lv_v.end(), (double*)(r.pin + r.o_lvh[(size_t)c * 4 + 1]));
+      std::copy(h.lv_k.begin(), h.lv_k.end(), (float*)(r.pin + r.o_lvh[(size_t)c * 4 + 2]));
+      std::copy(h.lv_v.begin(), h.lv_v.end(), (float*)(r.pin + r.o_lvh[(size_t)c * 4 + 3]));
+    }
+    hc[c] = C;
+  }
+  if (r.track) {
+    unsigned long long* bits0 = (unsigned long long*)(r.pin + r.o_bits0);
+    for (int c = 0; c < nc; ++c)  // identity of max (put) / min (call) over positive doubles
+      std::fill(bits0 + (size_t)c * (r.steps + 1), bits0 + (size_t)(c + 1) * (r.steps + 1),
+                r.hs[(size_t)c].C.put ? 0ULL : 0x7FF0000000000000ULL);
+  }
+  if (cudaEventCreateWithFlags(&r.gen_done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming) != cudaSuccess)
+    return of_fail(ctx, OF_ERR_CUDA, "LSM event creation failed");
+  return OF_OK;
+}
+
+// Enqueues a bound run: its tables, the path generation and the `gen_done`
+// event on `gs`; on `ms`, after `gen_done`, the passes, the final kernel, the
+// readback of the results into the pinned staging and the `done` event.
+of_status lsm_enqueue(of_ctx* ctx, LsmRun& r, const of_lsm_config* cfg, cudaStream_t gs, cudaStream_t ms) {
+  const bool fp64 = cfg->precision == OF_PREC_FP64_REFERENCE;
+  const int nc = r.nc();
+  const size_t ns = r.ns();
+  LsmBatch& B = r.B;
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)B.c, r.pin + r.o_hc, (size_t)nc * sizeof(LsmC), cudaMemcpyHostToDevice, gs));
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)B.can_ex, r.pin + r.o_can, ns, cudaMemcpyHostToDevice, gs));
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)B.st, r.pin + r.o_st, ns * sizeof(LsmStep), cudaMemcpyHostToDevice, gs));
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)B.disc_pow, r.pin + r.o_dpow, ns * sizeof(double), cudaMemcpyHostToDevice,
+                                   gs));
+  const LsmC* hc = (const LsmC*)(r.pin + r.o_hc);
+  for (int c = 0; c < nc; ++c) {
+    const LsmHost& h = r.hs[(size_t)c];
+    if (h.lv_k.empty()) continue;
+    const size_t nk = h.lv_k.size(), nv = h.lv_v.size();
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)hc[c].lv_k, r.pin + r.o_lvh[(size_t)c * 4 + 0], nk * sizeof(double),
+                                     cudaMemcpyHostToDevice, gs));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)hc[c].lv_v, r.pin + r.o_lvh[(size_t)c * 4 + 1], nv * sizeof(double),
+                                     cudaMemcpyHostToDevice, gs));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)hc[c].lv_kf, r.pin + r.o_lvh[(size_t)c * 4 + 2], nk * sizeof(float),
+                                     cudaMemcpyHostToDevice, gs));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync((void*)hc[c].lv_vf, r.pin + r.o_lvh[(size_t)c * 4 + 3], nv * sizeof(float),
+                                     cudaMemcpyHostToDevice, gs));
+  }
+  OF_CUDA_TRY(ctx, cudaMemsetAsync(B.beta_ok, 0, (size_t)nc * 2 * sizeof(int32_t), gs));
+  OF_CUDA_TRY(ctx, cudaMemsetAsync(B.regress_count, 0, (size_t)nc * sizeof(int32_t), gs));
+  OF_CUDA_TRY(ctx, cudaMemsetAsync(B.counters, 0, (size_t)nc * sizeof(uint32_t), gs));
+  OF_CUDA_TRY(ctx, cudaMemsetAsync(B.status, 0, sizeof(uint32_t), gs));
+  if (r.track) {
+    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.ex_count, 0, ns * sizeof(unsigned long long), gs));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(B.ex_bits, r.pin + r.o_bits0, ns * sizeof(unsigned long long),
+                                     cudaMemcpyHostToDevice, gs));
+    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.itm_count, 0, ns * sizeof(double), gs));
+    OF_CUDA_TRY(ctx, cudaMemsetAsync(B.term_itm, 0, (size_t)nc * sizeof(unsigned long long), gs));
+  }
+  if (r.inj_host) {
+    const size_t cnt = (size_t)B.n * r.steps * r.draws;
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(r.d_inj, r.inj_host, cnt * sizeof(double), cudaMemcpyHostToDevice, gs));
+    B.inj = (const double*)r.d_inj;
+  }
   if (fp64) {
-    const int64_t chunks = (N + B.chunk - 1) / B.chunk;
-    lsm_gen_ref<<<dim3((unsigned)((chunks + 127) / 128), nc), 128, 0, ctx->stream>>>(B);
+    const int64_t chunks = (B.n + B.chunk - 1) / B.chunk;
+    lsm_gen_ref<<<dim3((unsigned)((chunks + 127) / 128), nc), 128, 0, gs>>>(B);
   } else {
-    const int64_t quads = npad / 4;
-    const int dyn = hs[0].C.dynamics;
-    for (const LsmHost& h : hs)
-      if (h.C.dynamics != dyn) return of_fail(ctx, OF_ERR_INVALID_INPUT, "an LSM batch mixes path dynamics");
+    const int64_t quads = B.npad / 4;
+    const int dyn = r.hs[0].C.dynamics;
     void (*gen)(LsmBatch) = dyn == DYN_HESTON ? lsm_gen_philox<DYN_HESTON>
                             : dyn == DYN_LOCAL_VOL ? lsm_gen_philox<DYN_LOCAL_VOL> : lsm_gen_philox<DYN_GBM>;
-    gen<<<dim3((unsigned)((quads + 255) / 256), nc), 256, 0, ctx->stream>>>(B);
+    gen<<<dim3((unsigned)((quads + 255) / 256), nc), 256, 0, gs>>>(B);
   }
   OF_CUDA_TRY(ctx, cudaGetLastError());
-  const dim3 grid((unsigned)blocks, nc);
+  OF_CUDA_TRY(ctx, cudaEventRecord(r.gen_done, gs));
+  OF_CUDA_TRY(ctx, cudaStreamWaitEvent(ms, r.gen_done, 0));
   // The passes: one wave of resident blocks over the whole batch, each block
   // striding over its contract's chunks.
   void (*pass)(LsmBatch, int) = fp64 ? (B.degree == 2 ? lsm_pass<double, 2> : lsm_pass<double, 3>)
@@ -1306,52 +1404,107 @@ of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, co
   int64_t pass_blocks = 1;
   double best = 0.0;
   for (int k = 1; k <= 8; ++k) {
-    const int64_t bpc = std::max<int64_t>(1, std::min<int64_t>(blocks, k * wave / nc));
+    const int64_t bpc = std::max<int64_t>(1, std::min<int64_t>(B.blocks, k * wave / nc));
     const int64_t total = bpc * nc, waves = (total + wave - 1) / wave;
     const double fill = (double)total / (double)(waves * wave);
     if (fill > best + 1e-9) {
       best = fill;
       pass_blocks = bpc;
     }
-    if (fill >= 0.95 || bpc == blocks) break;
+    if (fill >= 0.95 || bpc == B.blocks) break;
   }
   const dim3 pgrid((unsigned)pass_blocks, nc);
-  for (int t = (int)steps - 1; t >= 1; --t) pass<<<pgrid, kPassThreads, 0, ctx->stream>>>(B, t);
-  if (fp64) lsm_final<double><<<grid, kPassThreads, 0, ctx->stream>>>(B);
-  else lsm_final<float><<<grid, kPassThreads, 0, ctx->stream>>>(B);
+  for (int t = (int)r.steps - 1; t >= 1; --t) pass<<<pgrid, kPassThreads, 0, ms>>>(B, t);
+  const dim3 grid((unsigned)B.blocks, nc);
+  if (fp64) lsm_final<double><<<grid, kPassThreads, 0, ms>>>(B);
+  else lsm_final<float><<<grid, kPassThreads, 0, ms>>>(B);
   OF_CUDA_TRY(ctx, cudaGetLastError());
-  OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
-  results.assign((size_t)nc * 3, 0.0);
-  regs.assign((size_t)nc, 0);
-  OF_CUDA_TRY(ctx, cudaMemcpyAsync(results.data(), B.results, results.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                                   ctx->stream));
-  OF_CUDA_TRY(ctx, cudaMemcpyAsync(regs.data(), B.regress_count, regs.size() * sizeof(int32_t),
-                                   cudaMemcpyDeviceToHost, ctx->stream));
-  uint32_t status = 0;
-  OF_CUDA_TRY(ctx, cudaMemcpyAsync(&status, B.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
-  std::vector<unsigned long long> hcnt(track ? ns : 0), hbits(track ? ns : 0), hterm(track ? (size_t)nc : 0);
-  std::vector<double> hitm(track ? ns : 0);
-  if (track) {
-    OF_CUDA_TRY(ctx, cudaMemcpyAsync(hcnt.data(), B.ex_count, ns * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    OF_CUDA_TRY(ctx, cudaMemcpyAsync(hbits.data(), B.ex_bits, ns * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    OF_CUDA_TRY(ctx, cudaMemcpyAsync(hitm.data(), B.itm_count, ns * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    OF_CUDA_TRY(ctx, cudaMemcpyAsync(hterm.data(), B.term_itm, (size_t)nc * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(r.pin + r.o_res, B.results, (size_t)nc * 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                                   ms));
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(r.pin + r.o_reg, B.regress_count, (size_t)nc * sizeof(int32_t),
+                                   cudaMemcpyDeviceToHost, ms));
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(r.pin + r.o_status, B.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, ms));
+  if (r.track) {
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(r.pin + r.o_cnt, B.ex_count, ns * 8, cudaMemcpyDeviceToHost, ms));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(r.pin + r.o_bits, B.ex_bits, ns * 8, cudaMemcpyDeviceToHost, ms));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(r.pin + r.o_itm, B.itm_count, ns * 8, cudaMemcpyDeviceToHost, ms));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(r.pin + r.o_term, B.term_itm, (size_t)nc * 8, cudaMemcpyDeviceToHost, ms));
   }
-  OF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-  OF_CUDA_TRY(ctx, cudaEventElapsedTime(ms_out, ctx->ev_start, ctx->ev_stop));
-  if (status) return of_fail(ctx, OF_ERR_TIMEOUT, "LSM pass: a bulk copy into shared memory did not complete in time");
-  if (track) {
+  OF_CUDA_TRY(ctx, cudaEventRecord(r.done, ms));
+  return OF_OK;
+}
+
+// Results of a run whose streams have drained: {price, stderr, delta} per
+// contract, the regression counts and, when tracked, the boundary statistics.
+of_status lsm_collect(of_ctx* ctx, const LsmRun& r, std::vector<double>& results, std::vector<int32_t>& regs,
+                      std::vector<LsmTrack>* track) {
+  const int nc = r.nc();
+  if (*(const uint32_t*)(r.pin + r.o_status))
+    return of_fail(ctx, OF_ERR_TIMEOUT, "LSM pass: a bulk copy into shared memory did not complete in time");
+  const double* hres = (const double*)(r.pin + r.o_res);
+  const int32_t* hreg = (const int32_t*)(r.pin + r.o_reg);
+  results.assign(hres, hres + (size_t)nc * 3);
+  regs.assign(hreg, hreg + nc);
+  if (track && r.track) {
+    const unsigned long long* hcnt = (const unsigned long long*)(r.pin + r.o_cnt);
+    const unsigned long long* hbits = (const unsigned long long*)(r.pin + r.o_bits);
+    const double* hitm = (const double*)(r.pin + r.o_itm);
+    const unsigned long long* hterm = (const unsigned long long*)(r.pin + r.o_term);
     track->assign((size_t)nc, LsmTrack{});
     for (int c = 0; c < nc; ++c) {
       LsmTrack& tr = (*track)[(size_t)c];
-      const size_t b = (size_t)c * (steps + 1), e = b + (size_t)steps + 1;
-      tr.ex_count.assign(hcnt.begin() + b, hcnt.begin() + e);
-      tr.ex_bits.assign(hbits.begin() + b, hbits.begin() + e);
-      tr.itm.assign(hitm.begin() + b, hitm.begin() + e);
-      tr.term_itm = hterm[(size_t)c];
+      const size_t b = (size_t)c * (r.steps + 1), e = b + (size_t)r.steps + 1;
+      tr.ex_count.assign(hcnt + b, hcnt + e);
+      tr.ex_bits.assign(hbits + b, hbits + e);
+      tr.itm.assign(hitm + b, hitm + e);
+      tr.term_itm = hterm[c];
     }
   }
   return OF_OK;
+}
+
+// The context's lowest-priority stream, created on first use.
+of_status lsm_side_stream(of_ctx* ctx, cudaStream_t* out) {
+  if (!ctx->side_stream) {
+    int least = 0, greatest = 0;
+    OF_CUDA_TRY(ctx, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    OF_CUDA_TRY(ctx, cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, least));
+  }
+  *out = ctx->side_stream;
+  return OF_OK;
+}
+
+// Generation, the backward passes and the final reduction for contracts that
+// share a step count, run synchronously on the context stream and buffer set
+// 0; results[c] = {price, stderr, delta}.
+of_status lsm_run_batch(of_ctx* ctx, std::vector<LsmHost>& hs, int64_t steps, const of_lsm_config* cfg,
+                        const uint64_t* jump, uint32_t contract_base, const double* inj_host, int draws,
+                        std::vector<LsmTrack>* track, std::vector<double>& results, std::vector<int32_t>& regs,
+                        float* ms_out) {
+  LsmRun r;
+  r.hs = hs;
+  r.steps = steps;
+  r.contract_base = contract_base;
+  r.inj_host = inj_host;
+  r.draws = draws;
+  r.track = track != nullptr;
+  lsm_layout(r, cfg);
+  void *dS = nullptr, *dVal = nullptr, *dAux = nullptr;
+  OF_TRY(of_scratch(ctx, SLOT_LSM_PATHS, r.path_bytes, &dS));
+  OF_TRY(of_scratch(ctx, SLOT_LSM_VALUES, r.value_bytes, &dVal));
+  OF_TRY(of_scratch(ctx, SLOT_LSM_AUX, r.aux_bytes, &dAux));
+  if (inj_host)
+    OF_TRY(of_scratch(ctx, SLOT_INJECT, (size_t)cfg->num_paths * steps * draws * sizeof(double), &r.d_inj));
+  OF_TRY(lsm_bind(ctx, r, cfg, dS, dVal, dAux, jump));
+  OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+  const of_status st = lsm_enqueue(ctx, r, cfg, ctx->stream, ctx->stream);
+  if (st == OF_OK) OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+  // drain before the staging goes away, error or not
+  const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  OF_TRY(st);
+  if (e != cudaSuccess) return of_fail(ctx, OF_ERR_CUDA, "LSM run failed: %s", cudaGetErrorString(e));
+  OF_CUDA_TRY(ctx, cudaEventElapsedTime(ms_out, ctx->ev_start, ctx->ev_stop));
+  return lsm_collect(ctx, r, results, regs, track);
 }
 
 }  // namespace
@@ -1392,7 +1545,7 @@ extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_
   std::vector<int64_t> inj_off((size_t)n, 0);
   for (int64_t i = 1; i < n; ++i) inj_off[(size_t)i] = inj_off[(size_t)i - 1] + N * ks[i - 1].num_steps;
 
-  float total_ms = 0.0f;
+  std::vector<std::unique_ptr<LsmRun>> runs;
   size_t pos = 0;
   while (pos < order.size()) {
     // trivial contracts (expiry == 0): intrinsic, stderr 0 (longstaff_schwartz.rs:440-447)
@@ -1448,15 +1601,72 @@ extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_
         ce[steps] = 1;
       }
     }
-    std::vector<double> hres;
-    std::vector<int32_t> hreg;
-    float ms = 0.0f;
-    OF_TRY(lsm_run_batch(ctx, hs, steps, cfg, jump, (uint32_t)batch[0],
-                         cfg->injected_normals ? cfg->injected_normals + inj_off[(size_t)batch[0]] : nullptr, 1,
-                         nullptr, hres, hreg, &ms));
-    total_ms += ms;
-    for (int c = 0; c < nc; ++c) {
-      of_lsm_result& r = res[batch[(size_t)c]];
+    std::unique_ptr<LsmRun> run(new LsmRun());
+    run->hs.swap(hs);
+    run->steps = steps;
+    run->contract_base = (uint32_t)batch[0];
+    run->inj_host = cfg->injected_normals ? cfg->injected_normals + inj_off[(size_t)batch[0]] : nullptr;
+    run->index = batch;
+    runs.push_back(std::move(run));
+  }
+  if (runs.empty()) return OF_OK;
+  // Two device buffer sets alternate: batch i generates into set i % 2 on the
+  // lowest-priority side stream (compute-bound, little HBM traffic) while
+  // batch i-1 runs its passes (HBM-bound) on the context stream.  Each set is
+  // sized for the largest of its batches before anything is enqueued.
+  const int sets = runs.size() > 1 ? 2 : 1;
+  const int slots[2][3] = {{SLOT_LSM_PATHS, SLOT_LSM_VALUES, SLOT_LSM_AUX},
+                           {SLOT_LSM_PATHS_B, SLOT_LSM_VALUES_B, SLOT_LSM_AUX_B}};
+  size_t need[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  size_t inj_need = 0;
+  for (size_t i = 0; i < runs.size(); ++i) {
+    LsmRun& r = *runs[i];
+    lsm_layout(r, cfg);
+    size_t* nd = need[i % 2];
+    nd[0] = std::max(nd[0], r.path_bytes);
+    nd[1] = std::max(nd[1], r.value_bytes);
+    nd[2] = std::max(nd[2], r.aux_bytes);
+    if (r.inj_host) inj_need = std::max(inj_need, (size_t)N * r.steps * sizeof(double));
+  }
+  void* dbuf[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  for (int s = 0; s < sets; ++s)
+    for (int k = 0; k < 3; ++k) OF_TRY(of_scratch(ctx, slots[s][k], need[s][k], &dbuf[s][k]));
+  void* d_inj = nullptr;
+  if (inj_need) OF_TRY(of_scratch(ctx, SLOT_INJECT, inj_need, &d_inj));  // fed by the side stream, in order
+  for (size_t i = 0; i < runs.size(); ++i) {
+    runs[i]->d_inj = d_inj;
+    const int s = (int)(i % 2);
+    OF_TRY(lsm_bind(ctx, *runs[i], cfg, dbuf[s][0], dbuf[s][1], dbuf[s][2], jump));
+  }
+  const cudaStream_t ms = ctx->stream;
+  cudaStream_t gs = ms;
+  if (sets == 2) OF_TRY(lsm_side_stream(ctx, &gs));
+  of_status st = OF_OK;
+  if (cudaEventRecord(ctx->ev_start, ms) != cudaSuccess ||
+      (gs != ms && cudaStreamWaitEvent(gs, ctx->ev_start, 0) != cudaSuccess))
+    st = of_fail(ctx, OF_ERR_CUDA, "LSM stream set-up failed");
+  for (size_t i = 0; i < runs.size() && st == OF_OK; ++i) {
+    // set i % 2 was last used by batch i-2: its passes, final kernel and readback
+    if (i >= 2 && cudaStreamWaitEvent(gs, runs[i - 2]->done, 0) != cudaSuccess)
+      st = of_fail(ctx, OF_ERR_CUDA, "LSM stream wait failed");
+    if (st == OF_OK) st = lsm_enqueue(ctx, *runs[i], cfg, gs, ms);
+  }
+  if (st == OF_OK && cudaEventRecord(ctx->ev_stop, ms) != cudaSuccess)
+    st = of_fail(ctx, OF_ERR_CUDA, "LSM stream set-up failed");
+  // drain both streams before the staging buffers go away, error or not
+  const cudaError_t e1 = cudaStreamSynchronize(ms);
+  const cudaError_t e2 = gs != ms ? cudaStreamSynchronize(gs) : cudaSuccess;
+  OF_TRY(st);
+  if (e1 != cudaSuccess || e2 != cudaSuccess)
+    return of_fail(ctx, OF_ERR_CUDA, "LSM run failed: %s", cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+  float total_ms = 0.0f;
+  OF_CUDA_TRY(ctx, cudaEventElapsedTime(&total_ms, ctx->ev_start, ctx->ev_stop));
+  std::vector<double> hres;
+  std::vector<int32_t> hreg;
+  for (const std::unique_ptr<LsmRun>& run : runs) {
+    OF_TRY(lsm_collect(ctx, *run, hres, hreg, nullptr));
+    for (int c = 0; c < run->nc(); ++c) {
+      of_lsm_result& r = res[run->index[(size_t)c]];
       r.price = hres[(size_t)c * 3];
       r.stderr_ = hres[(size_t)c * 3 + 1];
       r.delta = cfg->want_delta ? hres[(size_t)c * 3 + 2] : 0.0;

@@ -22,8 +22,9 @@ of_status of_scratch(of_ctx* ctx, int slot, size_t bytes, void** out) {
   if (bytes == 0) bytes = 16;
   if (ctx->slot_bytes[slot] < bytes) {
     if (ctx->slot_ptr[slot]) {
-      // The stream may still use the old buffer.
+      // The streams may still use the old buffer.
       OF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+      if (ctx->side_stream) OF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->side_stream));
       OF_CUDA_TRY(ctx, cudaFree(ctx->slot_ptr[slot]));
       ctx->slot_ptr[slot] = nullptr;
       ctx->slot_bytes[slot] = 0;
@@ -150,7 +151,11 @@ of_status of_ctx_create(int device, of_ctx** out) {
   if (device < 0 || device >= n) return OF_ERR_INVALID_INPUT;
   of_ctx* ctx = new of_ctx();
   ctx->device = device;
-  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+  // the context stream at the highest priority: work that overlaps it on the
+  // side stream (LSM path generation) yields to it
+  int least = 0, greatest = 0;
+  if (cudaSetDevice(device) != cudaSuccess || cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&ctx->own_stream, cudaStreamNonBlocking, greatest) != cudaSuccess ||
       cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev_stop) != cudaSuccess) {
     of_ctx_destroy(ctx);
     return OF_ERR_CUDA;
@@ -166,6 +171,10 @@ void of_ctx_destroy(of_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->side_stream) {
+    cudaStreamSynchronize(ctx->side_stream);
+    cudaStreamDestroy(ctx->side_stream);
+  }
   for (int i = 0; i < SLOT_COUNT; ++i)
     if (ctx->slot_ptr[i]) cudaFree(ctx->slot_ptr[i]);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);

@@ -31,7 +31,10 @@ enum OfSlot {
   SLOT_STATUS = 13,    // device error word + counters
   SLOT_MISC = 14,
   SLOT_JUMP = 15,      // xoshiro256++ GF(2) jump tables
-  SLOT_COUNT = 16
+  SLOT_LSM_PATHS_B = 16,   // second LSM buffer set: the next batch generates into it
+  SLOT_LSM_VALUES_B = 17,  // while the current one runs its passes
+  SLOT_LSM_AUX_B = 18,
+  SLOT_COUNT = 19
 };
 
 struct of_ctx {
@@ -40,6 +43,7 @@ struct of_ctx {
   int max_threads_per_sm = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  cudaStream_t side_stream = nullptr;  // lowest priority; created on first use (LSM path generation)
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   void* slot_ptr[SLOT_COUNT] = {};
   size_t slot_bytes[SLOT_COUNT] = {};
