@@ -45,7 +45,7 @@ def _store(table: Dict[str, dict]) -> bool:
     path = cache_path()
     try:
         os.makedirs(os.path.dirname(path), exist_ok=True)
-        tmp = path + ".tmp"
+        tmp = f"{path}.{os.getpid()}.tmp"  # one per process: ranks of a job may write at once
         with open(tmp, "w") as f:
             json.dump(table, f, indent=1, sort_keys=True)
         os.replace(tmp, path)
