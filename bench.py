@@ -185,6 +185,31 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def fp64_strip_check(paths, strip_prices):
+    """The strip's FP32 Philox prices against the FP64 engine on the
+    reference's own stream (xoshiro256++ + Acklam, MonteCarloEngine::run's
+    arithmetic) for the same Heston Euler workload: per strike
+    z = (FP32 - FP64) / sqrt(se32^2 + se64^2).  Both are unbiased estimates of
+    the same discretised price from independent streams, so |z| is a standard
+    normal; run outside the timed region."""
+    import openferric_b200 as of
+    gen = of.HestonPathGenerator(of.Heston(**HESTON), S0, T, STEPS)
+    eng = of.MonteCarloEngine(paths, SEED)
+    df = math.exp(-RATE * T)
+    zs, ms, k100 = [], 0.0, None
+    for k, (p32, s32) in zip(STRIKES, strip_prices):
+        r = eng.run_full(gen, of.VanillaOption.european_call(k, T), df)
+        ms += r.kernel_ms
+        z = (p32 - r.price) / math.sqrt(s32 * s32 + r.stderr_ * r.stderr_)
+        zs.append(z)
+        if k == 100.0:
+            k100 = {"fp64_price": r.price, "fp64_stderr": r.stderr_, "fp32_price": p32, "fp32_stderr": s32, "z": z}
+    return {"engine": "FP64 reference-stream MonteCarloEngine (xoshiro256++ seed 7, Acklam), same paths/steps",
+            "strikes": len(zs), "max_abs_z": max(abs(z) for z in zs),
+            "within_3_combined_se": sum(1 for z in zs if abs(z) <= 3.0), "K100": k100,
+            "fp64_kernel_ms_total": ms}
+
+
 ADJ_HESTON = dict(spot=100.0, rate=0.03, v0=0.04, kappa=2.0, theta=0.04, xi=0.5, rho=-0.7)
 
 
@@ -212,7 +237,7 @@ def greeks_comparison(paths=PATHS, steps=512, reps=3):
         return r.price, r.stderr_, r.kernel_ms
 
     fp64_run(ADJ_HESTON)
-    t64, base_se = 0.0, None
+    t64, base_price, base_se = 0.0, None, None
     for name in [None] + list(ADJ_HESTON):
         for sgn in ((0,) if name is None else (1, -1)):
             p = dict(ADJ_HESTON)
@@ -221,11 +246,15 @@ def greeks_comparison(paths=PATHS, steps=512, reps=3):
             price, se, ms = fp64_run(p)
             t64 += ms
             if name is None:
-                base_se = se
+                base_price, base_se = price, se
     return {"workload": "heston_qe_asian_adjoint", "paths": paths, "steps": steps, "strike": 100.0, "T": 2.0,
             "fp32_adjoint_ms": t_adj, "fp32_adjoint_options_per_s": 1e3 / t_adj,
             "fp32_adjoint_price": adj[0].price, "fp32_adjoint_se": adj[0].stderr,
-            "fp64_plain_bump_ms": t64, "fp64_plain_bump_options_per_s": 1e3 / t64, "fp64_plain_se": base_se,
+            "fp64_plain_bump_ms": t64, "fp64_plain_bump_options_per_s": 1e3 / t64,
+            "fp64_plain_price": base_price, "fp64_plain_se": base_se,
+            # QE (FP32) against Euler (FP64) at 512 steps: the two schemes'
+            # discretisation biases differ, so this z is not only rounding
+            "z_fp32_qe_vs_fp64_euler": (adj[0].price - base_price) / math.sqrt(adj[0].stderr ** 2 + base_se ** 2),
             "speedup": t64 / t_adj, "greeks": adj[0].greeks}
 
 
@@ -444,8 +473,10 @@ def main():
                   "e2e_price_K100": e2e_prices[20][0]},
     }
     if rank == 0 and not args.no_greeks:
-        # the priced+Greeks part of the metric (outside the timed region)
+        # the priced+Greeks part of the metric, and the FP32 strip's error
+        # against an FP64 run (both outside the timed region)
         line["greeks"] = greeks_comparison()
+        line["check"]["fp64"] = fp64_strip_check(args.paths, prices)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, sample = cpu_sample(os.cpu_count() or 1, 10.0)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",

@@ -168,16 +168,17 @@ __device__ __forceinline__ float uniform_from_u32(uint32_t r) {
 // Two independent standard normals from two u32 draws, Box-Muller transform
 // (Box & Muller, Ann. Math. Stat. 29, 1958): radius sqrt(-2 ln u1) with
 // u1 = (k + 0.5) 2^-23 from the top 23 bits of a (never 0 or 1, so the
-// radius is finite and at most sqrt(48 ln 2) = 5.77), angle pi x with
-// x = 2 f - 3 in [-1, 1) from the top 23 bits of b, which covers one turn
-// exactly once.  MUFU lg2, sqrt, sin and cos plus ~10 FP32/integer ops per
-// pair, against ~2 x 16 for two normal_from_u32 draws.
+// radius is finite and at most sqrt(48 ln 2) = 5.77), angle pi (2 f - 3) in
+// [-pi, pi) with f = 1 + k 2^-23 from the top 23 bits of b, which covers one
+// turn exactly once.  The angle is one fma, 2 pi f - 3 pi (the two rounded
+// constants move it by at most 3e-7 rad).  MUFU lg2, sqrt, sin and cos plus
+// ~9 FP32/integer ops per pair, against ~2 x 16 for two normal_from_u32 draws.
 __device__ __forceinline__ float2 normal_pair_from_u32(uint32_t a, uint32_t b) {
   const float u1 = uniform_from_u32(a);
   const float r = sqrtf(-1.3862943611198906f * __log2f(u1));  // -2 ln(2) log2(u1) = -2 ln(u1)
-  const float x = fmaf(2.0f, __uint_as_float(0x3F800000u | (b >> 9)), -3.0f);
+  const float ang = fmaf(6.28318530717959f, __uint_as_float(0x3F800000u | (b >> 9)), -9.42477796076938f);
   float s, c;
-  __sincosf(3.14159265358979f * x, &s, &c);
+  __sincosf(ang, &s, &c);
   return make_float2(r * c, r * s);
 }
 
