@@ -39,19 +39,20 @@ STRIKES = [80.0 + k for k in range(41)]
 PATHS, STEPS, SEED = 1 << 20, 256, 7
 PATH_STEPS = float(PATHS) * STEPS
 # Declared algorithmic work of one Heston Euler path-step in the FP32 kernel:
-# one Box-Muller pair (u1 2, -2 ln 2 scale 1, angle 3, r cos / r sin 2: 8
-# flops; lg2, sqrt, sin, cos on the MUFU unit) and the step (correlation 3,
-# log-spot 6, variance 5, floors 2: 16 flops; one sqrt): 24 FP32 flops
-# (FMA = 2) and 5 MUFU operations.  The Philox rounds (integer multiply and
-# xor, ~20 instructions per step) use neither pipe's budget in this count.
-FLOPS_PER_STEP = 24.0
+# one Box-Muller pair (u1 2, radius constant 1, angle fma 2, r cos / r sin 2:
+# 7 flops; lg2, sqrt, sin, cos on the MUFU unit; sqrt(dt) rides in the radius
+# constant) and the step (correlation 3, log-spot 5, variance 5, floors 2: 15
+# flops; one sqrt): 22 FP32 flops (FMA = 2) and 5 MUFU operations.  The
+# Philox rounds (integer multiply and xor, ~20 instructions per step) use
+# neither pipe's budget in this count.
+FLOPS_PER_STEP = 22.0
 SFU_PER_STEP = 5.0
 # Issued thread instructions per path-step of the strip kernel, Philox
 # included, from ncu captures (smsp__inst_executed.sum x 32 / path-steps) of
 # the bench's kernel at 2^20 paths, by samples in flight per thread.  With the
 # sampled SM clock they give the issue fraction: warp instructions per second
 # over 148 SMs x 4 schedulers x 1 instruction per cycle.
-INSTR_PER_STEP = {1: 51.8, 2: 47.8}
+INSTR_PER_STEP = {1: 48.8, 2: 45.7}
 INSTR_SOURCE = "ncu smsp__inst_executed.sum of strip_kernel at 2^20 paths (profiles/strip_kernel_heston_euler_*)"
 # DRAM bytes (read + write) of one strip launch from an ncu capture of the
 # kernel; the kernel reads no input from HBM, so the figure does not grow

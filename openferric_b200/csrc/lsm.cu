@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(256, DYN == DYN_GBM ? 4 : 2) lsm_gen_philox(co
         for (int q = 0; q < 4; ++q) {
           const uint32_t* w = &r[q].x;
           if (DYN == DYN_HESTON) {
-            const float2 z = of::normal_pair_from_u32(w[2 * k], w[2 * k + 1]);
+            const float2 z = of::normal_pair_scaled_from_u32(w[2 * k], w[2 * k + 1], C.hc.bm_k2);
             of::heston_euler_step(L[q], C.hc, z.x, z.y);
           } else {
             if ((k & 1) == 0) zp[q] = of::normal_pair_from_u32(w[k], w[k + 1]);
@@ -1805,7 +1805,8 @@ extern "C" of_status of_lsm_bermudan(of_ctx* ctx, const of_bermudan_contract* k,
   C.hc.kdt = (float)(k->kappa * dt);
   C.hc.kdt_theta = (float)(k->kappa * k->theta * dt);
   C.hc.one_m_kdt = (float)(1.0 - k->kappa * dt);
-  C.hc.xi_sqdt = (float)(k->xi * sqdt);
+  C.hc.xi = (float)k->xi;
+  C.hc.bm_k2 = (float)(-2.0 * 0.69314718055994531 * dt);
   C.hc.rho = (float)k->rho;
   C.hc.rho_c = (float)std::sqrt(1.0 - k->rho * k->rho);
   C.hc.v0 = (float)k->v0;

@@ -39,7 +39,8 @@ StepConsts make_consts(const of_model* m) {
   c.kdt = (float)(m->kappa * dt);
   c.kdt_theta = (float)(m->kappa * m->theta * dt);
   c.one_m_kdt = (float)(1.0 - m->kappa * dt);
-  c.xi_sqdt = (float)(m->xi * sqdt);
+  c.xi = (float)m->xi;
+  c.bm_k2 = (float)(-2.0 * 0.69314718055994531 * dt);
   c.rho = (float)m->rho;
   c.rho_c = (float)std::sqrt(1.0 - m->rho * m->rho);
   c.v0 = (float)m->v0;
@@ -83,16 +84,16 @@ __device__ __forceinline__ void simulate_terminal(const StepConsts& c, int32_t s
     const int32_t pairs = steps >> 1;  // full Philox calls; an odd last step below
     for (int32_t q = 0; q < pairs; ++q) {
       const uint4 r = of::philox4x32_10(make_uint4((uint32_t)q, lo, hi, stream), K);
-      float2 z = of::normal_pair_from_u32(r.x, r.y);
+      float2 z = of::normal_pair_scaled_from_u32(r.x, r.y, c.bm_k2);
       of::heston_euler_step(a, c, z.x, z.y);
       if (ANTI) of::heston_euler_step(b, c, -z.x, -z.y);
-      z = of::normal_pair_from_u32(r.z, r.w);
+      z = of::normal_pair_scaled_from_u32(r.z, r.w, c.bm_k2);
       of::heston_euler_step(a, c, z.x, z.y);
       if (ANTI) of::heston_euler_step(b, c, -z.x, -z.y);
     }
     if (steps & 1) {
       const uint4 r = of::philox4x32_10(make_uint4((uint32_t)pairs, lo, hi, stream), K);
-      const float2 z = of::normal_pair_from_u32(r.x, r.y);
+      const float2 z = of::normal_pair_scaled_from_u32(r.x, r.y, c.bm_k2);
       of::heston_euler_step(a, c, z.x, z.y);
       if (ANTI) of::heston_euler_step(b, c, -z.x, -z.y);
     }
@@ -163,10 +164,10 @@ __device__ __forceinline__ void simulate_terminal_n(const StepConsts& c, int32_t
 #pragma unroll
       for (int l = 0; l < ILP; ++l) {
         const uint4 r = of::philox4x32_10(make_uint4((uint32_t)q, lo[l], hi[l], stream), K);
-        float2 z = of::normal_pair_from_u32(r.x, r.y);
+        float2 z = of::normal_pair_scaled_from_u32(r.x, r.y, c.bm_k2);
         of::heston_euler_step(a[l], c, z.x, z.y);
         if (ANTI) of::heston_euler_step(b[l], c, -z.x, -z.y);
-        z = of::normal_pair_from_u32(r.z, r.w);
+        z = of::normal_pair_scaled_from_u32(r.z, r.w, c.bm_k2);
         of::heston_euler_step(a[l], c, z.x, z.y);
         if (ANTI) of::heston_euler_step(b[l], c, -z.x, -z.y);
       }
@@ -175,7 +176,7 @@ __device__ __forceinline__ void simulate_terminal_n(const StepConsts& c, int32_t
 #pragma unroll
       for (int l = 0; l < ILP; ++l) {
         const uint4 r = of::philox4x32_10(make_uint4((uint32_t)pairs, lo[l], hi[l], stream), K);
-        const float2 z = of::normal_pair_from_u32(r.x, r.y);
+        const float2 z = of::normal_pair_scaled_from_u32(r.x, r.y, c.bm_k2);
         of::heston_euler_step(a[l], c, z.x, z.y);
         if (ANTI) of::heston_euler_step(b[l], c, -z.x, -z.y);
       }
@@ -631,8 +632,10 @@ __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, const 
     // Box-Muller normals of the two draw pairs (GBM and Heston Euler)
     float2 p01 = make_float2(0.0f, 0.0f), p23 = make_float2(0.0f, 0.0f);
     if (MODEL != OF_MODEL_HESTON_QE) {
-      p01 = of::normal_pair_from_u32(r.x, r.y);
-      p23 = of::normal_pair_from_u32(r.z, r.w);
+      // Heston Euler takes its normals scaled by sqrt(dt) (heston_euler_step)
+      const float k2 = MODEL == OF_MODEL_HESTON_EULER ? c.bm_k2 : of::kBoxMullerK2;
+      p01 = of::normal_pair_scaled_from_u32(r.x, r.y, k2);
+      p23 = of::normal_pair_scaled_from_u32(r.z, r.w, k2);
     }
 #pragma unroll
     for (int q = 0; q < SPC; ++q) {

@@ -173,13 +173,23 @@ __device__ __forceinline__ float uniform_from_u32(uint32_t r) {
 // turn exactly once.  The angle is one fma, 2 pi f - 3 pi (the two rounded
 // constants move it by at most 3e-7 rad).  MUFU lg2, sqrt, sin and cos plus
 // ~9 FP32/integer ops per pair, against ~2 x 16 for two normal_from_u32 draws.
-__device__ __forceinline__ float2 normal_pair_from_u32(uint32_t a, uint32_t b) {
+//
+// normal_pair_scaled_from_u32 returns s (z1, z2) for a scale s > 0 folded
+// into the radius: k2 = -2 ln(2) s^2, r = sqrt(k2 log2(u1)) = s sqrt(-2 ln u1),
+// at the cost of the unscaled pair (the constant of the multiply changes).
+constexpr float kBoxMullerK2 = -1.3862943611198906f;  // -2 ln 2: unit scale
+
+__device__ __forceinline__ float2 normal_pair_scaled_from_u32(uint32_t a, uint32_t b, float k2) {
   const float u1 = uniform_from_u32(a);
-  const float r = sqrtf(-1.3862943611198906f * __log2f(u1));  // -2 ln(2) log2(u1) = -2 ln(u1)
+  const float r = sqrtf(k2 * __log2f(u1));  // k2 log2(u1) = -2 s^2 ln(u1)
   const float ang = fmaf(6.28318530717959f, __uint_as_float(0x3F800000u | (b >> 9)), -9.42477796076938f);
   float s, c;
   __sincosf(ang, &s, &c);
   return make_float2(r * c, r * s);
+}
+
+__device__ __forceinline__ float2 normal_pair_from_u32(uint32_t a, uint32_t b) {
+  return normal_pair_scaled_from_u32(a, b, kBoxMullerK2);
 }
 
 // ---------------------------------------------------------------------------

@@ -15,8 +15,10 @@ struct StepConsts {
   float drift, diff;
   // Heston Euler of the reference (src/models/stochastic.rs:56-71, with the
   // variance floored after every step as src/mc/simulation.rs:111-113 does):
-  // y += mudt - half_dt v + sqdt sqrt(v) zs ; v = max(v + kdt_theta - kdt v + xi_sqdt sqrt(v) z1, 0)
-  float mudt, half_dt, sqdt, kdt, kdt_theta, xi_sqdt, rho, rho_c, v0, y_floor, one_m_kdt;
+  // y += mudt - half_dt v + sqrt(v) sqdt zs ; v = max(v + kdt_theta - kdt v + xi sqrt(v) sqdt z1, 0)
+  // The normals arrive as sqdt (z1, z2): bm_k2 = -2 ln(2) dt is the radius
+  // constant of normal_pair_scaled_from_u32.
+  float mudt, half_dt, sqdt, kdt, kdt_theta, xi, rho, rho_c, v0, y_floor, one_m_kdt, bm_k2;
   // Heston QE (Andersen 2008, gamma1 = gamma2 = 1/2, psi_c = 1.5)
   float qe_e, qe_c1, qe_c2, qe_theta, qe_k0, qe_k1, qe_k2, qe_k3, qe_k4;
 };
@@ -26,12 +28,13 @@ struct LegState {
 };
 
 // Reference Heston Euler step in FP32 (variance kept >= 0 after each step).
-__device__ __forceinline__ void heston_euler_step(LegState& L, const StepConsts& c, float z1, float z2) {
+// w1, w2 = sqdt (z1, z2), the pair of normal_pair_scaled_from_u32(.., c.bm_k2).
+__device__ __forceinline__ void heston_euler_step(LegState& L, const StepConsts& c, float w1, float w2) {
   const float sq = sqrtf(L.v);
-  const float zs = fmaf(c.rho, z1, c.rho_c * z2);
-  const float y = fmaf(c.sqdt * sq, zs, fmaf(-c.half_dt, L.v, L.y + c.mudt));
+  const float ws = fmaf(c.rho, w1, c.rho_c * w2);  // sqdt zs
+  const float y = fmaf(sq, ws, fmaf(-c.half_dt, L.v, L.y + c.mudt));
   // v + kappa (theta - v) dt = (1 - kappa dt) v + kappa theta dt
-  const float vn = fmaf(c.xi_sqdt * sq, z1, fmaf(c.one_m_kdt, L.v, c.kdt_theta));
+  const float vn = fmaf(c.xi * sq, w1, fmaf(c.one_m_kdt, L.v, c.kdt_theta));
   L.v = fmaxf(vn, 0.0f);
   L.y = fmaxf(y, c.y_floor);
 }
