@@ -297,8 +297,20 @@ def run_workload(args, local_rank):
         # options/s with every option priced to SE <= 1e-4 S0: pilot launch,
         # then launches with the paths each option's pilot SE asks for
         import time
-        from openferric_b200.book import price_book_to_stderr, synthetic_book
+        from openferric_b200.book import BookEntry, price_book_to_stderr, synthetic_book
+        from openferric_b200.engines import VarianceReduction
+        from openferric_b200.instruments import AsianOption
         book = synthetic_book(4096)[:args.se_options]
+        vr_note = "none (plain Monte Carlo)"
+        if args.variance_reduction == "mixed":
+            # the reference's VarianceReduction per option: the geometric-Asian
+            # control variate for the arithmetic Asians; antithetic pairs for
+            # the Europeans (whose reference control variate is their own
+            # payoff, i.e. the closed form) and the barriers (no control variate)
+            book = [BookEntry(e.instrument, e.market, e.num_paths, e.num_steps,
+                              VarianceReduction.ControlVariate if isinstance(e.instrument, AsianOption)
+                              else VarianceReduction.Antithetic) for e in book]
+            vr_note = "geometric-Asian control variate for the Asians; antithetic for Europeans and barriers"
         price_book_to_stderr(book[:8], seed=1)  # warm-up (library load, clocks)
         times, rounds = [], None
         for k in range(max(1, args.steps)):
@@ -311,6 +323,7 @@ def run_workload(args, local_rank):
         line = {"metric": "options/s at SE<=1e-4*S0", "value": len(book) / s, "unit": "options/s", "n_gpus": 1,
                 "higher_is_better": True, "dtype": "f32", "data": "synthetic", "ms_per_step": s * 1e3,
                 "config": {"workload": f"batched_book_se_{len(book)}", "se_target": "1e-4*S0",
+                           "variance_reduction": vr_note,
                            "timing": "wall clock of the whole procedure (pilot + follow-up launches, host planning)",
                            "options_meeting_target": ok, "path_steps": ps, "path_steps_per_s": ps / s,
                            "rounds": [r.__dict__ for r in rounds]}}
@@ -357,6 +370,9 @@ def main():
                     help="paths per strip (profiling a smaller case; the benchmark workload is 2^20)")
     ap.add_argument("--book-options", type=int, default=4096,
                     help="book workload: number of options (4096 in the benchmark; fewer for a profiler capture)")
+    ap.add_argument("--variance-reduction", default="none", choices=["none", "mixed"],
+                    help="book_se workload: none (plain MC), or mixed (geometric-Asian control variate for the "
+                         "Asians, antithetic for the Europeans and barriers)")
     ap.add_argument("--contracts", type=int, default=256,
                     help="LSM workload: number of American puts (256 in the benchmark; fewer for a profiler capture)")
     args = ap.parse_args()

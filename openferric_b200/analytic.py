@@ -11,6 +11,8 @@ import math
 from fractions import Fraction
 from typing import Sequence
 
+import numpy as np
+
 from .core import OptionType
 
 _INV_SQRT_2PI = 0.3989422804014327
@@ -88,6 +90,19 @@ def bs_greeks(option_type: OptionType, spot: float, strike: float, rate: float, 
     return dict(delta=delta, gamma=gamma, vega=vega, theta=theta, rho=rho)
 
 
+def min_sum_in_order(times: Sequence[float], rows_per_block: int = 256) -> float:
+    """sum_i sum_j min(t_i, t_j) added in the reference's order (i outer, j
+    inner, one FP64 add at a time: src/pricing/asian.rs:86-136), so the
+    result is bit-identical to its double loop.  np.cumsum adds strictly left
+    to right; blocks of rows bound the temporary to rows_per_block x n."""
+    t = np.asarray(times, dtype=np.float64)
+    total = 0.0
+    for a in range(0, t.size, rows_per_block):
+        block = np.minimum.outer(t[a:a + rows_per_block], t).ravel()
+        total = float(np.cumsum(np.concatenate(([total], block)))[-1])
+    return total
+
+
 def geometric_asian_discrete_fixed(option_type: OptionType, s0: float, k: float, r: float, q: float, sigma: float,
                                    observation_times: Sequence[float]) -> float:
     obs = list(observation_times)
@@ -98,10 +113,7 @@ def geometric_asian_discrete_fixed(option_type: OptionType, s0: float, k: float,
         return math.exp(-r * maturity) * _vanilla(option_type, s0, k)
     n = float(len(obs))
     mean_t = sum(obs) / n
-    cov_sum = 0.0
-    for ti in obs:
-        for tj in obs:
-            cov_sum += min(ti, tj)
+    cov_sum = min_sum_in_order(obs)
     var = sigma * sigma * cov_sum / (n * n)
     m = math.log(s0) + _fma(-0.5 * sigma, sigma, r - q) * mean_t
     df = math.exp(-r * maturity)

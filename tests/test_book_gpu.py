@@ -120,9 +120,15 @@ def test_specialised_step_loops_match_the_general_loop(vr):
         assert x.price == y.price and x.stderr == y.stderr, (e.instrument, x.price, y.price)
 
 
-def test_price_book_to_stderr_meets_the_target():
+@pytest.mark.parametrize("mixed_vr", [False, True])
+def test_price_book_to_stderr_meets_the_target(mixed_vr):
     from openferric_b200.book import price_book_to_stderr
+    from openferric_b200.instruments import AsianOption
     book = synthetic_book(n=12, seed=8, min_log2_paths=10, max_log2_paths=11)
+    if mixed_vr:  # geometric control variate for the Asians, antithetic pairs elsewhere
+        book = [BookEntry(e.instrument, e.market, e.num_paths, e.num_steps,
+                          VarianceReduction.ControlVariate if isinstance(e.instrument, AsianOption)
+                          else VarianceReduction.Antithetic) for e in book]
     res, rounds = price_book_to_stderr(book, seed=3, se_rel=2e-3, pilot_paths=2048)
     for e, r in zip(book, res):
         assert r.stderr <= 2e-3 * e.market.spot, (e.instrument, r.stderr)
