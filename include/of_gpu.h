@@ -7,8 +7,7 @@
  * of_ctx_destroy).  All calls are synchronous to the caller unless stated.
  *
  * Each entry point names the openferric interface it replaces (path:line in
- * the rosssaunders/openferric source tree).  The Rust-side extern block that a
- * maintainer adds to bind these is shown in INTEGRATION.md.
+ * the rosssaunders/openferric source tree).
  *
  * Error behaviour follows openferric's `PricingError` (src/core/engine.rs:293-302):
  * OF_ERR_INVALID_INPUT  -> PricingError::InvalidInput
@@ -521,15 +520,18 @@ of_status of_heston_price_adjoint(of_ctx* ctx, const of_heston_adjoint_params* p
  * OF_STRIP_NOALLOC_MAX_STRIKES strikes and OF_STRIP_NOALLOC_MAX_BLOCKS blocks
  * (larger requests are rejected with OF_ERR_INVALID_INPUT and a message).
  *
- * Runs on the calling thread's current device and on `cuda_stream` (NULL =
- * the legacy default stream), and returns when the results are on the host.
- * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) once: make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (other
- * streams, other threads) race and must be serialised by the caller.  Every
- * call overwrites all of the scratch it reads, so nothing needs clearing
- * between calls.  `err`/`err_len` (may be NULL/0) receive the message of a
- * failure; kernel_ms is not measured (0). */
+ * Runs on the calling thread's current device and CUDA context, on
+ * `cuda_stream` (NULL = the legacy default stream), and returns when the
+ * results are on the host.  The first call in a context (per device, and
+ * again after cudaDeviceReset) looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current: make that first call
+ * before any stream capture.  The request is validated exactly as of_mc_strip
+ * validates it (same statuses and messages), then against the limits below.
+ * All calls share the array: calls that overlap on the GPU (other streams,
+ * other threads) race and must be serialised by the caller.  Every call
+ * overwrites all of the scratch it reads, so nothing needs clearing between
+ * calls.  `err`/`err_len` (may be NULL/0) receive the message of a failure;
+ * kernel_ms is not measured (0). */
 #define OF_STRIP_NOALLOC_MAX_STRIKES 64
 #define OF_STRIP_NOALLOC_MAX_BLOCKS 1024
 #define OF_STRIP_NOALLOC_SCRATCH_BYTES                            \

@@ -193,7 +193,7 @@ struct LsmBatch {
   unsigned long long* ex_bits;   // [nc][steps+1] bits of the max (put) / min (call) exercised spot
   double* itm_count;             // [nc][steps+1] in-the-money paths at each regression date
   const double* disc_pow;        // [nc][steps+1] disc^k by repeated multiplication, as V is discounted
-  uint32_t* status;              // nonzero: a pass gave up waiting for its bulk copies
+  uint32_t* status;              // bit 0: a pass gave up waiting for its bulk copies; bit 1: its drain gave up too
   unsigned long long* term_itm;  // [nc] paths in the money at expiry
   uint64_t seed;
   of::PhiloxKeys keys;
@@ -745,7 +745,10 @@ constexpr uint64_t kWaitLimitNs = 1000000000ull;               // a bulk copy la
 // both publishes the landed stage and frees the one consumed before it.  The
 // new cash flows go straight to global memory.  A copy that has not landed
 // after kWaitLimitNs sets B.status, and the block drains its outstanding
-// copies (bounded the same way) and returns without its moments.
+// copies (bounded the same way) and returns without its moments.  A drain
+// that gives up as well sets a second status bit: the host then marks the
+// context unusable, since copies may still land in shared memory that the
+// returned block no longer owns.
 template <int DEG, bool PUT>
 __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, float* ring, uint64_t* full,
                                                   double* red_sh, double* mom_sh) {
@@ -833,12 +836,15 @@ __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, floa
   }
   if (i < n_chunks) {  // a copy did not land: record it, drain what is in flight, give up
     if (threadIdx.x == 0) {
-      atomicOr(B.status, 1u);
       // issued so far: chunks 0 .. kStages-1, then chunk k-1+kStages at each completed iteration k >= 1
       const int issued = i >= 1 ? i - 2 + kStages : kStages - 1;
       const int last = issued < n_chunks - 1 ? issued : n_chunks - 1;
+      bool drained = true;
       for (int j = i; j <= last; ++j)
-        of::mbar_wait(of::smem_u32(full + j % kStages), (uint32_t)(j / kStages) & 1u, kWaitLimitNs);
+        drained &= of::mbar_wait(of::smem_u32(full + j % kStages), (uint32_t)(j / kStages) & 1u, kWaitLimitNs);
+      // bit 0: a copy timed out; bit 1: the drain timed out too, so copies
+      // may still land in shared memory the block no longer owns
+      atomicOr(B.status, drained ? 1u : 3u);
     }
     __syncthreads();
     return;
@@ -1439,7 +1445,14 @@ of_status lsm_enqueue(of_ctx* ctx, LsmRun& r, const of_lsm_config* cfg, cudaStre
 of_status lsm_collect(of_ctx* ctx, const LsmRun& r, std::vector<double>& results, std::vector<int32_t>& regs,
                       std::vector<LsmTrack>* track) {
   const int nc = r.nc();
-  if (*(const uint32_t*)(r.pin + r.o_status))
+  const uint32_t status = *(const uint32_t*)(r.pin + r.o_status);
+  if (status & 2u) {
+    ctx->unusable = true;
+    return of_fail(ctx, OF_ERR_TIMEOUT,
+                   "LSM pass: a bulk copy into shared memory did not complete in time and could not be drained; "
+                   "the context is unusable: destroy it and create a new one");
+  }
+  if (status)
     return of_fail(ctx, OF_ERR_TIMEOUT, "LSM pass: a bulk copy into shared memory did not complete in time");
   const double* hres = (const double*)(r.pin + r.o_res);
   const int32_t* hreg = (const int32_t*)(r.pin + r.o_reg);

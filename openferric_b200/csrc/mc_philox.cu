@@ -9,8 +9,11 @@
 // sums are compensated FP32 per thread and FP64 from the warp level up.
 // Compiled with -use_fast_math: sqrt/exp/log/div map to single MUFU
 // operations; the few places that need more accuracy say so.
+#include <cuda.h>  // CUcontext / CUresult types only; the driver functions are resolved at run time
+
 #include <algorithm>
 #include <cmath>
+#include <cstdarg>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -341,10 +344,12 @@ extern "C" void of_strip_plan_destroy(of_strip_plan* pl) {
   delete pl;
 }
 
-// Validates a strip request and fills the plan's parameters, kernel and
-// launch shape (no allocation).
-static of_status strip_setup(of_ctx* ctx, const of_model* m, int32_t option_type, const double* strikes,
-                             int64_t n_strikes, const of_mc_config* cfg, of_strip_plan* pl) {
+// Checks of a strip request that need no device: every strip entry point
+// (of_mc_strip, the plans, of_mc_strip_noalloc) runs exactly these.  `ctx`
+// only receives the message; it may be a stack context that owns nothing.
+static of_status strip_validate(of_ctx* ctx, const of_model* m, int32_t option_type, const double* strikes,
+                                int64_t n_strikes, const of_mc_config* cfg) {
+  if (!m || !cfg) return of_fail(ctx, OF_ERR_INVALID_INPUT, "null argument");
   of_payoff dummy{};
   dummy.kind = OF_PAYOFF_VANILLA;
   dummy.option_type = option_type;
@@ -360,6 +365,19 @@ static of_status strip_setup(of_ctx* ctx, const of_model* m, int32_t option_type
       return of_fail(ctx, OF_ERR_INVALID_INPUT, "strike %lld must be finite and > 0", (long long)k);
   if (cfg->control_variate != OF_CV_NONE)
     return of_fail(ctx, OF_ERR_UNSUPPORTED, "the strike strip has no control variate");
+  if (cfg->injected_normals)
+    return of_fail(ctx, OF_ERR_UNSUPPORTED, "injected normals are a FP64 reference-mode test hook");
+  if (cfg->tile_ilp < 0 || cfg->tile_ilp > 2)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "tile_ilp must be 0 (default), 1 or 2");
+  return OF_OK;
+}
+
+// Validates a strip request and fills the plan's parameters, kernel and
+// launch shape (no allocation).
+static of_status strip_setup(of_ctx* ctx, const of_model* m, int32_t option_type, const double* strikes,
+                             int64_t n_strikes, const of_mc_config* cfg, of_strip_plan* pl) {
+  OF_TRY(strip_validate(ctx, m, option_type, strikes, n_strikes, cfg));
+  OF_TRY(of_ctx_check(ctx));
   OF_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   pl->ctx = ctx;
   pl->n_strikes = (int)n_strikes;
@@ -375,8 +393,6 @@ static of_status strip_setup(of_ctx* ctx, const of_model* m, int32_t option_type
   P.s0 = (float)m->s0;
   P.keys = of::philox_keys(cfg->seed);
   const int kpl = (int)((n_strikes + 31) / 32);
-  if (cfg->tile_ilp < 0 || cfg->tile_ilp > 2)
-    return of_fail(ctx, OF_ERR_INVALID_INPUT, "tile_ilp must be 0 (default), 1 or 2");
   const int ilp = cfg->tile_ilp == 2 ? 2 : 1;
   pl->fn = pick_strip_ilp(kpl, ilp, m->kind, P.antithetic);
   pl->smem = (size_t)(pl->block / 32) * n_strikes * 2 * sizeof(double);
@@ -431,6 +447,7 @@ extern "C" of_status of_strip_plan_create(of_ctx* ctx, const of_model* m, int32_
 
 extern "C" of_status of_strip_plan_launch(of_strip_plan* pl) {
   if (!pl) return OF_ERR_INVALID_INPUT;
+  OF_TRY(of_ctx_check(pl->ctx));
   OF_CUDA_TRY(pl->ctx, cudaGraphLaunch(pl->exec, pl->ctx->stream));
   return OF_OK;
 }
@@ -868,6 +885,7 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
   *out = nullptr;
   if (n <= 0 || !e) return of_fail(ctx, OF_ERR_INVALID_INPUT, "book must hold at least one option");
   if (n > (1 << 24)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "book too large");
+  OF_TRY(of_ctx_check(ctx));
   OF_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   of_book_plan* pl = new of_book_plan();
   pl->ctx = ctx;
@@ -1051,6 +1069,7 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
 
 extern "C" of_status of_book_plan_launch(of_book_plan* pl) {
   if (!pl) return OF_ERR_INVALID_INPUT;
+  OF_TRY(of_ctx_check(pl->ctx));
   if (pl->use_graph) {
     OF_CUDA_TRY(pl->ctx, cudaGraphLaunch(pl->exec, pl->ctx->stream));
   } else {
@@ -1125,16 +1144,27 @@ of_status of_mc_run_fp32(of_ctx* ctx, const of_model* m, const of_payoff* p, con
 // Layout: [strikes: MAX_STRIKES floats][sums: 2*MAX_STRIKES doubles]
 //         [per-block partials: MAX_BLOCKS * 2*MAX_STRIKES doubles].
 // In host code `g_strip_noalloc_scratch` names a host-side stand-in, not the
-// device array: its device address is looked up with cudaGetSymbolAddress,
-// once per device with that device current, and that address is what the
-// kernels get.
+// device array: its device address is looked up with cudaGetSymbolAddress
+// with the caller's device current, once per CUDA context (a device's
+// primary context, or a context the caller made current), and that address
+// is what the kernels get.  The lookups are cached by the context's
+// process-unique ID, so a context created after cudaDeviceReset, whose copy
+// of the array may sit elsewhere, gets a lookup of its own.
 // ---------------------------------------------------------------------------
 static __device__ __align__(256) unsigned char g_strip_noalloc_scratch[OF_STRIP_NOALLOC_SCRATCH_BYTES];
 
 namespace {
 
-constexpr int kNoallocMaxDevices = 64;
-void* g_noalloc_addr[kNoallocMaxDevices] = {};
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext*);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long*);
+
+struct NoallocAddr {
+  unsigned long long ctx_id;
+  void* addr;
+};
+constexpr int kNoallocCache = 64;
+NoallocAddr g_noalloc_cache[kNoallocCache] = {};
+int g_noalloc_used = 0;
 std::mutex g_noalloc_mutex;
 
 void noalloc_msg(char* err, size_t len, const char* fmt, ...) {
@@ -1145,75 +1175,92 @@ void noalloc_msg(char* err, size_t len, const char* fmt, ...) {
   va_end(ap);
 }
 
+// The process-unique ID of the calling thread's current CUDA context (0 when
+// none is current).  The two driver functions are resolved once through the
+// runtime, so the library keeps no link-time dependency on libcuda.
+cudaError_t noalloc_ctx_id(unsigned long long* id) {
+  static PfnCtxGetCurrent get_current = nullptr;
+  static PfnCtxGetId get_id = nullptr;
+  static cudaError_t resolved = [] {
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = cudaDriverEntryPointSymbolNotFound;
+    cudaError_t e = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", (void**)&get_current, 12000,
+                                                     cudaEnableDefault, &q1);
+    if (e == cudaSuccess)
+      e = cudaGetDriverEntryPointByVersion("cuCtxGetId", (void**)&get_id, 12000, cudaEnableDefault, &q2);
+    if (e == cudaSuccess && (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !get_current ||
+                             !get_id))
+      e = cudaErrorSymbolNotFound;
+    return e;
+  }();
+  *id = 0;
+  if (resolved != cudaSuccess) return resolved;
+  CUcontext c = nullptr;
+  if (get_current(&c) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
+  if (!c) return cudaSuccess;
+  return get_id(c, id) == CUDA_SUCCESS ? cudaSuccess : cudaErrorDeviceUninitialized;
+}
+
+// Device address of the scratch array in the current context.  The first
+// call in a context makes the runtime's context current (cudaGetSymbolAddress
+// initialises the primary context of the current device if needed).
+cudaError_t noalloc_scratch_addr(void** out) {
+  unsigned long long id = 0;
+  cudaError_t e = noalloc_ctx_id(&id);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> guard(g_noalloc_mutex);
+  if (id != 0)
+    for (int k = 0; k < g_noalloc_used; ++k)
+      if (g_noalloc_cache[k].ctx_id == id) {
+        *out = g_noalloc_cache[k].addr;
+        return cudaSuccess;
+      }
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_strip_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  if (!p) return cudaErrorInvalidSymbol;
+  if (id == 0 && (e = noalloc_ctx_id(&id)) != cudaSuccess) return e;  // the lookup made a context current
+  if (id != 0 && g_noalloc_used < kNoallocCache) g_noalloc_cache[g_noalloc_used++] = {id, p};
+  *out = p;
+  return cudaSuccess;
+}
+
 }  // namespace
 
 extern "C" of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* m, int32_t option_type,
                                          const double* strikes, int64_t n_strikes, const of_mc_config* cfg,
                                          of_mc_result* results, char* err, size_t err_len) {
   if (err && err_len) err[0] = '\0';
-  if (!m || !cfg || !results || !strikes) {
+  if (!results) {
     noalloc_msg(err, err_len, "null argument");
     return OF_ERR_INVALID_INPUT;
   }
-  if (n_strikes <= 0 || n_strikes > OF_STRIP_NOALLOC_MAX_STRIKES) {
+  {
+    // The checks of of_mc_strip; the stack context only carries the message.
+    of_ctx sink;
+    const of_status st = strip_validate(&sink, m, option_type, strikes, n_strikes, cfg);
+    if (st != OF_OK) {
+      noalloc_msg(err, err_len, "%s", sink.last_error.c_str());
+      return st;
+    }
+  }
+  if (n_strikes > OF_STRIP_NOALLOC_MAX_STRIKES) {
     noalloc_msg(err, err_len, "n_strikes must be in [1, %d] (static scratch limit), got %lld",
                 OF_STRIP_NOALLOC_MAX_STRIKES, (long long)n_strikes);
     return OF_ERR_INVALID_INPUT;
   }
-  // Validation of of_mc_strip, restated without a context.
-  if (cfg->num_paths <= 0) return noalloc_msg(err, err_len, "num_paths must be > 0"), OF_ERR_INVALID_INPUT;
-  if (m->steps <= 0 || m->steps > 2147483647LL)
-    return noalloc_msg(err, err_len, "num_steps must be in [1, 2^31-1]"), OF_ERR_INVALID_INPUT;
-  if (!(m->maturity > 0.0) || !std::isfinite(m->maturity))
-    return noalloc_msg(err, err_len, "maturity must be finite and > 0"), OF_ERR_INVALID_INPUT;
-  if (!(m->s0 > 0.0) || !std::isfinite(m->s0) || !std::isfinite(m->mu))
-    return noalloc_msg(err, err_len, "spot must be > 0 and drift finite"), OF_ERR_INVALID_INPUT;
-  if (m->kind == OF_MODEL_GBM) {
-    if (!(m->sigma > 0.0) || !std::isfinite(m->sigma))
-      return noalloc_msg(err, err_len, "market volatility must be > 0"), OF_ERR_INVALID_INPUT;
-  } else if (m->kind == OF_MODEL_HESTON_EULER || m->kind == OF_MODEL_HESTON_QE) {
-    if (!(m->kappa > 0.0 && m->theta >= 0.0 && m->xi >= 0.0 && m->v0 >= 0.0 && m->rho > -1.0 && m->rho < 1.0))
-      return noalloc_msg(err, err_len, "invalid Heston parameters"), OF_ERR_INVALID_INPUT;
-    if (m->kind == OF_MODEL_HESTON_QE && !(m->xi > 0.0 && m->theta > 0.0))
-      return noalloc_msg(err, err_len, "the QE scheme needs xi > 0 and theta > 0"), OF_ERR_INVALID_INPUT;
-  } else {
-    return noalloc_msg(err, err_len, "unknown model kind %d", m->kind), OF_ERR_INVALID_INPUT;
-  }
-  if (m->n_dividends > 0)
-    return noalloc_msg(err, err_len, "the strike strip takes no discrete dividends"), OF_ERR_UNSUPPORTED;
-  if (option_type != OF_CALL && option_type != OF_PUT)
-    return noalloc_msg(err, err_len, "unknown option type %d", option_type), OF_ERR_INVALID_INPUT;
-  if (cfg->control_variate != OF_CV_NONE || cfg->injected_normals)
-    return noalloc_msg(err, err_len, "the strip has no control variate and no injected normals"),
-           OF_ERR_INVALID_INPUT;
-  if (!std::isfinite(cfg->discount_factor))
-    return noalloc_msg(err, err_len, "discount factor must be finite"), OF_ERR_INVALID_INPUT;
   float hk[OF_STRIP_NOALLOC_MAX_STRIKES];
-  for (int64_t k = 0; k < n_strikes; ++k) {
-    if (!(strikes[k] > 0.0) || !std::isfinite(strikes[k]))
-      return noalloc_msg(err, err_len, "strike %lld must be finite and > 0", (long long)k), OF_ERR_INVALID_INPUT;
-    hk[k] = (float)strikes[k];
-  }
+  for (int64_t k = 0; k < n_strikes; ++k) hk[k] = (float)strikes[k];
 
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) {
+  if (e != cudaSuccess) {
     noalloc_msg(err, err_len, "cudaGetDevice failed: %s", cudaGetErrorString(e));
     return OF_ERR_CUDA;
   }
   void* base = nullptr;
-  {
-    std::lock_guard<std::mutex> guard(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
-      void* p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_strip_noalloc_scratch);
-      if (e != cudaSuccess || !p) {
-        noalloc_msg(err, err_len, "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-        return OF_ERR_CUDA;
-      }
-      g_noalloc_addr[dev] = p;
-    }
-    base = g_noalloc_addr[dev];
+  if ((e = noalloc_scratch_addr(&base)) != cudaSuccess) {
+    noalloc_msg(err, err_len, "device address of the static scratch: %s", cudaGetErrorString(e));
+    return OF_ERR_CUDA;
   }
   float* d_strikes = (float*)base;
   double* d_sums = (double*)((char*)base + OF_STRIP_NOALLOC_MAX_STRIKES * 4);
@@ -1229,7 +1276,9 @@ extern "C" of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* m, i
   P.s0 = (float)m->s0;
   P.keys = of::philox_keys(cfg->seed);
   P.strikes = d_strikes;
-  const StripKernelFn fn = n_strikes <= 32 ? pick_strip<1>(m->kind, P.antithetic) : pick_strip<2>(m->kind, P.antithetic);
+  // the kernel of_mc_strip picks for the same request (strikes per lane, samples in flight)
+  const int ilp = cfg->tile_ilp == 2 ? 2 : 1;
+  const StripKernelFn fn = pick_strip_ilp((int)((n_strikes + 31) / 32), ilp, m->kind, P.antithetic);
   const int block = 256;
   const size_t smem = (size_t)(block / 32) * n_strikes * 2 * sizeof(double);
   int sms = 0, per_sm = 0;
@@ -1238,7 +1287,7 @@ extern "C" of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* m, i
     noalloc_msg(err, err_len, "device query failed: %s", cudaGetErrorString(e));
     return OF_ERR_CUDA;
   }
-  const int64_t want = (P.samples + block - 1) / block;
+  const int64_t want = (P.samples + (int64_t)block * ilp - 1) / ((int64_t)block * ilp);
   int64_t grid = std::min<int64_t>(want, (int64_t)sms * std::max(per_sm, 1));
   grid = std::max<int64_t>(1, std::min<int64_t>(grid, OF_STRIP_NOALLOC_MAX_BLOCKS));
 

@@ -17,7 +17,15 @@ of_status of_fail(of_ctx* ctx, of_status st, const char* fmt, ...) {
   return st;
 }
 
+of_status of_ctx_check(of_ctx* ctx) {
+  if (ctx && ctx->unusable)
+    return of_fail(ctx, OF_ERR_CUDA,
+                   "context unusable: an earlier kernel gave up with copies in flight; destroy it and create a new one");
+  return OF_OK;
+}
+
 of_status of_scratch(of_ctx* ctx, int slot, size_t bytes, void** out) {
+  OF_TRY(of_ctx_check(ctx));
   if (slot < 0 || slot >= SLOT_COUNT) return of_fail(ctx, OF_ERR_INVALID_INPUT, "bad scratch slot %d", slot);
   if (bytes == 0) bytes = 16;
   if (ctx->slot_bytes[slot] < bytes) {
@@ -43,6 +51,7 @@ of_status of_scratch(of_ctx* ctx, int slot, size_t bytes, void** out) {
 }
 
 of_status of_pinned(of_ctx* ctx, size_t bytes, void** out) {
+  OF_TRY(of_ctx_check(ctx));
   if (ctx->pinned_bytes < bytes) {
     if (ctx->pinned) {
       OF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));

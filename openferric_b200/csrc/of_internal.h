@@ -50,10 +50,17 @@ struct of_ctx {
   void* pinned = nullptr;  // pinned host staging for results
   size_t pinned_bytes = 0;
   std::string last_error;
+  // Set when a kernel gave up on asynchronous copies that were still in
+  // flight into shared memory it no longer owns: from then on the context
+  // refuses work, and the caller destroys it and creates a new one.
+  bool unusable = false;
 };
 
 // Records a formatted message as the context's last error and returns `st`.
 of_status of_fail(of_ctx* ctx, of_status st, const char* fmt, ...);
+
+// OF_OK, or OF_ERR_CUDA with a message once the context is marked unusable.
+of_status of_ctx_check(of_ctx* ctx);
 
 // Returns a device buffer of at least `bytes` for `slot`, growing it if needed.
 of_status of_scratch(of_ctx* ctx, int slot, size_t bytes, void** out);

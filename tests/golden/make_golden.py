@@ -11,7 +11,7 @@ Reads (once, in a container where the openferric source tree is mounted):
 The fixtures are committed so that the GPU tests need no access to the
 reference tree.
 
-    python tests/golden/make_golden.py [--reference PATH]
+    python tests/golden/make_golden.py --reference PATH
 """
 import argparse
 import json
@@ -127,7 +127,7 @@ def bermudan_quantlib(ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of an openferric source tree")
     a = ap.parse_args()
     fixtures = {
         "lsm_table1.json": lsm_table1(a.reference),

@@ -92,3 +92,34 @@ def test_no_gpu_fails_loudly_without_cpu_fallback():
     market = Market.builder().spot(100).rate(0.05).flat_vol(0.2).build()
     with pytest.raises(_lib.GpuUnavailable):
         MonteCarloPricingEngine(1000, 10, 1).price(VanillaOption.european_call(100, 1.0), market)
+
+
+def _noalloc(model, strikes, **cfg_fields):
+    """of_mc_strip_noalloc on host arguments only; the requests below fail in
+    its validation, before any CUDA call, so this runs without a GPU."""
+    L = _lib.load()
+    ks = (C.c_double * len(strikes))(*strikes)
+    cfg = A.OfMcConfig(num_paths=1024, seed=1, precision=A.OF_PREC_FP32_PHILOX, discount_factor=1.0, **cfg_fields)
+    out = (A.OfMcResult * len(strikes))()
+    err = C.create_string_buffer(256)
+    st = L.of_mc_strip_noalloc(None, C.byref(model), A.OF_CALL, ks, len(strikes), C.byref(cfg), out, err, len(err))
+    return st, err.value.decode()
+
+
+def test_noalloc_strip_validates_like_of_mc_strip():
+    """The no-allocation strip runs of_mc_strip's own validation: the same
+    status for the same request, then its static-scratch strike limit."""
+    from openferric_b200 import Heston, HestonPathGenerator
+    gen = HestonPathGenerator(Heston(0.03, 2.0, 0.04, 0.5, -0.7, 0.04), 100.0, 1.0, 8)
+    model = gen.to_abi()
+    st, msg = _noalloc(model, [100.0], tile_ilp=3)
+    assert st == A.OF_ERR_INVALID_INPUT and "tile_ilp" in msg
+    st, msg = _noalloc(model, [100.0], control_variate=A.OF_CV_TERMINAL_SPOT)
+    assert st == A.OF_ERR_UNSUPPORTED and "control variate" in msg
+    big = HestonPathGenerator(Heston(0.03, 2.0, 0.04, 0.5, -0.7, 0.04), 100.0, 1.0, (1 << 30) + 1).to_abi()
+    st, msg = _noalloc(big, [100.0])
+    assert st == A.OF_ERR_INVALID_INPUT and "num_steps" in msg
+    st, msg = _noalloc(model, [100.0 + k for k in range(65)])
+    assert st == A.OF_ERR_INVALID_INPUT and "64" in msg
+    st, msg = _noalloc(model, [100.0 + k for k in range(129)])
+    assert st == A.OF_ERR_UNSUPPORTED and "128" in msg

@@ -14,7 +14,7 @@ import math
 
 import pytest
 
-from openferric_b200 import Heston, HestonPathGenerator, OptionType, price_strike_strip
+from openferric_b200 import Gbm, GbmPathGenerator, Heston, HestonPathGenerator, OptionType, price_strike_strip
 from openferric_b200 import _abi as A
 from openferric_b200 import _lib
 
@@ -23,10 +23,11 @@ pytestmark = pytest.mark.gpu
 STRIKES = [80.0 + 2.0 * k for k in range(21)]
 
 
-def noalloc_strip(model, option_type, strikes, num_paths, seed, df):
+def noalloc_strip(model, option_type, strikes, num_paths, seed, df, antithetic=False, tile_ilp=0):
     L = _lib.load()
-    ks =(C.c_double * len(strikes))(*strikes)
-    cfg = A.OfMcConfig(num_paths=num_paths, seed=seed, precision=A.OF_PREC_FP32_PHILOX, discount_factor=df)
+    ks = (C.c_double * len(strikes))(*strikes)
+    cfg = A.OfMcConfig(num_paths=num_paths, seed=seed, precision=A.OF_PREC_FP32_PHILOX, discount_factor=df,
+                       antithetic=int(antithetic), tile_ilp=tile_ilp)
     out = (A.OfMcResult * len(strikes))()
     err = C.create_string_buffer(256)
     st = L.of_mc_strip_noalloc(None, C.byref(model), option_type, ks, len(strikes), C.byref(cfg), out, err,
@@ -43,6 +44,22 @@ def test_noalloc_strip_matches_existing_entry_point_on_two_calls():
         assert st == A.OF_OK, msg
         for (p, s), (rp, rs) in zip(got, ref):
             # same kernel, same draws: equal up to the FP32 partial-sum grouping
+            assert abs(p - rp) <= 1e-9 * abs(rp) + 1e-12, (p, rp)
+            assert abs(s - rs) <= 1e-9 * abs(rs) + 1e-12
+
+
+def test_noalloc_strip_full_strike_layout_gbm_antithetic_two_samples_per_thread():
+    """64 strikes fill the static scratch's strike and sum rows (two strikes
+    per lane), with GBM antithetic pairs and two samples in flight per thread:
+    the same kernel of_mc_strip picks for that request."""
+    gen = GbmPathGenerator(Gbm(0.05, 0.25), 100.0, 1.0, 52)
+    df = math.exp(-0.05)
+    strikes = [70.0 + k for k in range(64)]
+    ref = price_strike_strip(gen, OptionType.Put, strikes, 1 << 17, 11, df, antithetic=True, tile_ilp=2)
+    for _ in range(2):
+        st, msg, got = noalloc_strip(gen.to_abi(), A.OF_PUT, strikes, 1 << 17, 11, df, antithetic=True, tile_ilp=2)
+        assert st == A.OF_OK, msg
+        for (p, s), (rp, rs) in zip(got, ref):
             assert abs(p - rp) <= 1e-9 * abs(rp) + 1e-12, (p, rp)
             assert abs(s - rs) <= 1e-9 * abs(rs) + 1e-12
 
