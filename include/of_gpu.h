@@ -157,19 +157,22 @@ of_status of_ctx_get_stream(of_ctx* ctx, void** cuda_stream);
 int of_abi_version(void);
 int of_device_sm_count(of_ctx* ctx);
 
-/* Throughput of this GPU's FP32 pipe and special-function unit (MUFU),
- * measured by two short probe kernels on the context's stream: the
+/* Throughput of this GPU's FP32 and FP64 pipes and special-function unit
+ * (MUFU), measured by three short probe kernels on the context's stream: the
  * denominators of a compute-bound roofline at the clocks of the moment.  No
  * counterpart in the reference.
  *   sfu_ops_per_s: MUFU results per second for the mix that the FP32 Philox
  *     kernels issue (lg2, sqrt, sin, cos), 8 independent chains per thread;
  *   fp32_flops_per_s: FP32 FMA throughput, 2 flops per FMA, 8 independent
  *     chains per thread;
- *   probe_ms: device time of the two probes together. */
+ *   probe_ms: device time of the three probes together;
+ *   fp64_flops_per_s: FP64 FMA throughput, 2 flops per FMA, 8 independent
+ *     chains per thread. */
 typedef struct {
   double sfu_ops_per_s;
   double fp32_flops_per_s;
   double probe_ms;
+  double fp64_flops_per_s;
 } of_device_peaks;
 of_status of_measure_device_peaks(of_ctx* ctx, of_device_peaks* out);
 
@@ -215,13 +218,40 @@ typedef struct of_book_entry {
   double discount_factor;
 } of_book_entry;
 
+/* What a book launch computes (of_book_config.mode).
+ * OF_BOOK_PRICE:      FP32 prices (the estimator of MonteCarloPricingEngine::price).
+ * OF_BOOK_GREEKS:     FP32 prices and pathwise Greeks (delta, vega, rho, theta)
+ *                     of GBM options without discrete dividends, the Greeks of
+ *                     MonteCarloPricingEngine::price_with_greeks_aad
+ *                     (src/engines/monte_carlo/mc_engine.rs:977-987,
+ *                     mc_aad.rs:15-219) for every payoff of the book.  Barrier
+ *                     options are priced by one-step survival (each step drawn
+ *                     on the alive side of the barrier, the path weighted by
+ *                     its survival probability), which is unbiased for the
+ *                     same discretely monitored price and differentiable; a
+ *                     barrier option takes no control variate in this mode.
+ * OF_BOOK_PRICE_FP64: the prices of OF_BOOK_GREEKS in FP64 path arithmetic on
+ *                     the same draws, for bump-and-revalue checks of the Greeks
+ *                     with common random numbers. */
+enum { OF_BOOK_PRICE = 0, OF_BOOK_GREEKS = 1, OF_BOOK_PRICE_FP64 = 2 };
+
 typedef struct of_book_config {
   uint64_t seed;
   int32_t block;            /* threads per block, 0 = autotuned */
   int32_t paths_per_thread; /* samples per thread per tile, 0 = autotuned */
   int32_t use_graph;        /* capture the launch in a CUDA graph */
-  int32_t reserved0;
+  int32_t mode;             /* OF_BOOK_* */
 } of_book_config;
+
+/* Greeks of one book option (openferric core::Greeks, src/core/engine.rs:17-28):
+ * d PV / d spot, d PV / d sigma, d PV / d r (with the drift r - q and the
+ * discount exp(-r T), r = -ln(discount_factor) / T), theta = -d PV / d T
+ * (steps fixed, dt = T / steps).  gamma is 0, as the reference's pathwise AAD
+ * returns it.  Each comes with its Monte Carlo standard error. */
+typedef struct of_book_greeks {
+  double delta, gamma, vega, theta, rho;
+  double delta_se, gamma_se, vega_se, theta_se, rho_se;
+} of_book_greeks;
 
 /* Prices every entry of a book in one persistent kernel launch: the work is
  * cut into (option, path-block) tiles, longest first, and CTAs pull tiles
@@ -238,7 +268,17 @@ of_status of_book_plan_results(of_book_plan* plan, of_mc_result* results);
 /* Tile shape the plan uses (after autotuning) and its total path-steps. */
 of_status of_book_plan_info(of_book_plan* plan, int32_t* block, int32_t* paths_per_thread,
                             int64_t* n_tiles, double* path_steps);
+/* Greeks of the plan's last launch (plan created with mode OF_BOOK_GREEKS);
+ * waits for the launch like of_book_plan_results. */
+of_status of_book_plan_greeks(of_book_plan* plan, of_book_greeks* greeks);
 void of_book_plan_destroy(of_book_plan* plan);
+
+/* MonteCarloPricingEngine::price_with_greeks_aad
+ * (src/engines/monte_carlo/mc_engine.rs:977-987) for a whole book in one
+ * persistent launch: of_mc_price_book in mode OF_BOOK_GREEKS (cfg->mode is
+ * ignored).  results[i] and greeks[i] belong to entries[i]. */
+of_status of_mc_price_book_greeks(of_ctx* ctx, const of_book_entry* entries, int64_t n, const of_book_config* cfg,
+                                  of_mc_result* results, of_book_greeks* greeks);
 
 /* ---- book priced to a standard-error target ----------------------------- */
 /* No single reference counterpart: the target is the one the batched-book
@@ -257,6 +297,7 @@ typedef struct of_stderr_round {
   int64_t paths;      /* their total paths */
   double path_steps;  /* their total path-steps */
   int64_t converged;  /* of them, how many met their target */
+  double kernel_ms;   /* device time of the launch (CUDA events) */
 } of_stderr_round;
 
 /* A pilot launch prices every entry with target->pilot_paths paths
@@ -275,6 +316,13 @@ typedef struct of_stderr_round {
 of_status of_book_price_to_stderr(of_ctx* ctx, const of_book_entry* entries, int64_t n, const of_book_config* cfg,
                                   const of_stderr_target* target, of_mc_result* results, int64_t* paths_out,
                                   of_stderr_round* rounds, int32_t* n_rounds);
+/* The same in mode OF_BOOK_GREEKS (cfg->mode is ignored): every option priced
+ * to its standard-error target with its pathwise Greeks from the same launch
+ * (greeks[i] from option i's last launch). */
+of_status of_book_price_to_stderr_greeks(of_ctx* ctx, const of_book_entry* entries, int64_t n,
+                                         const of_book_config* cfg, const of_stderr_target* target,
+                                         of_mc_result* results, of_book_greeks* greeks, int64_t* paths_out,
+                                         of_stderr_round* rounds, int32_t* n_rounds);
 
 /* ---- tile-shape autotuner ----------------------------------------------- */
 /* The reference has no counterpart (its GPU engine uses one fixed launch
@@ -441,6 +489,30 @@ typedef struct of_boundary_point {
 of_status of_lsm_bermudan(of_ctx* ctx, const of_bermudan_contract* contract, const of_lsm_config* cfg,
                           of_lsm_result* result, of_boundary_point* boundary, int64_t capacity,
                           int64_t* n_boundary);
+
+/* A European barrier option priced by the LSM engine
+ * (LongstaffSchwartzEngine::price(BarrierOption),
+ * src/engines/lsm/longstaff_schwartz.rs:632-736). */
+typedef struct of_lsm_barrier_contract {
+  int32_t option_type;        /* OF_CALL / OF_PUT */
+  int32_t barrier_direction;  /* OF_BARRIER_UP / OF_BARRIER_DOWN */
+  int32_t barrier_style;      /* OF_BARRIER_IN / OF_BARRIER_OUT */
+  int32_t reserved0;
+  double spot, strike, rate;
+  double dividend_yield;      /* market.effective_dividend_yield(expiry) */
+  double vol;                 /* market.vol_for(strike, expiry) */
+  double expiry, barrier_level, rebate;
+  int64_t num_steps;
+} of_lsm_barrier_contract;
+
+/* The LSM engine's European barrier Monte Carlo on its single xoshiro256++
+ * stream (FP64_REFERENCE only): path-major draws, log-Euler steps, the barrier
+ * monitored on path[0..=steps] (>= up, <= down), the vanilla payoff of the
+ * terminal spot when active and the rebate otherwise, discounted by
+ * exp(-r T); `result` gets price, stderr_ (mean_and_stderr, :125-140) and
+ * kernel_ms.  cfg->injected_normals ([path][step]) replaces the stream. */
+of_status of_lsm_barrier(of_ctx* ctx, const of_lsm_barrier_contract* contract, const of_lsm_config* cfg,
+                         of_lsm_result* result);
 
 /* xoshiro256++ jump-ahead: the state of the stream seeded with `seed`
  * (Xoshiro256PlusPlus::seed_from_u64, src/math/fast_rng.rs:36-48) after

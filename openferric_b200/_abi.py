@@ -100,14 +100,24 @@ class OfBookEntry(C.Structure):
     ]
 
 
+OF_BOOK_PRICE = 0
+OF_BOOK_GREEKS = 1
+OF_BOOK_PRICE_FP64 = 2
+
+
 class OfBookConfig(C.Structure):
     _fields_ = [
         ("seed", C.c_uint64),
         ("block", C.c_int32),
         ("paths_per_thread", C.c_int32),
         ("use_graph", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("mode", C.c_int32),
     ]
+
+
+class OfBookGreeks(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("delta", "gamma", "vega", "theta", "rho",
+                                           "delta_se", "gamma_se", "vega_se", "theta_se", "rho_se")]
 
 
 class OfStderrTarget(C.Structure):
@@ -125,6 +135,7 @@ class OfStderrRound(C.Structure):
         ("paths", C.c_int64),
         ("path_steps", C.c_double),
         ("converged", C.c_int64),
+        ("kernel_ms", C.c_double),
     ]
 
 
@@ -192,6 +203,24 @@ class OfLsmContract(C.Structure):
         ("num_steps", C.c_int64),
         ("exercise_dates", C.POINTER(C.c_double)),
         ("n_exercise_dates", C.c_int64),
+    ]
+
+
+class OfLsmBarrierContract(C.Structure):
+    _fields_ = [
+        ("option_type", C.c_int32),
+        ("barrier_direction", C.c_int32),
+        ("barrier_style", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("spot", C.c_double),
+        ("strike", C.c_double),
+        ("rate", C.c_double),
+        ("dividend_yield", C.c_double),
+        ("vol", C.c_double),
+        ("expiry", C.c_double),
+        ("barrier_level", C.c_double),
+        ("rebate", C.c_double),
+        ("num_steps", C.c_int64),
     ]
 
 
@@ -276,6 +305,7 @@ class OfDevicePeaks(C.Structure):
         ("sfu_ops_per_s", C.c_double),
         ("fp32_flops_per_s", C.c_double),
         ("probe_ms", C.c_double),
+        ("fp64_flops_per_s", C.c_double),
     ]
 
 

@@ -24,7 +24,8 @@ EXPORTED = [
     "of_book_plan_destroy", "of_mc_european_pathwise_aad", "of_heston_price_delta_aad", "of_mc_greek_estimators",
     "of_lsm_price", "of_xoshiro_jump", "of_heston_price_adjoint", "of_mc_european_gpu", "of_mc_strip_noalloc",
     "of_measure_device_peaks", "of_lsm_bermudan", "of_mc_european_qmc", "of_autotune_strip", "of_autotune_book",
-    "of_test_bounded_wait", "of_book_price_to_stderr",
+    "of_test_bounded_wait", "of_book_price_to_stderr", "of_book_plan_greeks", "of_mc_price_book_greeks",
+    "of_book_price_to_stderr_greeks", "of_lsm_barrier",
 ]
 
 
@@ -79,6 +80,8 @@ def _declare(L):
         getattr(L, name).restype = C.c_int
     L.of_lsm_price.argtypes = [vp, P(A.OfLsmContract), C.c_int64, P(A.OfLsmConfig), P(A.OfLsmResult)]
     L.of_lsm_price.restype = C.c_int
+    L.of_lsm_barrier.argtypes = [vp, P(A.OfLsmBarrierContract), P(A.OfLsmConfig), P(A.OfLsmResult)]
+    L.of_lsm_barrier.restype = C.c_int
     L.of_xoshiro_jump.argtypes = [vp, C.c_uint64, P(C.c_uint64), C.c_int64, P(C.c_uint64)]
     L.of_xoshiro_jump.restype = C.c_int
     L.of_heston_price_adjoint.argtypes = [vp, P(A.OfHestonAdjointParams), P(A.OfAdjointResult)]
@@ -107,6 +110,15 @@ def _declare(L):
     L.of_book_price_to_stderr.argtypes = [vp, P(A.OfBookEntry), C.c_int64, P(A.OfBookConfig), P(A.OfStderrTarget),
                                           P(A.OfMcResult), P(C.c_int64), P(A.OfStderrRound), P(C.c_int32)]
     L.of_book_price_to_stderr.restype = C.c_int
+    L.of_book_plan_greeks.argtypes = [vp, P(A.OfBookGreeks)]
+    L.of_book_plan_greeks.restype = C.c_int
+    L.of_mc_price_book_greeks.argtypes = [vp, P(A.OfBookEntry), C.c_int64, P(A.OfBookConfig), P(A.OfMcResult),
+                                          P(A.OfBookGreeks)]
+    L.of_mc_price_book_greeks.restype = C.c_int
+    L.of_book_price_to_stderr_greeks.argtypes = [vp, P(A.OfBookEntry), C.c_int64, P(A.OfBookConfig),
+                                                 P(A.OfStderrTarget), P(A.OfMcResult), P(A.OfBookGreeks),
+                                                 P(C.c_int64), P(A.OfStderrRound), P(C.c_int32)]
+    L.of_book_price_to_stderr_greeks.restype = C.c_int
     for name in ["of_ctx_create", "of_ctx_set_stream", "of_ctx_get_stream", "of_mc_run", "of_mc_strip",
                  "of_strip_plan_create", "of_strip_plan_launch", "of_strip_plan_results", "of_mc_price_book",
                  "of_book_plan_create", "of_book_plan_launch", "of_book_plan_results", "of_book_plan_info"]:
@@ -176,12 +188,12 @@ class Context:
         self.check(self._L.of_ctx_set_stream(self.handle, C.c_void_p(ptr or None)))
 
     def device_peaks(self) -> dict:
-        """MUFU and FP32 FMA throughput of this GPU, measured by probe kernels."""
+        """MUFU, FP32 FMA and FP64 FMA throughput of this GPU, measured by probe kernels."""
         out = A.OfDevicePeaks()
         with self.lock:
             self.check(self._L.of_measure_device_peaks(self.handle, C.byref(out)))
         return {"sfu_ops_per_s": out.sfu_ops_per_s, "fp32_flops_per_s": out.fp32_flops_per_s,
-                "probe_ms": out.probe_ms}
+                "fp64_flops_per_s": out.fp64_flops_per_s, "probe_ms": out.probe_ms}
 
     def close(self):
         if getattr(self, "handle", None) and self.handle.value:

@@ -3,10 +3,13 @@ in one persistent kernel launch (of_mc_price_book / of_book_plan_*).
 
 `BookEntry` carries what MonteCarloPricingEngine::price derives per instrument
 (src/engines/monte_carlo/mc_engine.rs:875-975); `price_book` returns one
-PricingResult per entry.  `BookPlan` keeps the device tables and the captured
-CUDA graph for repeated launches.  `synthetic_book` builds the seeded mixed
-book (European / daily-fixing arithmetic Asian / up-and-out call) used by the
-benchmarks.
+PricingResult per entry.  `price_book_greeks` is
+MonteCarloPricingEngine::price_with_greeks_aad (mc_engine.rs:977-987) for a
+whole book: price, delta, vega, rho and theta of every GBM option from the
+same launch (of_mc_price_book_greeks).  `BookPlan` keeps the device tables and
+the captured CUDA graph for repeated launches.  `synthetic_book` builds the
+seeded mixed book (European / daily-fixing arithmetic Asian / up-and-out call)
+used by the benchmarks.
 """
 from __future__ import annotations
 
@@ -19,8 +22,8 @@ import numpy as np
 
 from . import _abi as A
 from ._lib import context
-from .core import (AsianSpec, Averaging, BarrierDirection, BarrierSpec, BarrierStyle, Diagnostics, OptionType,
-                   PricingResult, StrikeType)
+from .core import (AsianSpec, Averaging, BarrierDirection, BarrierSpec, BarrierStyle, Diagnostics, Greeks,
+                   OptionType, PricingResult, StrikeType)
 from .engines import (Gbm, GbmPathGenerator, VarianceReduction, _payoff_abi, instrument_control_variate,
                       reference_strike)
 from .instruments import AsianOption, BarrierOption, VanillaOption
@@ -62,16 +65,43 @@ def book_entries_abi(entries: Sequence[BookEntry]):
     return arr, keep, vols
 
 
+@dataclass
+class BookGreeksResult:
+    """One option of `price_book_greeks`: its PricingResult with `greeks`
+    filled (gamma = 0, as the reference's pathwise AAD returns it) and the
+    Monte Carlo standard error of each Greek."""
+    result: PricingResult
+    greeks_stderr: Greeks
+
+
+def _greeks_of(g: A.OfBookGreeks):
+    return (Greeks(delta=g.delta, gamma=g.gamma, vega=g.vega, theta=g.theta, rho=g.rho),
+            Greeks(delta=g.delta_se, gamma=g.gamma_se, vega=g.vega_se, theta=g.theta_se, rho=g.rho_se))
+
+
+def _diagnostics(paths, steps, vol):
+    d = Diagnostics()
+    d.insert("num_paths", float(paths))
+    d.insert("num_steps", float(steps))
+    d.insert("vol", vol)
+    return d
+
+
 class BookPlan:
-    """Device tables + CUDA graph for a book; launch() replays without a host sync."""
+    """Device tables + CUDA graph for a book; launch() replays without a host sync.
+
+    mode: A.OF_BOOK_PRICE (prices), A.OF_BOOK_GREEKS (prices and pathwise
+    Greeks; `greeks()` reads them) or A.OF_BOOK_PRICE_FP64 (the Greeks mode's
+    prices in FP64 on the same draws, for bump-and-revalue checks)."""
 
     def __init__(self, entries: Sequence[BookEntry], seed: int, block: int = 0, paths_per_thread: int = 0,
-                 use_graph: bool = True, device: int = 0):
+                 use_graph: bool = True, device: int = 0, mode: int = A.OF_BOOK_PRICE):
         self.ctx = context(device)
         self.n = len(entries)
+        self.mode = int(mode)
         arr, self._keep, self._vols = book_entries_abi(entries)
         cfg = A.OfBookConfig(seed=int(seed) & 0xFFFFFFFFFFFFFFFF, block=block, paths_per_thread=paths_per_thread,
-                             use_graph=int(use_graph))
+                             use_graph=int(use_graph), mode=self.mode)
         h = C.c_void_p()
         with self.ctx.lock:
             self.ctx.check(self.ctx._L.of_book_plan_create(self.ctx.handle, arr, self.n, C.byref(cfg), C.byref(h)))
@@ -92,14 +122,21 @@ class BookPlan:
         return list(out)
 
     def results(self) -> List[PricingResult]:
-        res = []
-        for e, r, vol in zip(self.entries, self.raw_results(), self._vols):
-            d = Diagnostics()
-            d.insert("num_paths", float(e.num_paths))
-            d.insert("num_steps", float(e.num_steps))
-            d.insert("vol", vol)
-            res.append(PricingResult(price=r.price, stderr=r.stderr_, diagnostics=d))
-        return res
+        return [PricingResult(price=r.price, stderr=r.stderr_, diagnostics=_diagnostics(e.num_paths, e.num_steps, vol))
+                for e, r, vol in zip(self.entries, self.raw_results(), self._vols)]
+
+    def raw_greeks(self) -> List[A.OfBookGreeks]:
+        out = (A.OfBookGreeks * self.n)()
+        self.ctx.check(self.ctx._L.of_book_plan_greeks(self.handle, out))
+        return list(out)
+
+    def greeks_results(self) -> List[BookGreeksResult]:
+        """Prices and Greeks of the last launch (mode OF_BOOK_GREEKS)."""
+        out = []
+        for r, g in zip(self.results(), self.raw_greeks()):
+            r.greeks, se = _greeks_of(g)
+            out.append(BookGreeksResult(r, se))
+        return out
 
     def close(self):
         if self.handle and self.handle.value:
@@ -123,14 +160,44 @@ def price_book(entries: Sequence[BookEntry], seed: int, block: int = 0, paths_pe
         plan.close()
 
 
+def price_book_greeks(entries: Sequence[BookEntry], seed: int, block: int = 0, paths_per_thread: int = 0,
+                      device: int = 0) -> List[BookGreeksResult]:
+    """Price and pathwise Greeks (delta, vega, rho, theta) of every entry in
+    one persistent launch (of_mc_price_book_greeks).  GBM options without
+    discrete dividends; barrier options are priced by one-step survival (no
+    control variate), the other payoffs by the book's own estimator."""
+    plan = BookPlan(entries, seed, block, paths_per_thread, use_graph=False, device=device, mode=A.OF_BOOK_GREEKS)
+    try:
+        plan.launch()
+        return plan.greeks_results()
+    finally:
+        plan.close()
+
+
+def price_book_fp64(entries: Sequence[BookEntry], seed: int, block: int = 0, paths_per_thread: int = 0,
+                    device: int = 0) -> List[PricingResult]:
+    """The prices of `price_book_greeks` in FP64 path arithmetic on the same
+    draws (same seed, entries and path counts): the revaluations of a
+    bump-and-revalue check with common random numbers."""
+    plan = BookPlan(entries, seed, block, paths_per_thread, use_graph=False, device=device,
+                    mode=A.OF_BOOK_PRICE_FP64)
+    try:
+        plan.launch()
+        return plan.results()
+    finally:
+        plan.close()
+
+
 @dataclass
 class StderrRound:
     """One book launch of `price_book_to_stderr`: how many options it priced,
-    their total paths and path-steps, and how many met the target."""
+    their total paths and path-steps, how many met the target, and the
+    launch's device time."""
     options: int
     paths: int
     path_steps: float
     converged: int
+    kernel_ms: float = 0.0
 
 
 def paths_for_stderr(paths: int, stderr: float, target: float, margin: float = 1.1, granule: int = 256) -> int:
@@ -146,7 +213,7 @@ def paths_for_stderr(paths: int, stderr: float, target: float, margin: float = 1
 
 
 def price_book_to_stderr(entries: Sequence[BookEntry], seed: int, se_rel: float = 1e-4, pilot_paths: int = 8192,
-                         max_rounds: int = 4, device: int = 0):
+                         max_rounds: int = 4, device: int = 0, greeks: bool = False):
     """Prices every entry to a standard error of at most `se_rel` x its spot
     (of_book_price_to_stderr).
 
@@ -156,7 +223,11 @@ def price_book_to_stderr(entries: Sequence[BookEntry], seed: int, se_rel: float 
     that estimate, and so on until all meet the target or `max_rounds`
     launches have run.  Each round draws from its own seed (seed + round), and
     an option's result is the one of its last round (its diagnostics carry
-    that round's path count).  Returns the results and the rounds."""
+    that round's path count).  Returns the results and the rounds.
+
+    greeks=True prices every launch with the pathwise Greeks
+    (of_book_price_to_stderr_greeks): the results are then BookGreeksResult,
+    each option's Greeks from the launch of its price."""
     ctx = context(device)
     n = len(entries)
     arr, keep, vols = book_entries_abi(entries)
@@ -166,18 +237,24 @@ def price_book_to_stderr(entries: Sequence[BookEntry], seed: int, se_rel: float 
     paths = (C.c_int64 * n)()
     rounds = (A.OfStderrRound * max(1, int(max_rounds)))()
     n_rounds = C.c_int32()
+    gr = (A.OfBookGreeks * n)() if greeks else None
     with ctx.lock:
-        ctx.check(ctx._L.of_book_price_to_stderr(ctx.handle, arr, n, C.byref(cfg), C.byref(tgt), out, paths, rounds,
-                                                 C.byref(n_rounds)))
+        if greeks:
+            ctx.check(ctx._L.of_book_price_to_stderr_greeks(ctx.handle, arr, n, C.byref(cfg), C.byref(tgt), out, gr,
+                                                            paths, rounds, C.byref(n_rounds)))
+        else:
+            ctx.check(ctx._L.of_book_price_to_stderr(ctx.handle, arr, n, C.byref(cfg), C.byref(tgt), out, paths,
+                                                     rounds, C.byref(n_rounds)))
     del keep
     results = []
-    for e, r, p, vol in zip(entries, out, paths, vols):
-        d = Diagnostics()
-        d.insert("num_paths", float(p))
-        d.insert("num_steps", float(e.num_steps))
-        d.insert("vol", vol)
-        results.append(PricingResult(price=r.price, stderr=r.stderr_, diagnostics=d))
-    return results, [StderrRound(rd.options, rd.paths, rd.path_steps, rd.converged) for rd in rounds[:n_rounds.value]]
+    for k, (e, r, p, vol) in enumerate(zip(entries, out, paths, vols)):
+        res = PricingResult(price=r.price, stderr=r.stderr_, diagnostics=_diagnostics(p, e.num_steps, vol))
+        if greeks:
+            res.greeks, se = _greeks_of(gr[k])
+            res = BookGreeksResult(res, se)
+        results.append(res)
+    return results, [StderrRound(rd.options, rd.paths, rd.path_steps, rd.converged, rd.kernel_ms)
+                     for rd in rounds[:n_rounds.value]]
 
 
 def synthetic_book(n: int = 4096, seed: int = 20261203, steps_per_year: int = 252, min_log2_paths: int = 14,

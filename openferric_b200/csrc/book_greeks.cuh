@@ -1,0 +1,503 @@
+// book_greeks.cuh - per-sample kernels of the batched book's Greeks modes.
+//
+// Two modes share this code and the same draws:
+//   R = float,  G = true : price and the pathwise Greeks of a GBM option
+//                          (delta, vega, rho, theta), FP32 path arithmetic;
+//   R = double, G = false: price only, FP64 path arithmetic on the same
+//                          Philox draws (the revaluations of a bump-and-
+//                          revalue check with common random numbers).
+//
+// The Greeks are the ones of MonteCarloPricingEngine::price_with_greeks_aad
+// (src/engines/monte_carlo/mc_engine.rs:977-987 -> mc_european_pathwise_aad,
+// src/engines/monte_carlo/mc_aad.rs:15-219): d PV / d(S0, sigma, r) and
+// theta = -d PV / dT with the step count fixed (dt = T / steps), the rate
+// entering the drift r - q and the discount exp(-r T).  The reference's tape
+// differentiates exp(drift + diffusion z) step by step; for GBM every step's
+// adjoint collapses to closed forms in the path's log-returns y_i:
+//   dy_i/dsigma = (y_i - a t_i) / sigma - sigma t_i,  dy_i/dr = t_i,
+//   dy_i/dT = (y_i + a t_i) / (2T),                   a = r - q - sigma^2/2,
+// so a vanilla needs y_T only and an arithmetic average needs three running
+// sums (sum w S, sum w S y, sum w S i), a geometric one sum w y.
+//
+// A discretely monitored barrier has a payoff that jumps where a path
+// touches the barrier; its pathwise derivative misses the jump.  The barrier
+// options are priced here by one-step survival (Glasserman & Staum, "Conditioning
+// on one-step survival for barrier option simulations", Oper. Res. 49, 2001):
+// at every step the next log-return is drawn conditioned to stay on the alive
+// side of the barrier, z = Phi^-1(u p) with p = Phi(h) the probability of
+// staying alive over the step, and the path carries the weight L = prod p.
+// A knock-out pays L f(S_T) + (1 - L) R, a knock-in f(S_T') - L (f(S_T) - R)
+// with S_T' the unconditioned path of the same uniforms.  Both estimators
+// are unbiased for the discretely monitored price, and smooth in the
+// parameters, so their pathwise derivatives (forward tangents of y and ln L
+// through every step) are unbiased too.
+#pragma once
+
+#include "of_device.cuh"
+
+namespace of {
+
+// The book's Greeks-mode kinds (which step loop an option takes).
+enum : int32_t { GK_TERMINAL = 0, GK_ASIAN_DAILY = 1, GK_ASIAN_WEIGHTS = 2, GK_BARRIER_OUT = 3, GK_BARRIER_IN = 4 };
+enum : int32_t {
+  GF_CALL = 1,
+  GF_ANTI = 2,
+  GF_FLOATING = 4,       // Asian floating strike: max(+-(S_T - avg), 0)
+  GF_GEOMETRIC = 8,      // Asian geometric average
+  GF_TERMINAL_ONLY = 16  // Asian with no observations: the terminal spot is the average
+};
+// Control variates of the Greeks modes (the price only; the Greeks carry none).
+enum : int32_t { GCV_NONE = 0, GCV_VANILLA_TERMINAL = 1, GCV_GEOMETRIC_ASIAN = 2, GCV_TERMINAL_SPOT = 3 };
+
+// Per-option constants in the path's arithmetic type R, built on the host
+// in FP64 and rounded once.
+template <typename R>
+struct GreekConsts {
+  R alpha, beta;        // per step: log drift (r - q - sigma^2/2) dt and sigma sqrt(dt)
+  R a, dt, T, sigma, r, df;
+  R s0, strike, rebate;
+  R inv_n;              // Asian: 1 / number of observations
+  R w1;                 // Asian: sum_i w_i i over the observed step indices
+  R bar, sgn, sib;      // barrier: log(B/S0); +1 up, -1 down; sgn / beta
+  // tangent coefficients (parameters in the order ln S0, sigma, r, T)
+  R sig_dt, inv_sig, beta_over_sig, alpha_over_T, inv_2T, beta_over_2T;
+  int32_t kind, flags, steps, obs_offset, cv_kind;
+  uint32_t stream;
+};
+
+// One sample (antithetic pairs averaged): the undiscounted payoff x, the
+// control variate y, and the discounted pathwise derivatives
+// g = (delta, vega, rho, theta) of df x.
+template <typename R>
+struct GreekSample {
+  R x, y;
+  R g[4];
+};
+
+template <typename R>
+struct GMath;
+
+template <>
+struct GMath<float> {
+  static constexpr float kTiny = 1e-30f;  // floor of the survival-draw uniform (above FLT_MIN)
+  static constexpr float kHMin = -12.0f;  // Phi(-12) = 1.8e-33 is still a normal float
+  static __device__ __forceinline__ float exp(float x) { return __expf(x); }
+  static __device__ __forceinline__ float cdf(float x) { return normcdff(x); }
+  static __device__ __forceinline__ float icdf(float x) { return normcdfinvf(x); }
+  static __device__ __forceinline__ float unif(uint32_t r) { return uniform_from_u32(r); }
+  static __device__ __forceinline__ void pair(uint32_t a, uint32_t b, float& z1, float& z2) {
+    const float2 p = normal_pair_from_u32(a, b);
+    z1 = p.x;
+    z2 = p.y;
+  }
+};
+
+template <>
+struct GMath<double> {
+  static constexpr double kTiny = 1e-300;
+  static constexpr double kHMin = -37.0;
+  static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
+  static __device__ __forceinline__ double cdf(double x) { return ::normcdf(x); }
+  static __device__ __forceinline__ double icdf(double x) { return ::normcdfinv(x); }
+  // the grid of uniform_from_u32: (k + 0.5) 2^-23, k = the top 23 bits (exact in either type)
+  static __device__ __forceinline__ double unif(uint32_t r) { return ((double)(r >> 9) + 0.5) * 0x1p-23; }
+  // normal_pair_from_u32's transform in FP64: radius sqrt(-2 ln u1), angle pi (2 f - 3)
+  static __device__ __forceinline__ void pair(uint32_t a, uint32_t b, double& z1, double& z2) {
+    const double rad = ::sqrt(-2.0 * ::log(unif(a)));
+    const double f = 1.0 + (double)(b >> 9) * 0x1p-23;
+    double s, c;
+    ::sincospi(2.0 * f - 3.0, &s, &c);
+    z1 = rad * c;
+    z2 = rad * s;
+  }
+};
+
+// The four draws of Philox block q of sample i: Box-Muller normals (the
+// book's draws for GBM steps) or uniforms (survival draws).
+template <typename R>
+__device__ __forceinline__ void gk_normals(const GreekConsts<R>& c, uint32_t q, uint32_t lo, uint32_t hi,
+                                           const PhiloxKeys& K, R (&z)[4]) {
+  const uint4 r = philox4x32_10(make_uint4(q, lo, hi, c.stream), K);
+  GMath<R>::pair(r.x, r.y, z[0], z[1]);
+  GMath<R>::pair(r.z, r.w, z[2], z[3]);
+}
+
+template <typename R>
+__device__ __forceinline__ void gk_uniforms(const GreekConsts<R>& c, uint32_t q, uint32_t lo, uint32_t hi,
+                                            const PhiloxKeys& K, R (&u)[4]) {
+  const uint4 r = philox4x32_10(make_uint4(q, lo, hi, c.stream), K);
+  u[0] = GMath<R>::unif(r.x);
+  u[1] = GMath<R>::unif(r.y);
+  u[2] = GMath<R>::unif(r.z);
+  u[3] = GMath<R>::unif(r.w);
+}
+
+// The terminal spot S_T = s0 e^y and its derivatives along (ln S0, sigma, r, T)
+// for an unconditioned GBM path.
+template <typename R>
+__device__ __forceinline__ R gk_spot(const GreekConsts<R>& c, R y, R (&d)[4]) {
+  const R s = c.s0 * GMath<R>::exp(y);
+  d[0] = s;
+  d[1] = s * ((y - c.a * c.T) * c.inv_sig - c.sigma * c.T);
+  d[2] = s * c.T;
+  d[3] = s * (y + c.a * c.T) * c.inv_2T;
+  return s;
+}
+
+// f = max(phi (u - v), 0) and, where G, its derivative df = phi (du - dv) on
+// the exercised side (0 elsewhere).
+template <typename R, bool G>
+__device__ __forceinline__ R gk_vanilla(bool call, R u, R v, const R (&du)[4], const R (&dv)[4], R (&df)[4]) {
+  const R diff = call ? u - v : v - u;
+  const R f = diff > (R)0 ? diff : (R)0;
+  if (G) {
+    const R m = diff > (R)0 ? (call ? (R)1 : (R)-1) : (R)0;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) df[t] = m * (du[t] - dv[t]);
+  }
+  return f;
+}
+
+// Discounted Greeks of one leg from its undiscounted payoff x and dx along
+// (ln S0, sigma, r, T): delta = df dx0 / s0, vega = df dx1,
+// rho = df dx2 - T df x, theta = -(df dx3 - r df x).
+template <typename R>
+__device__ __forceinline__ void gk_discount(const GreekConsts<R>& c, R x, const R (&dx)[4], R (&g)[4]) {
+  const R pv = c.df * x;
+  g[0] = c.df * dx[0] / c.s0;
+  g[1] = c.df * dx[1];
+  g[2] = c.df * dx[2] - c.T * pv;
+  g[3] = c.r * pv - c.df * dx[3];
+}
+
+// ---- vanilla / terminal-only Asian: the path needs y_T only --------------
+template <typename R, bool G, bool ANTI>
+__device__ __forceinline__ void gk_terminal(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
+                                            GreekSample<R>& out) {
+  const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
+  R w = (R)0;  // sum of the path's normals
+  const int32_t full = c.steps & ~3;
+  for (int32_t j = 0; j < full; j += 4) {
+    R z[4];
+    gk_normals(c, (uint32_t)(j >> 2), lo, hi, K, z);
+    w += (z[0] + z[1]) + (z[2] + z[3]);
+  }
+  if (full < c.steps) {
+    R z[4];
+    gk_normals(c, (uint32_t)(full >> 2), lo, hi, K, z);
+    w += z[0];
+    if (full + 1 < c.steps) w += z[1];
+    if (full + 2 < c.steps) w += z[2];
+  }
+  const R base = (R)c.steps * c.alpha;
+  const bool call = c.flags & GF_CALL;
+  const bool floating = (c.flags & GF_TERMINAL_ONLY) && (c.flags & GF_FLOATING);
+  R xs = (R)0, ys = (R)0, gs[4] = {(R)0, (R)0, (R)0, (R)0};
+#pragma unroll
+  for (int leg = 0; leg < (ANTI ? 2 : 1); ++leg) {
+    const R y = leg == 0 ? base + c.beta * w : base - c.beta * w;
+    R ds[4], dk[4] = {(R)0, (R)0, (R)0, (R)0}, dx[4];
+    const R s = gk_spot(c, y, ds);
+    // a floating-strike Asian on the terminal spot alone pays max(+-(S_T - S_T), 0) = 0
+    const R x = floating ? (R)0 : gk_vanilla<R, G>(call, s, c.strike, ds, dk, dx);
+    if (floating)
+      for (int t = 0; t < 4; ++t) dx[t] = (R)0;
+    R y_cv = (R)0;
+    if (c.cv_kind == GCV_VANILLA_TERMINAL || c.cv_kind == GCV_GEOMETRIC_ASIAN)
+      y_cv = call ? (s > c.strike ? s - c.strike : (R)0) : (c.strike > s ? c.strike - s : (R)0);
+    else if (c.cv_kind == GCV_TERMINAL_SPOT)
+      y_cv = s;
+    xs += x;
+    ys += y_cv;
+    if (G) {
+      R g[4];
+      gk_discount(c, x, dx, g);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) gs[t] += g[t];
+    }
+  }
+  const R h = ANTI ? (R)0.5 : (R)1;
+  out.x = h * xs;
+  out.y = h * ys;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) out.g[t] = h * gs[t];
+}
+
+// ---- Asian: running sums of the observed spots ----------------------------
+template <typename R>
+struct AsianLeg {
+  R y;
+  R p0, p0c;  // sum w e^y (compensated in FP32)
+  R p1, p2;   // sum w e^y y, sum w e^y i
+  R q;        // sum w y
+};
+
+template <typename R, bool G, bool NEED_ARITH, bool NEED_GEO>
+__device__ __forceinline__ void gk_observe(AsianLeg<R>& L, R w, R idx) {
+  if (NEED_ARITH) {
+    const R e = w * GMath<R>::exp(L.y);
+    const R yk = e - L.p0c;
+    const R t = L.p0 + yk;
+    L.p0c = (t - L.p0) - yk;
+    L.p0 = t;
+    if (G) {
+      L.p1 = fma(e, L.y, L.p1);
+      L.p2 = fma(e, idx, L.p2);
+    }
+  }
+  if (NEED_GEO) L.q = fma(w, L.y, L.q);
+}
+
+template <typename R, bool G, bool ANTI, bool DAILY, bool NEED_ARITH, bool NEED_GEO>
+__device__ __forceinline__ void gk_asian(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
+                                         const float* __restrict__ obs_w, GreekSample<R>& out) {
+  const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
+  AsianLeg<R> A{}, B{};
+  if (!DAILY) {  // an observation at t = 0: e^0 = 1, y = 0, i = 0
+    const R w0 = (R)__ldg(obs_w + c.obs_offset);
+    if (NEED_ARITH) A.p0 = B.p0 = w0;
+  }
+  R idx = (R)0;
+  auto step = [&](R z, int32_t j) {
+    idx += (R)1;
+    A.y = fma(c.beta, z, A.y + c.alpha);
+    if (ANTI) B.y = fma(-c.beta, z, B.y + c.alpha);
+    const R w = DAILY ? (R)1 : (R)__ldg(obs_w + c.obs_offset + j + 1);
+    if (DAILY || w != (R)0) {
+      gk_observe<R, G, NEED_ARITH, NEED_GEO>(A, w, idx);
+      if (ANTI) gk_observe<R, G, NEED_ARITH, NEED_GEO>(B, w, idx);
+    }
+  };
+  const int32_t full = c.steps & ~3;
+  for (int32_t j = 0; j < full; j += 4) {
+    R z[4];
+    gk_normals(c, (uint32_t)(j >> 2), lo, hi, K, z);
+    step(z[0], j);
+    step(z[1], j + 1);
+    step(z[2], j + 2);
+    step(z[3], j + 3);
+  }
+  if (full < c.steps) {
+    R z[4];
+    gk_normals(c, (uint32_t)(full >> 2), lo, hi, K, z);
+    step(z[0], full);
+    if (full + 1 < c.steps) step(z[1], full + 1);
+    if (full + 2 < c.steps) step(z[2], full + 2);
+  }
+  const bool call = c.flags & GF_CALL;
+  const bool floating = c.flags & GF_FLOATING;
+  R xs = (R)0, ys = (R)0, gs[4] = {(R)0, (R)0, (R)0, (R)0};
+#pragma unroll
+  for (int leg = 0; leg < (ANTI ? 2 : 1); ++leg) {
+    const AsianLeg<R>& L = leg == 0 ? A : B;
+    R ds[4], da[4], dg[4], dk[4] = {(R)0, (R)0, (R)0, (R)0}, dx[4];
+    const R s = gk_spot(c, L.y, ds);
+    R geo = (R)0;
+    if (NEED_GEO) {  // G = s0 exp(q / n); d/dtheta = G sum_i w_i dy_i/dtheta / n
+      geo = c.s0 * GMath<R>::exp(L.q * c.inv_n);
+      dg[0] = geo;
+      dg[1] = geo * c.inv_n * (L.q * c.inv_sig - (c.a * c.inv_sig + c.sigma) * c.dt * c.w1);
+      dg[2] = geo * c.inv_n * c.dt * c.w1;
+      dg[3] = geo * c.inv_n * (L.q + c.a * c.dt * c.w1) * c.inv_2T;
+    }
+    R avg;
+    if (c.flags & GF_GEOMETRIC) {
+      avg = geo;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) da[t] = dg[t];
+    } else {
+      const R sn = c.s0 * c.inv_n;
+      avg = sn * (L.p0 - L.p0c);
+      if (G) {
+        da[0] = avg;
+        da[1] = sn * (L.p1 * c.inv_sig - (c.a * c.inv_sig + c.sigma) * c.dt * L.p2);
+        da[2] = sn * c.dt * L.p2;
+        da[3] = sn * (L.p1 + c.a * c.dt * L.p2) * c.inv_2T;
+      }
+    }
+    const R x = floating ? gk_vanilla<R, G>(call, s, avg, ds, da, dx) : gk_vanilla<R, G>(call, avg, c.strike, da, dk, dx);
+    R y_cv = (R)0;
+    if (c.cv_kind == GCV_VANILLA_TERMINAL)
+      y_cv = call ? (s > c.strike ? s - c.strike : (R)0) : (c.strike > s ? c.strike - s : (R)0);
+    else if (c.cv_kind == GCV_GEOMETRIC_ASIAN)
+      y_cv = call ? (geo > c.strike ? geo - c.strike : (R)0) : (c.strike > geo ? c.strike - geo : (R)0);
+    else if (c.cv_kind == GCV_TERMINAL_SPOT)
+      y_cv = s;
+    xs += x;
+    ys += y_cv;
+    if (G) {
+      R g[4];
+      gk_discount(c, x, dx, g);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) gs[t] += g[t];
+    }
+  }
+  const R h = ANTI ? (R)0.5 : (R)1;
+  out.x = h * xs;
+  out.y = h * ys;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) out.g[t] = h * gs[t];
+}
+
+// ---- barrier: one-step survival -------------------------------------------
+template <typename R, bool G>
+struct SurvLeg {
+  R y, L;    // log-return of the conditioned path and its survival weight
+  R ypl;     // knock-in: the unconditioned path of the same uniforms
+  R yd[4];   // tangents of y along (ln S0, sigma, r, T)
+  R ld[4];   // tangents of ln L
+};
+
+template <typename R, bool G>
+__device__ __forceinline__ void surv_init(SurvLeg<R, G>& s, const GreekConsts<R>& c) {
+  s.y = (R)0;
+  s.ypl = (R)0;
+  s.L = c.sgn * c.bar > (R)0 ? (R)1 : (R)0;  // the scan includes path[0]: a spot already beyond the barrier is out
+#pragma unroll
+  for (int t = 0; t < 4; ++t) s.yd[t] = s.ld[t] = (R)0;
+}
+
+// One step: h = sgn (bar - y - alpha) / beta is the standardised distance to
+// the barrier, p = Phi(h) the probability of staying alive, and the step's
+// normal is drawn from the alive side, z = sgn Phi^-1(u p).  Tangents (for
+// each parameter with b' = d bar, alpha', beta'):
+//   h' = sgn (b' - y' - alpha') / beta - h beta' / beta,
+//   (ln p)' = g h' with g = phi(h) / p,
+//   z' = sgn u p' / phi(Phi^-1(u p)) = sgn (v / phi(zeta)) g h',   v = u p,
+//   y_next' = y' + alpha' + beta' z + beta z'.
+template <typename R, bool G, bool IN>
+__device__ __forceinline__ void surv_step(SurvLeg<R, G>& s, const GreekConsts<R>& c, R u) {
+  R h = c.sib * (c.bar - s.y - c.alpha);
+  h = h > GMath<R>::kHMin ? h : GMath<R>::kHMin;
+  const R p = GMath<R>::cdf(h);
+  const R v = u * p;
+  const R q = fma(-u, p, (R)1);  // 1 - u p with one rounding
+  const bool upper = v > (R)0.5;
+  R lo = upper ? q : v;
+  lo = lo > GMath<R>::kTiny ? lo : GMath<R>::kTiny;
+  R zeta = GMath<R>::icdf(lo);
+  zeta = upper ? -zeta : zeta;
+  const R z = c.sgn * zeta;
+  if (G) {
+    const R kInvSqrt2Pi = (R)0.398942280401432677939946;
+    const R phih = kInvSqrt2Pi * GMath<R>::exp((R)-0.5 * h * h);
+    const R phiz = kInvSqrt2Pi * GMath<R>::exp((R)-0.5 * zeta * zeta);
+    const R g = phih / p;
+    const R k = c.beta * c.sgn * (v / phiz) * g;  // d y_next / d h
+    // ln S0: b' = -1
+    const R h0 = c.sib * ((R)-1 - s.yd[0]);
+    s.ld[0] = fma(g, h0, s.ld[0]);
+    s.yd[0] = fma(k, h0, s.yd[0]);
+    // sigma: alpha' = -sigma dt, beta' / beta = 1 / sigma
+    const R h1 = fma(c.sib, c.sig_dt - s.yd[1], -h * c.inv_sig);
+    s.ld[1] = fma(g, h1, s.ld[1]);
+    s.yd[1] = fma(k, h1, s.yd[1] + fma(c.beta_over_sig, z, -c.sig_dt));
+    // r: alpha' = dt
+    const R h2 = c.sib * (-c.dt - s.yd[2]);
+    s.ld[2] = fma(g, h2, s.ld[2]);
+    s.yd[2] = fma(k, h2, s.yd[2] + c.dt);
+    // T (steps fixed): alpha' = alpha / T, beta' / beta = 1 / (2T)
+    const R h3 = fma(c.sib, -c.alpha_over_T - s.yd[3], -h * c.inv_2T);
+    s.ld[3] = fma(g, h3, s.ld[3]);
+    s.yd[3] = fma(k, h3, s.yd[3] + fma(c.beta_over_2T, z, c.alpha_over_T));
+  }
+  s.y = fma(c.beta, z, s.y + c.alpha);
+  s.L *= p;
+  if (IN) s.ypl = fma(c.beta, GMath<R>::icdf(u), s.ypl + c.alpha);
+}
+
+template <typename R, bool G, bool IN>
+__device__ __forceinline__ void surv_payoff(const SurvLeg<R, G>& s, const GreekConsts<R>& c, R& x, R (&g)[4]) {
+  const bool call = c.flags & GF_CALL;
+  R ds[4], dk[4] = {(R)0, (R)0, (R)0, (R)0}, dfo[4], dx[4];
+  const R so = c.s0 * GMath<R>::exp(s.y);
+  if (G) {  // S = s0 e^y with y depending on ln S0 through the barrier: dS/dlnS0 = S (1 + y')
+    ds[0] = so * ((R)1 + s.yd[0]);
+#pragma unroll
+    for (int t = 1; t < 4; ++t) ds[t] = so * s.yd[t];
+  }
+  const R fo = gk_vanilla<R, G>(call, so, c.strike, ds, dk, dfo);
+  if (!IN) {
+    x = s.L * fo + ((R)1 - s.L) * c.rebate;  // L f + (1 - L) R
+    if (G) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) dx[t] = s.L * fma(s.ld[t], fo - c.rebate, dfo[t]);
+    }
+  } else {
+    R dp[4], dfp[4];
+    const R sp = gk_spot(c, s.ypl, dp);
+    const R fp = gk_vanilla<R, G>(call, sp, c.strike, dp, dk, dfp);
+    x = fp - s.L * (fo - c.rebate);  // f(S') - L (f(S) - R)
+    if (G) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) dx[t] = dfp[t] - s.L * fma(s.ld[t], fo - c.rebate, dfo[t]);
+    }
+  }
+  if (G) gk_discount(c, x, dx, g);
+}
+
+template <typename R, bool G, bool ANTI, bool IN>
+__device__ __forceinline__ void gk_barrier(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
+                                           GreekSample<R>& out) {
+  const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
+  SurvLeg<R, G> A, B;
+  surv_init(A, c);
+  if (ANTI) surv_init(B, c);
+  for (int32_t j = 0; j < c.steps; j += 4) {
+    R u[4];
+    gk_uniforms(c, (uint32_t)(j >> 2), lo, hi, K, u);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (j + q >= c.steps) break;
+      surv_step<R, G, IN>(A, c, u[q]);
+      if (ANTI) surv_step<R, G, IN>(B, c, (R)1 - u[q]);  // antithetic in the uniform
+    }
+  }
+  R x, g[4];
+  surv_payoff<R, G, IN>(A, c, x, g);
+  out.x = x;
+  out.y = (R)0;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) out.g[t] = g[t];
+  if (ANTI) {
+    surv_payoff<R, G, IN>(B, c, x, g);
+    out.x = (R)0.5 * (out.x + x);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) out.g[t] = (R)0.5 * (out.g[t] + g[t]);
+  }
+}
+
+// ---- dispatch ---------------------------------------------------------------
+template <typename R, bool G, bool ANTI>
+__device__ __forceinline__ void gk_sample_anti(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
+                                               const float* obs_w, GreekSample<R>& out) {
+  switch (c.kind) {
+    case GK_TERMINAL:
+      gk_terminal<R, G, ANTI>(c, i, K, out);
+      return;
+    case GK_ASIAN_DAILY:
+      if (c.flags & GF_GEOMETRIC) gk_asian<R, G, ANTI, true, false, true>(c, i, K, obs_w, out);
+      else if (c.cv_kind == GCV_GEOMETRIC_ASIAN) gk_asian<R, G, ANTI, true, true, true>(c, i, K, obs_w, out);
+      else gk_asian<R, G, ANTI, true, true, false>(c, i, K, obs_w, out);
+      return;
+    case GK_ASIAN_WEIGHTS:
+      if (c.flags & GF_GEOMETRIC) gk_asian<R, G, ANTI, false, false, true>(c, i, K, obs_w, out);
+      else gk_asian<R, G, ANTI, false, true, true>(c, i, K, obs_w, out);
+      return;
+    case GK_BARRIER_OUT:
+      gk_barrier<R, G, ANTI, false>(c, i, K, out);
+      return;
+    default:
+      gk_barrier<R, G, ANTI, true>(c, i, K, out);
+      return;
+  }
+}
+
+template <typename R, bool G>
+__device__ __forceinline__ void gk_sample(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
+                                          const float* obs_w, GreekSample<R>& out) {
+  if (c.flags & GF_ANTI) gk_sample_anti<R, G, true>(c, i, K, obs_w, out);
+  else gk_sample_anti<R, G, false>(c, i, K, obs_w, out);
+}
+
+}  // namespace of

@@ -1,6 +1,7 @@
-// book_stderr.cu - of_book_price_to_stderr: a book priced until every option
-// meets a standard-error target.  Host-only: each round is one batched-book
-// launch (of_mc_price_book) over the options still above their target.
+// book_stderr.cu - of_book_price_to_stderr(_greeks): a book priced until
+// every option meets a standard-error target.  Host-only: each round is one
+// batched-book launch (of_mc_price_book, or of_mc_price_book_greeks with the
+// pathwise Greeks) over the options still above their target.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -21,10 +22,12 @@ int64_t paths_for_stderr(int64_t paths, double se, double target) {
 
 }  // namespace
 
-extern "C" of_status of_book_price_to_stderr(of_ctx* ctx, const of_book_entry* entries, int64_t n,
-                                             const of_book_config* cfg, const of_stderr_target* target,
-                                             of_mc_result* results, int64_t* paths_out, of_stderr_round* rounds,
-                                             int32_t* n_rounds) {
+// The rounds of of_book_price_to_stderr(_greeks): `greeks` non-null prices
+// every launch in mode OF_BOOK_GREEKS and keeps each option's Greeks from its
+// last launch.
+static of_status price_to_stderr(of_ctx* ctx, const of_book_entry* entries, int64_t n, const of_book_config* cfg,
+                                 const of_stderr_target* target, of_mc_result* results, of_book_greeks* greeks,
+                                 int64_t* paths_out, of_stderr_round* rounds, int32_t* n_rounds) {
   if (!ctx) return OF_ERR_INVALID_INPUT;
   if (!entries || !cfg || !target || !results || !n_rounds || n <= 0)
     return of_fail(ctx, OF_ERR_INVALID_INPUT, "book, config, target, results and n_rounds are required");
@@ -40,6 +43,7 @@ extern "C" of_status of_book_price_to_stderr(of_ctx* ctx, const of_book_entry* e
   for (int64_t i = 0; i < n; ++i) pending[(size_t)i] = i;
   std::vector<of_book_entry> sub;
   std::vector<of_mc_result> res;
+  std::vector<of_book_greeks> gr;
   int32_t r = 0;
   for (; r < target->max_rounds && !pending.empty(); ++r) {
     sub.clear();
@@ -60,11 +64,17 @@ extern "C" of_status of_book_price_to_stderr(of_ctx* ctx, const of_book_entry* e
       c.paths_per_thread = ppt;
     }
     res.assign(sub.size(), of_mc_result{});
-    OF_TRY(of_mc_price_book(ctx, sub.data(), (int64_t)sub.size(), &c, res.data()));
+    if (greeks) {
+      gr.assign(sub.size(), of_book_greeks{});
+      OF_TRY(of_mc_price_book_greeks(ctx, sub.data(), (int64_t)sub.size(), &c, res.data(), gr.data()));
+    } else {
+      OF_TRY(of_mc_price_book(ctx, sub.data(), (int64_t)sub.size(), &c, res.data()));
+    }
     std::vector<int64_t> still;
     for (size_t k = 0; k < pending.size(); ++k) {
       const int64_t i = pending[k];
       results[i] = res[k];
+      if (greeks) greeks[i] = gr[k];
       used[(size_t)i] = cur[(size_t)i].num_paths;
       const double tgt = target->se_rel * entries[i].model.s0;
       if (res[k].stderr_ > tgt) {
@@ -78,6 +88,7 @@ extern "C" of_status of_book_price_to_stderr(of_ctx* ctx, const of_book_entry* e
       o.paths = total;
       o.path_steps = steps;
       o.converged = (int64_t)(pending.size() - still.size());
+      o.kernel_ms = res.empty() ? 0.0 : res[0].kernel_ms;
     }
     pending.swap(still);
   }
@@ -85,4 +96,19 @@ extern "C" of_status of_book_price_to_stderr(of_ctx* ctx, const of_book_entry* e
     for (int64_t i = 0; i < n; ++i) paths_out[i] = used[(size_t)i];
   *n_rounds = r;
   return OF_OK;
+}
+
+extern "C" of_status of_book_price_to_stderr(of_ctx* ctx, const of_book_entry* entries, int64_t n,
+                                             const of_book_config* cfg, const of_stderr_target* target,
+                                             of_mc_result* results, int64_t* paths_out, of_stderr_round* rounds,
+                                             int32_t* n_rounds) {
+  return price_to_stderr(ctx, entries, n, cfg, target, results, nullptr, paths_out, rounds, n_rounds);
+}
+
+extern "C" of_status of_book_price_to_stderr_greeks(of_ctx* ctx, const of_book_entry* entries, int64_t n,
+                                                    const of_book_config* cfg, const of_stderr_target* target,
+                                                    of_mc_result* results, of_book_greeks* greeks, int64_t* paths_out,
+                                                    of_stderr_round* rounds, int32_t* n_rounds) {
+  if (ctx && !greeks) return of_fail(ctx, OF_ERR_INVALID_INPUT, "greeks is required");
+  return price_to_stderr(ctx, entries, n, cfg, target, results, greeks, paths_out, rounds, n_rounds);
 }

@@ -1865,3 +1865,138 @@ extern "C" of_status of_lsm_bermudan(of_ctx* ctx, const of_bermudan_contract* k,
   for (int64_t i = 0; i < (int64_t)pts.size() && i < capacity; ++i) boundary[i] = pts[(size_t)i];
   return OF_OK;
 }
+
+// ---------------------------------------------------------------------------
+// LongstaffSchwartzEngine::price(BarrierOption)
+// (src/engines/lsm/longstaff_schwartz.rs:632-736): European barrier Monte
+// Carlo on the engine's single xoshiro256++ stream.  A thread owns kBarChunk
+// consecutive paths and jumps its copy of the stream to the chunk's first
+// draw; each path runs log-Euler with the barrier tested at every point of
+// path[0..=steps] and adds its discounted payoff (or rebate) to FP64 sums.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kBarThreads = 128;
+constexpr int kBarChunk = 8;
+
+struct LsmBarrierParams {
+  double spot, strike, level, rebate, drift, step_vol, discount;
+  int64_t n, steps;
+  uint64_t seed;
+  int32_t call, up, knock_in;
+  const uint64_t* jump;
+  const double* inj;  // [path][step] test hook, or null
+  double* partials;   // [block][2]: sum and sum of squares of the discounted values
+};
+
+__global__ void __launch_bounds__(kBarThreads) lsm_barrier_ref(const __grid_constant__ LsmBarrierParams P) {
+  __shared__ double red_sh[2 * (kBarThreads / 32)];
+  const int64_t chunk0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * kBarChunk;
+  double acc[2] = {0.0, 0.0};
+  if (chunk0 < P.n) {
+    of::Xoshiro256pp rng;
+    if (!P.inj) {
+      rng.seed(P.seed);
+      xoshiro_jump(rng, (uint64_t)chunk0 * (uint64_t)P.steps, P.jump);
+    }
+    const int64_t end = chunk0 + kBarChunk < P.n ? chunk0 + kBarChunk : P.n;
+    for (int64_t p = chunk0; p < end; ++p) {
+      const double* z = P.inj ? P.inj + (size_t)p * P.steps : nullptr;
+      double s = P.spot;
+      bool hit = P.up ? s >= P.level : s <= P.level;  // the scan includes path[0]
+      for (int64_t t = 0; t < P.steps; ++t) {
+        const double zt = z ? z[t] : of::acklam_inv_cdf(rng.next_f64());
+        s = s * exp(fma(P.step_vol, zt, P.drift));
+        hit |= P.up ? s >= P.level : s <= P.level;
+      }
+      const bool active = P.knock_in ? hit : !hit;
+      const double intrinsic = P.call ? s - P.strike : P.strike - s;
+      const double v = P.discount * (active ? (intrinsic > 0.0 ? intrinsic : 0.0) : P.rebate);
+      acc[0] += v;
+      acc[1] += v * v;
+    }
+  }
+  of::block_sum<2>(acc, red_sh);
+  if (threadIdx.x == 0) {
+    P.partials[(int64_t)blockIdx.x * 2] = acc[0];
+    P.partials[(int64_t)blockIdx.x * 2 + 1] = acc[1];
+  }
+}
+
+}  // namespace
+
+extern "C" of_status of_lsm_barrier(of_ctx* ctx, const of_lsm_barrier_contract* k, const of_lsm_config* cfg,
+                                    of_lsm_result* out) {
+  if (!ctx || !k || !cfg || !out) return OF_ERR_INVALID_INPUT;
+  // BarrierOption::validate (src/instruments/barrier.rs:36-60), then :640-657
+  if (k->option_type != OF_CALL && k->option_type != OF_PUT)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown option type %d", k->option_type);
+  if (!(k->strike > 0.0)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "barrier strike must be > 0");
+  if (!(k->expiry >= 0.0)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "barrier expiry must be >= 0");
+  if (!(k->barrier_level > 0.0)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "barrier level must be > 0");
+  if (!(k->rebate >= 0.0)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "barrier rebate must be >= 0");
+  if (k->barrier_direction != OF_BARRIER_UP && k->barrier_direction != OF_BARRIER_DOWN)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown barrier direction %d", k->barrier_direction);
+  if (k->barrier_style != OF_BARRIER_IN && k->barrier_style != OF_BARRIER_OUT)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown barrier style %d", k->barrier_style);
+  if (k->num_steps <= 0) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_steps must be > 0");
+  if (k->num_steps > (int64_t)1 << 30) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_steps too large");
+  if (cfg->num_paths <= 0) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_paths must be > 0");
+  if (!(k->vol > 0.0)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "market volatility must be > 0");
+  if (cfg->precision != OF_PREC_FP64_REFERENCE)
+    return of_fail(ctx, OF_ERR_UNSUPPORTED,
+                   "the LSM engine's barrier pricing runs on the reference stream (FP32 barriers: the batched book)");
+  if (cfg->injected_normals && cfg->n_injected < cfg->num_paths * k->num_steps)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "injected normals: need num_paths x num_steps values");
+  OF_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  LsmBarrierParams P{};
+  const double dt = k->expiry / (double)k->num_steps;
+  P.spot = k->spot;
+  P.strike = k->strike;
+  P.level = k->barrier_level;
+  P.rebate = k->rebate;
+  P.drift = (k->rate - k->dividend_yield - 0.5 * k->vol * k->vol) * dt;
+  P.step_vol = k->vol * std::sqrt(dt);
+  P.discount = std::exp(-k->rate * k->expiry);
+  P.n = cfg->num_paths;
+  P.steps = k->num_steps;
+  P.seed = cfg->seed;
+  P.call = k->option_type == OF_CALL;
+  P.up = k->barrier_direction == OF_BARRIER_UP;
+  P.knock_in = k->barrier_style == OF_BARRIER_IN;
+  const int64_t per_block = (int64_t)kBarThreads * kBarChunk;
+  const int64_t blocks = (P.n + per_block - 1) / per_block;
+  if (blocks > 2147483647LL) return of_fail(ctx, OF_ERR_INVALID_INPUT, "num_paths too large");
+  if (cfg->injected_normals) {
+    void* d = nullptr;
+    const size_t bytes = (size_t)(P.n * P.steps) * sizeof(double);
+    OF_TRY(of_scratch(ctx, SLOT_INJECT, bytes, &d));
+    OF_CUDA_TRY(ctx, cudaMemcpyAsync(d, cfg->injected_normals, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    P.inj = (const double*)d;
+  } else {
+    OF_TRY(upload_jump_tables(ctx, &P.jump));
+  }
+  void *d_part = nullptr, *d_sums = nullptr, *h = nullptr;
+  OF_TRY(of_scratch(ctx, SLOT_PARTIALS, (size_t)blocks * 2 * sizeof(double), &d_part));
+  OF_TRY(of_scratch(ctx, SLOT_SUMS, 2 * sizeof(double), &d_sums));
+  OF_TRY(of_pinned(ctx, 2 * sizeof(double), &h));
+  P.partials = (double*)d_part;
+  OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+  lsm_barrier_ref<<<(unsigned)blocks, kBarThreads, 0, ctx->stream>>>(P);
+  OF_CUDA_TRY(ctx, cudaGetLastError());
+  OF_TRY(of_reduce_rows(ctx, (const double*)d_part, blocks, 2, (double*)d_sums));
+  OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+  OF_CUDA_TRY(ctx, cudaMemcpyAsync(h, d_sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  OF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  float ms = 0.0f;
+  OF_CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+  // mean_and_stderr, longstaff_schwartz.rs:125-140
+  const double sum = ((const double*)h)[0], sum_sq = ((const double*)h)[1], n = (double)P.n;
+  const double var = P.n > 1 ? (sum_sq - sum * sum / n) / (n - 1.0) : 0.0;
+  out->price = sum / n;
+  out->stderr_ = std::sqrt(var / n);
+  out->delta = 0.0;
+  out->regressions = 0;
+  out->kernel_ms = ms;
+  return OF_OK;
+}

@@ -19,6 +19,7 @@
 #include <numeric>
 #include <vector>
 
+#include "book_greeks.cuh"
 #include "of_internal.h"
 #include "path_fp32.cuh"
 
@@ -814,26 +815,226 @@ __global__ void __launch_bounds__(256, 3) book_kernel(const __grid_constant__ Bo
   }
 }
 
-// Per-option sums over its tile slots [begin[o], begin[o+1]) in fixed order.
+// Running sums of the Greeks modes.  FP32 (with Greeks): the five sums of
+// MonteCarloEngine::run compensated, then per Greek its compensated sum and
+// plain sum of squares (a few samples per thread per tile; only the standard
+// error reads them).  FP64: the five sums.
+template <typename R, bool G>
+struct GreekAcc;
+
+template <>
+struct GreekAcc<float, true> {
+  of::Kahan32 s[5], g[4];
+  float g2[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  __device__ __forceinline__ void add(const of::GreekSample<float>& v) {
+    s[0].add(v.x);
+    s[1].add(v.x * v.x);
+    s[2].add(v.y);
+    s[3].add(v.x * v.y);
+    s[4].add(v.y * v.y);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      g[t].add(v.g[t]);
+      g2[t] = fmaf(v.g[t], v.g[t], g2[t]);
+    }
+  }
+  __device__ __forceinline__ void values(double (&out)[13]) const {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = s[k].value();
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      out[5 + t] = g[t].value();
+      out[9 + t] = (double)g2[t];
+    }
+  }
+};
+
+template <>
+struct GreekAcc<double, false> {
+  double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  __device__ __forceinline__ void add(const of::GreekSample<double>& v) {
+    s[0] += v.x;
+    s[1] += v.x * v.x;
+    s[2] += v.y;
+    s[3] += v.x * v.y;
+    s[4] += v.y * v.y;
+  }
+  __device__ __forceinline__ void values(double (&out)[5]) const {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = s[k];
+  }
+};
+
+// The book's Greeks modes: the persistent tile loop of book_kernel over the
+// per-sample kernels of book_greeks.cuh.  <float, true>: prices and pathwise
+// Greeks (13 sums per tile); <double, false>: FP64 prices on the same draws.
+template <typename R, bool G>
+__global__ void __launch_bounds__(256, 2) book_greeks_kernel(const __grid_constant__ BookParams P,
+                                                              const of::GreekConsts<R>* __restrict__ gc) {
+  constexpr int NC = G ? 13 : 5;
+  __shared__ int tile_sh;
+  __shared__ double red_sh[NC * 8];
+  for (;;) {
+    if (threadIdx.x == 0) tile_sh = atomicAdd(P.counter, 1);
+    __syncthreads();
+    const int t = tile_sh;
+    if (t >= P.n_tiles) break;
+    const BookTile tile = P.tiles[t];
+    const of::GreekConsts<R>& c = gc[tile.opt];
+    GreekAcc<R, G> acc;
+    for (int k = 0; k < P.ppt; ++k) {
+      const int local = k * blockDim.x + threadIdx.x;
+      if (local >= tile.count) break;
+      of::GreekSample<R> v;
+      of::gk_sample<R, G>(c, (uint64_t)(tile.first + local), P.keys, P.obs_w, v);
+      acc.add(v);
+    }
+    double v[NC];
+    acc.values(v);
+    of::block_sum<NC>(v, red_sh);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < NC; ++k) P.partials[(int64_t)tile.slot * NC + k] = v[k];
+    __syncthreads();
+  }
+}
+
+// Per-option sums over its tile slots [begin[o], begin[o+1]) in fixed order;
+// NC sums per slot.
+template <int NC>
 __global__ void book_reduce_kernel(const double* __restrict__ partials, const int32_t* __restrict__ begin, int n_opts,
                                    double* __restrict__ sums) {
   const int o = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (o >= n_opts) return;
-  double acc[5] = {0, 0, 0, 0, 0};
+  double acc[NC];
+#pragma unroll
+  for (int k = 0; k < NC; ++k) acc[k] = 0.0;
   for (int s = begin[o] + lane; s < begin[o + 1]; s += 32)
-    for (int k = 0; k < 5; ++k) acc[k] += partials[(int64_t)s * 5 + k];
-  for (int k = 0; k < 5; ++k) {
+#pragma unroll
+    for (int k = 0; k < NC; ++k) acc[k] += partials[(int64_t)s * NC + k];
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
     const double v = of::warp_sum(acc[k]);
-    if (lane == 0) sums[(int64_t)o * 5 + k] = v;
+    if (lane == 0) sums[(int64_t)o * NC + k] = v;
   }
 }
 
 }  // namespace
 
+static_assert(OF_CV_NONE == of::GCV_NONE && OF_CV_VANILLA_TERMINAL == of::GCV_VANILLA_TERMINAL &&
+                  OF_CV_GEOMETRIC_ASIAN == of::GCV_GEOMETRIC_ASIAN && OF_CV_TERMINAL_SPOT == of::GCV_TERMINAL_SPOT,
+              "the Greeks modes read the control-variate kinds of the ABI");
+
+// Constants of one entry in the Greeks modes (FP64; the FP32 mode rounds
+// them once).  `d` is the entry's price-mode record (flags, observation
+// weights' offset), `w` its observation weights by step index (empty when it
+// has none) and `daily` whether they are the daily fixings 1..steps.
+static of_status book_greek_consts(of_ctx* ctx, const of_book_entry& b, int64_t o, const BookOpt& d,
+                                   const std::vector<double>& w, bool daily, of::GreekConsts<double>& g) {
+  const of_model& m = b.model;
+  const of_payoff& p = b.payoff;
+  if (m.kind != OF_MODEL_GBM)
+    return of_fail(ctx, OF_ERR_UNSUPPORTED, "the Greeks modes price GBM options (Heston: of_heston_price_adjoint)");
+  if (m.n_dividends > 0) return of_fail(ctx, OF_ERR_UNSUPPORTED, "the Greeks modes take no discrete dividends");
+  if (!(b.discount_factor > 0.0) || !std::isfinite(b.discount_factor))
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "the Greeks modes need a discount factor exp(-r T) > 0");
+  g = of::GreekConsts<double>{};
+  const double T = m.maturity, M = (double)m.steps, dt = T / M, sig = m.sigma;
+  g.dt = dt;
+  g.T = T;
+  g.sigma = sig;
+  g.a = m.mu - 0.5 * sig * sig;
+  g.alpha = g.a * dt;
+  g.beta = sig * std::sqrt(dt);
+  g.df = b.discount_factor;
+  g.r = -std::log(b.discount_factor) / T;
+  g.s0 = m.s0;
+  g.strike = p.strike;
+  g.sig_dt = sig * dt;
+  g.inv_sig = 1.0 / sig;
+  g.beta_over_sig = std::sqrt(dt);
+  g.alpha_over_T = g.alpha / T;
+  g.inv_2T = 0.5 / T;
+  g.beta_over_2T = g.beta / (2.0 * T);
+  g.steps = (int32_t)m.steps;
+  g.obs_offset = d.obs_offset;
+  g.cv_kind = b.control_variate;
+  g.stream = d.stream;
+  int32_t f = 0;
+  if (p.option_type == OF_CALL) f |= of::GF_CALL;
+  if (b.antithetic) f |= of::GF_ANTI;
+  switch (p.kind) {
+    case OF_PAYOFF_VANILLA:
+      g.kind = of::GK_TERMINAL;
+      break;
+    case OF_PAYOFF_ASIAN:
+      if (p.strike_type == OF_STRIKE_FLOATING) f |= of::GF_FLOATING;
+      if (p.averaging == OF_AVG_GEOMETRIC) f |= of::GF_GEOMETRIC;
+      if (d.flags & BF_TERMINAL_ONLY) {
+        f |= of::GF_TERMINAL_ONLY;
+        g.kind = of::GK_TERMINAL;
+      } else {
+        g.kind = daily ? of::GK_ASIAN_DAILY : of::GK_ASIAN_WEIGHTS;
+        g.inv_n = 1.0 / (double)p.n_observations;
+        double w1 = 0.0;
+        for (size_t i = 1; i < w.size(); ++i) w1 += w[i] * (double)i;
+        g.w1 = w1;
+      }
+      break;
+    default:  // barrier
+      if (!(p.barrier_level > 0.0) || !std::isfinite(p.barrier_level))
+        return of_fail(ctx, OF_ERR_INVALID_INPUT, "barrier level must be > 0");
+      if (b.control_variate != OF_CV_NONE)
+        return of_fail(ctx, OF_ERR_UNSUPPORTED, "a barrier option takes no control variate in the Greeks modes");
+      g.kind = p.barrier_style == OF_BARRIER_IN ? of::GK_BARRIER_IN : of::GK_BARRIER_OUT;
+      g.rebate = p.rebate;
+      g.bar = std::log(p.barrier_level / m.s0);
+      g.sgn = p.barrier_direction == OF_BARRIER_UP ? 1.0 : -1.0;
+      g.sib = g.sgn / g.beta;
+  }
+  g.flags = f;
+  (void)o;
+  return OF_OK;
+}
+
+static of::GreekConsts<float> round_greek_consts(const of::GreekConsts<double>& d) {
+  of::GreekConsts<float> f{};
+  f.alpha = (float)d.alpha;
+  f.beta = (float)d.beta;
+  f.a = (float)d.a;
+  f.dt = (float)d.dt;
+  f.T = (float)d.T;
+  f.sigma = (float)d.sigma;
+  f.r = (float)d.r;
+  f.df = (float)d.df;
+  f.s0 = (float)d.s0;
+  f.strike = (float)d.strike;
+  f.rebate = (float)d.rebate;
+  f.inv_n = (float)d.inv_n;
+  f.w1 = (float)d.w1;
+  f.bar = (float)d.bar;
+  f.sgn = (float)d.sgn;
+  f.sib = (float)d.sib;
+  f.sig_dt = (float)d.sig_dt;
+  f.inv_sig = (float)d.inv_sig;
+  f.beta_over_sig = (float)d.beta_over_sig;
+  f.alpha_over_T = (float)d.alpha_over_T;
+  f.inv_2T = (float)d.inv_2T;
+  f.beta_over_2T = (float)d.beta_over_2T;
+  f.kind = d.kind;
+  f.flags = d.flags;
+  f.steps = d.steps;
+  f.obs_offset = d.obs_offset;
+  f.cv_kind = d.cv_kind;
+  f.stream = d.stream;
+  return f;
+}
+
 struct of_book_plan {
   of_ctx* ctx = nullptr;
   int64_t n = 0;
+  int mode = OF_BOOK_PRICE;
+  int nc = 5;  // sums per option: 5, or 13 with the Greeks
   int block = 256, ppt = 4, grid = 0;
   int64_t n_tiles = 0;
   double path_steps = 0.0;
@@ -845,6 +1046,7 @@ struct of_book_plan {
   BookTile* d_tiles = nullptr;
   float* d_obs = nullptr;
   BookDiv* d_divs = nullptr;
+  void* d_gc = nullptr;  // GreekConsts<float> (Greeks mode) or <double> (FP64 mode)
   int* d_counter = nullptr;
   double* d_partials = nullptr;
   int32_t* d_begin = nullptr;
@@ -855,11 +1057,26 @@ struct of_book_plan {
   cudaGraphExec_t exec = nullptr;
 };
 
+static const void* book_kernel_for(int mode) {
+  if (mode == OF_BOOK_GREEKS) return (const void*)book_greeks_kernel<float, true>;
+  if (mode == OF_BOOK_PRICE_FP64) return (const void*)book_greeks_kernel<double, false>;
+  return (const void*)book_kernel;
+}
+
 static void book_enqueue(of_book_plan* pl, cudaStream_t s) {
   cudaMemsetAsync(pl->d_counter, 0, sizeof(int), s);
-  book_kernel<<<pl->grid, pl->block, 0, s>>>(pl->P);
-  book_reduce_kernel<<<(unsigned)((pl->n + 7) / 8), 256, 0, s>>>(pl->d_partials, pl->d_begin, (int)pl->n, pl->d_sums);
-  cudaMemcpyAsync(pl->h_sums, pl->d_sums, (size_t)pl->n * 5 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  const unsigned rgrid = (unsigned)((pl->n + 7) / 8);
+  if (pl->mode == OF_BOOK_GREEKS) {
+    book_greeks_kernel<float, true><<<pl->grid, pl->block, 0, s>>>(pl->P, (const of::GreekConsts<float>*)pl->d_gc);
+    book_reduce_kernel<13><<<rgrid, 256, 0, s>>>(pl->d_partials, pl->d_begin, (int)pl->n, pl->d_sums);
+  } else if (pl->mode == OF_BOOK_PRICE_FP64) {
+    book_greeks_kernel<double, false><<<pl->grid, pl->block, 0, s>>>(pl->P, (const of::GreekConsts<double>*)pl->d_gc);
+    book_reduce_kernel<5><<<rgrid, 256, 0, s>>>(pl->d_partials, pl->d_begin, (int)pl->n, pl->d_sums);
+  } else {
+    book_kernel<<<pl->grid, pl->block, 0, s>>>(pl->P);
+    book_reduce_kernel<5><<<rgrid, 256, 0, s>>>(pl->d_partials, pl->d_begin, (int)pl->n, pl->d_sums);
+  }
+  cudaMemcpyAsync(pl->h_sums, pl->d_sums, (size_t)pl->n * pl->nc * sizeof(double), cudaMemcpyDeviceToHost, s);
 }
 
 extern "C" void of_book_plan_destroy(of_book_plan* pl) {
@@ -871,6 +1088,7 @@ extern "C" void of_book_plan_destroy(of_book_plan* pl) {
   cudaFree(pl->d_tiles);
   cudaFree(pl->d_obs);
   cudaFree(pl->d_divs);
+  cudaFree(pl->d_gc);
   cudaFree(pl->d_counter);
   cudaFree(pl->d_partials);
   cudaFree(pl->d_begin);
@@ -893,6 +1111,13 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
   pl->block = cfg->block > 0 ? cfg->block : 256;
   pl->ppt = cfg->paths_per_thread > 0 ? cfg->paths_per_thread : 4;
   pl->use_graph = cfg->use_graph != 0;
+  pl->mode = cfg->mode;
+  if (pl->mode != OF_BOOK_PRICE && pl->mode != OF_BOOK_GREEKS && pl->mode != OF_BOOK_PRICE_FP64) {
+    const int m = pl->mode;
+    of_book_plan_destroy(pl);
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown book mode %d", m);
+  }
+  pl->nc = pl->mode == OF_BOOK_GREEKS ? 13 : 5;
   if (pl->block % 32 != 0 || pl->block > 256) {
     of_book_plan_destroy(pl);
     return of_fail(ctx, OF_ERR_INVALID_INPUT, "block must be a multiple of 32 and <= 256");
@@ -902,6 +1127,8 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
     return st;
   };
   std::vector<BookOpt> opts((size_t)n);
+  std::vector<of::GreekConsts<double>> gcs;  // Greeks modes only
+  if (pl->mode != OF_BOOK_PRICE) gcs.resize((size_t)n);
   std::vector<float> obs;
   std::vector<BookDiv> divs;
   std::vector<of_div_trigger> trig;
@@ -964,8 +1191,9 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
     const bool asian = b.payoff.kind == OF_PAYOFF_ASIAN;
     bool need_arith = asian && b.payoff.averaging == OF_AVG_ARITHMETIC;
     bool need_geo = (asian && b.payoff.averaging == OF_AVG_GEOMETRIC) || b.control_variate == OF_CV_GEOMETRIC_ASIAN;
+    std::vector<double> w;
+    bool daily_obs = false;
     if (need_arith || need_geo) {
-      std::vector<double> w;
       bool terminal_only = true;
       of_observation_weights(&b.payoff, b.model.steps, w, terminal_only);
       if (terminal_only) {
@@ -974,6 +1202,7 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
       } else {
         bool daily = w[0] == 0.0;
         for (size_t k = 1; k < w.size() && daily; ++k) daily = w[k] == 1.0;
+        daily_obs = daily;
         if (daily) {
           f |= BF_DAILY;
         } else {
@@ -992,6 +1221,13 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
       if (b.payoff.kind == OF_PAYOFF_VANILLA || (f & BF_TERMINAL_ONLY)) d.kind = BK_TERMINAL;
       else if (b.payoff.kind == OF_PAYOFF_BARRIER) d.kind = BK_BARRIER;
       else if (need_arith && (f & BF_DAILY)) d.kind = BK_ASIAN_DAILY;
+    }
+    if (pl->mode != OF_BOOK_PRICE) {
+      st = book_greek_consts(ctx, b, o, d, w, daily_obs, gcs[(size_t)o]);
+      if (st != OF_OK) {
+        ctx->last_error = "book entry " + std::to_string(o) + ": " + ctx->last_error;
+        return fail(st);
+      }
     }
     const int64_t samples = b.antithetic ? (b.num_paths + 1) / 2 : b.num_paths;
     pl->samples[(size_t)o] = samples;
@@ -1025,11 +1261,24 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
       cudaMalloc(&pl->d_obs, std::max<size_t>(1, obs.size()) * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&pl->d_divs, std::max<size_t>(1, divs.size()) * sizeof(BookDiv)) != cudaSuccess ||
       cudaMalloc(&pl->d_counter, sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&pl->d_partials, nt * 5 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&pl->d_partials, nt * pl->nc * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&pl->d_begin, begin.size() * sizeof(int32_t)) != cudaSuccess ||
-      cudaMalloc(&pl->d_sums, (size_t)n * 5 * sizeof(double)) != cudaSuccess ||
-      cudaMallocHost(&pl->h_sums, (size_t)n * 5 * sizeof(double)) != cudaSuccess)
+      cudaMalloc(&pl->d_sums, (size_t)n * pl->nc * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&pl->h_sums, (size_t)n * pl->nc * sizeof(double)) != cudaSuccess)
     return fail(of_fail(ctx, OF_ERR_ALLOC, "book plan allocation failed"));
+  if (pl->mode == OF_BOOK_GREEKS) {  // the constants rounded once to FP32
+    std::vector<of::GreekConsts<float>> gf(gcs.size());
+    for (size_t k = 0; k < gcs.size(); ++k) gf[k] = round_greek_consts(gcs[k]);
+    if (cudaMalloc(&pl->d_gc, gf.size() * sizeof(gf[0])) != cudaSuccess)
+      return fail(of_fail(ctx, OF_ERR_ALLOC, "book plan allocation failed"));
+    if (cudaMemcpy(pl->d_gc, gf.data(), gf.size() * sizeof(gf[0]), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(of_fail(ctx, OF_ERR_CUDA, "book upload failed"));
+  } else if (pl->mode == OF_BOOK_PRICE_FP64) {
+    if (cudaMalloc(&pl->d_gc, gcs.size() * sizeof(gcs[0])) != cudaSuccess)
+      return fail(of_fail(ctx, OF_ERR_ALLOC, "book plan allocation failed"));
+    if (cudaMemcpy(pl->d_gc, gcs.data(), gcs.size() * sizeof(gcs[0]), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(of_fail(ctx, OF_ERR_CUDA, "book upload failed"));
+  }
   if (cudaMemcpy(pl->d_opts, opts.data(), opts.size() * sizeof(BookOpt), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(pl->d_tiles, sorted.data(), nt * sizeof(BookTile), cudaMemcpyHostToDevice) != cudaSuccess ||
       (!obs.empty() && cudaMemcpy(pl->d_obs, obs.data(), obs.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) ||
@@ -1047,7 +1296,7 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
   P.keys = of::philox_keys(cfg->seed);
   P.counter = pl->d_counter;
   P.partials = pl->d_partials;
-  const int per_sm = of_blocks_per_sm((const void*)book_kernel, pl->block, 0);
+  const int per_sm = of_blocks_per_sm(book_kernel_for(pl->mode), pl->block, 0);
   const int64_t cap = (int64_t)ctx->sm_count * per_sm;
   pl->grid = (int)std::max<int64_t>(1, std::min<int64_t>(cap, (int64_t)nt));
   if (pl->use_graph) {
@@ -1083,9 +1332,38 @@ extern "C" of_status of_book_plan_results(of_book_plan* pl, of_mc_result* res) {
   if (!pl || !res) return OF_ERR_INVALID_INPUT;
   OF_CUDA_TRY(pl->ctx, cudaStreamSynchronize(pl->ctx->stream));
   for (int64_t o = 0; o < pl->n; ++o) {
-    of_mc_finish(pl->h_sums + o * 5, pl->samples[(size_t)o], pl->cv_kind[(size_t)o], pl->cv_expected[(size_t)o],
+    of_mc_finish(pl->h_sums + o * pl->nc, pl->samples[(size_t)o], pl->cv_kind[(size_t)o], pl->cv_expected[(size_t)o],
                  pl->discount[(size_t)o], &res[o]);
     res[o].kernel_ms = 0.0;
+  }
+  return OF_OK;
+}
+
+extern "C" of_status of_book_plan_greeks(of_book_plan* pl, of_book_greeks* out) {
+  if (!pl || !out) return OF_ERR_INVALID_INPUT;
+  if (pl->mode != OF_BOOK_GREEKS)
+    return of_fail(pl->ctx, OF_ERR_INVALID_INPUT, "the plan was not created in mode OF_BOOK_GREEKS");
+  OF_CUDA_TRY(pl->ctx, cudaStreamSynchronize(pl->ctx->stream));
+  for (int64_t o = 0; o < pl->n; ++o) {
+    const double* s = pl->h_sums + o * pl->nc;
+    const double n = (double)pl->samples[(size_t)o];
+    double mean[4], se[4];
+    for (int t = 0; t < 4; ++t) {  // the sums are of discounted per-sample derivatives
+      mean[t] = s[5 + t] / n;
+      const double var = n > 1.0 ? std::fmax(s[9 + t] - s[5 + t] * s[5 + t] / n, 0.0) / (n - 1.0) : 0.0;
+      se[t] = std::sqrt(var / n);
+    }
+    of_book_greeks& g = out[o];
+    g.delta = mean[0];
+    g.vega = mean[1];
+    g.rho = mean[2];
+    g.theta = mean[3];
+    g.gamma = 0.0;
+    g.delta_se = se[0];
+    g.vega_se = se[1];
+    g.rho_se = se[2];
+    g.theta_se = se[3];
+    g.gamma_se = 0.0;
   }
   return OF_OK;
 }
@@ -1100,20 +1378,35 @@ extern "C" of_status of_book_plan_info(of_book_plan* pl, int32_t* block, int32_t
   return OF_OK;
 }
 
-extern "C" of_status of_mc_price_book(of_ctx* ctx, const of_book_entry* e, int64_t n, const of_book_config* cfg,
-                                      of_mc_result* res) {
-  if (!ctx || !res) return OF_ERR_INVALID_INPUT;
+// One launch of a book: plan, launch, results (and Greeks when `greeks`).
+static of_status book_run(of_ctx* ctx, const of_book_entry* e, int64_t n, const of_book_config* cfg,
+                          of_mc_result* res, of_book_greeks* greeks) {
   of_book_plan* pl = nullptr;
   OF_TRY(of_book_plan_create(ctx, e, n, cfg, &pl));
   cudaEventRecord(ctx->ev_start, ctx->stream);
   of_status st = of_book_plan_launch(pl);
   cudaEventRecord(ctx->ev_stop, ctx->stream);
   if (st == OF_OK) st = of_book_plan_results(pl, res);
+  if (st == OF_OK && greeks) st = of_book_plan_greeks(pl, greeks);
   float ms = 0.0f;
   if (st == OF_OK && cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess)
     for (int64_t o = 0; o < n; ++o) res[o].kernel_ms = ms;
   of_book_plan_destroy(pl);
   return st;
+}
+
+extern "C" of_status of_mc_price_book(of_ctx* ctx, const of_book_entry* e, int64_t n, const of_book_config* cfg,
+                                      of_mc_result* res) {
+  if (!ctx || !res || !cfg) return OF_ERR_INVALID_INPUT;
+  return book_run(ctx, e, n, cfg, res, nullptr);
+}
+
+extern "C" of_status of_mc_price_book_greeks(of_ctx* ctx, const of_book_entry* e, int64_t n, const of_book_config* cfg,
+                                             of_mc_result* res, of_book_greeks* greeks) {
+  if (!ctx || !res || !cfg || !greeks) return OF_ERR_INVALID_INPUT;
+  of_book_config c = *cfg;
+  c.mode = OF_BOOK_GREEKS;
+  return book_run(ctx, e, n, &c, res, greeks);
 }
 
 // FP32 branch of of_mc_run: a one-option book.
@@ -1363,6 +1656,22 @@ __global__ void __launch_bounds__(kProbeBlock) fma_probe_kernel(int iters, float
   if (s < 0.0f) sink[blockIdx.x] = s;  // never taken; keeps the chains live
 }
 
+// kProbeChains independent FP64 FMA chains per thread converging to 1.
+__global__ void __launch_bounds__(kProbeBlock) dfma_probe_kernel(int iters, double* sink) {
+  double a[kProbeChains];
+#pragma unroll
+  for (int k = 0; k < kProbeChains; ++k) a[k] = 0.5 + 0.01 * k + 1e-7 * threadIdx.x;
+#pragma unroll 16
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < kProbeChains; ++k) a[k] = fma(a[k], 0.99993896484375, 6.103515625e-5);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < kProbeChains; ++k) s += a[k];
+  if (s < 0.0) sink[blockIdx.x] = s;  // never taken; keeps the chains live
+}
+
 }  // namespace
 
 extern "C" of_status of_measure_device_peaks(of_ctx* ctx, of_device_peaks* out) {
@@ -1370,9 +1679,11 @@ extern "C" of_status of_measure_device_peaks(of_ctx* ctx, of_device_peaks* out) 
   OF_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   const int per_sm_s = of_blocks_per_sm((const void*)sfu_probe_kernel, kProbeBlock, 0);
   const int per_sm_f = of_blocks_per_sm((const void*)fma_probe_kernel, kProbeBlock, 0);
+  const int per_sm_d = of_blocks_per_sm((const void*)dfma_probe_kernel, kProbeBlock, 0);
   const int grid_s = ctx->sm_count * std::max(per_sm_s, 1), grid_f = ctx->sm_count * std::max(per_sm_f, 1);
+  const int grid_d = ctx->sm_count * std::max(per_sm_d, 1);
   void* sink = nullptr;
-  OF_TRY(of_scratch(ctx, SLOT_MISC, (size_t)std::max(grid_s, grid_f) * sizeof(float), &sink));
+  OF_TRY(of_scratch(ctx, SLOT_MISC, (size_t)std::max(std::max(grid_s, grid_f), grid_d) * sizeof(double), &sink));
   const int it_s = 2048, it_f = 65536;
   // warm-up (clocks up), then the best of three timed launches of each probe
   sfu_probe_kernel<<<grid_s, kProbeBlock, 0, ctx->stream>>>(it_s / 8, (float*)sink);
@@ -1394,10 +1705,25 @@ extern "C" of_status of_measure_device_peaks(of_ctx* ctx, of_device_peaks* out) 
     OF_CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
     best_f = std::min(best_f, ms);
   }
+  // FP64: warm-up, then the best of three
+  const int it_d = 4096;
+  float best_d = 1e30f;
+  dfma_probe_kernel<<<grid_d, kProbeBlock, 0, ctx->stream>>>(it_d / 8, (double*)sink);
+  for (int rep = 0; rep < 3; ++rep) {
+    float ms = 0.0f;
+    OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+    dfma_probe_kernel<<<grid_d, kProbeBlock, 0, ctx->stream>>>(it_d, (double*)sink);
+    OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+    OF_CUDA_TRY(ctx, cudaEventSynchronize(ctx->ev_stop));
+    OF_CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+    best_d = std::min(best_d, ms);
+  }
   OF_CUDA_TRY(ctx, cudaGetLastError());
   const double threads_s = (double)grid_s * kProbeBlock, threads_f = (double)grid_f * kProbeBlock;
+  const double threads_d = (double)grid_d * kProbeBlock;
   out->sfu_ops_per_s = threads_s * it_s * kProbeChains * 5.0 / (best_s * 1e-3);
   out->fp32_flops_per_s = threads_f * (double)it_f * kProbeChains * 2.0 / (best_f * 1e-3);
-  out->probe_ms = (double)best_s + (double)best_f;
+  out->fp64_flops_per_s = threads_d * (double)it_d * kProbeChains * 2.0 / (best_d * 1e-3);
+  out->probe_ms = (double)best_s + (double)best_f + (double)best_d;
   return OF_OK;
 }

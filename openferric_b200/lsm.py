@@ -7,7 +7,9 @@ in FP64 reference mode, basis {1,S,S^2}); `with_precision(Fp32Philox)` and
 {1,x,x^2,x^3} (x = S/K) solved by Cholesky; `price_batch` prices many
 contracts through one date loop.  `price_bermudan_with_boundary` prices a
 BermudanOption (a strike per exercise date) under GBM, local-vol Euler or
-Heston Euler paths and returns the exercise boundary.
+Heston Euler paths and returns the exercise boundary.  A BarrierOption is
+priced by the engine's European barrier Monte Carlo on its single stream
+(of_lsm_barrier).
 """
 from __future__ import annotations
 
@@ -20,9 +22,9 @@ import numpy as np
 
 from . import _abi as A
 from ._lib import context
-from .core import Diagnostics, Greeks, OptionType, PricingError, PricingResult
+from .core import BarrierDirection, BarrierStyle, Diagnostics, Greeks, OptionType, PricingError, PricingResult
 from .engines import Precision
-from .instruments import BermudanOption, VanillaOption
+from .instruments import BarrierOption, BermudanOption, VanillaOption
 from .market import Market
 
 
@@ -211,11 +213,52 @@ class LongstaffSchwartzEngine:
                                           int(p.itm_paths), int(p.exercised_paths)) for p in pts[:nb.value]]
         return BermudanLsmOutput(PricingResult(price=out.price, stderr=out.stderr_, diagnostics=d), boundary)
 
+    def price_barrier(self, instrument: BarrierOption, market: Market) -> PricingResult:
+        """PricingEngine<BarrierOption>::price (longstaff_schwartz.rs:632-736):
+        the engine's single xoshiro256++ stream, path-major, log-Euler steps,
+        the barrier monitored on every point of the path including the spot,
+        the vanilla payoff when active and the rebate otherwise, discounted by
+        exp(-r T).  FP64 reference draws only."""
+        instrument.validate()
+        if self.num_steps == 0:
+            raise PricingError.InvalidInput("num_steps must be > 0")
+        if self.num_paths == 0:
+            raise PricingError.InvalidInput("num_paths must be > 0")
+        vol = market.vol_for(instrument.strike, instrument.expiry)
+        if vol <= 0.0:
+            raise PricingError.InvalidInput("market volatility must be > 0")
+        b = instrument.barrier
+        k = A.OfLsmBarrierContract(
+            option_type=instrument.option_type.value,
+            barrier_direction=A.OF_BARRIER_UP if b.direction is BarrierDirection.Up else A.OF_BARRIER_DOWN,
+            barrier_style=A.OF_BARRIER_IN if b.style is BarrierStyle.In else A.OF_BARRIER_OUT,
+            spot=market.spot, strike=instrument.strike, rate=market.rate,
+            dividend_yield=market.effective_dividend_yield(instrument.expiry), vol=vol, expiry=instrument.expiry,
+            barrier_level=b.level, rebate=b.rebate, num_steps=self.num_steps)
+        cfg = A.OfLsmConfig(num_paths=self.num_paths, seed=self.seed & 0xFFFFFFFFFFFFFFFF,
+                            precision=self.precision.value, basis_degree=self.basis_degree, want_delta=0)
+        if self.injected_normals is not None:
+            cfg.injected_normals = self.injected_normals.ctypes.data_as(C.POINTER(C.c_double))
+            cfg.n_injected = self.injected_normals.size
+        out = A.OfLsmResult()
+        ctx = context(self.device)
+        with ctx.lock:
+            ctx.check(ctx._L.of_lsm_barrier(ctx.handle, C.byref(k), C.byref(cfg), C.byref(out)))
+        self.last_kernel_ms = out.kernel_ms
+        d = Diagnostics()
+        d.insert("num_paths", float(self.num_paths))
+        d.insert("num_steps", float(self.num_steps))
+        d.insert("vol", vol)
+        return PricingResult(price=out.price, stderr=out.stderr_, diagnostics=d)
+
     def price(self, instrument, market: Market) -> PricingResult:
         """PricingEngine<VanillaOption>::price (longstaff_schwartz.rs:421-618);
-        a BermudanOption goes through price_bermudan_with_boundary (:620-630)."""
+        a BermudanOption goes through price_bermudan_with_boundary (:620-630),
+        a BarrierOption through price_barrier (:632-736)."""
         if isinstance(instrument, BermudanOption):
             return self.price_bermudan_with_boundary(instrument, market).result
+        if isinstance(instrument, BarrierOption):
+            return self.price_barrier(instrument, market)
         if instrument.expiry == 0.0:
             instrument.validate()
             v = market.spot - instrument.strike if instrument.option_type is OptionType.Call else \

@@ -927,6 +927,48 @@ static int chol_solve4(double a[4][4], const double b[4], double x[4]) {
   return 1;
 }
 
+/* LongstaffSchwartzEngine::price(BarrierOption), src/engines/lsm/longstaff_schwartz.rs:632-736
+ * (the portable branch, :691-697): ONE xoshiro256++ stream seeded with `seed`
+ * feeds all paths in path-major order; path[0] = spot and
+ * path[t+1] = path[t] * exp(mul_add(step_vol, z, drift)) with the Acklam normal
+ * of uniform_open01(next_f64); the barrier is monitored on path[0..=steps]
+ * (path_hits_barrier, :115-123: >= for up, <= for down); an active path pays
+ * the vanilla intrinsic of path[steps], an inactive one the rebate; each
+ * value is discounted by exp(-r T) and mean_and_stderr (:125-140) gives the
+ * result.  `normals` ([path][step], optional) replaces the stream.
+ * out2 = {price, stderr}. */
+int orc_lsm_barrier(int option_type, double strike, double expiry, int up, int knock_in, double level, double rebate,
+                    double spot, double rate, double q, double vol, int64_t num_paths, int64_t num_steps,
+                    uint64_t seed, const double* normals, double* out2) {
+  if (num_steps <= 0 || num_paths <= 0) return OF_ERR_INVALID_INPUT;
+  const double dt = expiry / (double)num_steps;
+  const double drift = (rate - q - 0.5 * vol * vol) * dt;
+  const double step_vol = vol * sqrt(dt);
+  const double discount = exp(-rate * expiry);
+  orc_xoshiro rng;
+  orc_xoshiro_seed(&rng, seed);
+  double sum = 0.0, sum_sq = 0.0;
+  for (int64_t pi = 0; pi < num_paths; ++pi) {
+    double s = spot;
+    int hit = up ? s >= level : s <= level;
+    for (int64_t ti = 0; ti < num_steps; ++ti) {
+      const double z = normals ? normals[pi * num_steps + ti] : draw_normal(&rng);
+      s = s * exp(fma(step_vol, z, drift));
+      hit |= up ? s >= level : s <= level;
+    }
+    const int active = knock_in ? hit : !hit;
+    const double v = discount * (active ? vanilla_payoff(option_type, s, strike) : rebate);
+    sum += v;
+    sum_sq += v * v;
+  }
+  const double n = (double)num_paths;
+  const double mean = sum / n;
+  const double var = num_paths > 1 ? (sum_sq - sum * sum / n) / (n - 1.0) : 0.0;
+  out2[0] = mean;
+  out2[1] = sqrt(var / n);
+  return OF_OK;
+}
+
 int orc_lsm_price(int option_type, double strike, double expiry, int exercise, const double* dates, int64_t n_dates,
                   double spot, double rate, double q, double vol, int64_t num_paths, int64_t num_steps,
                   uint64_t seed, int degree, const double* normals, double* out) {

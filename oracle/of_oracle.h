@@ -89,6 +89,12 @@ int orc_mc_greek_estimators(int option_type, double strike, double spot, double 
  * degree 3 = basis {1,x,x^2,x^3}, x = S/K, Cholesky (the build's extension).
  * normals: NULL draws one sequential xoshiro stream (the reference order),
  * else [path][step] normals are used.  out[0]=price out[1]=stderr. */
+/* LongstaffSchwartzEngine::price(BarrierOption) (longstaff_schwartz.rs:632-736):
+ * out2 = {price, stderr}; normals [path][step] replaces the stream if non-null. */
+int orc_lsm_barrier(int option_type, double strike, double expiry, int up, int knock_in, double level, double rebate,
+                    double spot, double rate, double q, double vol, int64_t num_paths, int64_t num_steps,
+                    uint64_t seed, const double* normals, double* out2);
+
 int orc_lsm_price(int option_type, double strike, double expiry, int exercise, const double* dates, int64_t n_dates,
                   double spot, double rate, double q, double vol, int64_t num_paths, int64_t num_steps,
                   uint64_t seed, int degree, const double* normals, double* out2);

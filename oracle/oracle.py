@@ -214,6 +214,22 @@ def mc_greek_estimators(option_type, strike, spot, rate, q, vol, expiry, num_pat
     return dict(zip(["pathwise_delta", "pathwise_gamma", "lr_delta", "lr_gamma", "lr_vega"], out.tolist()))
 
 
+def lsm_barrier(option_type, strike, expiry, up, knock_in, level, rebate, spot, rate, q, vol, num_paths, num_steps,
+                seed, normals=None):
+    """LongstaffSchwartzEngine::price(BarrierOption) restated: (price, stderr)."""
+    L = lib()
+    f = L.orc_lsm_barrier
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, D, D, C.c_int, C.c_int, D, D, D, D, D, D, I64, I64, C.c_uint64, PD, PD]
+    out = np.zeros(2)
+    z = None if normals is None else np.ascontiguousarray(normals, dtype=np.float64)
+    st = f(option_type, strike, expiry, int(up), int(knock_in), level, rebate, spot, rate, q, vol, num_paths,
+           num_steps, seed, _ptr(z) if z is not None else None, _ptr(out))
+    if st != 0:
+        raise RuntimeError(f"orc_lsm_barrier status {st}")
+    return float(out[0]), float(out[1])
+
+
 def lsm_price(option_type, strike, expiry, exercise, spot, rate, q, vol, num_paths, num_steps, seed, degree=2,
               dates=None, normals=None):
     out = np.zeros(2)

@@ -55,6 +55,8 @@ STRUCTS = {
     "of_boundary_point": A.OfBoundaryPoint,
     "of_qmc_params": A.OfQmcParams,
     "of_dividend_event": A.OfDividendEvent,
+    "of_book_greeks": A.OfBookGreeks,
+    "of_lsm_barrier_contract": A.OfLsmBarrierContract,
 }
 
 

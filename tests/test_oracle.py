@@ -381,6 +381,24 @@ def test_lsm_degree3_agrees_with_degree2_and_crr(orc):
     assert abs(p3 - p2) < 4 * s2
 
 
+def test_lsm_barrier_in_plus_out_is_the_european_on_the_same_stream(orc):
+    """LongstaffSchwartzEngine::price(BarrierOption) (longstaff_schwartz.rs:632-736)
+    draws the engine's single stream in the same path-major order as its
+    vanilla pricing (:467-509): on one seed, knock-in + knock-out (no rebate)
+    equals the European-exercise LSM price path by path, up to the discount
+    exp(-rT) against disc^steps."""
+    args = dict(spot=100.0, rate=0.05, q=0.0, vol=0.25, num_paths=20000, num_steps=50, seed=42)
+    ko, _ = orc.lsm_barrier(OF_PUT, 105.0, 0.5, False, False, 90.0, 0.0, **args)
+    ki, _ = orc.lsm_barrier(OF_PUT, 105.0, 0.5, False, True, 90.0, 0.0, **args)
+    plain, _ = orc.lsm_price(OF_PUT, 105.0, 0.5, 0, **args)
+    assert abs((ki + ko) - plain) <= 1e-12 * plain
+    assert 0.0 < ko < plain and 0.0 < ki < plain
+    # a rebate is paid on the inactive paths: in + out with rebate R = plain + R e^(-rT)
+    kor, _ = orc.lsm_barrier(OF_PUT, 105.0, 0.5, False, False, 90.0, 2.0, **args)
+    kir, _ = orc.lsm_barrier(OF_PUT, 105.0, 0.5, False, True, 90.0, 2.0, **args)
+    assert abs((kir + kor) - (plain + 2.0 * math.exp(-0.05 * 0.5))) <= 1e-12 * plain
+
+
 def test_lsm_european_exercise_is_discounted_payoff(orc):
     p, s = orc.lsm_price(OF_PUT, 40, 1.0, 0, 40, 0.06, 0.0, 0.2, 100000, 50, 3)
     bs = orc.bs_price(OF_PUT, 40, 40, 0.06, 0, 0.2, 1.0)
