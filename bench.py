@@ -669,7 +669,7 @@ def leg_book_greeks(n=256, per_kind=8, seed=BOOK_SEED):
 LSM_ALG_BYTES_PER_PATH_DATE = 16.0  # store 4 + reload 4 + cash flow read/write 8
 
 
-def leg_lsm(paths, contracts, seed=7):
+def leg_lsm(paths, contracts, seed=7, batch_contracts=0):
     import numpy as np
     import openferric_b200 as of
     from openferric_b200.lsm import LongstaffSchwartzEngine
@@ -684,7 +684,7 @@ def leg_lsm(paths, contracts, seed=7):
         for T in (1.0, 2.0):
             sub = [it for it in items if it[0].expiry == T]
             eng = LongstaffSchwartzEngine(paths, int(50 * T), seed).with_precision(
-                of.Precision.Fp32Philox).with_basis_degree(3)
+                of.Precision.Fp32Philox).with_basis_degree(3).with_batch_contracts(batch_contracts)
             eng.price_batch(sub[:2], with_delta=True)
             out = eng.price_batch(sub, with_delta=True)
             prices += [r.price for r in out]
@@ -700,6 +700,7 @@ def leg_lsm(paths, contracts, seed=7):
                          "peak_source": src, "per_path_date_bytes": LSM_ALG_BYTES_PER_PATH_DATE,
                          "scope": "all kernels of the workload (generation, passes, final), device time from CUDA "
                                   "events around each batch"},
+            "batch_contracts": batch_contracts or "automatic (L2-sized)",
             "price_range": [min(prices), max(prices)], "clocks": clocks.summary()}
 
 
@@ -729,7 +730,7 @@ def run_workload(args, local_rank):
     elif args.workload == "book_greeks":
         line = leg_book_greeks(args.se_options)
     else:  # lsm
-        line = leg_lsm(args.paths, args.contracts)
+        line = leg_lsm(args.paths, args.contracts, batch_contracts=args.lsm_batch)
     print(json.dumps(line), flush=True)
 
 
@@ -757,6 +758,8 @@ def main():
     ap.add_argument("--variance-reduction", default="none", choices=["none", "mixed"],
                     help="book_se workload: none (plain MC), or mixed (geometric-Asian control variate for the "
                          "Asians, antithetic for the Europeans and barriers)")
+    ap.add_argument("--lsm-batch", type=int, default=0,
+                    help="lsm workload: contracts per date loop (0 = automatic)")
     ap.add_argument("--book-mode", default="price", choices=["price", "greeks"],
                     help="book workload: prices only, or prices with the pathwise Greeks")
     ap.add_argument("--contracts", type=int, default=256,

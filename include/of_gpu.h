@@ -123,7 +123,9 @@ typedef struct of_mc_config {
   int32_t antithetic; /* 0/1 */
   int32_t precision; /* OF_PREC_* */
   int32_t control_variate; /* OF_CV_* */
-  int32_t tile_ilp; /* FP32 strip: samples in flight per thread (0 = default, 1 or 2) */
+  int32_t tile_ilp; /* FP32 strip tile shape: 0 = default (1), 1 or 2 samples in flight per thread,
+                       3 = warp-specialised (half the warps generate the Philox draws into a
+                       shared-memory ring, half simulate and price) */
   double cv_expected; /* E[Y] of the control variate, undiscounted */
   double discount_factor;
   /* Test hook (the injection point PathGenerator::generate_from_normals,
@@ -331,7 +333,7 @@ of_status of_book_price_to_stderr_greeks(of_ctx* ctx, const of_book_entry* entri
  * its measured time. */
 typedef struct of_tune_candidate {
   int32_t block;            /* book: threads per block; strip: written as 0 */
-  int32_t paths_per_thread; /* book: samples per thread per tile; strip: samples in flight per thread (1 or 2) */
+  int32_t paths_per_thread; /* book: samples per thread per tile; strip: the tile_ilp shape (1, 2 or 3) */
   double ms;                /* out: median device milliseconds of the timed replays */
 } of_tune_candidate;
 
@@ -397,7 +399,9 @@ typedef struct of_lsm_config {
                            paths; FP32_PHILOX: Philox normals, FP32 path store */
   int32_t basis_degree; /* 2: {1,S,S^2} + LU (the reference); 3: {1,x,x^2,x^3}, x=S/K, Cholesky */
   int32_t want_delta;   /* also return the pathwise delta under the fitted exercise policy */
-  int32_t reserved0;
+  int32_t batch_contracts; /* of_lsm_price: contracts per date loop (0 = automatic: in FP32 mode as
+                              many as keep a date's cash flows and two path columns within half
+                              the L2 cache) */
   /* Test hook: [contract][path][step] normals replacing the device stream
    * (FP64_REFERENCE only), NULL to draw on the device. */
   const double* injected_normals;
@@ -606,8 +610,8 @@ of_status of_heston_price_adjoint(of_ctx* ctx, const of_heston_adjoint_params* p
  * kernel_ms is not measured (0). */
 #define OF_STRIP_NOALLOC_MAX_STRIKES 64
 #define OF_STRIP_NOALLOC_MAX_BLOCKS 1024
-#define OF_STRIP_NOALLOC_SCRATCH_BYTES                            \
-  (OF_STRIP_NOALLOC_MAX_STRIKES * 4 + OF_STRIP_NOALLOC_MAX_STRIKES * 2 * 8 + \
+#define OF_STRIP_NOALLOC_SCRATCH_BYTES                                  \
+  (OF_STRIP_NOALLOC_MAX_STRIKES * 4 + (OF_STRIP_NOALLOC_MAX_STRIKES * 2 + 1) * 8 + \
    OF_STRIP_NOALLOC_MAX_BLOCKS * OF_STRIP_NOALLOC_MAX_STRIKES * 2 * 8)
 of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* model, int32_t option_type,
                               const double* strikes, int64_t n_strikes, const of_mc_config* cfg,

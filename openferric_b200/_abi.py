@@ -231,7 +231,7 @@ class OfLsmConfig(C.Structure):
         ("precision", C.c_int32),
         ("basis_degree", C.c_int32),
         ("want_delta", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("batch_contracts", C.c_int32),
         ("injected_normals", C.POINTER(C.c_double)),
         ("n_injected", C.c_int64),
     ]

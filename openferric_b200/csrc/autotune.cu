@@ -54,8 +54,10 @@ extern "C" of_status of_autotune_strip(of_ctx* ctx, const of_model* model, int32
   OF_TRY(check_args(ctx, cands, n_cands, reps, best));
   if (!cfg) return of_fail(ctx, OF_ERR_INVALID_INPUT, "null config");
   for (int32_t i = 0; i < n_cands; ++i) {
-    if (cands[i].paths_per_thread < 1 || cands[i].paths_per_thread > 2)
-      return of_fail(ctx, OF_ERR_INVALID_INPUT, "strip candidate %d: samples in flight per thread must be 1 or 2", i);
+    if (cands[i].paths_per_thread < 1 || cands[i].paths_per_thread > 3)
+      return of_fail(ctx, OF_ERR_INVALID_INPUT,
+                     "strip candidate %d: tile shape must be 1 or 2 samples in flight per thread, or 3 "
+                     "(warp-specialised)", i);
   }
   for (int32_t i = 0; i < n_cands; ++i) {
     of_mc_config c = *cfg;

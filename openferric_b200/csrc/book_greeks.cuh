@@ -83,7 +83,8 @@ struct GMath<float> {
   static constexpr float kHMin = -12.0f;  // Phi(-12) = 1.8e-33 is still a normal float
   static __device__ __forceinline__ float exp(float x) { return __expf(x); }
   static __device__ __forceinline__ float cdf(float x) { return normcdff(x); }
-  static __device__ __forceinline__ float icdf(float x) { return normcdfinvf(x); }
+  // Phi^-1(v) with q = 1 - v: the fitted single-log inverse of the Philox kernels
+  static __device__ __forceinline__ float icdf2(float v, float q) { return inv_normal_vq(v, q); }
   static __device__ __forceinline__ float unif(uint32_t r) { return uniform_from_u32(r); }
   static __device__ __forceinline__ void pair(uint32_t a, uint32_t b, float& z1, float& z2) {
     const float2 p = normal_pair_from_u32(a, b);
@@ -98,7 +99,9 @@ struct GMath<double> {
   static constexpr double kHMin = -37.0;
   static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
   static __device__ __forceinline__ double cdf(double x) { return ::normcdf(x); }
-  static __device__ __forceinline__ double icdf(double x) { return ::normcdfinv(x); }
+  static __device__ __forceinline__ double icdf2(double v, double q) {
+    return v <= 0.5 ? ::normcdfinv(v) : -::normcdfinv(q);
+  }
   // the grid of uniform_from_u32: (k + 0.5) 2^-23, k = the top 23 bits (exact in either type)
   static __device__ __forceinline__ double unif(uint32_t r) { return ((double)(r >> 9) + 0.5) * 0x1p-23; }
   // normal_pair_from_u32's transform in FP64: radius sqrt(-2 ln u1), angle pi (2 f - 3)
@@ -370,13 +373,11 @@ __device__ __forceinline__ void surv_step(SurvLeg<R, G>& s, const GreekConsts<R>
   R h = c.sib * (c.bar - s.y - c.alpha);
   h = h > GMath<R>::kHMin ? h : GMath<R>::kHMin;
   const R p = GMath<R>::cdf(h);
-  const R v = u * p;
-  const R q = fma(-u, p, (R)1);  // 1 - u p with one rounding
-  const bool upper = v > (R)0.5;
-  R lo = upper ? q : v;
-  lo = lo > GMath<R>::kTiny ? lo : GMath<R>::kTiny;
-  R zeta = GMath<R>::icdf(lo);
-  zeta = upper ? -zeta : zeta;
+  R v = u * p;
+  R q = fma(-u, p, (R)1);  // 1 - u p with one rounding
+  v = v > GMath<R>::kTiny ? v : GMath<R>::kTiny;
+  q = q > GMath<R>::kTiny ? q : GMath<R>::kTiny;
+  const R zeta = GMath<R>::icdf2(v, q);
   const R z = c.sgn * zeta;
   if (G) {
     const R kInvSqrt2Pi = (R)0.398942280401432677939946;
@@ -403,7 +404,7 @@ __device__ __forceinline__ void surv_step(SurvLeg<R, G>& s, const GreekConsts<R>
   }
   s.y = fma(c.beta, z, s.y + c.alpha);
   s.L *= p;
-  if (IN) s.ypl = fma(c.beta, GMath<R>::icdf(u), s.ypl + c.alpha);
+  if (IN) s.ypl = fma(c.beta, GMath<R>::icdf2(u, (R)1 - u), s.ypl + c.alpha);
 }
 
 template <typename R, bool G, bool IN>

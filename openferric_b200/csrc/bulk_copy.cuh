@@ -1,5 +1,6 @@
 // bulk_copy.cuh - 1-D bulk asynchronous copies (global -> shared) completed on
-// an mbarrier, for sm_90+ (cp.async.bulk, PTX ISA 8.0).  Each copy lands in
+// an mbarrier, for sm_90+ (cp.async.bulk, PTX ISA 8.0), and the mbarrier
+// operations of producer/consumer rings in shared memory.  Each copy lands in
 // the issuing CTA's own shared memory, and the sources are this GPU's own
 // memory.
 //
@@ -26,6 +27,11 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
 
 // Makes the initialised barriers visible to the async proxy (the bulk copies).
 __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// One plain arrival (release at CTA scope).
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
 
 // One arrival that also announces `bytes` of transactions for the phase.
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "book_greeks.cuh"
+#include "bulk_copy.cuh"
 #include "of_internal.h"
 #include "path_fp32.cuh"
 
@@ -206,6 +207,7 @@ struct StripParams {
   float s0;
   of::PhiloxKeys keys;
   const float* strikes;
+  uint32_t* status;  // warp-specialised kernel: nonzero when a ring wait gave up
 };
 
 template <int KPL, int MODEL, bool ANTI, int ILP = 1>
@@ -273,6 +275,177 @@ __global__ void __launch_bounds__(256, 5) strip_kernel(const __grid_constant__ S
   }
 }
 
+// ---------------------------------------------------------------------------
+// Warp-specialised strike strip (tile_ilp = 3).
+//
+// The step loop of strip_kernel alternates two instruction mixes: the Philox
+// rounds (32x32->64 integer multiplies on the FMA-heavy pipe, three-input
+// XORs on the ALU) and the Box-Muller pair plus the Heston step (lg2, sqrt,
+// sin, cos and sqrt on the MUFU pipe, FP32 FMAs).  All warps of an SM run the
+// same phase at about the same time, so one pipe waits while the other is
+// saturated.  Here half of the warps only generate: producer warp c + 4
+// computes the Philox blocks of the 32 samples its consumer warp c simulates
+// and writes them to a ring in shared memory; the consumer warps only turn
+// draws into normals, steps and payoffs.  The scheduler then always has
+// warps of both mixes to issue.  Same draws, same steps and same payoffs per
+// sample as strip_kernel<..., ILP = 1>; the per-warp sums group samples
+// differently, so results agree to the rounding of the FP32 partial sums.
+//
+// Ring: per consumer kWsSlots chunks of kWsChunk Philox blocks x 32 lanes
+// (uint4), with a full and an empty mbarrier per chunk (32 arrivals each).
+// Every wait is bounded (kWsWaitNs of the global timer) and its outcome is
+// made warp-uniform; a warp whose wait gives up sets P.status and leaves its
+// loops, so its partner's next wait gives up too and the block still reaches
+// its final reduction.
+// ---------------------------------------------------------------------------
+constexpr int kWsPairs = 4;   // consumer warps 0..3, producer warps 4..7
+constexpr int kWsChunk = 4;   // Philox blocks per ring chunk
+constexpr int kWsSlots = 3;   // chunks in flight per pair
+constexpr uint64_t kWsWaitNs = 1000000000ull;
+constexpr size_t kWsRingBytes = (size_t)kWsPairs * kWsSlots * kWsChunk * 32 * sizeof(uint4);
+
+// The steps of Philox block q of one sample (and its antithetic twin), as
+// simulate_terminal consumes them.
+template <int MODEL, bool ANTI>
+__device__ __forceinline__ void ws_consume(const StepConsts& c, const uint4 r, int32_t q, int32_t steps,
+                                           LegState& a, LegState& b, float& w) {
+  if (MODEL == OF_MODEL_GBM) {
+    const int32_t j = q * 4;
+    const float2 p = of::normal_pair_from_u32(r.x, r.y), pq = of::normal_pair_from_u32(r.z, r.w);
+    w += p.x;
+    if (j + 1 < steps) w += p.y;
+    if (j + 2 < steps) w += pq.x;
+    if (j + 3 < steps) w += pq.y;
+  } else if (MODEL == OF_MODEL_HESTON_EULER) {
+    float2 z = of::normal_pair_scaled_from_u32(r.x, r.y, c.bm_k2);
+    of::heston_euler_step(a, c, z.x, z.y);
+    if (ANTI) of::heston_euler_step(b, c, -z.x, -z.y);
+    if (2 * q + 1 < steps) {
+      z = of::normal_pair_scaled_from_u32(r.z, r.w, c.bm_k2);
+      of::heston_euler_step(a, c, z.x, z.y);
+      if (ANTI) of::heston_euler_step(b, c, -z.x, -z.y);
+    }
+  } else {
+    float u = of::uniform_from_u32(r.x), zx = of::normal_from_u32(r.y);
+    of::heston_qe_step(a, c, u, 1.0f, zx, r.x);
+    if (ANTI) of::heston_qe_step(b, c, 1.0f - u, -1.0f, -zx, r.x);
+    if (2 * q + 1 < steps) {
+      u = of::uniform_from_u32(r.z);
+      zx = of::normal_from_u32(r.w);
+      of::heston_qe_step(a, c, u, 1.0f, zx, r.z);
+      if (ANTI) of::heston_qe_step(b, c, 1.0f - u, -1.0f, -zx, r.z);
+    }
+  }
+}
+
+template <int KPL, int MODEL, bool ANTI>
+__global__ void __launch_bounds__(256, 5) strip_kernel_ws(const __grid_constant__ StripParams P,
+                                                       double* __restrict__ partials) {
+  extern __shared__ __align__(16) unsigned char ws_smem[];
+  uint4* ring = reinterpret_cast<uint4*>(ws_smem);                       // [pair][slot][block][lane]
+  double* sh_strip = reinterpret_cast<double*>(ws_smem + kWsRingBytes);  // [warps][n_strikes][2]
+  __shared__ __align__(8) uint64_t full[kWsPairs * kWsSlots], empty[kWsPairs * kWsSlots];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const bool producer = warp >= kWsPairs;
+  const int pair = producer ? warp - kWsPairs : warp;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kWsPairs * kWsSlots; ++k) {
+      of::mbar_init(of::smem_u32(full + k), 32);
+      of::mbar_init(of::smem_u32(empty + k), 32);
+    }
+    of::mbar_fence_init();
+  }
+  __syncthreads();
+  float K[KPL];
+  of::Kahan32 s1[KPL], s2[KPL];
+#pragma unroll
+  for (int q = 0; q < KPL; ++q) {
+    const int k = lane + 32 * q;
+    K[q] = k < P.n_strikes ? P.strikes[k] : 0.0f;
+  }
+  const bool call = P.option_type == OF_CALL;
+  const int32_t spb = MODEL == OF_MODEL_GBM ? 4 : 2;  // steps per Philox block
+  const int32_t nq = (P.steps + spb - 1) / spb;       // Philox blocks per sample
+  const int64_t stride = (int64_t)gridDim.x * kWsPairs * 32;
+  uint4* my_ring = ring + (size_t)pair * kWsSlots * kWsChunk * 32;
+  uint32_t g = 0;  // chunks this pair has passed through its ring
+  bool ok = true;
+  for (int64_t base = ((int64_t)blockIdx.x * kWsPairs + pair) * 32; base < P.samples && ok; base += stride) {
+    const uint64_t i = (uint64_t)(base + lane);
+    const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
+    LegState a{0.0f, P.c.v0}, b{0.0f, P.c.v0};
+    float w = 0.0f;
+    for (int32_t q0 = 0; q0 < nq; q0 += kWsChunk, ++g) {
+      const int slot = (int)(g % kWsSlots);
+      const uint32_t use = g / kWsSlots;
+      uint4* chunk = my_ring + (size_t)slot * kWsChunk * 32;
+      if (producer) {
+        const bool free_ok =
+            use == 0 || of::mbar_wait(of::smem_u32(empty + pair * kWsSlots + slot), (use - 1) & 1u, kWsWaitNs);
+        if (!__all_sync(of::kFullMask, free_ok)) {  // the warp leaves together
+          ok = false;
+          break;
+        }
+#pragma unroll
+        for (int k = 0; k < kWsChunk; ++k)
+          if (q0 + k < nq)
+            chunk[k * 32 + lane] = of::philox4x32_10(make_uint4((uint32_t)(q0 + k), lo, hi, kStripStreamTag), P.keys);
+        of::mbar_arrive(of::smem_u32(full + pair * kWsSlots + slot));
+      } else {
+        const bool full_ok = of::mbar_wait(of::smem_u32(full + pair * kWsSlots + slot), use & 1u, kWsWaitNs);
+        if (!__all_sync(of::kFullMask, full_ok)) {
+          ok = false;
+          break;
+        }
+#pragma unroll
+        for (int k = 0; k < kWsChunk; ++k)
+          if (q0 + k < nq) ws_consume<MODEL, ANTI>(P.c, chunk[k * 32 + lane], q0 + k, P.steps, a, b, w);
+        of::mbar_arrive(of::smem_u32(empty + pair * kWsSlots + slot));
+      }
+    }
+    if (producer || !ok) continue;
+    float ya, yb;
+    if (MODEL == OF_MODEL_GBM) {
+      const float basev = (float)P.steps * P.c.drift;
+      ya = fmaf(P.c.diff, w, basev);
+      yb = fmaf(-P.c.diff, w, basev);
+    } else {
+      ya = a.y;
+      yb = b.y;
+    }
+    const float sa = P.s0 * __expf(ya), sb = P.s0 * __expf(yb);
+    const int64_t rem = P.samples - base;
+    const int nvalid = rem < 32 ? (int)rem : 32;
+    for (int j = 0; j < nvalid; ++j) {
+      const float st = __shfl_sync(of::kFullMask, sa, j);
+      const float sta = ANTI ? __shfl_sync(of::kFullMask, sb, j) : 0.0f;
+#pragma unroll
+      for (int q = 0; q < KPL; ++q) {
+        float x = fmaxf(call ? st - K[q] : K[q] - st, 0.0f);
+        if (ANTI) x = 0.5f * (x + fmaxf(call ? sta - K[q] : K[q] - sta, 0.0f));
+        s1[q].add(x);
+        s2[q].add(x * x);
+      }
+    }
+  }
+  if (!ok && lane == 0) atomicOr(P.status, 1u);
+  const int n = P.n_strikes;
+#pragma unroll
+  for (int q = 0; q < KPL; ++q) {
+    const int k = lane + 32 * q;
+    if (k < n) {
+      sh_strip[(warp * n + k) * 2] = s1[q].value();
+      sh_strip[(warp * n + k) * 2 + 1] = s2[q].value();
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 2 * n; t += blockDim.x) {
+    double acc = 0.0;
+    for (int w2 = 0; w2 < nw; ++w2) acc += sh_strip[w2 * 2 * n + t];
+    partials[(int64_t)blockIdx.x * 2 * n + t] = acc;
+  }
+}
+
 typedef void (*StripKernelFn)(StripParams, double*);
 
 template <int KPL, int ILP = 1>
@@ -283,6 +456,39 @@ StripKernelFn pick_strip(int model, bool anti) {
     return anti ? strip_kernel<KPL, OF_MODEL_HESTON_EULER, true, ILP>
                 : strip_kernel<KPL, OF_MODEL_HESTON_EULER, false, ILP>;
   return anti ? strip_kernel<KPL, OF_MODEL_HESTON_QE, true, ILP> : strip_kernel<KPL, OF_MODEL_HESTON_QE, false, ILP>;
+}
+
+template <int KPL>
+StripKernelFn pick_strip_ws_kpl(int model, bool anti) {
+  if (model == OF_MODEL_GBM) return anti ? strip_kernel_ws<KPL, OF_MODEL_GBM, true> : strip_kernel_ws<KPL, OF_MODEL_GBM, false>;
+  if (model == OF_MODEL_HESTON_EULER)
+    return anti ? strip_kernel_ws<KPL, OF_MODEL_HESTON_EULER, true> : strip_kernel_ws<KPL, OF_MODEL_HESTON_EULER, false>;
+  return anti ? strip_kernel_ws<KPL, OF_MODEL_HESTON_QE, true> : strip_kernel_ws<KPL, OF_MODEL_HESTON_QE, false>;
+}
+
+StripKernelFn pick_strip_ilp(int kpl, int ilp, int model, bool anti);
+
+// The kernel, its dynamic shared memory and the samples one block covers per
+// round, for a strip tile shape: tile 1 or 2 = strip_kernel with that many
+// samples in flight per thread (0 = 1), tile 3 = the warp-specialised
+// strip_kernel_ws.
+struct StripShape {
+  StripKernelFn fn;
+  size_t smem;
+  int64_t samples_per_block;
+  bool ws;
+};
+
+StripShape strip_shape(int tile, int64_t n_strikes, int model, bool anti, int block) {
+  const int kpl = (int)((n_strikes + 31) / 32);
+  const size_t sums = (size_t)(block / 32) * (size_t)n_strikes * 2 * sizeof(double);
+  if (tile == 3) {
+    const StripKernelFn fn = kpl <= 1 ? pick_strip_ws_kpl<1>(model, anti)
+                             : kpl <= 2 ? pick_strip_ws_kpl<2>(model, anti) : pick_strip_ws_kpl<4>(model, anti);
+    return {fn, kWsRingBytes + sums, (int64_t)kWsPairs * 32, true};
+  }
+  const int ilp = tile == 2 ? 2 : 1;
+  return {pick_strip_ilp(kpl, ilp, model, anti), sums, (int64_t)block * ilp, false};
 }
 
 // Kernel for KPL strikes per lane and ILP samples in flight per thread.
@@ -315,6 +521,7 @@ struct of_strip_plan {
   int n_strikes = 0, grid = 0, block = 256;
   size_t smem = 0;
   StripKernelFn fn = nullptr;
+  bool ws = false;  // warp-specialised kernel: clears and reads back the status word after the sums
   double discount = 1.0;
   int64_t samples = 0;
   float* d_strikes = nullptr;
@@ -325,11 +532,21 @@ struct of_strip_plan {
   cudaGraphExec_t exec = nullptr;
 };
 
+// d_sums holds the 2n sums and one more double whose first word is the
+// status of the warp-specialised kernel.
 static of_status strip_enqueue(of_strip_plan* pl, cudaStream_t s) {
-  pl->fn<<<pl->grid, pl->block, pl->smem, s>>>(pl->P, pl->d_partials);
   const int64_t cols = 2 * (int64_t)pl->n_strikes;
+  if (pl->ws) cudaMemsetAsync(pl->d_sums + cols, 0, sizeof(double), s);
+  pl->fn<<<pl->grid, pl->block, pl->smem, s>>>(pl->P, pl->d_partials);
   of_launch_reduce_rows(pl->d_partials, pl->grid, cols, pl->d_sums, s);
-  cudaMemcpyAsync(pl->h_sums, pl->d_sums, cols * sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(pl->h_sums, pl->d_sums, (cols + (pl->ws ? 1 : 0)) * sizeof(double), cudaMemcpyDeviceToHost, s);
+  return OF_OK;
+}
+
+// OF_ERR_TIMEOUT when the warp-specialised kernel's ring gave up.
+static of_status strip_status(of_ctx* ctx, const of_strip_plan* pl) {
+  if (pl->ws && *(const uint32_t*)(pl->h_sums + 2 * pl->n_strikes))
+    return of_fail(ctx, OF_ERR_TIMEOUT, "strike strip: a producer/consumer ring wait did not complete in time");
   return OF_OK;
 }
 
@@ -368,8 +585,8 @@ static of_status strip_validate(of_ctx* ctx, const of_model* m, int32_t option_t
     return of_fail(ctx, OF_ERR_UNSUPPORTED, "the strike strip has no control variate");
   if (cfg->injected_normals)
     return of_fail(ctx, OF_ERR_UNSUPPORTED, "injected normals are a FP64 reference-mode test hook");
-  if (cfg->tile_ilp < 0 || cfg->tile_ilp > 2)
-    return of_fail(ctx, OF_ERR_INVALID_INPUT, "tile_ilp must be 0 (default), 1 or 2");
+  if (cfg->tile_ilp < 0 || cfg->tile_ilp > 3)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "tile_ilp must be 0 (default), 1, 2 or 3");
   return OF_OK;
 }
 
@@ -393,12 +610,12 @@ static of_status strip_setup(of_ctx* ctx, const of_model* m, int32_t option_type
   P.antithetic = cfg->antithetic ? 1 : 0;
   P.s0 = (float)m->s0;
   P.keys = of::philox_keys(cfg->seed);
-  const int kpl = (int)((n_strikes + 31) / 32);
-  const int ilp = cfg->tile_ilp == 2 ? 2 : 1;
-  pl->fn = pick_strip_ilp(kpl, ilp, m->kind, P.antithetic);
-  pl->smem = (size_t)(pl->block / 32) * n_strikes * 2 * sizeof(double);
+  const StripShape sh = strip_shape(cfg->tile_ilp, n_strikes, m->kind, P.antithetic, pl->block);
+  pl->fn = sh.fn;
+  pl->smem = sh.smem;
+  pl->ws = sh.ws;
   const int per_sm = of_blocks_per_sm((const void*)pl->fn, pl->block, pl->smem);
-  const int64_t want = (pl->samples + (int64_t)pl->block * ilp - 1) / ((int64_t)pl->block * ilp);
+  const int64_t want = (pl->samples + sh.samples_per_block - 1) / sh.samples_per_block;
   const int64_t cap = (int64_t)ctx->sm_count * per_sm;
   pl->grid = (int)std::max<int64_t>(1, std::min(want, cap));
   return OF_OK;
@@ -424,12 +641,13 @@ extern "C" of_status of_strip_plan_create(of_ctx* ctx, const of_model* m, int32_
   for (int64_t k = 0; k < n_strikes; ++k) ks[(size_t)k] = (float)strikes[k];
   if (cudaMalloc(&pl->d_strikes, ks.size() * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&pl->d_partials, (size_t)pl->grid * 2 * n_strikes * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&pl->d_sums, 2 * n_strikes * sizeof(double)) != cudaSuccess ||
-      cudaMallocHost(&pl->h_sums, 2 * n_strikes * sizeof(double)) != cudaSuccess)
+      cudaMalloc(&pl->d_sums, (2 * n_strikes + 1) * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&pl->h_sums, (2 * n_strikes + 1) * sizeof(double)) != cudaSuccess)
     return fail(of_fail(ctx, OF_ERR_ALLOC, "strip plan allocation failed"));
   if (cudaMemcpy(pl->d_strikes, ks.data(), ks.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(of_fail(ctx, OF_ERR_CUDA, "strike upload failed"));
   pl->P.strikes = pl->d_strikes;
+  pl->P.status = (uint32_t*)(pl->d_sums + 2 * n_strikes);
   // Capture kernel + reduction + readback once; launches replay the graph.
   cudaStream_t cap_stream = nullptr;
   if (cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -456,6 +674,7 @@ extern "C" of_status of_strip_plan_launch(of_strip_plan* pl) {
 extern "C" of_status of_strip_plan_results(of_strip_plan* pl, of_mc_result* res) {
   if (!pl || !res) return OF_ERR_INVALID_INPUT;
   OF_CUDA_TRY(pl->ctx, cudaStreamSynchronize(pl->ctx->stream));
+  OF_TRY(strip_status(pl->ctx, pl));
   for (int k = 0; k < pl->n_strikes; ++k) {
     const double s[5] = {pl->h_sums[2 * k], pl->h_sums[2 * k + 1], 0.0, 0.0, 0.0};
     of_mc_finish(s, pl->samples, OF_CV_NONE, 0.0, pl->discount, &res[k]);
@@ -475,12 +694,13 @@ extern "C" of_status of_mc_strip(of_ctx* ctx, const of_model* m, int32_t option_
   void *d_k = nullptr, *d_part = nullptr, *d_sums = nullptr, *h = nullptr;
   OF_TRY(of_scratch(ctx, SLOT_STRIKES, (size_t)n_strikes * sizeof(float), &d_k));
   OF_TRY(of_scratch(ctx, SLOT_PARTIALS, (size_t)pl.grid * cols * sizeof(double), &d_part));
-  OF_TRY(of_scratch(ctx, SLOT_SUMS, (size_t)cols * sizeof(double), &d_sums));
-  OF_TRY(of_pinned(ctx, (size_t)cols * sizeof(double) + (size_t)n_strikes * sizeof(float), &h));
-  float* hk = (float*)((double*)h + cols);
+  OF_TRY(of_scratch(ctx, SLOT_SUMS, (size_t)(cols + 1) * sizeof(double), &d_sums));
+  OF_TRY(of_pinned(ctx, (size_t)(cols + 1) * sizeof(double) + (size_t)n_strikes * sizeof(float), &h));
+  float* hk = (float*)((double*)h + cols + 1);
   for (int64_t k = 0; k < n_strikes; ++k) hk[k] = (float)strikes[k];
   OF_CUDA_TRY(ctx, cudaMemcpyAsync(d_k, hk, (size_t)n_strikes * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
   pl.P.strikes = (const float*)d_k;
+  pl.P.status = (uint32_t*)((double*)d_sums + cols);
   pl.d_partials = (double*)d_part;
   pl.d_sums = (double*)d_sums;
   pl.h_sums = (double*)h;
@@ -491,7 +711,8 @@ extern "C" of_status of_mc_strip(of_ctx* ctx, const of_model* m, int32_t option_
   OF_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   float ms = 0.0f;
   OF_CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
-  for (int64_t k = 0; k < n_strikes; ++k) {
+  const of_status st = strip_status(ctx, &pl);
+  for (int64_t k = 0; k < n_strikes && st == OF_OK; ++k) {
     const double s[5] = {pl.h_sums[2 * k], pl.h_sums[2 * k + 1], 0.0, 0.0, 0.0};
     of_mc_finish(s, pl.samples, OF_CV_NONE, 0.0, pl.discount, &results[k]);
     results[k].kernel_ms = ms;
@@ -500,7 +721,7 @@ extern "C" of_status of_mc_strip(of_ctx* ctx, const of_model* m, int32_t option_
   pl.d_partials = nullptr;
   pl.d_sums = nullptr;
   pl.h_sums = nullptr;
-  return OF_OK;
+  return st;
 }
 
 // ---------------------------------------------------------------------------
@@ -1557,7 +1778,8 @@ extern "C" of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* m, i
   }
   float* d_strikes = (float*)base;
   double* d_sums = (double*)((char*)base + OF_STRIP_NOALLOC_MAX_STRIKES * 4);
-  double* d_partials = d_sums + OF_STRIP_NOALLOC_MAX_STRIKES * 2;
+  double* d_status = d_sums + OF_STRIP_NOALLOC_MAX_STRIKES * 2;  // the warp-specialised kernel's status word
+  double* d_partials = d_status + 1;
 
   StripParams P{};
   P.c = make_consts(m);
@@ -1569,36 +1791,43 @@ extern "C" of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* m, i
   P.s0 = (float)m->s0;
   P.keys = of::philox_keys(cfg->seed);
   P.strikes = d_strikes;
-  // the kernel of_mc_strip picks for the same request (strikes per lane, samples in flight)
-  const int ilp = cfg->tile_ilp == 2 ? 2 : 1;
-  const StripKernelFn fn = pick_strip_ilp((int)((n_strikes + 31) / 32), ilp, m->kind, P.antithetic);
+  P.status = (uint32_t*)d_status;
+  // the kernel of_mc_strip picks for the same request (strikes per lane, tile shape)
   const int block = 256;
-  const size_t smem = (size_t)(block / 32) * n_strikes * 2 * sizeof(double);
+  const StripShape sh = strip_shape(cfg->tile_ilp, n_strikes, m->kind, P.antithetic, block);
+  const StripKernelFn fn = sh.fn;
+  const size_t smem = sh.smem;
   int sms = 0, per_sm = 0;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
       (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, block, smem)) != cudaSuccess) {
     noalloc_msg(err, err_len, "device query failed: %s", cudaGetErrorString(e));
     return OF_ERR_CUDA;
   }
-  const int64_t want = (P.samples + (int64_t)block * ilp - 1) / ((int64_t)block * ilp);
+  const int64_t want = (P.samples + sh.samples_per_block - 1) / sh.samples_per_block;
   int64_t grid = std::min<int64_t>(want, (int64_t)sms * std::max(per_sm, 1));
   grid = std::max<int64_t>(1, std::min<int64_t>(grid, OF_STRIP_NOALLOC_MAX_BLOCKS));
 
   cudaStream_t s = (cudaStream_t)cuda_stream;
   const int64_t cols = 2 * n_strikes;
-  double hs[2 * OF_STRIP_NOALLOC_MAX_STRIKES];
+  double hs[2 * OF_STRIP_NOALLOC_MAX_STRIKES + 1];
   if ((e = cudaMemcpyAsync(d_strikes, hk, (size_t)n_strikes * sizeof(float), cudaMemcpyHostToDevice, s)) !=
-      cudaSuccess) {
+          cudaSuccess ||
+      (sh.ws && (e = cudaMemsetAsync(d_status, 0, sizeof(double), s)) != cudaSuccess)) {
     noalloc_msg(err, err_len, "strike upload failed: %s", cudaGetErrorString(e));
     return OF_ERR_CUDA;
   }
   fn<<<(unsigned)grid, block, smem, s>>>(P, d_partials);
   of_launch_reduce_rows(d_partials, grid, cols, d_sums, s);
   if ((e = cudaGetLastError()) != cudaSuccess ||
-      (e = cudaMemcpyAsync(hs, d_sums, (size_t)cols * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(hs, d_sums, (size_t)(cols + 1) * sizeof(double), cudaMemcpyDeviceToHost, s)) !=
+          cudaSuccess ||
       (e = cudaStreamSynchronize(s)) != cudaSuccess) {
     noalloc_msg(err, err_len, "strip launch failed: %s", cudaGetErrorString(e));
     return OF_ERR_CUDA;
+  }
+  if (sh.ws && *(const uint32_t*)(hs + cols)) {
+    noalloc_msg(err, err_len, "strike strip: a producer/consumer ring wait did not complete in time");
+    return OF_ERR_TIMEOUT;
   }
   for (int64_t k = 0; k < n_strikes; ++k) {
     const double sums[5] = {hs[2 * k], hs[2 * k + 1], 0.0, 0.0, 0.0};

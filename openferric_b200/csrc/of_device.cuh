@@ -157,6 +157,31 @@ __device__ __forceinline__ float normal_from_u32(uint32_t r) {
   return x * p;
 }
 
+// Phi^-1(v) for v in (0,1) given q = 1 - v (each exact or rounded once, so
+// that either tail keeps its relative precision): the polynomials of
+// normal_from_u32 on x = v - q = 2v - 1 and w = -log2(4 v q), whose fit
+// covers w <= 26 (v or q down to ~3.7e-9); CUDA's normcdfinvf beyond that.
+__device__ __forceinline__ float inv_normal_vq(float v, float q) {
+  const float t = 4.0f * v * q;  // 1 - x^2
+  if (t < 1.4901161193847656e-8f)  // 2^-26: past the tail fit (probability ~1e-8 per draw)
+    return v <= 0.5f ? normcdfinvf(v) : -normcdfinvf(q);
+  const float x = v - q;
+  const float w = -__log2f(t);
+  float p;
+  if (w < OF_INVN_W_SPLIT) {
+    const float s = w - OF_INVN_C_CENTER;
+    p = kInvnCentral[OF_INVN_DEG_C];
+#pragma unroll
+    for (int i = OF_INVN_DEG_C - 1; i >= 0; --i) p = fmaf(p, s, kInvnCentral[i]);
+  } else {
+    const float s = sqrtf(w) - OF_INVN_T_CENTER;
+    p = kInvnTail[OF_INVN_DEG_T];
+#pragma unroll
+    for (int i = OF_INVN_DEG_T - 1; i >= 0; --i) p = fmaf(p, s, kInvnTail[i]);
+  }
+  return x * p;
+}
+
 // u32 -> uniform in (0,1), the same grid as normal_from_u32: (k + 0.5) 2^-23.
 __device__ __forceinline__ float uniform_from_u32(uint32_t r) {
   const float f = __uint_as_float(0x3F800000u | (r >> 9));

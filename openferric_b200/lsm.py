@@ -76,6 +76,7 @@ class LongstaffSchwartzEngine:
         self.device = device
         self.dynamics = LsmDynamics.Gbm
         self.injected_normals: Optional[np.ndarray] = None
+        self.batch_contracts = 0
         self.last_kernel_ms = 0.0
 
     @staticmethod
@@ -100,6 +101,15 @@ class LongstaffSchwartzEngine:
         if degree not in (2, 3):
             raise PricingError.InvalidInput("basis degree must be 2 or 3")
         self.basis_degree = degree
+        return self
+
+    def with_batch_contracts(self, n: int) -> "LongstaffSchwartzEngine":
+        """Contracts per date loop of price_batch (0 = automatic: in FP32 mode
+        as many as keep a date's cash flows and two path columns within half
+        the L2 cache)."""
+        if n < 0:
+            raise PricingError.InvalidInput("batch_contracts must be >= 0")
+        self.batch_contracts = int(n)
         return self
 
     def with_injected_normals(self, normals: Optional[np.ndarray]) -> "LongstaffSchwartzEngine":
@@ -136,7 +146,7 @@ class LongstaffSchwartzEngine:
         arr = (A.OfLsmContract * len(built))(*[b[0] for b in built])
         cfg = A.OfLsmConfig(num_paths=self.num_paths, seed=self.seed & 0xFFFFFFFFFFFFFFFF,
                             precision=self.precision.value, basis_degree=self.basis_degree,
-                            want_delta=int(want_delta))
+                            want_delta=int(want_delta), batch_contracts=self.batch_contracts)
         if self.injected_normals is not None:
             cfg.injected_normals = self.injected_normals.ctypes.data_as(C.POINTER(C.c_double))
             cfg.n_injected = self.injected_normals.size

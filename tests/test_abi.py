@@ -114,7 +114,7 @@ def test_noalloc_strip_validates_like_of_mc_strip():
     from openferric_b200 import Heston, HestonPathGenerator
     gen = HestonPathGenerator(Heston(0.03, 2.0, 0.04, 0.5, -0.7, 0.04), 100.0, 1.0, 8)
     model = gen.to_abi()
-    st, msg = _noalloc(model, [100.0], tile_ilp=3)
+    st, msg = _noalloc(model, [100.0], tile_ilp=4)
     assert st == A.OF_ERR_INVALID_INPUT and "tile_ilp" in msg
     st, msg = _noalloc(model, [100.0], control_variate=A.OF_CV_TERMINAL_SPOT)
     assert st == A.OF_ERR_UNSUPPORTED and "control variate" in msg

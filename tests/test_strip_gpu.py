@@ -111,7 +111,43 @@ def test_strip_gbm_two_samples_in_flight_matches_one():
         assert abs(p1 - p2) <= 2e-6 * max(1.0, abs(p1)), (p1, p2)
 
 
+@pytest.mark.parametrize("scheme", ["euler", "qe", "gbm"])
+@pytest.mark.parametrize("anti", [False, True])
+@pytest.mark.parametrize("n_paths,strikes", [(1 << 16, 37), (100_003, 41), (333, 64), (4099, 5)])
+def test_strip_warp_specialised_matches_one_sample_per_thread(scheme, anti, n_paths, strikes):
+    """tile_ilp=3: producer warps write the same Philox blocks to a shared-memory
+    ring and consumer warps run the same steps and payoffs per sample, so the
+    prices agree with tile_ilp=1 up to the FP32 accumulation order.  Odd step
+    counts exercise the partial last Philox block, ragged path counts the
+    partial last warp round, 64 strikes two strikes per lane, and 333 paths
+    fewer samples than one block's round."""
+    gen = GbmPathGenerator(Gbm(0.05, 0.2), 100.0, 1.0, 29) if scheme == "gbm" else \
+        HestonPathGenerator(HESTON, 100.0, 1.0, 63, scheme=scheme)
+    ks = [60.0 + 80.0 * k / max(1, strikes - 1) for k in range(strikes)]
+    one = price_strike_strip(gen, OptionType.Call, ks, n_paths, 9, 0.97, antithetic=anti, tile_ilp=1)
+    ws = price_strike_strip(gen, OptionType.Call, ks, n_paths, 9, 0.97, antithetic=anti, tile_ilp=3)
+    for (p1, s1), (p3, s3) in zip(one, ws):
+        assert abs(p1 - p3) <= 2e-6 * max(1.0, abs(p1)), (p1, p3)
+        assert abs(s1 - s3) <= 2e-6 * max(1.0, s1), (s1, s3)
+
+
+def test_strip_warp_specialised_plan_replays():
+    """The plan (CUDA graph with the status-word reset) replays the
+    warp-specialised kernel and returns the same prices every time."""
+    from openferric_b200.engines import StripPlan
+    gen = HestonPathGenerator(HESTON, 100.0, 1.0, 64)
+    plan = StripPlan(gen, OptionType.Call, STRIKES, 1 << 16, 5, 0.97, tile_ilp=3)
+    try:
+        plan.launch()
+        first = plan.results()
+        for _ in range(3):
+            plan.launch()
+        assert plan.results() == first
+    finally:
+        plan.close()
+
+
 def test_strip_rejects_bad_tile_ilp():
     gen = GbmPathGenerator(Gbm(0.05, 0.2), 100.0, 1.0, 8)
     with pytest.raises(PricingError):
-        price_strike_strip(gen, OptionType.Call, [100.0], 1000, 3, 1.0, tile_ilp=3)
+        price_strike_strip(gen, OptionType.Call, [100.0], 1000, 3, 1.0, tile_ilp=4)

@@ -64,6 +64,20 @@ def test_noalloc_strip_full_strike_layout_gbm_antithetic_two_samples_per_thread(
             assert abs(s - rs) <= 1e-9 * abs(rs) + 1e-12
 
 
+def test_noalloc_strip_warp_specialised_shape():
+    """tile_ilp=3 runs the warp-specialised kernel from the static array (its
+    ring status word included) and matches of_mc_strip with the same shape."""
+    gen = HestonPathGenerator(Heston(0.03, 2.0, 0.04, 0.5, -0.7, 0.04), 100.0, 1.0, 63)
+    df = math.exp(-0.03)
+    ref = price_strike_strip(gen, OptionType.Call, STRIKES, 100_003, 3, df, tile_ilp=3)
+    for _ in range(2):
+        st, msg, got = noalloc_strip(gen.to_abi(), A.OF_CALL, STRIKES, 100_003, 3, df, tile_ilp=3)
+        assert st == A.OF_OK, msg
+        for (p, s), (rp, rs) in zip(got, ref):
+            assert abs(p - rp) <= 1e-9 * abs(rp) + 1e-12, (p, rp)
+            assert abs(s - rs) <= 1e-9 * abs(rs) + 1e-12
+
+
 def test_noalloc_strip_rejects_sizes_beyond_its_static_scratch():
     gen = HestonPathGenerator(Heston(0.03, 2.0, 0.04, 0.5, -0.7, 0.04), 100.0, 1.0, 8)
     too_many = [90.0 + 0.1 * k for k in range(65)]
