@@ -856,20 +856,25 @@ def main():
         ("sfu", sfu_line, "fp32", fp32_line) if sfu_frac >= fp32_frac else ("fp32", fp32_line, "sfu", sfu_line))
     # issue slots: Philox, conversions and control flow included
     sm_run = clk.get("sm_mhz") or sm_max
-    ips = INSTR_PER_STEP.get(tile_ilp, INSTR_PER_STEP[1])
+    ips = INSTR_PER_STEP.get(tile_ilp)
     issue_peak = 148 * 4 * sm_run * 1e6
-    issue_line = {"achieved": per_gpu * ips / 32.0 / 1e12, "peak": issue_peak / 1e12, "unit": "T warp-inst/s",
-                  "frac": per_gpu * ips / 32.0 / issue_peak, "per_step": ips,
+    issue_line = {"achieved": per_gpu * ips / 32.0 / 1e12 if ips else None, "peak": issue_peak / 1e12,
+                  "unit": "T warp-inst/s", "frac": per_gpu * ips / 32.0 / issue_peak if ips else None,
+                  "per_step": ips,
                   "peak_source": f"148 SMs x 4 schedulers x 1 warp instruction per cycle at the sampled "
                                  f"{sm_run:.0f} MHz",
-                  "per_step_source": INSTR_SOURCE}
+                  "per_step_source": INSTR_SOURCE if ips else "no ncu instruction count for this tile shape"}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": dict(CONFIG, parallelism=f"replicas{world}", tile_ilp=tile_ilp,
                                                           tile_ilp_ms={str(k): v for k, v in tune_ms.items()}),
         "roofline": dict(main_line, bound=bound, traffic=STRIP_DRAM_BYTES, traffic_source=STRIP_DRAM_SOURCE,
-                         issue=issue_line, **{other_name: other_line}),
+                         issue=issue_line, **{other_name: other_line},
+                         # the survey's declared count: a single-log inverse normal per draw
+                         # (2 lg2 per step) + sqrt + ex2; Box-Muller issues 5 (lg2, sqrt, sin, cos per
+                         # pair of normals, sqrt of the variance)
+                         frac_at_4_mufu_per_step=per_gpu * 4.0 / sfu_peak),
         "e2e": {"value": world * PATH_STEPS * args.steps / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": 41 * 4, "d2h_bytes_per_step": 41 * 2 * 8},
         "gpu_launches": 2 * args.steps,

@@ -160,3 +160,48 @@ def test_greeks_mode_rejects_what_it_cannot_differentiate():
         DividendSchedule([DividendEvent.cash(0.5, 1.0)])).build()
     with pytest.raises(PricingError):
         price_book_greeks([BookEntry(VanillaOption.european_call(100.0, 1.0), md, 4096, 16)], seed=1)
+
+
+def _oracle_option(kind, k, steps=48, anti=False):
+    from oracle.book_oracle import GreekOption
+    base = dict(s0=BASE["spot"], r=BASE["rate"], q=BASE["q"], sigma=BASE["vol"], T=1.25, steps=steps, stream=k,
+                antithetic=anti)
+    daily = [0.0] + [1.0] * steps
+    monthly = [0.0] * (steps + 1)
+    for j in range(1, 13):
+        monthly[round(j / 12.0 * steps)] += 1.0
+    monthly0 = list(monthly)
+    monthly0[0] += 1.0
+    return {
+        "euro_call": GreekOption("vanilla", True, strike=105.0, **base),
+        "euro_put": GreekOption("vanilla", False, strike=95.0, **base),
+        "asian_daily": GreekOption("asian", True, strike=100.0, weights=daily, **base),
+        "asian_monthly_put": GreekOption("asian", False, strike=102.0, weights=monthly, **base),
+        "asian_geometric": GreekOption("asian", True, strike=98.0, weights=daily, geometric=True, **base),
+        "asian_floating": GreekOption("asian", True, strike=1.0, weights=monthly0, floating=True, **base),
+        "up_out_call": GreekOption("barrier", True, strike=100.0, up=True, barrier=135.0, **base),
+        "down_out_put": GreekOption("barrier", False, strike=100.0, up=False, barrier=75.0, rebate=1.5, **base),
+        "up_in_call": GreekOption("barrier", True, strike=100.0, up=True, knock_in=True, barrier=125.0, rebate=0.5,
+                                  **base),
+        "down_in_put": GreekOption("barrier", False, strike=100.0, up=False, knock_in=True, barrier=85.0, **base),
+    }[kind]
+
+
+@pytest.mark.parametrize("anti", [False, True])
+def test_book_greeks_mode_matches_the_oracle_on_the_same_draws(anti):
+    """The CPU restatement (oracle/book_oracle.py) draws the kernel's own
+    Philox blocks: the FP64 mode equals it to FP64 rounding, and the FP32
+    Greeks mode's price and Greeks to FP32 path precision."""
+    from oracle.book_oracle import book_greeks
+    paths, seed = 4096, 77
+    base = (BASE["spot"], BASE["vol"], BASE["rate"], 1.25)
+    book = [_entry(k, *base, paths=paths, anti=anti) for k in KINDS]
+    g32 = price_book_greeks(book, seed)
+    p64 = price_book_fp64(book, seed)
+    for k, kind in enumerate(KINDS):
+        price, g = book_greeks(_oracle_option(kind, k, anti=anti), paths, seed)
+        assert abs(p64[k].price - price) <= 1e-9 * abs(price) + 1e-12, (kind, p64[k].price, price)
+        assert abs(g32[k].result.price - price) <= 2e-5 * abs(price) + 1e-6, (kind, g32[k].result.price, price)
+        gg = g32[k].result.greeks
+        for name, value, ref in zip(("delta", "vega", "rho", "theta"), (gg.delta, gg.vega, gg.rho, gg.theta), g):
+            assert abs(value - ref) <= 1e-4 * abs(ref) + 2e-5, (kind, name, value, ref)
