@@ -619,7 +619,8 @@ def leg_book_greeks(n=256, per_kind=8, seed=BOOK_SEED):
         dt, base, g64, _ = fp64_plain_bump_greeks(e, 1e-4 * e.market.spot, seed=42)
         t64 += dt
         r = res[i]
-        zs.append(max(abs(r.result.price - base.price) / math.hypot(r.result.stderr, base.stderr), 0.0))
+        se = math.hypot(r.result.stderr, base.stderr)
+        zs.append(abs(r.result.price - base.price) / se if se > 0.0 else 0.0)
     # accuracy on the same draws: FP32 pathwise Greeks against central differences
     # of FP64 revaluations of the same launch (bumps 1e-4 relative)
     fixed = [BookEntry(e.instrument, e.market, int(r.result.diagnostics.get("num_paths")), e.num_steps,
@@ -700,7 +701,7 @@ def leg_lsm(paths, contracts, seed=7, batch_contracts=0):
                          "peak_source": src, "per_path_date_bytes": LSM_ALG_BYTES_PER_PATH_DATE,
                          "scope": "all kernels of the workload (generation, passes, final), device time from CUDA "
                                   "events around each batch"},
-            "batch_contracts": batch_contracts or "automatic (L2-sized)",
+            "batch_contracts": batch_contracts or "automatic (path-store budget)",
             "price_range": [min(prices), max(prices)], "clocks": clocks.summary()}
 
 

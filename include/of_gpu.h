@@ -399,9 +399,8 @@ typedef struct of_lsm_config {
                            paths; FP32_PHILOX: Philox normals, FP32 path store */
   int32_t basis_degree; /* 2: {1,S,S^2} + LU (the reference); 3: {1,x,x^2,x^3}, x=S/K, Cholesky */
   int32_t want_delta;   /* also return the pathwise delta under the fitted exercise policy */
-  int32_t batch_contracts; /* of_lsm_price: contracts per date loop (0 = automatic: in FP32 mode as
-                              many as keep a date's cash flows and two path columns within half
-                              the L2 cache) */
+  int32_t batch_contracts; /* of_lsm_price: at most this many contracts per date loop (0 = as many
+                              as the path-store budget allows) */
   /* Test hook: [contract][path][step] normals replacing the device stream
    * (FP64_REFERENCE only), NULL to draw on the device. */
   const double* injected_normals;

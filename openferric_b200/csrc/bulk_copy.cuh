@@ -70,4 +70,18 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_
   return true;
 }
 
+// mbar_wait with a pause of `sleep_ns` between polls: a warp waiting on a
+// slower partner warp then leaves the issue slots to the warps doing work
+// instead of spinning on the barrier and the global timer.
+__device__ __forceinline__ bool mbar_wait_backoff(uint32_t bar, uint32_t parity, uint64_t limit_ns,
+                                                  uint32_t sleep_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    __nanosleep(sleep_ns);
+    if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > limit_ns) return false;
+  }
+}
+
 }  // namespace of

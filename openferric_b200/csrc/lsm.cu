@@ -1552,13 +1552,6 @@ extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_
   const size_t esz = fp64 ? sizeof(double) : sizeof(float);
   const int64_t npad = (N + kPathsPerBlock - 1) / kPathsPerBlock * kPathsPerBlock;
   if (cfg->batch_contracts < 0) return of_fail(ctx, OF_ERR_INVALID_INPUT, "batch_contracts must be >= 0");
-  // FP32: a pass reads S(t+1), S(t) and V and writes V, and the next pass
-  // reads S(t) again and V again.  With a batch whose V and two path columns
-  // fit in half the L2, those second reads hit L2 instead of HBM.
-  int l2_bytes = 0;
-  if (cudaDeviceGetAttribute(&l2_bytes, cudaDevAttrL2CacheSize, ctx->device) != cudaSuccess || l2_bytes <= 0)
-    l2_bytes = 64 << 20;
-  const size_t l2_cap = std::max<size_t>(1, (size_t)l2_bytes / 2 / ((size_t)npad * 3 * sizeof(float)));
   // Contracts sharing a step count go through the date loop together, in
   // batches bounded by a path-store budget.
   const size_t budget = (size_t)24 << 30;
@@ -1584,7 +1577,6 @@ extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_
     const size_t per = (size_t)steps * npad * esz;
     size_t cap = std::max<size_t>(1, budget / per);
     if (cfg->batch_contracts > 0) cap = std::min<size_t>(cap, (size_t)cfg->batch_contracts);
-    else if (!fp64) cap = std::min<size_t>(cap, l2_cap);
     if (cfg->injected_normals) cap = 1;  // one contract per batch keeps the injected layout simple
     std::vector<int64_t> batch;
     while (pos < order.size() && batch.size() < cap && ks[order[pos]].num_steps == steps &&

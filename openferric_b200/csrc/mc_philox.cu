@@ -293,8 +293,9 @@ __global__ void __launch_bounds__(256, 5) strip_kernel(const __grid_constant__ S
 //
 // Ring: per consumer kWsSlots chunks of kWsChunk Philox blocks x 32 lanes
 // (uint4), with a full and an empty mbarrier per chunk (32 arrivals each).
-// Every wait is bounded (kWsWaitNs of the global timer) and its outcome is
-// made warp-uniform; a warp whose wait gives up sets P.status and leaves its
+// Every wait is bounded (kWsWaitNs of the global timer), pauses between
+// polls so a waiting warp leaves the issue slots to working ones, and its
+// outcome is made warp-uniform; a warp whose wait gives up sets P.status and leaves its
 // loops, so its partner's next wait gives up too and the block still reaches
 // its final reduction.
 // ---------------------------------------------------------------------------
@@ -302,6 +303,7 @@ constexpr int kWsPairs = 4;   // consumer warps 0..3, producer warps 4..7
 constexpr int kWsChunk = 4;   // Philox blocks per ring chunk
 constexpr int kWsSlots = 3;   // chunks in flight per pair
 constexpr uint64_t kWsWaitNs = 1000000000ull;
+constexpr uint32_t kWsSleepNs = 128;  // pause between polls of a ring barrier
 constexpr size_t kWsRingBytes = (size_t)kWsPairs * kWsSlots * kWsChunk * 32 * sizeof(uint4);
 
 // The steps of Philox block q of one sample (and its antithetic twin), as
@@ -381,7 +383,8 @@ __global__ void __launch_bounds__(256, 5) strip_kernel_ws(const __grid_constant_
       uint4* chunk = my_ring + (size_t)slot * kWsChunk * 32;
       if (producer) {
         const bool free_ok =
-            use == 0 || of::mbar_wait(of::smem_u32(empty + pair * kWsSlots + slot), (use - 1) & 1u, kWsWaitNs);
+            use == 0 || of::mbar_wait_backoff(of::smem_u32(empty + pair * kWsSlots + slot), (use - 1) & 1u,
+                                              kWsWaitNs, kWsSleepNs);
         if (!__all_sync(of::kFullMask, free_ok)) {  // the warp leaves together
           ok = false;
           break;
@@ -392,7 +395,8 @@ __global__ void __launch_bounds__(256, 5) strip_kernel_ws(const __grid_constant_
             chunk[k * 32 + lane] = of::philox4x32_10(make_uint4((uint32_t)(q0 + k), lo, hi, kStripStreamTag), P.keys);
         of::mbar_arrive(of::smem_u32(full + pair * kWsSlots + slot));
       } else {
-        const bool full_ok = of::mbar_wait(of::smem_u32(full + pair * kWsSlots + slot), use & 1u, kWsWaitNs);
+        const bool full_ok =
+            of::mbar_wait_backoff(of::smem_u32(full + pair * kWsSlots + slot), use & 1u, kWsWaitNs, kWsSleepNs);
         if (!__all_sync(of::kFullMask, full_ok)) {
           ok = false;
           break;
@@ -1809,7 +1813,8 @@ extern "C" of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* m, i
 
   cudaStream_t s = (cudaStream_t)cuda_stream;
   const int64_t cols = 2 * n_strikes;
-  double hs[2 * OF_STRIP_NOALLOC_MAX_STRIKES + 1];
+  double hs[2 * OF_STRIP_NOALLOC_MAX_STRIKES];
+  uint32_t h_status = 0;
   if ((e = cudaMemcpyAsync(d_strikes, hk, (size_t)n_strikes * sizeof(float), cudaMemcpyHostToDevice, s)) !=
           cudaSuccess ||
       (sh.ws && (e = cudaMemsetAsync(d_status, 0, sizeof(double), s)) != cudaSuccess)) {
@@ -1819,13 +1824,14 @@ extern "C" of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* m, i
   fn<<<(unsigned)grid, block, smem, s>>>(P, d_partials);
   of_launch_reduce_rows(d_partials, grid, cols, d_sums, s);
   if ((e = cudaGetLastError()) != cudaSuccess ||
-      (e = cudaMemcpyAsync(hs, d_sums, (size_t)(cols + 1) * sizeof(double), cudaMemcpyDeviceToHost, s)) !=
-          cudaSuccess ||
+      (e = cudaMemcpyAsync(hs, d_sums, (size_t)cols * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (sh.ws &&
+       (e = cudaMemcpyAsync(&h_status, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s)) != cudaSuccess) ||
       (e = cudaStreamSynchronize(s)) != cudaSuccess) {
     noalloc_msg(err, err_len, "strip launch failed: %s", cudaGetErrorString(e));
     return OF_ERR_CUDA;
   }
-  if (sh.ws && *(const uint32_t*)(hs + cols)) {
+  if (h_status) {
     noalloc_msg(err, err_len, "strike strip: a producer/consumer ring wait did not complete in time");
     return OF_ERR_TIMEOUT;
   }

@@ -104,9 +104,8 @@ class LongstaffSchwartzEngine:
         return self
 
     def with_batch_contracts(self, n: int) -> "LongstaffSchwartzEngine":
-        """Contracts per date loop of price_batch (0 = automatic: in FP32 mode
-        as many as keep a date's cash flows and two path columns within half
-        the L2 cache)."""
+        """At most this many contracts per date loop of price_batch (0 = as
+        many as the path-store budget allows)."""
         if n < 0:
             raise PricingError.InvalidInput("batch_contracts must be >= 0")
         self.batch_contracts = int(n)

@@ -50,7 +50,7 @@ def test_native_autotune_rejects_bad_candidates(tmp_path, monkeypatch):
     from openferric_b200 import PricingError
     gen = HestonPathGenerator(HESTON, 100.0, 1.0, 8)
     with pytest.raises(PricingError, match="1 or 2"):
-        autotune.tune_strip(gen, [100.0], 1 << 12, candidates=(1, 3))
+        autotune.tune_strip(gen, [100.0], 1 << 12, candidates=(1, 4))
     with pytest.raises(PricingError, match="reps"):
         autotune.tune_strip(gen, [100.0], 1 << 12, reps=0)
     book = synthetic_book(4, seed=3, min_log2_paths=10, max_log2_paths=11)
