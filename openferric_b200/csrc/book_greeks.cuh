@@ -368,9 +368,27 @@ __device__ __forceinline__ void surv_init(SurvLeg<R, G>& s, const GreekConsts<R>
 //   (ln p)' = g h' with g = phi(h) / p,
 //   z' = sgn u p' / phi(Phi^-1(u p)) = sgn (v / phi(zeta)) g h',   v = u p,
 //   y_next' = y' + alpha' + beta' z + beta z'.
+// Distance to the barrier, in step standard deviations, beyond which the FP32
+// Greeks mode takes the unconditioned step (phi(8) = 5e-15).
+constexpr float kSurvFar = 8.0f;
+
 template <typename R, bool G, bool IN>
 __device__ __forceinline__ void surv_step(SurvLeg<R, G>& s, const GreekConsts<R>& c, R u) {
   R h = c.sib * (c.bar - s.y - c.alpha);
+  if (G && __all_sync(__activemask(), h > (R)kSurvFar)) {
+    // Every path of the warp is more than kSurvFar step deviations from the
+    // barrier: p = Phi(h) rounds to 1 in FP32 and phi(h) / p < 3e-15, so the
+    // step is the unconditioned one and only the drift and volatility
+    // tangents move.
+    const R zeta = GMath<R>::icdf2(u, (R)1 - u);
+    const R z = c.sgn * zeta;
+    s.yd[1] += fma(c.beta_over_sig, z, -c.sig_dt);
+    s.yd[2] += c.dt;
+    s.yd[3] += fma(c.beta_over_2T, z, c.alpha_over_T);
+    s.y = fma(c.beta, z, s.y + c.alpha);
+    if (IN) s.ypl = fma(c.beta, zeta, s.ypl + c.alpha);
+    return;
+  }
   h = h > GMath<R>::kHMin ? h : GMath<R>::kHMin;
   const R p = GMath<R>::cdf(h);
   R v = u * p;
@@ -469,36 +487,42 @@ __device__ __forceinline__ void gk_barrier(const GreekConsts<R>& c, uint64_t i, 
 }
 
 // ---- dispatch ---------------------------------------------------------------
-template <typename R, bool G, bool ANTI>
-__device__ __forceinline__ void gk_sample_anti(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
-                                               const float* obs_w, GreekSample<R>& out) {
-  switch (c.kind) {
-    case GK_TERMINAL:
-      gk_terminal<R, G, ANTI>(c, i, K, out);
-      return;
-    case GK_ASIAN_DAILY:
+// Kind groups: each is priced by a persistent launch of its own, so that the
+// registers of the survival step (the largest) do not set the occupancy of
+// the vanilla and Asian loops.
+enum : int { KG_TERMINAL = 0, KG_ASIAN = 1, KG_BARRIER = 2, KG_COUNT = 3 };
+
+__host__ __device__ __forceinline__ int gk_group(int kind) {
+  return kind == GK_TERMINAL ? KG_TERMINAL : (kind == GK_ASIAN_DAILY || kind == GK_ASIAN_WEIGHTS) ? KG_ASIAN
+                                                                                                  : KG_BARRIER;
+}
+
+template <typename R, bool G, int KG, bool ANTI>
+__device__ __forceinline__ void gk_sample_group_anti(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
+                                                     const float* obs_w, GreekSample<R>& out) {
+  if (KG == KG_TERMINAL) {
+    gk_terminal<R, G, ANTI>(c, i, K, out);
+  } else if (KG == KG_ASIAN) {
+    if (c.kind == GK_ASIAN_DAILY) {
       if (c.flags & GF_GEOMETRIC) gk_asian<R, G, ANTI, true, false, true>(c, i, K, obs_w, out);
       else if (c.cv_kind == GCV_GEOMETRIC_ASIAN) gk_asian<R, G, ANTI, true, true, true>(c, i, K, obs_w, out);
       else gk_asian<R, G, ANTI, true, true, false>(c, i, K, obs_w, out);
-      return;
-    case GK_ASIAN_WEIGHTS:
+    } else {
       if (c.flags & GF_GEOMETRIC) gk_asian<R, G, ANTI, false, false, true>(c, i, K, obs_w, out);
-      else gk_asian<R, G, ANTI, false, true, true>(c, i, K, obs_w, out);
-      return;
-    case GK_BARRIER_OUT:
-      gk_barrier<R, G, ANTI, false>(c, i, K, out);
-      return;
-    default:
-      gk_barrier<R, G, ANTI, true>(c, i, K, out);
-      return;
+      else if (c.cv_kind == GCV_GEOMETRIC_ASIAN) gk_asian<R, G, ANTI, false, true, true>(c, i, K, obs_w, out);
+      else gk_asian<R, G, ANTI, false, true, false>(c, i, K, obs_w, out);
+    }
+  } else {
+    if (c.kind == GK_BARRIER_OUT) gk_barrier<R, G, ANTI, false>(c, i, K, out);
+    else gk_barrier<R, G, ANTI, true>(c, i, K, out);
   }
 }
 
-template <typename R, bool G>
-__device__ __forceinline__ void gk_sample(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
-                                          const float* obs_w, GreekSample<R>& out) {
-  if (c.flags & GF_ANTI) gk_sample_anti<R, G, true>(c, i, K, obs_w, out);
-  else gk_sample_anti<R, G, false>(c, i, K, obs_w, out);
+template <typename R, bool G, int KG>
+__device__ __forceinline__ void gk_sample_group(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
+                                                const float* obs_w, GreekSample<R>& out) {
+  if (c.flags & GF_ANTI) gk_sample_group_anti<R, G, KG, true>(c, i, K, obs_w, out);
+  else gk_sample_group_anti<R, G, KG, false>(c, i, K, obs_w, out);
 }
 
 }  // namespace of

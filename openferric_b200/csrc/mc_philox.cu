@@ -1091,11 +1091,14 @@ struct GreekAcc<double, false> {
 };
 
 // The book's Greeks modes: the persistent tile loop of book_kernel over the
-// per-sample kernels of book_greeks.cuh.  <float, true>: prices and pathwise
-// Greeks (13 sums per tile); <double, false>: FP64 prices on the same draws.
-template <typename R, bool G>
-__global__ void __launch_bounds__(256, 2) book_greeks_kernel(const __grid_constant__ BookParams P,
-                                                              const of::GreekConsts<R>* __restrict__ gc) {
+// per-sample kernels of book_greeks.cuh, one launch per kind group (the
+// group's tiles only).  <float, true>: prices and pathwise Greeks (13 sums
+// per tile); <double, false>: FP64 prices on the same draws.  The survival
+// step of the barrier group needs the most registers: two blocks per SM;
+// the vanilla and Asian groups fit three.
+template <typename R, bool G, int KG>
+__global__ void __launch_bounds__(256, (KG == of::KG_BARRIER || !G) ? 2 : 3)
+    book_greeks_kernel(const __grid_constant__ BookParams P, const of::GreekConsts<R>* __restrict__ gc) {
   constexpr int NC = G ? 13 : 5;
   __shared__ int tile_sh;
   __shared__ double red_sh[NC * 8];
@@ -1111,7 +1114,7 @@ __global__ void __launch_bounds__(256, 2) book_greeks_kernel(const __grid_consta
       const int local = k * blockDim.x + threadIdx.x;
       if (local >= tile.count) break;
       of::GreekSample<R> v;
-      of::gk_sample<R, G>(c, (uint64_t)(tile.first + local), P.keys, P.obs_w, v);
+      of::gk_sample_group<R, G, KG>(c, (uint64_t)(tile.first + local), P.keys, P.obs_w, v);
       acc.add(v);
     }
     double v[NC];
@@ -1267,6 +1270,8 @@ struct of_book_plan {
   std::vector<int32_t> cv_kind;
   std::vector<double> cv_expected, discount;
   BookParams P{};
+  BookParams Pg[of::KG_COUNT]{};  // Greeks modes: one launch per kind group
+  int grid_g[of::KG_COUNT] = {0, 0, 0};
   BookOpt* d_opts = nullptr;
   BookTile* d_tiles = nullptr;
   float* d_obs = nullptr;
@@ -1282,20 +1287,39 @@ struct of_book_plan {
   cudaGraphExec_t exec = nullptr;
 };
 
-static const void* book_kernel_for(int mode) {
-  if (mode == OF_BOOK_GREEKS) return (const void*)book_greeks_kernel<float, true>;
-  if (mode == OF_BOOK_PRICE_FP64) return (const void*)book_greeks_kernel<double, false>;
+template <typename R, bool G>
+static const void* book_greeks_kernel_for(int kg) {
+  return kg == of::KG_TERMINAL ? (const void*)book_greeks_kernel<R, G, of::KG_TERMINAL>
+         : kg == of::KG_ASIAN  ? (const void*)book_greeks_kernel<R, G, of::KG_ASIAN>
+                               : (const void*)book_greeks_kernel<R, G, of::KG_BARRIER>;
+}
+
+static const void* book_kernel_for(int mode, int kg) {
+  if (mode == OF_BOOK_GREEKS) return book_greeks_kernel_for<float, true>(kg);
+  if (mode == OF_BOOK_PRICE_FP64) return book_greeks_kernel_for<double, false>(kg);
   return (const void*)book_kernel;
 }
 
+template <typename R, bool G>
+static void book_greeks_enqueue(of_book_plan* pl, cudaStream_t s) {
+  const of::GreekConsts<R>* gc = (const of::GreekConsts<R>*)pl->d_gc;
+  for (int kg = 0; kg < of::KG_COUNT; ++kg) {
+    if (pl->Pg[kg].n_tiles == 0) continue;
+    const dim3 grid((unsigned)pl->grid_g[kg]);
+    if (kg == of::KG_TERMINAL) book_greeks_kernel<R, G, of::KG_TERMINAL><<<grid, pl->block, 0, s>>>(pl->Pg[kg], gc);
+    else if (kg == of::KG_ASIAN) book_greeks_kernel<R, G, of::KG_ASIAN><<<grid, pl->block, 0, s>>>(pl->Pg[kg], gc);
+    else book_greeks_kernel<R, G, of::KG_BARRIER><<<grid, pl->block, 0, s>>>(pl->Pg[kg], gc);
+  }
+}
+
 static void book_enqueue(of_book_plan* pl, cudaStream_t s) {
-  cudaMemsetAsync(pl->d_counter, 0, sizeof(int), s);
+  cudaMemsetAsync(pl->d_counter, 0, of::KG_COUNT * sizeof(int), s);
   const unsigned rgrid = (unsigned)((pl->n + 7) / 8);
   if (pl->mode == OF_BOOK_GREEKS) {
-    book_greeks_kernel<float, true><<<pl->grid, pl->block, 0, s>>>(pl->P, (const of::GreekConsts<float>*)pl->d_gc);
+    book_greeks_enqueue<float, true>(pl, s);
     book_reduce_kernel<13><<<rgrid, 256, 0, s>>>(pl->d_partials, pl->d_begin, (int)pl->n, pl->d_sums);
   } else if (pl->mode == OF_BOOK_PRICE_FP64) {
-    book_greeks_kernel<double, false><<<pl->grid, pl->block, 0, s>>>(pl->P, (const of::GreekConsts<double>*)pl->d_gc);
+    book_greeks_enqueue<double, false>(pl, s);
     book_reduce_kernel<5><<<rgrid, 256, 0, s>>>(pl->d_partials, pl->d_begin, (int)pl->n, pl->d_sums);
   } else {
     book_kernel<<<pl->grid, pl->block, 0, s>>>(pl->P);
@@ -1476,6 +1500,10 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
   std::vector<size_t> order(pend.size());
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return pend[a].cost > pend[b].cost; });
+  if (pl->mode != OF_BOOK_PRICE)  // Greeks modes: the tiles of each kind group together, longest first within
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+      return of::gk_group(gcs[(size_t)pend[a].opt].kind) < of::gk_group(gcs[(size_t)pend[b].opt].kind);
+    });
   std::vector<BookTile> sorted(pend.size());
   for (size_t k = 0; k < order.size(); ++k) sorted[k] = tiles[order[k]];
   pl->n_tiles = (int64_t)sorted.size();
@@ -1485,7 +1513,7 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
       cudaMalloc(&pl->d_tiles, nt * sizeof(BookTile)) != cudaSuccess ||
       cudaMalloc(&pl->d_obs, std::max<size_t>(1, obs.size()) * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&pl->d_divs, std::max<size_t>(1, divs.size()) * sizeof(BookDiv)) != cudaSuccess ||
-      cudaMalloc(&pl->d_counter, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&pl->d_counter, of::KG_COUNT * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&pl->d_partials, nt * pl->nc * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&pl->d_begin, begin.size() * sizeof(int32_t)) != cudaSuccess ||
       cudaMalloc(&pl->d_sums, (size_t)n * pl->nc * sizeof(double)) != cudaSuccess ||
@@ -1521,9 +1549,24 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
   P.keys = of::philox_keys(cfg->seed);
   P.counter = pl->d_counter;
   P.partials = pl->d_partials;
-  const int per_sm = of_blocks_per_sm(book_kernel_for(pl->mode), pl->block, 0);
+  const int per_sm = of_blocks_per_sm(book_kernel_for(pl->mode, of::KG_TERMINAL), pl->block, 0);
   const int64_t cap = (int64_t)ctx->sm_count * per_sm;
   pl->grid = (int)std::max<int64_t>(1, std::min<int64_t>(cap, (int64_t)nt));
+  if (pl->mode != OF_BOOK_PRICE) {
+    size_t start = 0;
+    for (int kg = 0; kg < of::KG_COUNT; ++kg) {
+      size_t end = start;
+      while (end < nt && of::gk_group(gcs[(size_t)sorted[end].opt].kind) == kg) ++end;
+      BookParams& Q = pl->Pg[kg];
+      Q = P;
+      Q.tiles = pl->d_tiles + start;
+      Q.n_tiles = (int32_t)(end - start);
+      Q.counter = pl->d_counter + kg;
+      const int per = of_blocks_per_sm(book_kernel_for(pl->mode, kg), pl->block, 0);
+      pl->grid_g[kg] = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->sm_count * per, (int64_t)(end - start)));
+      start = end;
+    }
+  }
   if (pl->use_graph) {
     cudaStream_t cs = nullptr;
     if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)
