@@ -859,11 +859,17 @@ __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, floa
 }
 
 template <int DEG>
+// Launched with programmatic stream serialisation: the next date's pass may
+// be scheduled while this one finishes (its last blocks reduce the moments
+// and solve for the betas); it waits here for this grid to complete and its
+// writes (betas, cash flows, flag rows) to be visible before it reads any.
 __global__ void __launch_bounds__(kPassThreads, 4) lsm_pass_f32(const __grid_constant__ LsmBatch B, int t) {
   __shared__ __align__(128) float ring[kStages * 3 * kPathsPerBlock];
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ double red_sh[kPassThreads];
   __shared__ double mom_sh[kMaxMoments];
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (B.c[blockIdx.y].put) lsm_pass_f32_body<DEG, true>(B, t, ring, full, red_sh, mom_sh);
   else lsm_pass_f32_body<DEG, false>(B, t, ring, full, red_sh, mom_sh);
 }
@@ -1423,7 +1429,23 @@ of_status lsm_enqueue(of_ctx* ctx, LsmRun& r, const of_lsm_config* cfg, cudaStre
     if (fill >= 0.95 || bpc == B.blocks) break;
   }
   const dim3 pgrid((unsigned)pass_blocks, nc);
-  for (int t = (int)r.steps - 1; t >= 1; --t) pass<<<pgrid, kPassThreads, 0, ms>>>(B, t);
+  if (fp64) {
+    for (int t = (int)r.steps - 1; t >= 1; --t) pass<<<pgrid, kPassThreads, 0, ms>>>(B, t);
+  } else {
+    // FP32 passes: programmatic dependent launches (lsm_pass_f32 waits on its
+    // predecessor grid before reading anything it wrote)
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = pgrid;
+    lc.blockDim = dim3(kPassThreads);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = ms;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    for (int t = (int)r.steps - 1; t >= 1; --t) OF_CUDA_TRY(ctx, cudaLaunchKernelEx(&lc, pass, B, t));
+  }
   const dim3 grid((unsigned)B.blocks, nc);
   if (fp64) lsm_final<double><<<grid, kPassThreads, 0, ms>>>(B);
   else lsm_final<float><<<grid, kPassThreads, 0, ms>>>(B);
