@@ -78,6 +78,15 @@ CONFIG = {"workload": "heston_euler_strike_strip", "paths": PATHS, "steps": STEP
           "l2": "flushed between timed iterations (256 MiB write); the kernel reads no HBM input"}
 
 
+def _json_default(o):
+    """numpy scalars and arrays in a line become plain numbers and lists."""
+    if hasattr(o, "item") and getattr(o, "ndim", 0) == 0:
+        return o.item()
+    if hasattr(o, "tolist"):
+        return o.tolist()
+    raise TypeError(f"Object of type {type(o).__name__} is not JSON serializable")
+
+
 def env_int(name, default):
     try:
         return int(os.environ.get(name, default))
@@ -204,7 +213,7 @@ def run_reference(args, rank, world):
             "note": "oracle/of_oracle.c: C restatement of openferric's MonteCarloEngine::run with the Heston "
                     "Euler generator (no Rust toolchain on either machine to build the reference); OpenMP over "
                     "all host cores"}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(line, default=_json_default), flush=True)
 
 
 def fp64_strip_check(paths, strip_prices):
@@ -732,7 +741,7 @@ def run_workload(args, local_rank):
         line = leg_book_greeks(args.se_options)
     else:  # lsm
         line = leg_lsm(args.paths, args.contracts, batch_contracts=args.lsm_batch)
-    print(json.dumps(line), flush=True)
+    print(json.dumps(line, default=_json_default), flush=True)
 
 
 def main():
@@ -903,15 +912,20 @@ def main():
     if rank == 0 and world == 1 and not args.no_legs:
         # configurations 1, 3 and 5 and the target form, each with its own
         # device timing, clock samples and roofline (outside the timed region)
-        line["config1"] = leg_config1(args.steps, args.warmup, peaks, os.cpu_count() or 1)
-        line["book"] = leg_book(stream, flush, min(args.steps, 5), 3, peaks)
-        line["book_greeks_launch"] = leg_book(stream, flush, min(args.steps, 5), 3, peaks, greeks=True)
-        line["book_se"] = leg_book_se(1)
-        line["book_greeks"] = leg_book_greeks()
-        line["lsm"] = leg_lsm(PATHS, 256)
+        legs = {"config1": lambda: leg_config1(args.steps, args.warmup, peaks, os.cpu_count() or 1),
+                "book": lambda: leg_book(stream, flush, min(args.steps, 5), 3, peaks),
+                "book_greeks_launch": lambda: leg_book(stream, flush, min(args.steps, 5), 3, peaks, greeks=True),
+                "book_se": lambda: leg_book_se(1),
+                "book_greeks": lambda: leg_book_greeks(),
+                "lsm": lambda: leg_lsm(PATHS, 256)}
+        for name, leg in legs.items():
+            try:
+                line[name] = leg()
+            except Exception as exc:  # one failing leg does not take the benchmark line with it
+                line[name] = {"error": f"{type(exc).__name__}: {exc}"}
     plan.close()
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line, default=_json_default), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
