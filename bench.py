@@ -632,8 +632,12 @@ def leg_book_greeks(n=256, per_kind=8, seed=BOOK_SEED):
         zs.append(abs(r.result.price - base.price) / se if se > 0.0 else 0.0)
     # accuracy on the same draws: FP32 pathwise Greeks against central differences
     # of FP64 revaluations of the same launch (bumps 1e-4 relative)
+    # the Greeks carry no control variate: revalue the estimator they differentiate
+    # (antithetic pairs kept, the Asians' control variate dropped)
+    from openferric_b200.engines import VarianceReduction
     fixed = [BookEntry(e.instrument, e.market, int(r.result.diagnostics.get("num_paths")), e.num_steps,
-                       e.variance_reduction) for e, r in zip(sub, res_sub)]
+                       e.variance_reduction if e.variance_reduction is VarianceReduction.Antithetic
+                       else VarianceReduction.None_) for e, r in zip(sub, res_sub)]
     acc_seed = seed + 7
     g32 = price_book_greeks(fixed, acc_seed)
     worst = {}
@@ -646,7 +650,7 @@ def leg_book_greeks(n=256, per_kind=8, seed=BOOK_SEED):
             fd = (a.price - b.price) / (2e-4 * _bump_param(e, name))
             fd = -fd if name == "theta" else fd
             v = getattr(g.result.greeks, name)
-            errs.append(abs(v - fd) / max(abs(fd), 1e-300))
+            errs.append(abs(v - fd) / max(abs(fd), 1e-2))
             within += abs(v - fd) <= max(1e-3 * abs(fd), 2e-4)
         worst[name] = max(errs)
     v32, v64 = n / t32, len(sub) / t64
@@ -667,7 +671,8 @@ def leg_book_greeks(n=256, per_kind=8, seed=BOOK_SEED):
             "fp32_same_options": {"options": len(sub), "seconds": t32_sub, "options_per_s": len(sub) / t32_sub},
             "speedup": v32 / v64, "speedup_same_options": (len(sub) / t32_sub) / v64,
             "greeks_vs_crn_fd_same_draws": {
-                "max_rel_err": worst, "within_1e-3_rel_or_2e-4_abs": within, "of": 4 * len(sub),
+                "max_rel_err": worst, "rel_err_floor": "relative to max(|fd|, 0.01)",
+                "within_1e-3_rel_or_2e-4_abs": within, "of": 4 * len(sub),
                 "how": "FP32 pathwise Greeks vs central differences (bump 1e-4 relative) of FP64 revaluations of "
                        "the same launch on the same Philox draws, at each option's SE-target path count"},
             "clocks": clocks.summary()}
