@@ -33,6 +33,7 @@
 // through every step) are unbiased too.
 #pragma once
 
+#include "mills_coeffs.h"
 #include "of_device.cuh"
 
 namespace of {
@@ -82,7 +83,23 @@ struct GMath<float> {
   static constexpr float kTiny = 1e-30f;  // floor of the survival-draw uniform (above FLT_MIN)
   static constexpr float kHMin = -12.0f;  // Phi(-12) = 1.8e-33 is still a normal float
   static __device__ __forceinline__ float exp(float x) { return __expf(x); }
-  static __device__ __forceinline__ float cdf(float x) { return normcdff(x); }
+  // Phi(h) and phi(h) / Phi(h): the normal tail Phi(-|h|) = phi(|h|) M(|h|)
+  // with the fitted Mills ratio M of mills_coeffs.h (Hastings' form) and
+  // phi from an exact split of h^2, so that the tail keeps its relative
+  // precision; for h < 0 the ratio is 1 / M.
+  static __device__ __forceinline__ void cdf_ratio(float h, float& p, float& g) {
+    const float a = fabsf(h);
+    const float t = 1.0f / fmaf(OF_MILLS_C, a, 1.0f);
+    float m = kMills[OF_MILLS_DEG];
+#pragma unroll
+    for (int i = OF_MILLS_DEG - 1; i >= 0; --i) m = fmaf(m, t, kMills[i]);
+    m *= t;
+    const float a2 = a * a, a2lo = fmaf(a, a, -a2);  // a^2 = a2 + a2lo exactly
+    const float phi = 0.398942280401432677939946f * __expf(-0.5f * a2) * fmaf(-0.5f, a2lo, 1.0f);
+    const float tail = phi * m;
+    p = h < 0.0f ? tail : 1.0f - tail;
+    g = h < 0.0f ? 1.0f / m : phi / p;
+  }
   // Phi^-1(v) with q = 1 - v: the fitted single-log inverse of the Philox kernels
   static __device__ __forceinline__ float icdf2(float v, float q) { return inv_normal_vq(v, q); }
   static __device__ __forceinline__ float unif(uint32_t r) { return uniform_from_u32(r); }
@@ -98,7 +115,10 @@ struct GMath<double> {
   static constexpr double kTiny = 1e-300;
   static constexpr double kHMin = -37.0;
   static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
-  static __device__ __forceinline__ double cdf(double x) { return ::normcdf(x); }
+  static __device__ __forceinline__ void cdf_ratio(double h, double& p, double& g) {
+    p = ::normcdf(h);
+    g = 0.398942280401432677939946 * ::exp(-0.5 * h * h) / p;
+  }
   static __device__ __forceinline__ double icdf2(double v, double q) {
     return v <= 0.5 ? ::normcdfinv(v) : -::normcdfinv(q);
   }
@@ -368,29 +388,12 @@ __device__ __forceinline__ void surv_init(SurvLeg<R, G>& s, const GreekConsts<R>
 //   (ln p)' = g h' with g = phi(h) / p,
 //   z' = sgn u p' / phi(Phi^-1(u p)) = sgn (v / phi(zeta)) g h',   v = u p,
 //   y_next' = y' + alpha' + beta' z + beta z'.
-// Distance to the barrier, in step standard deviations, beyond which the FP32
-// Greeks mode takes the unconditioned step (phi(8) = 5e-15).
-constexpr float kSurvFar = 8.0f;
-
 template <typename R, bool G, bool IN>
 __device__ __forceinline__ void surv_step(SurvLeg<R, G>& s, const GreekConsts<R>& c, R u) {
   R h = c.sib * (c.bar - s.y - c.alpha);
-  if (G && __all_sync(__activemask(), h > (R)kSurvFar)) {
-    // Every path of the warp is more than kSurvFar step deviations from the
-    // barrier: p = Phi(h) rounds to 1 in FP32 and phi(h) / p < 3e-15, so the
-    // step is the unconditioned one and only the drift and volatility
-    // tangents move.
-    const R zeta = GMath<R>::icdf2(u, (R)1 - u);
-    const R z = c.sgn * zeta;
-    s.yd[1] += fma(c.beta_over_sig, z, -c.sig_dt);
-    s.yd[2] += c.dt;
-    s.yd[3] += fma(c.beta_over_2T, z, c.alpha_over_T);
-    s.y = fma(c.beta, z, s.y + c.alpha);
-    if (IN) s.ypl = fma(c.beta, zeta, s.ypl + c.alpha);
-    return;
-  }
   h = h > GMath<R>::kHMin ? h : GMath<R>::kHMin;
-  const R p = GMath<R>::cdf(h);
+  R p, g;  // Phi(h) and phi(h) / Phi(h)
+  GMath<R>::cdf_ratio(h, p, g);
   R v = u * p;
   R q = fma(-u, p, (R)1);  // 1 - u p with one rounding
   v = v > GMath<R>::kTiny ? v : GMath<R>::kTiny;
@@ -399,9 +402,7 @@ __device__ __forceinline__ void surv_step(SurvLeg<R, G>& s, const GreekConsts<R>
   const R z = c.sgn * zeta;
   if (G) {
     const R kInvSqrt2Pi = (R)0.398942280401432677939946;
-    const R phih = kInvSqrt2Pi * GMath<R>::exp((R)-0.5 * h * h);
     const R phiz = kInvSqrt2Pi * GMath<R>::exp((R)-0.5 * zeta * zeta);
-    const R g = phih / p;
     const R k = c.beta * c.sgn * (v / phiz) * g;  // d y_next / d h
     // ln S0: b' = -1
     const R h0 = c.sib * ((R)-1 - s.yd[0]);

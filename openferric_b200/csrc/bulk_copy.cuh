@@ -70,16 +70,31 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_
   return true;
 }
 
-// mbar_wait with a pause of `sleep_ns` between polls: a warp waiting on a
-// slower partner warp then leaves the issue slots to the warps doing work
-// instead of spinning on the barrier and the global timer.
+// try_wait with a suspend-time hint: the thread sleeps in the barrier until
+// the phase completes or about `hint_ns` pass, instead of polling.
+__device__ __forceinline__ bool mbar_try_wait_suspend(uint32_t bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n"
+      " .reg .pred p;\n"
+      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+      " selp.u32 %0, 1, 0, p;\n"
+      "}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
+// mbar_wait whose polls suspend the waiting warp in the barrier for up to
+// `hint_ns` each: a warp waiting on a slower partner warp then leaves the
+// issue slots to the warps doing work instead of spinning.
 __device__ __forceinline__ bool mbar_wait_backoff(uint32_t bar, uint32_t parity, uint64_t limit_ns,
-                                                  uint32_t sleep_ns) {
-  if (mbar_try_wait(bar, parity)) return true;
+                                                  uint32_t hint_ns) {
+  if (mbar_try_wait_suspend(bar, parity, hint_ns)) return true;
   const uint64_t t0 = global_ns();
   for (;;) {
-    __nanosleep(sleep_ns);
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait_suspend(bar, parity, hint_ns)) return true;
     if (global_ns() - t0 > limit_ns) return false;
   }
 }

@@ -293,9 +293,9 @@ __global__ void __launch_bounds__(256, 5) strip_kernel(const __grid_constant__ S
 //
 // Ring: per consumer kWsSlots chunks of kWsChunk Philox blocks x 32 lanes
 // (uint4), with a full and an empty mbarrier per chunk (32 arrivals each).
-// Every wait is bounded (kWsWaitNs of the global timer), pauses between
-// polls so a waiting warp leaves the issue slots to working ones, and its
-// outcome is made warp-uniform; a warp whose wait gives up sets P.status and leaves its
+// Every wait is bounded (kWsWaitNs of the global timer), suspends the warp in
+// the barrier between polls so a waiting warp leaves the issue slots to
+// working ones, and its outcome is made warp-uniform; a warp whose wait gives up sets P.status and leaves its
 // loops, so its partner's next wait gives up too and the block still reaches
 // its final reduction.
 // ---------------------------------------------------------------------------
@@ -303,7 +303,7 @@ constexpr int kWsPairs = 4;   // consumer warps 0..3, producer warps 4..7
 constexpr int kWsChunk = 4;   // Philox blocks per ring chunk
 constexpr int kWsSlots = 3;   // chunks in flight per pair
 constexpr uint64_t kWsWaitNs = 1000000000ull;
-constexpr uint32_t kWsSleepNs = 128;  // pause between polls of a ring barrier
+constexpr uint32_t kWsSleepNs = 20000;  // suspend-time hint of a ring barrier poll
 constexpr size_t kWsRingBytes = (size_t)kWsPairs * kWsSlots * kWsChunk * 32 * sizeof(uint4);
 
 // The steps of Philox block q of one sample (and its antithetic twin), as
