@@ -104,7 +104,11 @@ def min_sum_in_order(times: Sequence[float], rows_per_block: int = 256) -> float
 
 
 def geometric_asian_discrete_fixed(option_type: OptionType, s0: float, k: float, r: float, q: float, sigma: float,
-                                   observation_times: Sequence[float]) -> float:
+                                   observation_times: Sequence[float], exact_order: bool = True) -> float:
+    """exact_order=True adds the covariance sum in the reference's order
+    (bit-identical to its double loop, O(n^2)); False uses the sorted O(n log n)
+    form, equal up to summation order (about 1e-16 relative), for callers that
+    need no bit-level parity with the reference (the FP32 batched book)."""
     obs = list(observation_times)
     if not obs:
         return _vanilla(option_type, s0, k)
@@ -113,7 +117,7 @@ def geometric_asian_discrete_fixed(option_type: OptionType, s0: float, k: float,
         return math.exp(-r * maturity) * _vanilla(option_type, s0, k)
     n = float(len(obs))
     mean_t = sum(obs) / n
-    cov_sum = min_sum_in_order(obs)
+    cov_sum = min_sum_in_order(obs) if exact_order else geometric_asian_cov_sum_sorted(obs)
     var = sigma * sigma * cov_sum / (n * n)
     m = math.log(s0) + _fma(-0.5 * sigma, sigma, r - q) * mean_t
     df = math.exp(-r * maturity)

@@ -212,8 +212,12 @@ def reference_strike(instrument, spot: float) -> float:
     return instrument.strike
 
 
-def instrument_control_variate(instrument, market: Market, vol: float) -> Optional[ControlVariate]:
-    """MonteCarloInstrument::control_variate (mc_engine.rs:458-485, 546-583)."""
+def instrument_control_variate(instrument, market: Market, vol: float,
+                               exact_order: bool = True) -> Optional[ControlVariate]:
+    """MonteCarloInstrument::control_variate (mc_engine.rs:458-485, 546-583).
+    exact_order=False computes the geometric-Asian mean's covariance sum in
+    O(n log n) instead of the reference's order (see
+    geometric_asian_discrete_fixed)."""
     if market.has_discrete_dividends():
         return None
     if isinstance(instrument, VanillaOption):
@@ -230,7 +234,7 @@ def instrument_control_variate(instrument, market: Market, vol: float) -> Option
             return None
         expected_disc = geometric_asian_discrete_fixed(instrument.option_type, market.spot, instrument.strike,
                                                        market.rate, market.dividend_yield, vol,
-                                                       s.observation_times)
+                                                       s.observation_times, exact_order=exact_order)
         df = math.exp(-market.rate * instrument.expiry)
         return ControlVariate(expected_disc / df, ControlVariateKind.GeometricAsian)
     return None
