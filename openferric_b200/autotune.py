@@ -73,10 +73,11 @@ def _strip_key(device: int, generator, n_strikes: int, antithetic: bool) -> str:
 
 
 def tune_strip(generator, strikes: Sequence[float], num_paths: int, antithetic: bool = False, device: int = 0,
-               candidates: Sequence[int] = (1, 2, 3), reps: int = 5) -> Tuple[int, Dict[int, float]]:
+               candidates: Sequence[int] = (1, 2), reps: int = 5) -> Tuple[int, Dict[int, float]]:
     """Times the strip for each tile shape (1 or 2 samples in flight per
-    thread, 3 = warp-specialised producer/consumer warps); stores and returns
-    the best."""
+    thread; 3 = warp-specialised producer/consumer warps, measured slower on
+    the B200 and therefore not a default candidate); stores and returns the
+    best."""
     from .core import OptionType
     ctx = context(device)
     ks = np.ascontiguousarray(strikes, dtype=np.float64)

@@ -386,8 +386,13 @@ __device__ __forceinline__ void surv_init(SurvLeg<R, G>& s, const GreekConsts<R>
 // each parameter with b' = d bar, alpha', beta'):
 //   h' = sgn (b' - y' - alpha') / beta - h beta' / beta,
 //   (ln p)' = g h' with g = phi(h) / p,
-//   z' = sgn u p' / phi(Phi^-1(u p)) = sgn (v / phi(zeta)) g h',   v = u p,
+//   z' = sgn u p' / phi(Phi^-1(u p)) = sgn w h',   w = u phi(h) / phi(zeta),
 //   y_next' = y' + alpha' + beta' z + beta z'.
+// w = u exp((zeta - h)(zeta + h) / 2) in [0, 1] (the Mills ratio Phi / phi
+// increases and zeta <= h).  Written this way its exponent is small where a
+// draw lands at the barrier (u -> 1, zeta -> h), the steps whose w ~ 1 carries
+// the barrier's sensitivity into y', so that w keeps its relative precision
+// there; the relative error of w adds up over the steps near the barrier.
 template <typename R, bool G, bool IN>
 __device__ __forceinline__ void surv_step(SurvLeg<R, G>& s, const GreekConsts<R>& c, R u) {
   R h = c.sib * (c.bar - s.y - c.alpha);
@@ -401,9 +406,8 @@ __device__ __forceinline__ void surv_step(SurvLeg<R, G>& s, const GreekConsts<R>
   const R zeta = GMath<R>::icdf2(v, q);
   const R z = c.sgn * zeta;
   if (G) {
-    const R kInvSqrt2Pi = (R)0.398942280401432677939946;
-    const R phiz = kInvSqrt2Pi * GMath<R>::exp((R)-0.5 * zeta * zeta);
-    const R k = c.beta * c.sgn * (v / phiz) * g;  // d y_next / d h
+    const R w = u * GMath<R>::exp((R)0.5 * (zeta - h) * (zeta + h));
+    const R k = c.beta * c.sgn * w;  // d y_next / d h
     // ln S0: b' = -1
     const R h0 = c.sib * ((R)-1 - s.yd[0]);
     s.ld[0] = fma(g, h0, s.ld[0]);

@@ -10,12 +10,14 @@
 // mode one dense row of exercise flags per date (a bit per path) from which
 // the final kernel takes the first flagged date.  The final kernel derives
 // dV = +-S_tau disc^tau / S0 from V and tau.  One kernel per exercise date does
-//   exercise(t+1) with the betas of the previous pass -> discount -> FP64
+//   exercise(t+1) with the betas of the previous pass -> discount ->
 //   in-the-money basis moments at t -> block partials,
 // and the last block of each contract (last-block-done counter, no spin)
 // reduces the partials in a fixed order and solves the normal equations:
 // degree 2 = the reference's {1,S,S^2} with partially pivoted LU (nalgebra),
-// degree 3 = {1,x,x^2,x^3}, x = S/K, with Cholesky.
+// degree 3 = {1,x,x^2,x^3} with Cholesky, x = S/K in the FP64 mode and
+// x = S/K - 1 (centred at the strike) in the FP32 mode, whose cubic moments
+// are FP32 sums carried into FP64 per warp.
 //
 // FP64 reference mode reproduces the reference's draws: ONE xoshiro256++
 // stream seeded with `seed` feeds all paths in path-major order
@@ -38,6 +40,7 @@
 #include "of_internal.h"
 #include "bulk_copy.cuh"
 #include "path_fp32.cuh"
+#include "f32x2.cuh"
 
 namespace {
 
@@ -346,6 +349,41 @@ __global__ void __launch_bounds__(256, DYN == DYN_GBM ? 4 : 2) lsm_gen_philox(co
 #pragma unroll
       for (int q = 0; q < 4; ++q)
         r[q] = of::philox4x32_10(make_uint4(blk, (uint32_t)(p0 + q), cid, kLsmStreamTag), B.keys);
+      if (DYN == DYN_GBM) {
+        // paths (0,1) and (2,3) in packed pairs: each half is the scalar
+        // loop's arithmetic below, bit for bit
+#pragma unroll
+        for (int k = 0; k < kStepsPerBlock; k += 2) {
+          float2 za[2], zb[2];  // the normals of steps tb+k and tb+k+1
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const uint32_t* w0 = &r[2 * h].x;
+            const uint32_t* w1 = &r[2 * h + 1].x;
+            of::normal_pairs_scaled2_from_u32(w0[k], w0[k + 1], w1[k], w1[k + 1], of::kBoxMullerK2, za[h], zb[h]);
+          }
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int t = tb + k + e;
+            if (t >= B.steps) break;
+            float4 out;
+            float* o = &out.x;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              float2 y = make_float2(L[2 * h].y, L[2 * h + 1].y);
+              y = of::fma2(of::splat2(C.fstep_vol), e ? zb[h] : za[h], of::add2(y, of::splat2(C.fdrift)));
+              L[2 * h].y = y.x;
+              L[2 * h + 1].y = y.y;
+              const float2 sp = of::mul2(of::splat2(fspot), make_float2(__expf(y.x), __expf(y.y)));
+              s[2 * h] = sp.x;
+              s[2 * h + 1] = sp.y;
+              o[2 * h] = in[2 * h] ? sp.x : pad;
+              o[2 * h + 1] = in[2 * h + 1] ? sp.y : pad;
+            }
+            __stcs(reinterpret_cast<float4*>(S + (size_t)t * B.npad), out);
+          }
+        }
+        continue;
+      }
       float2 zp[4];  // Box-Muller pair of words (0,1) or (2,3) of the counter block
 #pragma unroll
       for (int k = 0; k < kStepsPerBlock; ++k) {
@@ -399,9 +437,12 @@ __global__ void __launch_bounds__(256, DYN == DYN_GBM ? 4 : 2) lsm_gen_philox(co
 }
 
 // Continuation value of the fitted basis, FP64 (longstaff_schwartz.rs:597).
-__device__ __forceinline__ double continuation(int degree, const double* b, double s, double inv_k) {
+// Degree 3: the cubic in x = S/K_t - shift (shift 0 in the FP64 mode, 1 in
+// the FP32 mode's centred basis).
+__device__ __forceinline__ double continuation(int degree, const double* b, double s, double inv_k,
+                                               double shift = 0.0) {
   if (degree == 2) return b[0] + b[1] * s + b[2] * s * s;
-  const double x = s * inv_k;
+  const double x = s * inv_k - shift;
   return b[0] + x * (b[1] + x * (b[2] + x * b[3]));
 }
 
@@ -736,6 +777,82 @@ __device__ __forceinline__ unsigned f32_quad(const F32Pass& P, float4& v4, const
   return exm;
 }
 
+// The cubic-basis quad with packed pair arithmetic (paths 0,1 and 2,3 of the
+// quad share each instruction).  The FP32 mode's cubic basis is 1, x, x^2, x^3
+// in x = S/K_t - 1 (one fma, exact near the money): the same span as the
+// monomials of S/K_t, but centred at the strike, where the in-the-money paths
+// lie, so that the normal equations are some 10-100x better conditioned and
+// moments with FP32 rounding fit the same continuation to about 1e-6 (with
+// monomials of S/K_t, FP32 moments moved fitted values by up to 0.2 on
+// near-expiry dates, whose in-the-money spots span a narrow range).
+// The basis moments of the in-the-money paths (x as above, y = discounted cash
+// flow; out-of-the-money paths enter as x = y = 0 and add nothing) go into FP32
+// pair accumulators instead of FP64 registers: acc[0..5] = sum x^1..x^6,
+// acc[6] = sum y, acc[7..9] = sum y x^1..x^3; the count is n_itm.  Every kFlushChunks chunks the pass
+// adds each accumulator's two halves, sums them over the warp in FP32 and adds
+// the warp's total to the warp's FP64 moments in shared memory; so an FP32 sum
+// covers at most 2 kFlushChunks paths of one lane half and 32 lanes, whatever
+// the path count, and the FP64 sums carry the rest.  (The rounding of these
+// short FP32 sums, about 1e-6 relative at worst, moves the fitted betas far
+// less than the FP32 rounding of the betas themselves does.)
+template <bool PUT>
+__device__ __forceinline__ unsigned f32_quad3_packed(const F32Pass& P, float4& v4, const float4& a4, const float4& p4,
+                                                     float2* acc, unsigned& n_ex, unsigned& n_itm, float& ext) {
+  using of::add2;
+  using of::fma2;
+  using of::mul2;
+  using of::splat2;
+  using of::sub2;
+  float2 v[2] = {make_float2(v4.x, v4.y), make_float2(v4.z, v4.w)};
+  const float2 s1[2] = {make_float2(a4.x, a4.y), make_float2(a4.z, a4.w)};
+  const float2 s0[2] = {make_float2(p4.x, p4.y), make_float2(p4.z, p4.w)};
+  unsigned exm = 0;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    if (P.have_beta) {
+      const float2 ex = PUT ? sub2(splat2(P.k1), s1[h]) : sub2(s1[h], splat2(P.k1));
+      const float2 x1 = fma2(s1[h], splat2(P.ik1), splat2(-1.0f));
+      const float2 cont = fma2(x1, fma2(x1, fma2(x1, splat2(P.b3), splat2(P.b2)), splat2(P.b1)), splat2(P.b0));
+      if (ex.x > 0.0f && ex.x > cont.x) {
+        v[h].x = ex.x;
+        ++n_ex;
+        ext = PUT ? fmaxf(ext, s1[h].x) : fminf(ext, s1[h].x);
+        exm |= 1u << (2 * h);
+      }
+      if (ex.y > 0.0f && ex.y > cont.y) {
+        v[h].y = ex.y;
+        ++n_ex;
+        ext = PUT ? fmaxf(ext, s1[h].y) : fminf(ext, s1[h].y);
+        exm |= 2u << (2 * h);
+      }
+    }
+    v[h] = fma2(v[h], splat2(P.dh), mul2(v[h], splat2(P.dl)));
+    if (P.ex_now) {
+      const bool ia = (PUT ? P.k0 - s0[h].x : s0[h].x - P.k0) > 0.0f;
+      const bool ib = (PUT ? P.k0 - s0[h].y : s0[h].y - P.k0) > 0.0f;
+      n_itm += (unsigned)ia + (unsigned)ib;
+      const float2 x0 = fma2(s0[h], splat2(P.ik0), splat2(-1.0f));
+      const float2 x = make_float2(ia ? x0.x : 0.0f, ib ? x0.y : 0.0f);
+      const float2 y = make_float2(ia ? v[h].x : 0.0f, ib ? v[h].y : 0.0f);
+      const float2 x2 = mul2(x, x), x3 = mul2(x2, x);
+      acc[0] = add2(acc[0], x);
+      acc[1] = add2(acc[1], x2);
+      acc[2] = add2(acc[2], x3);
+      acc[3] = fma2(x2, x2, acc[3]);
+      acc[4] = fma2(x2, x3, acc[4]);
+      acc[5] = fma2(x3, x3, acc[5]);
+      acc[6] = add2(acc[6], y);
+      acc[7] = fma2(y, x, acc[7]);
+      acc[8] = fma2(y, x2, acc[8]);
+      acc[9] = fma2(y, x3, acc[9]);
+    }
+  }
+  v4 = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+  return exm;
+}
+
+constexpr int kFlushChunks = 32;  // FP32 moment accumulators flushed into FP64 this often
+
 constexpr int kStages = 3;                                     // ring depth of the FP32 pass
 constexpr uint32_t kChunkBytes = kPathsPerBlock * sizeof(float);  // one array's share of a chunk
 constexpr uint64_t kWaitLimitNs = 1000000000ull;               // a bulk copy lands in microseconds
@@ -754,7 +871,7 @@ constexpr uint64_t kWaitLimitNs = 1000000000ull;               // a bulk copy la
 // returned block no longer owns.
 template <int DEG, bool PUT>
 __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, float* ring, uint64_t* full,
-                                                  double* red_sh, double* mom_sh) {
+                                                  double* red_sh, double* mom_sh, double* warp_mom) {
   constexpr int nm = DEG == 2 ? 8 : 11;
   const int c = blockIdx.y;
   const float* S = (const float*)B.S + (size_t)c * B.steps * B.npad;
@@ -809,6 +926,23 @@ __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, floa
   double mom[nm];
 #pragma unroll
   for (int k = 0; k < nm; ++k) mom[k] = 0.0;
+  float2 acc[10];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) acc[k] = make_float2(0.f, 0.f);
+  // lane 0 of each warp owns the warp's 10 FP64 moments in shared memory
+  double* wm = warp_mom + (threadIdx.x >> 5) * 10;
+  if (DEG == 3 && (threadIdx.x & 31u) == 0)
+    for (int k = 0; k < 10; ++k) wm[k] = 0.0;
+  auto flush = [&]() {  // called by all lanes of the warp
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+      float a = acc[k].x + acc[k].y;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(of::kFullMask, a, o);
+      if ((threadIdx.x & 31u) == 0) wm[k] += (double)a;
+      acc[k] = make_float2(0.f, 0.f);
+    }
+  };
   const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
   int i = 0;
   for (; i < n_chunks; ++i) {
@@ -822,7 +956,13 @@ __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, floa
     const float4 p4 = P.ex_now ? reinterpret_cast<const float4*>(src + kPathsPerBlock)[threadIdx.x] : zero;
     float4 v4 = reinterpret_cast<const float4*>(src + 2 * kPathsPerBlock)[threadIdx.x];
     const int64_t q = ((int64_t)blockIdx.x + (int64_t)i * gridDim.x) * kPassThreads + threadIdx.x;
-    const unsigned exm = f32_quad<DEG, PUT>(P, v4, a4, p4, mom, n_ex, n_itm, ext);
+    unsigned exm;
+    if (DEG == 3) {
+      exm = f32_quad3_packed<PUT>(P, v4, a4, p4, acc, n_ex, n_itm, ext);
+      if (P.ex_now && (i % kFlushChunks) == kFlushChunks - 1) flush();
+    } else {
+      exm = f32_quad<DEG, PUT>(P, v4, a4, p4, mom, n_ex, n_itm, ext);
+    }
     reinterpret_cast<float4*>(gV)[q] = v4;
     if (P.want_delta) {
       // word 4g+e of the date's flag row: bit L = path 4(32g+L)+e exercised,
@@ -854,6 +994,11 @@ __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, floa
   }
   if (B.track && P.have_beta) record_exercise(B, c, t + 1, PUT, n_ex, (double)ext);  // block-uniform condition
   if (!P.ex_now) return;
+  if (DEG == 3) {
+    flush();
+#pragma unroll
+    for (int k = 0; k < 10; ++k) mom[k + 1] = (threadIdx.x & 31u) == 0 ? wm[k] : 0.0;
+  }
   mom[0] = (double)n_itm;
   block_moments<nm>(B, c, t, mom, red_sh, mom_sh);
 }
@@ -868,10 +1013,11 @@ __global__ void __launch_bounds__(kPassThreads, 4) lsm_pass_f32(const __grid_con
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ double red_sh[kPassThreads];
   __shared__ double mom_sh[kMaxMoments];
+  __shared__ double warp_mom[kPassThreads / 32 * 10];
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  if (B.c[blockIdx.y].put) lsm_pass_f32_body<DEG, true>(B, t, ring, full, red_sh, mom_sh);
-  else lsm_pass_f32_body<DEG, false>(B, t, ring, full, red_sh, mom_sh);
+  if (B.c[blockIdx.y].put) lsm_pass_f32_body<DEG, true>(B, t, ring, full, red_sh, mom_sh, warp_mom);
+  else lsm_pass_f32_body<DEG, false>(B, t, ring, full, red_sh, mom_sh, warp_mom);
 }
 
 // 32 x 32 bit transpose across a warp: lane i holds row i on entry and column
@@ -946,7 +1092,7 @@ __global__ void __launch_bounds__(kPassThreads) lsm_final(LsmBatch B) {
   auto path_final = [&](double v, double s1, int tp) {
     if (have_beta) {
       const double ex = intrinsic_v<double>(C.put, s1, st1.strike);
-      if (ex > 0.0 && ex > continuation(B.degree, beta, s1, st1.inv_strike)) {
+      if (ex > 0.0 && ex > continuation(B.degree, beta, s1, st1.inv_strike, sizeof(T) == 4 ? 1.0 : 0.0)) {
         v = ex;
         tp = 1;
         ++n_ex;

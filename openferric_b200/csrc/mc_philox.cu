@@ -160,6 +160,29 @@ __device__ __forceinline__ void simulate_terminal_n(const StepConsts& c, int32_t
       ya[l] = fmaf(c.diff, w[l], base);
       yb[l] = fmaf(-c.diff, w[l], base);
     }
+  } else if (MODEL == OF_MODEL_HESTON_EULER && ILP == 2 && !ANTI) {
+    // the two samples' legs in packed pairs: each half is the one-sample
+    // loop's arithmetic, bit for bit (antithetic pairs keep the scalar loop,
+    // whose four legs fit the register budget without the pair alignment)
+    of::LegState2 a{make_float2(0.0f, 0.0f), make_float2(c.v0, c.v0)};
+    const int32_t pairs = steps >> 1;
+    float2 w1, w2;
+    for (int32_t q = 0; q < pairs; ++q) {
+      const uint4 r0 = of::philox4x32_10(make_uint4((uint32_t)q, lo[0], hi[0], stream), K);
+      const uint4 r1 = of::philox4x32_10(make_uint4((uint32_t)q, lo[1], hi[1], stream), K);
+      of::normal_pairs_scaled2_from_u32(r0.x, r0.y, r1.x, r1.y, c.bm_k2, w1, w2);
+      of::heston_euler_step2(a, c, w1, w2);
+      of::normal_pairs_scaled2_from_u32(r0.z, r0.w, r1.z, r1.w, c.bm_k2, w1, w2);
+      of::heston_euler_step2(a, c, w1, w2);
+    }
+    if (steps & 1) {
+      const uint4 r0 = of::philox4x32_10(make_uint4((uint32_t)pairs, lo[0], hi[0], stream), K);
+      const uint4 r1 = of::philox4x32_10(make_uint4((uint32_t)pairs, lo[1], hi[1], stream), K);
+      of::normal_pairs_scaled2_from_u32(r0.x, r0.y, r1.x, r1.y, c.bm_k2, w1, w2);
+      of::heston_euler_step2(a, c, w1, w2);
+    }
+    ya[0] = a.y.x;  // yb stays 0: there is no antithetic leg
+    ya[1] = a.y.y;
   } else if (MODEL == OF_MODEL_HESTON_EULER) {
     LegState a[ILP], b[ILP];
 #pragma unroll

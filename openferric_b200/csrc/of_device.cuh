@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "f32x2.cuh"
 #include "invnorm_coeffs.h"
 
 namespace of {
@@ -215,6 +216,26 @@ __device__ __forceinline__ float2 normal_pair_scaled_from_u32(uint32_t a, uint32
 
 __device__ __forceinline__ float2 normal_pair_from_u32(uint32_t a, uint32_t b) {
   return normal_pair_scaled_from_u32(a, b, kBoxMullerK2);
+}
+
+// normal_pair_scaled_from_u32 of two samples' draw pairs (a0, b0) and (a1, b1)
+// with the FP32 arithmetic in packed pairs: w1 = (z1 of sample 0, z1 of
+// sample 1), w2 likewise for z2; each half is bit-identical to the scalar
+// transform (the same operations in the same order).
+__device__ __forceinline__ void normal_pairs_scaled2_from_u32(uint32_t a0, uint32_t b0, uint32_t a1, uint32_t b1,
+                                                              float k2, float2& w1, float2& w2) {
+  const float2 u1 = sub2(make_float2(__uint_as_float(0x3F800000u | (a0 >> 9)), __uint_as_float(0x3F800000u | (a1 >> 9))),
+                         splat2(0.999999940395355224609375f));
+  const float2 rr = mul2(splat2(k2), make_float2(__log2f(u1.x), __log2f(u1.y)));
+  const float2 r = make_float2(sqrtf(rr.x), sqrtf(rr.y));
+  const float2 ang = fma2(splat2(6.28318530717959f),
+                          make_float2(__uint_as_float(0x3F800000u | (b0 >> 9)), __uint_as_float(0x3F800000u | (b1 >> 9))),
+                          splat2(-9.42477796076938f));
+  float s0, c0, s1, c1;
+  __sincosf(ang.x, &s0, &c0);
+  __sincosf(ang.y, &s1, &c1);
+  w1 = mul2(r, make_float2(c0, c1));
+  w2 = mul2(r, make_float2(s0, s1));
 }
 
 // ---------------------------------------------------------------------------

@@ -4,6 +4,7 @@
 // of each step is relative to |y| (~0.1-1) instead of |ln S| (~4.6).
 #pragma once
 
+#include "f32x2.cuh"
 #include "of_device.cuh"
 
 namespace of {
@@ -37,6 +38,22 @@ __device__ __forceinline__ void heston_euler_step(LegState& L, const StepConsts&
   const float vn = fmaf(c.xi * sq, w1, fmaf(c.one_m_kdt, L.v, c.kdt_theta));
   L.v = fmaxf(vn, 0.0f);
   L.y = fmaxf(y, c.y_floor);
+}
+
+// Two samples' Heston Euler legs in one packed pair each (.x = the first
+// sample, .y = the second): heston_euler_step's operations in its order, two
+// samples per instruction, so each half is bit-identical to the scalar step.
+struct LegState2 {
+  float2 y, v;
+};
+
+__device__ __forceinline__ void heston_euler_step2(LegState2& L, const StepConsts& c, float2 w1, float2 w2) {
+  const float2 sq = make_float2(sqrtf(L.v.x), sqrtf(L.v.y));
+  const float2 ws = fma2(splat2(c.rho), w1, mul2(splat2(c.rho_c), w2));
+  const float2 y = fma2(sq, ws, fma2(splat2(-c.half_dt), L.v, add2(L.y, splat2(c.mudt))));
+  const float2 vn = fma2(mul2(splat2(c.xi), sq), w1, fma2(splat2(c.one_m_kdt), L.v, splat2(c.kdt_theta)));
+  L.v = make_float2(fmaxf(vn.x, 0.0f), fmaxf(vn.y, 0.0f));
+  L.y = make_float2(fmaxf(y.x, c.y_floor), fmaxf(y.y, c.y_floor));
 }
 
 // Andersen QE step.  uv: uniform for the variance, zv = Phi^-1(uv) is
