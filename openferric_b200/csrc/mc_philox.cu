@@ -946,9 +946,24 @@ __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, const 
 // and flags resolved at compile time instead of tested every step.  Whole
 // Philox counter blocks (four steps) run without a bounds test; the last,
 // partial block follows.
+template <int KIND, bool TWIN>
+__device__ __forceinline__ void book_gbm_legs2(const BookOpt& o, uint64_t i0, uint64_t i1, const of::PhiloxKeys& K,
+                                               float2& y, PathObs& oa, PathObs& ob);
+
 template <int KIND, bool ANTI>
 __device__ __forceinline__ void book_sample_gbm(const BookOpt& o, uint64_t i, const of::PhiloxKeys& K, float& x,
                                                 float& cvy) {
+  if (ANTI) {  // the sample and its antithetic twin as the two halves of packed pairs
+    float2 y;
+    PathObs oa, ob;
+    book_gbm_legs2<KIND, true>(o, i, i, K, y, oa, ob);
+    float xb, yb2;
+    book_payoff(o, oa, y.x, x, cvy);
+    book_payoff(o, ob, y.y, xb, yb2);
+    x = 0.5f * (x + xb);
+    cvy = 0.5f * (cvy + yb2);
+    return;
+  }
   const float drift = o.c.drift, diff = o.c.diff;
   // barrier test as sg*y >= sg*b: sg = +1 for an up barrier, -1 for a down one
   const float sg = (o.flags & BF_UP) ? 1.0f : -1.0f, sgb = sg * o.barrier_y;
@@ -998,6 +1013,81 @@ __device__ __forceinline__ void book_sample_gbm(const BookOpt& o, uint64_t i, co
   }
 }
 
+// Two legs of the specialised GBM loop in packed pairs (.x and .y), each half
+// the arithmetic of book_sample_gbm bit for bit.  TWIN: the legs are sample
+// i0 and its antithetic twin (one Philox stream, normals z and -z); otherwise
+// the independent samples i0 and i1 (two streams, Box-Muller of both in packed
+// pairs).
+template <int KIND, bool TWIN>
+__device__ __forceinline__ void book_gbm_legs2(const BookOpt& o, uint64_t i0, uint64_t i1, const of::PhiloxKeys& K,
+                                               float2& y, PathObs& oa, PathObs& ob) {
+  using of::add2;
+  using of::fma2;
+  using of::mul2;
+  using of::splat2;
+  using of::sub2;
+  const float2 drift = splat2(o.c.drift);
+  const float2 diff = TWIN ? make_float2(o.c.diff, -o.c.diff) : splat2(o.c.diff);
+  const float sg = (o.flags & BF_UP) ? 1.0f : -1.0f, sgb = sg * o.barrier_y;
+  y = make_float2(0.0f, 0.0f);
+  float2 as = make_float2(0.0f, 0.0f), ac = make_float2(0.0f, 0.0f);  // Kahan sums of the daily fixings
+  bool ha = false, hb = false;
+  if (KIND == BK_BARRIER) ha = hb = 0.0f >= sgb;  // the scan includes path[0]
+  auto step = [&](float2 z) {
+    y = fma2(diff, z, add2(y, drift));
+    if (KIND == BK_BARRIER) {
+      const float2 t = mul2(splat2(sg), y);
+      ha |= t.x >= sgb;
+      hb |= t.y >= sgb;
+    } else if (KIND == BK_ASIAN_DAILY) {
+      const float2 yk = sub2(make_float2(__expf(y.x), __expf(y.y)), ac);
+      const float2 t = add2(as, yk);
+      ac = sub2(sub2(t, as), yk);
+      as = t;
+    }
+  };
+  const uint32_t lo0 = (uint32_t)i0, hi0 = (uint32_t)(i0 >> 32), lo1 = (uint32_t)i1, hi1 = (uint32_t)(i1 >> 32);
+  for (int32_t j = 0; j < o.steps; j += 4) {
+    const uint4 r0 = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo0, hi0, o.stream), K);
+    float2 w1, w2, w3, w4;
+    if (TWIN) {  // w1 = (z_j, z_j+2), w2 = (z_j+1, z_j+3)
+      of::normal_pairs_scaled2_from_u32(r0.x, r0.y, r0.z, r0.w, of::kBoxMullerK2, w1, w2);
+      w3 = splat2(w1.y);
+      w4 = splat2(w2.y);
+      w1 = splat2(w1.x);
+      w2 = splat2(w2.x);
+    } else {  // wk = step j+k-1 of (i0, i1)
+      const uint4 r1 = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo1, hi1, o.stream), K);
+      of::normal_pairs_scaled2_from_u32(r0.x, r0.y, r1.x, r1.y, of::kBoxMullerK2, w1, w2);
+      of::normal_pairs_scaled2_from_u32(r0.z, r0.w, r1.z, r1.w, of::kBoxMullerK2, w3, w4);
+    }
+    if (j + 4 <= o.steps) {
+      step(w1);
+      step(w2);
+      step(w3);
+      step(w4);
+    } else {
+      step(w1);
+      if (j + 1 < o.steps) step(w2);
+      if (j + 2 < o.steps) step(w3);
+    }
+  }
+  oa = PathObs{as.x, ac.x, 0.0f, ha};
+  ob = PathObs{as.y, ac.y, 0.0f, hb};
+}
+
+// book_sample_gbm<KIND, false> of two samples in one packed loop.
+template <int KIND>
+__device__ __forceinline__ void book_sample_gbm_pair(const BookOpt& o, uint64_t i0, uint64_t i1,
+                                                     const of::PhiloxKeys& K, float& x0, float& cv0, float& x1,
+                                                     float& cv1) {
+  float2 y;
+  PathObs oa, ob;
+  book_gbm_legs2<KIND, false>(o, i0, i1, K, y, oa, ob);
+  book_payoff(o, oa, y.x, x0, cv0);
+  book_payoff(o, ob, y.y, x1, cv1);
+}
+
 // One sample of option o: the specialised GBM loop when the option has one,
 // the general loop otherwise.
 __device__ __forceinline__ void book_dispatch(const BookOpt& o, uint64_t i, const BookParams& P, float& x, float& y) {
@@ -1041,17 +1131,34 @@ __global__ void __launch_bounds__(256, 3) book_kernel(const __grid_constant__ Bo
     const BookTile tile = P.tiles[t];
     const BookOpt o = P.opts[tile.opt];
     of::Kahan32 acc[5];
-    for (int k = 0; k < P.ppt; ++k) {
-      const int local = k * blockDim.x + threadIdx.x;
-      if (local >= tile.count) break;
-      const uint64_t i = (uint64_t)(tile.first + local);
-      float x, y;
-      book_dispatch(o, i, P, x, y);
+    auto add = [&](float x, float y) {
       acc[0].add(x);
       acc[1].add(x * x);
       acc[2].add(y);
       acc[3].add(x * y);
       acc[4].add(y * y);
+    };
+    // specialised GBM kinds without antithetic twins run two samples at a
+    // time in packed pairs; the sums take them in the same order
+    const bool pairs = o.kind != BK_GENERIC && !(o.flags & BF_ANTI);
+    for (int k = 0; k < P.ppt; ++k) {
+      const int local = k * blockDim.x + threadIdx.x;
+      if (local >= tile.count) break;
+      const uint64_t i = (uint64_t)(tile.first + local);
+      float x, y;
+      if (pairs && k + 1 < P.ppt && local + (int)blockDim.x < tile.count) {
+        const uint64_t i1 = i + blockDim.x;
+        float x1, y1;
+        if (o.kind == BK_TERMINAL) book_sample_gbm_pair<BK_TERMINAL>(o, i, i1, P.keys, x, y, x1, y1);
+        else if (o.kind == BK_BARRIER) book_sample_gbm_pair<BK_BARRIER>(o, i, i1, P.keys, x, y, x1, y1);
+        else book_sample_gbm_pair<BK_ASIAN_DAILY>(o, i, i1, P.keys, x, y, x1, y1);
+        add(x, y);
+        add(x1, y1);
+        ++k;
+        continue;
+      }
+      book_dispatch(o, i, P, x, y);
+      add(x, y);
     }
     double v[5];
 #pragma unroll
