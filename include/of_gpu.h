@@ -134,7 +134,16 @@ typedef struct of_mc_config {
    * the normals on the device.  FP64_REFERENCE mode only. */
   const double* injected_normals;
   int64_t n_injected;
+  /* The reproducible stream kind of FP64_REFERENCE mode (FastRngKind,
+   * src/math/fast_rng.rs:20-27): OF_RNG_XOSHIRO256PP (the default) or
+   * OF_RNG_PCG64 (PCG XSL-RR 128/64, fast_rng.rs:86-128).  Each sample's
+   * stream is seeded with stream_seed(seed, i) either way.  FP32 Philox mode
+   * takes OF_RNG_XOSHIRO256PP only (its draws are Philox's). */
+  int32_t rng_kind;
+  int32_t reserved0;
 } of_mc_config;
+
+enum { OF_RNG_XOSHIRO256PP = 0, OF_RNG_PCG64 = 1 };
 
 typedef struct of_mc_result {
   double price;

@@ -85,7 +85,12 @@ class OfMcConfig(C.Structure):
         ("discount_factor", C.c_double),
         ("injected_normals", C.POINTER(C.c_double)),
         ("n_injected", C.c_int64),
+        ("rng_kind", C.c_int32),
+        ("reserved0", C.c_int32),
     ]
+
+
+OF_RNG_XOSHIRO256PP, OF_RNG_PCG64 = 0, 1
 
 
 class OfBookEntry(C.Structure):

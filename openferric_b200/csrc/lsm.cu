@@ -159,6 +159,7 @@ struct LsmC {
   const float* lv_vf;
   float fdrift, fstep_vol, fspot, fmudt, fsqrt_dt, fdt, fy_floor;
   of::StepConsts hc;         // FP32 Heston Euler constants
+  uint32_t cid;              // FP32 mode: the contract's Philox stream, its index in the caller's list
 };
 
 // Per simulation step: the strike of an exercise date there (the terminal
@@ -325,7 +326,7 @@ __global__ void __launch_bounds__(256, DYN == DYN_GBM ? 4 : 2) lsm_gen_philox(co
   const int64_t p0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
   const bool live = p0 < B.npad;  // the grid's last block may reach past the padded path count
   const LsmStep* st = B.st + (size_t)c * (B.steps + 1);
-  const uint32_t cid = B.contract_base + (uint32_t)c;
+  const uint32_t cid = C.cid;
   const bool put = C.put != 0;
   const float fspot = C.fspot;
   int itm = 0;
@@ -795,7 +796,7 @@ __device__ __forceinline__ unsigned f32_quad(const F32Pass& P, float4& v4, const
 // the path count, and the FP64 sums carry the rest.  (The rounding of these
 // short FP32 sums, about 1e-6 relative at worst, moves the fitted betas far
 // less than the FP32 rounding of the betas themselves does.)
-template <bool PUT>
+template <bool PUT, bool TRACK>
 __device__ __forceinline__ unsigned f32_quad3_packed(const F32Pass& P, float4& v4, const float4& a4, const float4& p4,
                                                      float2* acc, unsigned& n_ex, unsigned& n_itm, float& ext) {
   using of::add2;
@@ -815,14 +816,18 @@ __device__ __forceinline__ unsigned f32_quad3_packed(const F32Pass& P, float4& v
       const float2 cont = fma2(x1, fma2(x1, fma2(x1, splat2(P.b3), splat2(P.b2)), splat2(P.b1)), splat2(P.b0));
       if (ex.x > 0.0f && ex.x > cont.x) {
         v[h].x = ex.x;
-        ++n_ex;
-        ext = PUT ? fmaxf(ext, s1[h].x) : fminf(ext, s1[h].x);
+        if (TRACK) {  // the Bermudan boundary statistics
+          ++n_ex;
+          ext = PUT ? fmaxf(ext, s1[h].x) : fminf(ext, s1[h].x);
+        }
         exm |= 1u << (2 * h);
       }
       if (ex.y > 0.0f && ex.y > cont.y) {
         v[h].y = ex.y;
-        ++n_ex;
-        ext = PUT ? fmaxf(ext, s1[h].y) : fminf(ext, s1[h].y);
+        if (TRACK) {
+          ++n_ex;
+          ext = PUT ? fmaxf(ext, s1[h].y) : fminf(ext, s1[h].y);
+        }
         exm |= 2u << (2 * h);
       }
     }
@@ -869,7 +874,7 @@ constexpr uint64_t kWaitLimitNs = 1000000000ull;               // a bulk copy la
 // that gives up as well sets a second status bit: the host then marks the
 // context unusable, since copies may still land in shared memory that the
 // returned block no longer owns.
-template <int DEG, bool PUT>
+template <int DEG, bool PUT, bool TRACK>
 __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, float* ring, uint64_t* full,
                                                   double* red_sh, double* mom_sh, double* warp_mom) {
   constexpr int nm = DEG == 2 ? 8 : 11;
@@ -958,7 +963,7 @@ __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, floa
     const int64_t q = ((int64_t)blockIdx.x + (int64_t)i * gridDim.x) * kPassThreads + threadIdx.x;
     unsigned exm;
     if (DEG == 3) {
-      exm = f32_quad3_packed<PUT>(P, v4, a4, p4, acc, n_ex, n_itm, ext);
+      exm = f32_quad3_packed<PUT, TRACK>(P, v4, a4, p4, acc, n_ex, n_itm, ext);
       if (P.ex_now && (i % kFlushChunks) == kFlushChunks - 1) flush();
     } else {
       exm = f32_quad<DEG, PUT>(P, v4, a4, p4, mom, n_ex, n_itm, ext);
@@ -992,7 +997,7 @@ __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, floa
     __syncthreads();
     return;
   }
-  if (B.track && P.have_beta) record_exercise(B, c, t + 1, PUT, n_ex, (double)ext);  // block-uniform condition
+  if (TRACK && P.have_beta) record_exercise(B, c, t + 1, PUT, n_ex, (double)ext);  // block-uniform condition
   if (!P.ex_now) return;
   if (DEG == 3) {
     flush();
@@ -1016,8 +1021,14 @@ __global__ void __launch_bounds__(kPassThreads, 4) lsm_pass_f32(const __grid_con
   __shared__ double warp_mom[kPassThreads / 32 * 10];
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  if (B.c[blockIdx.y].put) lsm_pass_f32_body<DEG, true>(B, t, ring, full, red_sh, mom_sh, warp_mom);
-  else lsm_pass_f32_body<DEG, false>(B, t, ring, full, red_sh, mom_sh, warp_mom);
+  const bool put = B.c[blockIdx.y].put;
+  if (B.track) {
+    if (put) lsm_pass_f32_body<DEG, true, true>(B, t, ring, full, red_sh, mom_sh, warp_mom);
+    else lsm_pass_f32_body<DEG, false, true>(B, t, ring, full, red_sh, mom_sh, warp_mom);
+  } else {
+    if (put) lsm_pass_f32_body<DEG, true, false>(B, t, ring, full, red_sh, mom_sh, warp_mom);
+    else lsm_pass_f32_body<DEG, false, false>(B, t, ring, full, red_sh, mom_sh, warp_mom);
+  }
 }
 
 // 32 x 32 bit transpose across a warp: lane i holds row i on entry and column
@@ -1467,6 +1478,9 @@ of_status lsm_bind(of_ctx* ctx, LsmRun& r, const of_lsm_config* cfg, void* dS, v
   for (int c = 0; c < nc; ++c) {
     const LsmHost& h = r.hs[(size_t)c];
     LsmC C = h.C;
+    // the stream follows the contract, not its batch slot, so that the draws
+    // do not depend on how the contracts were batched
+    C.cid = r.index.empty() ? r.contract_base + (uint32_t)c : (uint32_t)r.index[(size_t)c];
     std::copy(h.can.begin(), h.can.end(), can + (size_t)c * (r.steps + 1));
     std::copy(h.st.begin(), h.st.end(), st + (size_t)c * (r.steps + 1));
     double* dp = dpow + (size_t)c * (r.steps + 1);
@@ -1744,7 +1758,21 @@ extern "C" of_status of_lsm_price(of_ctx* ctx, const of_lsm_contract* ks, int64_
     const int64_t steps = k0.num_steps;
     const size_t per = (size_t)steps * npad * esz;
     size_t cap = std::max<size_t>(1, budget / per);
-    if (cfg->batch_contracts > 0) cap = std::min<size_t>(cap, (size_t)cfg->batch_contracts);
+    if (cfg->batch_contracts > 0) {
+      cap = std::min<size_t>(cap, (size_t)cfg->batch_contracts);
+    } else {
+      // Automatic sizes: the group's contracts in equal batches under the
+      // budget, rather than full batches and a small remainder whose passes
+      // cost the same launches for little work.  (A small first batch, so
+      // that less generation runs before the first passes, measured slower:
+      // the passes fill every SM, so the next batch's generation runs in
+      // their gaps rather than beside them, and more batches mean more passes.)
+      size_t g = 0;
+      for (size_t q = pos; q < order.size() && ks[order[q]].num_steps == steps && ks[order[q]].expiry != 0.0; ++q)
+        ++g;
+      const size_t nb = (g + cap - 1) / cap;
+      cap = (g + nb - 1) / nb;
+    }
     if (cfg->injected_normals) cap = 1;  // one contract per batch keeps the injected layout simple
     std::vector<int64_t> batch;
     while (pos < order.size() && batch.size() < cap && ks[order[pos]].num_steps == steps &&

@@ -119,6 +119,8 @@ __device__ __forceinline__ double dividend_jump(const of_div_trigger& e, double 
   return s * (1.0 - e.amount);
 }
 
+// RNG: of::Xoshiro256pp or of::Pcg64, the FastRngKind of the engine.
+template <typename RNG>
 __global__ void __launch_bounds__(128) mc_ref_kernel(RefParams P, double* __restrict__ partials) {
   __shared__ double sh[5 * 4];
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -126,7 +128,7 @@ __global__ void __launch_bounds__(128) mc_ref_kernel(RefParams P, double* __rest
   const int streams = heston ? 2 : 1;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.samples; i += stride) {
-    of::Xoshiro256pp rng;
+    RNG rng;
     const double* inj = P.inj ? P.inj + i * P.steps * streams : nullptr;
     if (!inj) rng.seed(P.seed + (uint64_t)i * 7919ULL);  // stream_seed, fast_rng.rs:203-205
     Leg a, b;
@@ -249,6 +251,10 @@ of_status of_validate_mc(of_ctx* ctx, const of_model* m, const of_payoff* p, con
   if (!std::isfinite(p->strike)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "strike must be finite");
   if (p->kind == OF_PAYOFF_ASIAN && p->n_observations > 0 && !p->observation_times)
     return of_fail(ctx, OF_ERR_INVALID_INPUT, "observation_times is null");
+  if (c->rng_kind != OF_RNG_XOSHIRO256PP && c->rng_kind != OF_RNG_PCG64)
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown rng kind %d", c->rng_kind);
+  if (c->rng_kind != OF_RNG_XOSHIRO256PP && c->precision != OF_PREC_FP64_REFERENCE)
+    return of_fail(ctx, OF_ERR_UNSUPPORTED, "the FP32 Philox mode draws from Philox streams only");
   if (c->control_variate < OF_CV_NONE || c->control_variate > OF_CV_TERMINAL_SPOT)
     return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown control variate %d", c->control_variate);
   if (!std::isfinite(c->discount_factor)) return of_fail(ctx, OF_ERR_INVALID_INPUT, "discount factor must be finite");
@@ -354,8 +360,10 @@ extern "C" of_status of_mc_run(of_ctx* ctx, const of_model* m, const of_payoff* 
   }
 
   const int block = 128;
+  const void* kern = c->rng_kind == OF_RNG_PCG64 ? (const void*)mc_ref_kernel<of::Pcg64>
+                                                 : (const void*)mc_ref_kernel<of::Xoshiro256pp>;
   const int64_t want = (P.samples + block - 1) / block;
-  const int64_t cap = (int64_t)ctx->sm_count * of_blocks_per_sm((const void*)mc_ref_kernel, block, 0);
+  const int64_t cap = (int64_t)ctx->sm_count * of_blocks_per_sm(kern, block, 0);
   const int grid = (int)(want < cap ? want : cap);
   void *d_part = nullptr, *d_sums = nullptr, *h = nullptr;
   OF_TRY(of_scratch(ctx, SLOT_PARTIALS, (size_t)grid * 5 * sizeof(double), &d_part));
@@ -363,7 +371,8 @@ extern "C" of_status of_mc_run(of_ctx* ctx, const of_model* m, const of_payoff* 
   OF_TRY(of_pinned(ctx, 5 * sizeof(double), &h));
 
   OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
-  mc_ref_kernel<<<grid, block, 0, ctx->stream>>>(P, (double*)d_part);
+  if (c->rng_kind == OF_RNG_PCG64) mc_ref_kernel<of::Pcg64><<<grid, block, 0, ctx->stream>>>(P, (double*)d_part);
+  else mc_ref_kernel<of::Xoshiro256pp><<<grid, block, 0, ctx->stream>>>(P, (double*)d_part);
   OF_CUDA_TRY(ctx, cudaGetLastError());
   OF_TRY(of_reduce_rows(ctx, (const double*)d_part, grid, 5, (double*)d_sums));
   OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));

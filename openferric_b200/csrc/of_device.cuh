@@ -54,6 +54,50 @@ struct Xoshiro256pp {
   __device__ __forceinline__ double next_f64() { return (double)(next_u64() >> 11) * (1.0 / 9007199254740992.0); }
 };
 
+// PCG XSL-RR 128/64 (O'Neill 2014), the reference's Pcg64
+// (src/math/fast_rng.rs:86-128): a 128-bit LCG with PCG's default multiplier
+// 0x2360ED051FC65DA4_4385DF649FCCF645, odd increment (stream << 1) | 1; the
+// output is (hi ^ lo) rotated right by the top 6 bits of the old state.
+// Seeded by SplitMix64 (state hi, state lo, stream) and advanced once.  The
+// 128-bit state is two 64-bit words; the product keeps its low 128 bits.
+struct Pcg64 {
+  uint64_t hi, lo, inc_hi, inc_lo;
+
+  static constexpr uint64_t kMulHi = 0x2360ED051FC65DA4ULL, kMulLo = 0x4385DF649FCCF645ULL;
+
+  __device__ __forceinline__ static uint64_t splitmix(uint64_t& sm) {
+    sm += 0x9E3779B97F4A7C15ULL;
+    uint64_t z = sm;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+  }
+
+  __device__ __forceinline__ void seed(uint64_t seed) {
+    uint64_t sm = seed;
+    hi = splitmix(sm);
+    lo = splitmix(sm);
+    const uint64_t stream = splitmix(sm);
+    inc_hi = stream >> 63;
+    inc_lo = (stream << 1) | 1ULL;
+    (void)next_u64();
+  }
+
+  __device__ __forceinline__ uint64_t next_u64() {
+    const uint64_t ohi = hi, olo = lo;
+    // state = old * M + inc (mod 2^128)
+    const uint64_t plo = olo * kMulLo;
+    const uint64_t phi = __umul64hi(olo, kMulLo) + olo * kMulHi + ohi * kMulLo;
+    lo = plo + inc_lo;
+    hi = phi + inc_hi + (lo < plo ? 1ULL : 0ULL);
+    const uint64_t x = ohi ^ olo;
+    const unsigned rot = (unsigned)(ohi >> 58);
+    return (x >> rot) | (x << ((64u - rot) & 63u));
+  }
+
+  __device__ __forceinline__ double next_f64() { return (double)(next_u64() >> 11) * (1.0 / 9007199254740992.0); }
+};
+
 // uniform_open01 (fast_rng.rs:219-221) then the Acklam inverse
 // (beasley_springer_moro_inv_cdf, src/math/fast_norm.rs:54-139), FP64.
 // Translation units using this must be compiled with --fmad=false so that

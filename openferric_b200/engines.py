@@ -50,7 +50,9 @@ class Precision(enum.Enum):
 
 class FastRngKind(enum.Enum):
     """math::fast_rng::FastRngKind (src/math/fast_rng.rs:20-27).  The device
-    engine implements the default Xoshiro256PlusPlus stream."""
+    engine implements the two reproducible kinds, Xoshiro256PlusPlus (the
+    default) and Pcg64, in its FP64 reference mode; ThreadRng and StdRng
+    (the rand crate's generators) are not available."""
 
     Xoshiro256PlusPlus = 0
     Pcg64 = 1
@@ -293,12 +295,14 @@ class MonteCarloEngine:
     def run_full(self, generator: PathGenerator, instrument, discount_factor: float) -> A.OfMcResult:
         if self.num_paths <= 0:
             raise PricingError.InvalidInput("num_paths must be > 0")
-        if self.rng_kind is not FastRngKind.Xoshiro256PlusPlus or not self.reproducible:
-            raise PricingError.InvalidInput("the GPU engine supports the reproducible Xoshiro256PlusPlus stream only")
+        if self.rng_kind not in (FastRngKind.Xoshiro256PlusPlus, FastRngKind.Pcg64) or not self.reproducible:
+            raise PricingError.InvalidInput(
+                "the GPU engine supports the reproducible Xoshiro256PlusPlus and Pcg64 streams only")
         ctx = context(self.device)
         model = generator.to_abi()
         payoff, keep = _payoff_abi(instrument)
         cfg = A.OfMcConfig(num_paths=self.num_paths, seed=self.seed & 0xFFFFFFFFFFFFFFFF,
+                           rng_kind=A.OF_RNG_PCG64 if self.rng_kind is FastRngKind.Pcg64 else A.OF_RNG_XOSHIRO256PP,
                            antithetic=int(self.antithetic), precision=self.precision.value,
                            discount_factor=float(discount_factor))
         if self.control_variate is not None:

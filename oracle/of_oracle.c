@@ -61,6 +61,33 @@ double orc_xoshiro_next_f64(orc_xoshiro* rng) {
   return (double)x * (1.0 / 9007199254740992.0);
 }
 
+/* Pcg64::seed_from_u64, fast_rng.rs:92-108: SplitMix64 gives the state's
+ * high and low words and the stream; the increment is (stream << 1) | 1; one
+ * draw is discarded. */
+void orc_pcg64_seed(orc_pcg64* rng, uint64_t seed) {
+  uint64_t sm = seed;
+  const uint64_t hi = splitmix64_next(&sm), lo = splitmix64_next(&sm), stream = splitmix64_next(&sm);
+  rng->inc = ((unsigned __int128)stream << 1) | 1u;
+  rng->state = ((unsigned __int128)hi << 64) | lo;
+  (void)orc_pcg64_next_u64(rng);
+}
+
+/* Pcg64::next_u64, fast_rng.rs:111-121: the 128-bit LCG step with PCG's
+ * default multiplier, then the XSL-RR output of the old state. */
+uint64_t orc_pcg64_next_u64(orc_pcg64* rng) {
+  const unsigned __int128 mul = ((unsigned __int128)0x2360ED051FC65DA4ULL << 64) | 0x4385DF649FCCF645ULL;
+  const unsigned __int128 old = rng->state;
+  rng->state = old * mul + rng->inc;
+  const uint64_t x = (uint64_t)(old >> 64) ^ (uint64_t)old;
+  const unsigned rot = (unsigned)(old >> 122);
+  return (x >> rot) | (x << ((64u - rot) & 63u));
+}
+
+static inline double draw_normal_pcg(orc_pcg64* rng) {
+  const double u = (double)(orc_pcg64_next_u64(rng) >> 11) * (1.0 / 9007199254740992.0);
+  return orc_acklam_inv_cdf(orc_uniform_open01(u));
+}
+
 /* stream_seed, fast_rng.rs:203-205 (wrapping u64 arithmetic) */
 uint64_t orc_stream_seed(uint64_t base_seed, uint64_t stream_index) { return base_seed + stream_index * 7919ULL; }
 
@@ -453,6 +480,13 @@ static void mc_sample(const of_model* m, const of_payoff* p, const of_mc_config*
       z1[j] = inj[j * streams];
       if (streams >= 2) z2[j] = inj[j * streams + 1];
     }
+  } else if (c->rng_kind == OF_RNG_PCG64) {  /* FastRng::from_seed(Pcg64, stream_seed), simulation.rs:215-216 */
+    orc_pcg64 rng;
+    orc_pcg64_seed(&rng, orc_stream_seed(c->seed, (uint64_t)i));
+    for (int64_t j = 0; j < steps; ++j) {
+      z1[j] = draw_normal_pcg(&rng);
+      if (streams >= 2) z2[j] = draw_normal_pcg(&rng);
+    }
   } else {
     orc_xoshiro rng;
     orc_xoshiro_seed(&rng, orc_stream_seed(c->seed, (uint64_t)i));
@@ -517,6 +551,7 @@ static void mc_finish(const mc_acc* a, const of_mc_config* c, of_mc_result* out)
 
 int orc_mc_run(const of_model* m, const of_payoff* p, const of_mc_config* c, int threads, of_mc_result* out) {
   if (c->num_paths <= 0 || m->steps <= 0) return OF_ERR_INVALID_INPUT;
+  if (c->rng_kind != OF_RNG_XOSHIRO256PP && c->rng_kind != OF_RNG_PCG64) return OF_ERR_INVALID_INPUT;
   const int64_t samples = c->antithetic ? (c->num_paths + 1) / 2 : c->num_paths;
   const int64_t steps = m->steps;
   if (c->injected_normals && c->n_injected < samples * steps * model_streams(m)) return OF_ERR_INVALID_INPUT;

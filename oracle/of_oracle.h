@@ -29,6 +29,10 @@ typedef struct orc_xoshiro { uint64_t s[4]; } orc_xoshiro;
 void orc_xoshiro_seed(orc_xoshiro* rng, uint64_t seed);
 uint64_t orc_xoshiro_next_u64(orc_xoshiro* rng);
 double orc_xoshiro_next_f64(orc_xoshiro* rng);
+/* Pcg64 (PCG XSL-RR 128/64) of fast_rng.rs:86-128 */
+typedef struct orc_pcg64 { unsigned __int128 state, inc; } orc_pcg64;
+void orc_pcg64_seed(orc_pcg64* rng, uint64_t seed);
+uint64_t orc_pcg64_next_u64(orc_pcg64* rng);
 uint64_t orc_stream_seed(uint64_t base_seed, uint64_t stream_index);
 double orc_uniform_open01(double u);
 double orc_acklam_inv_cdf(double p);

@@ -45,6 +45,9 @@ def lib():
         L.orc_xoshiro_next_u64.argtypes = [C.c_void_p]
         L.orc_xoshiro_next_f64.restype = D
         L.orc_xoshiro_next_f64.argtypes = [C.c_void_p]
+        L.orc_pcg64_seed.argtypes = [C.c_void_p, C.c_uint64]
+        L.orc_pcg64_next_u64.restype = C.c_uint64
+        L.orc_pcg64_next_u64.argtypes = [C.c_void_p]
         L.orc_fill_run_normals.argtypes = [C.c_uint64, I64, I64, C.c_int, PD]
         L.orc_fill_sequential_normals.argtypes = [C.c_uint64, I64, PD]
         L.orc_bs_price.restype = D
@@ -111,6 +114,17 @@ class Xoshiro:
 
     def state(self):
         return list(self._state)
+
+
+class Pcg64:
+    """The C oracle's Pcg64 (two 128-bit words: state, increment)."""
+
+    def __init__(self, seed):
+        self._state = (C.c_uint64 * 4)()
+        lib().orc_pcg64_seed(C.byref(self._state), C.c_uint64(seed))
+
+    def next_u64(self):
+        return lib().orc_pcg64_next_u64(C.byref(self._state))
 
 
 def acklam(p):

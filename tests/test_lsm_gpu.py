@@ -141,3 +141,27 @@ def test_lsm_validation_messages():
         LongstaffSchwartzEngine(2, 10, 1).price(VanillaOption.american_put(40, 1), m)
     r = LongstaffSchwartzEngine(100, 10, 1).price(VanillaOption.american_put(40, 0.0), m)
     assert r.price == 0.0 and r.stderr == 0.0
+
+
+def test_fp32_batches_do_not_change_the_draws():
+    """Each contract draws from its own Philox stream (its index in the list),
+    whatever batch it lands in: batches of 1, 2 and the automatic sizes price
+    the same paths.  The FP32 moment sums group the chunks by block, and the
+    blocks per contract follow the batch size, so the fitted betas may move in
+    the last digits and flip a few exercise decisions at the boundary, each by
+    O(1) / n; independent draws would differ by about one standard error."""
+    items = []
+    for i, (s0, vol) in enumerate([(36.0, 0.2), (40.0, 0.4), (44.0, 0.2), (38.0, 0.3), (42.0, 0.25)]):
+        m = Market.builder().spot(s0).rate(0.06).flat_vol(vol).build()
+        items.append((VanillaOption.american_put(40.0, 1.0), m))
+    runs = []
+    for b in (0, 1, 2):
+        eng = LongstaffSchwartzEngine(1 << 17, 50, 11).with_precision(Precision.Fp32Philox) \
+            .with_basis_degree(3).with_batch_contracts(b)
+        runs.append(eng.price_batch(items, with_delta=True))
+    for k in range(len(items)):
+        ref = runs[0][k]
+        for other in runs[1:]:
+            r = other[k]
+            assert abs(r.price - ref.price) <= 0.05 * ref.stderr, (k, r.price, ref.price, ref.stderr)
+            assert abs(r.stderr - ref.stderr) <= 0.01 * ref.stderr, (k, r.stderr, ref.stderr)

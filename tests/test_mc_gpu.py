@@ -45,10 +45,10 @@ def _market(spot=100.0, r=0.05, q=0.0, vol=0.2):
     return Market.builder().spot(spot).rate(r).dividend_yield(q).flat_vol(vol).build()
 
 
-def _oracle_run(orc, gen, instrument, anti, cv, df, num_paths, seed, injected=None):
+def _oracle_run(orc, gen, instrument, anti, cv, df, num_paths, seed, injected=None, rng_kind=A.OF_RNG_XOSHIRO256PP):
     from openferric_b200.engines import _payoff_abi
     payoff, keep = _payoff_abi(instrument)
-    cfg = A.OfMcConfig(num_paths=num_paths, seed=seed, antithetic=int(anti), discount_factor=df)
+    cfg = A.OfMcConfig(num_paths=num_paths, seed=seed, antithetic=int(anti), discount_factor=df, rng_kind=rng_kind)
     if cv is not None:
         cfg.control_variate = cv.kind.value
         cfg.cv_expected = cv.expected
@@ -150,6 +150,36 @@ def test_odd_path_count_and_single_sample(orc):
         assert gpu.samples == ref.samples
         assert close(gpu.price, ref.price, PRICE_RTOL)
         assert gpu.stderr_ == ref.stderr_ or close(gpu.stderr_, ref.stderr_, SE_RTOL)
+
+
+@pytest.mark.parametrize("model", ["gbm", "heston"])
+@pytest.mark.parametrize("anti", [False, True])
+def test_fp64_pcg64_streams_match_oracle(orc, model, anti):
+    """with_rng_kind(FastRngKind::Pcg64): every sample draws from
+    Pcg64::seed_from_u64(stream_seed(seed, i)) (fast_rng.rs:86-128,
+    simulation.rs:215-216); the FP64 engine equals the oracle's restatement,
+    and the xoshiro run of the same seed differs."""
+    from openferric_b200.engines import FastRngKind
+    T, steps, paths, seed = 1.0, 24, 3001, 1234
+    gen = GENS[model](T, steps)
+    inst = _instruments(T)["asian_arith_call"]
+    gpu = MonteCarloEngine(paths, seed).with_antithetic(anti).with_rng_kind(FastRngKind.Pcg64).run_full(gen, inst, 0.97)
+    ref = _oracle_run(orc, gen, inst, anti, None, 0.97, paths, seed, rng_kind=A.OF_RNG_PCG64)
+    xo = MonteCarloEngine(paths, seed).with_antithetic(anti).run_full(gen, inst, 0.97)
+    assert close(gpu.price, ref.price, PRICE_RTOL), (gpu.price, ref.price)
+    assert se_close(gpu.stderr_, ref.stderr_, SE_RTOL, ref.price)
+    assert gpu.price != xo.price
+
+
+def test_pcg64_is_rejected_in_fp32_mode_and_thread_rng_everywhere():
+    from openferric_b200.engines import FastRngKind, Precision
+    gen = GENS["gbm"](1.0, 8)
+    inst = _instruments(1.0)["call"]
+    with pytest.raises(PricingError, match="Philox streams only"):
+        MonteCarloEngine(1000, 1).with_rng_kind(FastRngKind.Pcg64).with_precision(Precision.Fp32Philox) \
+            .run_full(gen, inst, 1.0)
+    with pytest.raises(PricingError, match="Xoshiro256PlusPlus and Pcg64"):
+        MonteCarloEngine(1000, 1).with_rng_kind(FastRngKind.ThreadRng).run_full(gen, inst, 1.0)
 
 
 def test_large_seed_wraps_like_reference(orc):

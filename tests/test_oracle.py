@@ -99,6 +99,62 @@ def test_xoshiro_matches_python_restatement(orc, seed):
         assert a.next_u64() == b.next_u64()
 
 
+class PyPcg64:
+    """Pcg64 of fast_rng.rs:86-128 in Python integers: a second restatement
+    that checks the C oracle's 128-bit arithmetic."""
+    MUL = 0x2360ED051FC65DA44385DF649FCCF645
+    M128 = (1 << 128) - 1
+
+    def __init__(self, seed):
+        st = seed & M64
+        st, hi = py_splitmix(st)
+        st, lo = py_splitmix(st)
+        st, stream = py_splitmix(st)
+        self.inc = ((stream << 1) | 1) & self.M128
+        self.state = (hi << 64) | lo
+        self.next_u64()
+
+    def next_u64(self):
+        old = self.state
+        self.state = (old * self.MUL + self.inc) & self.M128
+        x = ((old >> 64) ^ old) & M64
+        rot = old >> 122
+        return ((x >> rot) | (x << ((64 - rot) & 63))) & M64
+
+
+@pytest.mark.parametrize("seed", [0, 1, 42, M64, 0x0123456789ABCDEF])
+def test_pcg64_matches_python_restatement(orc, seed):
+    a, b = orc.Pcg64(seed), PyPcg64(seed)
+    for _ in range(2000):
+        assert a.next_u64() == b.next_u64()
+
+
+def test_mc_run_pcg64_draws_from_pcg_streams(orc):
+    """FastRng::from_seed(Pcg64, stream_seed(seed, i)) per sample
+    (simulation.rs:215-216): the oracle's MC on Pcg64 streams equals its MC on
+    the same streams' normals injected, and differs from the xoshiro run."""
+    import ctypes as C
+    from openferric_b200 import _abi as A
+    n, steps, seed = 64, 12, 9
+    model = A.OfModel(kind=A.OF_MODEL_GBM, s0=100.0, mu=0.03, sigma=0.25, maturity=1.0, steps=steps)
+    payoff = A.OfPayoff(kind=A.OF_PAYOFF_VANILLA, option_type=A.OF_CALL, strike=100.0)
+    z = []
+    for i in range(n):
+        g = PyPcg64((seed + i * 7919) & M64)
+        for _ in range(steps):
+            u = float(g.next_u64() >> 11) * (1.0 / 9007199254740992.0)
+            z.append(orc.acklam(min(max(u, 2.0 ** -52), 1.0 - 2.0 ** -52)))
+    zz = np.array(z)
+    pcg = orc.mc_run(model, payoff, A.OfMcConfig(num_paths=n, seed=seed, discount_factor=1.0,
+                                                   rng_kind=A.OF_RNG_PCG64))
+    inj = orc.mc_run(model, payoff, A.OfMcConfig(num_paths=n, seed=seed, discount_factor=1.0,
+                                                   injected_normals=zz.ctypes.data_as(C.POINTER(C.c_double)),
+                                                   n_injected=zz.size))
+    xo = orc.mc_run(model, payoff, A.OfMcConfig(num_paths=n, seed=seed, discount_factor=1.0))
+    assert pcg.price == inj.price and pcg.stderr_ == inj.stderr_
+    assert pcg.price != xo.price
+
+
 def test_xoshiro_reproducible_and_unit_interval(orc):
     # fast_rng.rs:250-277
     a, b = orc.Xoshiro(42), orc.Xoshiro(42)
