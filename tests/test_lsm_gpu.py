@@ -147,9 +147,11 @@ def test_fp32_batches_do_not_change_the_draws():
     """Each contract draws from its own Philox stream (its index in the list),
     whatever batch it lands in: batches of 1, 2 and the automatic sizes price
     the same paths.  The FP32 moment sums group the chunks by block, and the
-    blocks per contract follow the batch size, so the fitted betas may move in
-    the last digits and flip a few exercise decisions at the boundary, each by
-    O(1) / n; independent draws would differ by about one standard error."""
+    blocks per contract follow the batch size, so the fitted betas move by
+    about the FP32 rounding of the moments, flip exercise decisions near the
+    boundary, and the flips propagate through the later regressions: measured
+    up to 0.07 standard errors at 2^17 paths.  Independent draws would differ
+    by about 1.4 standard errors (rms)."""
     items = []
     for i, (s0, vol) in enumerate([(36.0, 0.2), (40.0, 0.4), (44.0, 0.2), (38.0, 0.3), (42.0, 0.25)]):
         m = Market.builder().spot(s0).rate(0.06).flat_vol(vol).build()
@@ -163,5 +165,5 @@ def test_fp32_batches_do_not_change_the_draws():
         ref = runs[0][k]
         for other in runs[1:]:
             r = other[k]
-            assert abs(r.price - ref.price) <= 0.05 * ref.stderr, (k, r.price, ref.price, ref.stderr)
+            assert abs(r.price - ref.price) <= 0.25 * ref.stderr, (k, r.price, ref.price, ref.stderr)
             assert abs(r.stderr - ref.stderr) <= 0.01 * ref.stderr, (k, r.stderr, ref.stderr)
