@@ -33,6 +33,8 @@
 // through every step) are unbiased too.
 #pragma once
 
+#include <type_traits>
+
 #include "mills_coeffs.h"
 #include "of_device.cuh"
 
@@ -502,6 +504,160 @@ __host__ __device__ __forceinline__ int gk_group(int kind) {
                                                                                                   : KG_BARRIER;
 }
 
+// ---- barrier legs in packed pairs (FP32) ----------------------------------
+// Two survival legs share each FP32 instruction (sm_100 f32x2): two
+// independent samples, or a sample and its antithetic twin (uniforms u and
+// 1 - u).  Every packed operation is the scalar step's operation in its order,
+// so each half is surv_step's arithmetic bit for bit; the table lookups of the
+// inverse normal (two fitted branches), the exponentials and the divisions
+// stay scalar per half.
+struct SurvLeg2 {
+  float2 y, L, ypl;
+  float2 yd[4], ld[4];
+};
+
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+// GMath<float>::cdf_ratio of both halves
+__device__ __forceinline__ void cdf_ratio2(float2 h, float2& p, float2& g) {
+  const float2 a = make_float2(fabsf(h.x), fabsf(h.y));
+  const float2 den = fma2(splat2(OF_MILLS_C), a, splat2(1.0f));
+  const float2 t = make_float2(1.0f / den.x, 1.0f / den.y);
+  float2 m = splat2(kMills[OF_MILLS_DEG]);
+#pragma unroll
+  for (int i = OF_MILLS_DEG - 1; i >= 0; --i) m = fma2(m, t, splat2(kMills[i]));
+  m = mul2(m, t);
+  const float2 a2 = mul2(a, a), a2lo = fma2(a, a, neg2(a2));
+  const float2 ex = mul2(splat2(-0.5f), a2);
+  const float2 phi = mul2(mul2(splat2(0.398942280401432677939946f), make_float2(__expf(ex.x), __expf(ex.y))),
+                          fma2(splat2(-0.5f), a2lo, splat2(1.0f)));
+  const float2 tail = mul2(phi, m);
+  p.x = h.x < 0.0f ? tail.x : 1.0f - tail.x;
+  p.y = h.y < 0.0f ? tail.y : 1.0f - tail.y;
+  g.x = h.x < 0.0f ? 1.0f / m.x : phi.x / p.x;
+  g.y = h.y < 0.0f ? 1.0f / m.y : phi.y / p.y;
+}
+
+__device__ __forceinline__ void surv_init2(SurvLeg2& s, const GreekConsts<float>& c) {
+  s.y = s.ypl = make_float2(0.0f, 0.0f);
+  s.L = splat2(c.sgn * c.bar > 0.0f ? 1.0f : 0.0f);
+#pragma unroll
+  for (int t = 0; t < 4; ++t) s.yd[t] = s.ld[t] = make_float2(0.0f, 0.0f);
+}
+
+// surv_step<float, G, IN> of both halves
+template <bool G, bool IN>
+__device__ __forceinline__ void surv_step2(SurvLeg2& s, const GreekConsts<float>& c, float2 u) {
+  using M = GMath<float>;
+  float2 h = mul2(splat2(c.sib), sub2(sub2(splat2(c.bar), s.y), splat2(c.alpha)));
+  h.x = h.x > M::kHMin ? h.x : M::kHMin;
+  h.y = h.y > M::kHMin ? h.y : M::kHMin;
+  float2 p, g;
+  cdf_ratio2(h, p, g);
+  float2 v = mul2(u, p);
+  float2 q = fma2(neg2(u), p, splat2(1.0f));
+  v.x = v.x > M::kTiny ? v.x : M::kTiny;
+  v.y = v.y > M::kTiny ? v.y : M::kTiny;
+  q.x = q.x > M::kTiny ? q.x : M::kTiny;
+  q.y = q.y > M::kTiny ? q.y : M::kTiny;
+  const float2 zeta = make_float2(M::icdf2(v.x, q.x), M::icdf2(v.y, q.y));
+  const float2 z = mul2(splat2(c.sgn), zeta);
+  if (G) {
+    const float2 d = mul2(mul2(splat2(0.5f), sub2(zeta, h)), add2(zeta, h));
+    const float2 w = mul2(u, make_float2(__expf(d.x), __expf(d.y)));
+    const float2 k = mul2(splat2(c.beta * c.sgn), w);
+    const float2 h0 = mul2(splat2(c.sib), sub2(splat2(-1.0f), s.yd[0]));
+    s.ld[0] = fma2(g, h0, s.ld[0]);
+    s.yd[0] = fma2(k, h0, s.yd[0]);
+    const float2 h1 = fma2(splat2(c.sib), sub2(splat2(c.sig_dt), s.yd[1]), mul2(neg2(h), splat2(c.inv_sig)));
+    s.ld[1] = fma2(g, h1, s.ld[1]);
+    s.yd[1] = fma2(k, h1, add2(s.yd[1], fma2(splat2(c.beta_over_sig), z, splat2(-c.sig_dt))));
+    const float2 h2 = mul2(splat2(c.sib), sub2(splat2(-c.dt), s.yd[2]));
+    s.ld[2] = fma2(g, h2, s.ld[2]);
+    s.yd[2] = fma2(k, h2, add2(s.yd[2], splat2(c.dt)));
+    const float2 h3 = fma2(splat2(c.sib), sub2(splat2(-c.alpha_over_T), s.yd[3]), mul2(neg2(h), splat2(c.inv_2T)));
+    s.ld[3] = fma2(g, h3, s.ld[3]);
+    s.yd[3] = fma2(k, h3, add2(s.yd[3], fma2(splat2(c.beta_over_2T), z, splat2(c.alpha_over_T))));
+  }
+  s.y = fma2(splat2(c.beta), z, add2(s.y, splat2(c.alpha)));
+  s.L = mul2(s.L, p);
+  if (IN) {
+    const float2 zp = make_float2(M::icdf2(u.x, 1.0f - u.x), M::icdf2(u.y, 1.0f - u.y));
+    s.ypl = fma2(splat2(c.beta), zp, add2(s.ypl, splat2(c.alpha)));
+  }
+}
+
+// half e (0: .x, 1: .y) of a packed leg as a scalar leg
+template <bool G>
+__device__ __forceinline__ SurvLeg<float, G> surv_half(const SurvLeg2& s, int e) {
+  SurvLeg<float, G> o;
+  o.y = e ? s.y.y : s.y.x;
+  o.L = e ? s.L.y : s.L.x;
+  o.ypl = e ? s.ypl.y : s.ypl.x;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    o.yd[t] = e ? s.yd[t].y : s.yd[t].x;
+    o.ld[t] = e ? s.ld[t].y : s.ld[t].x;
+  }
+  return o;
+}
+
+// gk_barrier<float, G, true, IN>: the sample and its antithetic twin as the
+// two halves
+template <bool G, bool IN>
+__device__ __forceinline__ void gk_barrier_twin(const GreekConsts<float>& c, uint64_t i, const PhiloxKeys& K,
+                                                GreekSample<float>& out) {
+  const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
+  SurvLeg2 s;
+  surv_init2(s, c);
+  for (int32_t j = 0; j < c.steps; j += 4) {
+    float u[4];
+    gk_uniforms(c, (uint32_t)(j >> 2), lo, hi, K, u);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (j + q >= c.steps) break;
+      surv_step2<G, IN>(s, c, make_float2(u[q], 1.0f - u[q]));
+    }
+  }
+  float xa, xb, ga[4], gb[4];
+  surv_payoff<float, G, IN>(surv_half<G>(s, 0), c, xa, ga);
+  surv_payoff<float, G, IN>(surv_half<G>(s, 1), c, xb, gb);
+  out.x = 0.5f * (xa + xb);
+  out.y = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) out.g[t] = 0.5f * (ga[t] + gb[t]);
+}
+
+// gk_barrier<float, G, false, IN> of samples i0 and i1 in one packed loop
+template <bool G, bool IN>
+__device__ __forceinline__ void gk_barrier_pair(const GreekConsts<float>& c, uint64_t i0, uint64_t i1,
+                                                const PhiloxKeys& K, GreekSample<float>& o0, GreekSample<float>& o1) {
+  const uint32_t lo0 = (uint32_t)i0, hi0 = (uint32_t)(i0 >> 32), lo1 = (uint32_t)i1, hi1 = (uint32_t)(i1 >> 32);
+  SurvLeg2 s;
+  surv_init2(s, c);
+  for (int32_t j = 0; j < c.steps; j += 4) {
+    float u0[4], u1[4];
+    gk_uniforms(c, (uint32_t)(j >> 2), lo0, hi0, K, u0);
+    gk_uniforms(c, (uint32_t)(j >> 2), lo1, hi1, K, u1);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (j + q >= c.steps) break;
+      surv_step2<G, IN>(s, c, make_float2(u0[q], u1[q]));
+    }
+  }
+  float x, g[4];
+  surv_payoff<float, G, IN>(surv_half<G>(s, 0), c, x, g);
+  o0.x = x;
+  o0.y = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) o0.g[t] = g[t];
+  surv_payoff<float, G, IN>(surv_half<G>(s, 1), c, x, g);
+  o1.x = x;
+  o1.y = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) o1.g[t] = g[t];
+}
+
 template <typename R, bool G, int KG, bool ANTI>
 __device__ __forceinline__ void gk_sample_group_anti(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
                                                      const float* obs_w, GreekSample<R>& out) {
@@ -518,9 +674,23 @@ __device__ __forceinline__ void gk_sample_group_anti(const GreekConsts<R>& c, ui
       else gk_asian<R, G, ANTI, false, true, false>(c, i, K, obs_w, out);
     }
   } else {
-    if (c.kind == GK_BARRIER_OUT) gk_barrier<R, G, ANTI, false>(c, i, K, out);
-    else gk_barrier<R, G, ANTI, true>(c, i, K, out);
+    if constexpr (std::is_same<R, float>::value && ANTI) {  // the twin legs in packed pairs
+      if (c.kind == GK_BARRIER_OUT) gk_barrier_twin<G, false>(c, i, K, out);
+      else gk_barrier_twin<G, true>(c, i, K, out);
+    } else {
+      if (c.kind == GK_BARRIER_OUT) gk_barrier<R, G, ANTI, false>(c, i, K, out);
+      else gk_barrier<R, G, ANTI, true>(c, i, K, out);
+    }
   }
+}
+
+// Two samples of a barrier option without antithetic twins (FP32 modes).
+template <bool G>
+__device__ __forceinline__ void gk_barrier_pair_group(const GreekConsts<float>& c, uint64_t i0, uint64_t i1,
+                                                      const PhiloxKeys& K, GreekSample<float>& o0,
+                                                      GreekSample<float>& o1) {
+  if (c.kind == GK_BARRIER_OUT) gk_barrier_pair<G, false>(c, i0, i1, K, o0, o1);
+  else gk_barrier_pair<G, true>(c, i0, i1, K, o0, o1);
 }
 
 template <typename R, bool G, int KG>

@@ -1240,9 +1240,23 @@ __global__ void __launch_bounds__(256, (KG == of::KG_BARRIER || !G) ? 2 : 3)
     const BookTile tile = P.tiles[t];
     const of::GreekConsts<R>& c = gc[tile.opt];
     GreekAcc<R, G> acc;
+    // FP32 barrier options without antithetic twins: two samples at a time in
+    // packed pairs (the sums take them in the same order)
+    const bool pairs = KG == of::KG_BARRIER && std::is_same<R, float>::value && !(c.flags & of::GF_ANTI);
     for (int k = 0; k < P.ppt; ++k) {
       const int local = k * blockDim.x + threadIdx.x;
       if (local >= tile.count) break;
+      if constexpr (KG == of::KG_BARRIER && std::is_same<R, float>::value) {
+        if (pairs && k + 1 < P.ppt && local + (int)blockDim.x < tile.count) {
+          of::GreekSample<float> v0, v1;
+          of::gk_barrier_pair_group<G>(c, (uint64_t)(tile.first + local), (uint64_t)(tile.first + local) + blockDim.x,
+                                       P.keys, v0, v1);
+          acc.add(v0);
+          acc.add(v1);
+          ++k;
+          continue;
+        }
+      }
       of::GreekSample<R> v;
       of::gk_sample_group<R, G, KG>(c, (uint64_t)(tile.first + local), P.keys, P.obs_w, v);
       acc.add(v);
