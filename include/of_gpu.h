@@ -309,6 +309,7 @@ typedef struct of_stderr_round {
   double path_steps;  /* their total path-steps */
   int64_t converged;  /* of them, how many met their target */
   double kernel_ms;   /* device time of the launch (CUDA events) */
+  double wall_ms;     /* host wall clock of the round: planning, uploads, launch and readback */
 } of_stderr_round;
 
 /* A pilot launch prices every entry with target->pilot_paths paths

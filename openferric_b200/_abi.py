@@ -141,6 +141,7 @@ class OfStderrRound(C.Structure):
         ("path_steps", C.c_double),
         ("converged", C.c_int64),
         ("kernel_ms", C.c_double),
+        ("wall_ms", C.c_double),
     ]
 
 

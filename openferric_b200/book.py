@@ -193,13 +193,15 @@ def price_book_fp64(entries: Sequence[BookEntry], seed: int, block: int = 0, pat
 @dataclass
 class StderrRound:
     """One book launch of `price_book_to_stderr`: how many options it priced,
-    their total paths and path-steps, how many met the target, and the
-    launch's device time."""
+    their total paths and path-steps, how many met the target, the
+    launch's device time and the round's host wall clock (planning, uploads,
+    launch and readback)."""
     options: int
     paths: int
     path_steps: float
     converged: int
     kernel_ms: float = 0.0
+    wall_ms: float = 0.0
 
 
 def paths_for_stderr(paths: int, stderr: float, target: float, margin: float = 1.1, granule: int = 256) -> int:
@@ -255,7 +257,7 @@ def price_book_to_stderr(entries: Sequence[BookEntry], seed: int, se_rel: float 
             res.greeks, se = _greeks_of(gr[k])
             res = BookGreeksResult(res, se)
         results.append(res)
-    return results, [StderrRound(rd.options, rd.paths, rd.path_steps, rd.converged, rd.kernel_ms)
+    return results, [StderrRound(rd.options, rd.paths, rd.path_steps, rd.converged, rd.kernel_ms, rd.wall_ms)
                      for rd in rounds[:n_rounds.value]]
 
 

@@ -2,6 +2,7 @@
 // every option meets a standard-error target.  Host-only: each round is one
 // batched-book launch (of_mc_price_book, or of_mc_price_book_greeks with the
 // pathwise Greeks) over the options still above their target.
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -63,6 +64,7 @@ static of_status price_to_stderr(of_ctx* ctx, const of_book_entry* entries, int6
       while (ppt < 256 && total > ((int64_t)c.block * ppt) << 18) ppt *= 2;
       c.paths_per_thread = ppt;
     }
+    const auto t0 = std::chrono::steady_clock::now();
     res.assign(sub.size(), of_mc_result{});
     if (greeks) {
       gr.assign(sub.size(), of_book_greeks{});
@@ -89,6 +91,7 @@ static of_status price_to_stderr(of_ctx* ctx, const of_book_entry* entries, int6
       o.path_steps = steps;
       o.converged = (int64_t)(pending.size() - still.size());
       o.kernel_ms = res.empty() ? 0.0 : res[0].kernel_ms;
+      o.wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     pending.swap(still);
   }

@@ -1404,6 +1404,7 @@ static of::GreekConsts<float> round_greek_consts(const of::GreekConsts<double>& 
 
 struct of_book_plan {
   of_ctx* ctx = nullptr;
+  bool scratch = false;  // buffers borrowed from the context (a plan that lives inside one call)
   int64_t n = 0;
   int mode = OF_BOOK_PRICE;
   int nc = 5;  // sums per option: 5, or 13 with the Greeks
@@ -1477,6 +1478,10 @@ extern "C" void of_book_plan_destroy(of_book_plan* pl) {
   if (pl->ctx) cudaStreamSynchronize(pl->ctx->stream);
   if (pl->exec) cudaGraphExecDestroy(pl->exec);
   if (pl->graph) cudaGraphDestroy(pl->graph);
+  if (pl->scratch) {  // the context owns the buffers
+    delete pl;
+    return;
+  }
   cudaFree(pl->d_opts);
   cudaFree(pl->d_tiles);
   cudaFree(pl->d_obs);
@@ -1490,8 +1495,10 @@ extern "C" void of_book_plan_destroy(of_book_plan* pl) {
   delete pl;
 }
 
-extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, int64_t n, const of_book_config* cfg,
-                                         of_book_plan** out) {
+// scratch: the plan lives inside one library call and borrows the context's
+// cached buffers (of_scratch / of_pinned) instead of allocating its own.
+static of_status book_plan_create(of_ctx* ctx, const of_book_entry* e, int64_t n, const of_book_config* cfg,
+                                  bool scratch, of_book_plan** out) {
   if (!ctx || !out || !cfg) return OF_ERR_INVALID_INPUT;
   *out = nullptr;
   if (n <= 0 || !e) return of_fail(ctx, OF_ERR_INVALID_INPUT, "book must hold at least one option");
@@ -1500,6 +1507,7 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
   OF_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   of_book_plan* pl = new of_book_plan();
   pl->ctx = ctx;
+  pl->scratch = scratch;
   pl->n = n;
   pl->block = cfg->block > 0 ? cfg->block : 256;
   pl->ppt = cfg->paths_per_thread > 0 ? cfg->paths_per_thread : 4;
@@ -1653,25 +1661,33 @@ extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, in
   pl->n_tiles = (int64_t)sorted.size();
 
   const size_t nt = sorted.size();
-  if (cudaMalloc(&pl->d_opts, opts.size() * sizeof(BookOpt)) != cudaSuccess ||
-      cudaMalloc(&pl->d_tiles, nt * sizeof(BookTile)) != cudaSuccess ||
-      cudaMalloc(&pl->d_obs, std::max<size_t>(1, obs.size()) * sizeof(float)) != cudaSuccess ||
-      cudaMalloc(&pl->d_divs, std::max<size_t>(1, divs.size()) * sizeof(BookDiv)) != cudaSuccess ||
-      cudaMalloc(&pl->d_counter, of::KG_COUNT * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&pl->d_partials, nt * pl->nc * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&pl->d_begin, begin.size() * sizeof(int32_t)) != cudaSuccess ||
-      cudaMalloc(&pl->d_sums, (size_t)n * pl->nc * sizeof(double)) != cudaSuccess ||
-      cudaMallocHost(&pl->h_sums, (size_t)n * pl->nc * sizeof(double)) != cudaSuccess)
-    return fail(of_fail(ctx, OF_ERR_ALLOC, "book plan allocation failed"));
+  // A plan that lives inside one call borrows the context's cached buffers:
+  // no cudaMalloc / cudaFree / cudaMallocHost per call.
+  auto dalloc = [&](void** p, size_t bytes, int slot) {
+    if (pl->scratch) return of_scratch(ctx, slot, bytes, p) == OF_OK;
+    return cudaMalloc(p, bytes) == cudaSuccess;
+  };
+  const size_t sum_bytes = (size_t)n * pl->nc * sizeof(double);
+  bool ok = dalloc((void**)&pl->d_opts, opts.size() * sizeof(BookOpt), SLOT_BOOK) &&
+            dalloc((void**)&pl->d_tiles, nt * sizeof(BookTile), SLOT_TILES) &&
+            dalloc((void**)&pl->d_obs, std::max<size_t>(1, obs.size()) * sizeof(float), SLOT_BOOK_OBS) &&
+            dalloc((void**)&pl->d_divs, std::max<size_t>(1, divs.size()) * sizeof(BookDiv), SLOT_BOOK_DIVS) &&
+            dalloc((void**)&pl->d_counter, of::KG_COUNT * sizeof(int), SLOT_BOOK_COUNTER) &&
+            dalloc((void**)&pl->d_partials, nt * pl->nc * sizeof(double), SLOT_BOOK_PARTIALS) &&
+            dalloc((void**)&pl->d_begin, begin.size() * sizeof(int32_t), SLOT_BOOK_BEGIN) &&
+            dalloc((void**)&pl->d_sums, sum_bytes, SLOT_BOOK_SUMS);
+  if (ok) ok = pl->scratch ? of_pinned(ctx, sum_bytes, (void**)&pl->h_sums) == OF_OK
+                           : cudaMallocHost(&pl->h_sums, sum_bytes) == cudaSuccess;
+  if (!ok) return fail(of_fail(ctx, OF_ERR_ALLOC, "book plan allocation failed"));
   if (pl->mode == OF_BOOK_GREEKS) {  // the constants rounded once to FP32
     std::vector<of::GreekConsts<float>> gf(gcs.size());
     for (size_t k = 0; k < gcs.size(); ++k) gf[k] = round_greek_consts(gcs[k]);
-    if (cudaMalloc(&pl->d_gc, gf.size() * sizeof(gf[0])) != cudaSuccess)
+    if (!dalloc(&pl->d_gc, gf.size() * sizeof(gf[0]), SLOT_BOOK_GC))
       return fail(of_fail(ctx, OF_ERR_ALLOC, "book plan allocation failed"));
     if (cudaMemcpy(pl->d_gc, gf.data(), gf.size() * sizeof(gf[0]), cudaMemcpyHostToDevice) != cudaSuccess)
       return fail(of_fail(ctx, OF_ERR_CUDA, "book upload failed"));
   } else if (pl->mode == OF_BOOK_PRICE_FP64) {
-    if (cudaMalloc(&pl->d_gc, gcs.size() * sizeof(gcs[0])) != cudaSuccess)
+    if (!dalloc(&pl->d_gc, gcs.size() * sizeof(gcs[0]), SLOT_BOOK_GC))
       return fail(of_fail(ctx, OF_ERR_ALLOC, "book plan allocation failed"));
     if (cudaMemcpy(pl->d_gc, gcs.data(), gcs.size() * sizeof(gcs[0]), cudaMemcpyHostToDevice) != cudaSuccess)
       return fail(of_fail(ctx, OF_ERR_CUDA, "book upload failed"));
@@ -1791,10 +1807,15 @@ extern "C" of_status of_book_plan_info(of_book_plan* pl, int32_t* block, int32_t
 }
 
 // One launch of a book: plan, launch, results (and Greeks when `greeks`).
+extern "C" of_status of_book_plan_create(of_ctx* ctx, const of_book_entry* e, int64_t n, const of_book_config* cfg,
+                                         of_book_plan** out) {
+  return book_plan_create(ctx, e, n, cfg, false, out);
+}
+
 static of_status book_run(of_ctx* ctx, const of_book_entry* e, int64_t n, const of_book_config* cfg,
                           of_mc_result* res, of_book_greeks* greeks) {
   of_book_plan* pl = nullptr;
-  OF_TRY(of_book_plan_create(ctx, e, n, cfg, &pl));
+  OF_TRY(book_plan_create(ctx, e, n, cfg, true, &pl));
   cudaEventRecord(ctx->ev_start, ctx->stream);
   of_status st = of_book_plan_launch(pl);
   cudaEventRecord(ctx->ev_stop, ctx->stream);

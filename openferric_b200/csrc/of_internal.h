@@ -34,7 +34,14 @@ enum OfSlot {
   SLOT_LSM_PATHS_B = 16,   // second LSM buffer set: the next batch generates into it
   SLOT_LSM_VALUES_B = 17,  // while the current one runs its passes
   SLOT_LSM_AUX_B = 18,
-  SLOT_COUNT = 19
+  SLOT_BOOK_DIVS = 19,     // book plans run inside one call (of_mc_price_book, the SE driver):
+  SLOT_BOOK_GC = 20,       // their device tables and sums come from these slots
+  SLOT_BOOK_COUNTER = 21,
+  SLOT_BOOK_PARTIALS = 22,
+  SLOT_BOOK_BEGIN = 23,
+  SLOT_BOOK_SUMS = 24,
+  SLOT_BOOK_OBS = 25,
+  SLOT_COUNT = 26
 };
 
 struct of_ctx {
