@@ -63,12 +63,13 @@ SFU_PER_STEP = 5.0
 # the bench's kernel at 2^20 paths, by samples in flight per thread.  With the
 # sampled SM clock they give the issue fraction: warp instructions per second
 # over 148 SMs x 4 schedulers x 1 instruction per cycle.
-INSTR_PER_STEP = {1: 48.8, 2: 45.7}
-INSTR_SOURCE = "ncu smsp__inst_executed.sum of strip_kernel at 2^20 paths (profiles/strip_kernel_heston_euler_*)"
+INSTR_PER_STEP = {1: 48.8, 2: 40.0}
+INSTR_SOURCE = ("ncu smsp__inst_executed.sum of strip_kernel at 2^20 paths (profiles/strip_kernel_heston_euler_ilp2_2p20.md "
+                "for two samples per thread, profiles/strip_kernel_pipe_mix_2p20.md for one)")
 # DRAM bytes (read + write) of one strip launch from an ncu capture of the
 # kernel; the kernel reads no input from HBM, so the figure does not grow
 # with the path count.
-STRIP_DRAM_BYTES = 31488
+STRIP_DRAM_BYTES = 30720
 STRIP_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of strip_kernel<ILP=2> at 2^20 paths "
                      "(the kernel reads no HBM input; the figure does not grow with paths)")
 CONFIG = {"workload": "heston_euler_strike_strip", "paths": PATHS, "steps": STEPS, "strikes": 41,
@@ -431,7 +432,7 @@ def leg_config1(steps, warmup, peaks, threads):
 # ---------------------------------------------------------------------------
 # Issued thread instructions per path-step of book_kernel on the synthetic
 # mixed book, from the ncu capture of 256 options (profiles/book_kernel_book256.md).
-BOOK_INSTR_PER_STEP = 23.3
+BOOK_INSTR_PER_STEP = 19.8
 BOOK_SEED = 20261203
 
 

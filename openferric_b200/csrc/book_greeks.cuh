@@ -197,6 +197,9 @@ __device__ __forceinline__ void gk_discount(const GreekConsts<R>& c, R x, const 
 
 // ---- vanilla / terminal-only Asian: the path needs y_T only --------------
 template <typename R, bool G, bool ANTI>
+__device__ __forceinline__ void gk_terminal_finish(const GreekConsts<R>& c, R w, GreekSample<R>& out);
+
+template <typename R, bool G, bool ANTI>
 __device__ __forceinline__ void gk_terminal(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
                                             GreekSample<R>& out) {
   const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
@@ -214,6 +217,13 @@ __device__ __forceinline__ void gk_terminal(const GreekConsts<R>& c, uint64_t i,
     if (full + 1 < c.steps) w += z[1];
     if (full + 2 < c.steps) w += z[2];
   }
+  gk_terminal_finish<R, G, ANTI>(c, w, out);
+}
+
+// The payoff, control variate and discounted Greeks of a terminal-only
+// sample from the sum w of its normals (and -w for the antithetic twin).
+template <typename R, bool G, bool ANTI>
+__device__ __forceinline__ void gk_terminal_finish(const GreekConsts<R>& c, R w, GreekSample<R>& out) {
   const R base = (R)c.steps * c.alpha;
   const bool call = c.flags & GF_CALL;
   const bool floating = (c.flags & GF_TERMINAL_ONLY) && (c.flags & GF_FLOATING);
@@ -273,42 +283,11 @@ __device__ __forceinline__ void gk_observe(AsianLeg<R>& L, R w, R idx) {
   if (NEED_GEO) L.q = fma(w, L.y, L.q);
 }
 
-template <typename R, bool G, bool ANTI, bool DAILY, bool NEED_ARITH, bool NEED_GEO>
-__device__ __forceinline__ void gk_asian(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
-                                         const float* __restrict__ obs_w, GreekSample<R>& out) {
-  const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
-  AsianLeg<R> A{}, B{};
-  if (!DAILY) {  // an observation at t = 0: e^0 = 1, y = 0, i = 0
-    const R w0 = (R)__ldg(obs_w + c.obs_offset);
-    if (NEED_ARITH) A.p0 = B.p0 = w0;
-  }
-  R idx = (R)0;
-  auto step = [&](R z, int32_t j) {
-    idx += (R)1;
-    A.y = fma(c.beta, z, A.y + c.alpha);
-    if (ANTI) B.y = fma(-c.beta, z, B.y + c.alpha);
-    const R w = DAILY ? (R)1 : (R)__ldg(obs_w + c.obs_offset + j + 1);
-    if (DAILY || w != (R)0) {
-      gk_observe<R, G, NEED_ARITH, NEED_GEO>(A, w, idx);
-      if (ANTI) gk_observe<R, G, NEED_ARITH, NEED_GEO>(B, w, idx);
-    }
-  };
-  const int32_t full = c.steps & ~3;
-  for (int32_t j = 0; j < full; j += 4) {
-    R z[4];
-    gk_normals(c, (uint32_t)(j >> 2), lo, hi, K, z);
-    step(z[0], j);
-    step(z[1], j + 1);
-    step(z[2], j + 2);
-    step(z[3], j + 3);
-  }
-  if (full < c.steps) {
-    R z[4];
-    gk_normals(c, (uint32_t)(full >> 2), lo, hi, K, z);
-    step(z[0], full);
-    if (full + 1 < c.steps) step(z[1], full + 1);
-    if (full + 2 < c.steps) step(z[2], full + 2);
-  }
+// The payoff, control variate and discounted Greeks of an Asian sample from
+// its leg(s) (B is the antithetic twin when ANTI).
+template <typename R, bool G, bool ANTI, bool NEED_GEO>
+__device__ __forceinline__ void gk_asian_finish(const GreekConsts<R>& c, const AsianLeg<R>& A, const AsianLeg<R>& B,
+                                                GreekSample<R>& out) {
   const bool call = c.flags & GF_CALL;
   const bool floating = c.flags & GF_FLOATING;
   R xs = (R)0, ys = (R)0, gs[4] = {(R)0, (R)0, (R)0, (R)0};
@@ -362,6 +341,164 @@ __device__ __forceinline__ void gk_asian(const GreekConsts<R>& c, uint64_t i, co
   out.y = h * ys;
 #pragma unroll
   for (int t = 0; t < 4; ++t) out.g[t] = h * gs[t];
+}
+
+template <typename R, bool G, bool ANTI, bool DAILY, bool NEED_ARITH, bool NEED_GEO>
+__device__ __forceinline__ void gk_asian(const GreekConsts<R>& c, uint64_t i, const PhiloxKeys& K,
+                                         const float* __restrict__ obs_w, GreekSample<R>& out) {
+  const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
+  AsianLeg<R> A{}, B{};
+  if (!DAILY) {  // an observation at t = 0: e^0 = 1, y = 0, i = 0
+    const R w0 = (R)__ldg(obs_w + c.obs_offset);
+    if (NEED_ARITH) A.p0 = B.p0 = w0;
+  }
+  R idx = (R)0;
+  auto step = [&](R z, int32_t j) {
+    idx += (R)1;
+    A.y = fma(c.beta, z, A.y + c.alpha);
+    if (ANTI) B.y = fma(-c.beta, z, B.y + c.alpha);
+    const R w = DAILY ? (R)1 : (R)__ldg(obs_w + c.obs_offset + j + 1);
+    if (DAILY || w != (R)0) {
+      gk_observe<R, G, NEED_ARITH, NEED_GEO>(A, w, idx);
+      if (ANTI) gk_observe<R, G, NEED_ARITH, NEED_GEO>(B, w, idx);
+    }
+  };
+  const int32_t full = c.steps & ~3;
+  for (int32_t j = 0; j < full; j += 4) {
+    R z[4];
+    gk_normals(c, (uint32_t)(j >> 2), lo, hi, K, z);
+    step(z[0], j);
+    step(z[1], j + 1);
+    step(z[2], j + 2);
+    step(z[3], j + 3);
+  }
+  if (full < c.steps) {
+    R z[4];
+    gk_normals(c, (uint32_t)(full >> 2), lo, hi, K, z);
+    step(z[0], full);
+    if (full + 1 < c.steps) step(z[1], full + 1);
+    if (full + 2 < c.steps) step(z[2], full + 2);
+  }
+  gk_asian_finish<R, G, ANTI, NEED_GEO>(c, A, B, out);
+}
+
+// gk_terminal<float, G, ANTI> of samples i0 and i1: the normals' sums in
+// packed pairs (each half bit for bit the scalar sum).
+template <bool G, bool ANTI>
+__device__ __forceinline__ void gk_terminal_pair(const GreekConsts<float>& c, uint64_t i0, uint64_t i1,
+                                                 const PhiloxKeys& K, GreekSample<float>& o0, GreekSample<float>& o1) {
+  const uint32_t lo0 = (uint32_t)i0, hi0 = (uint32_t)(i0 >> 32), lo1 = (uint32_t)i1, hi1 = (uint32_t)(i1 >> 32);
+  float2 w = make_float2(0.0f, 0.0f);
+  for (int32_t j = 0; j < c.steps; j += 4) {
+    const uint4 r0 = philox4x32_10(make_uint4((uint32_t)(j >> 2), lo0, hi0, c.stream), K);
+    const uint4 r1 = philox4x32_10(make_uint4((uint32_t)(j >> 2), lo1, hi1, c.stream), K);
+    float2 a1, a2, a3, a4;  // the normals of steps j .. j+3 of (i0, i1)
+    normal_pairs_scaled2_from_u32(r0.x, r0.y, r1.x, r1.y, kBoxMullerK2, a1, a2);
+    normal_pairs_scaled2_from_u32(r0.z, r0.w, r1.z, r1.w, kBoxMullerK2, a3, a4);
+    if (j + 4 <= c.steps) {
+      w = add2(w, add2(add2(a1, a2), add2(a3, a4)));
+    } else {
+      w = add2(w, a1);
+      if (j + 1 < c.steps) w = add2(w, a2);
+      if (j + 2 < c.steps) w = add2(w, a3);
+    }
+  }
+  gk_terminal_finish<float, G, ANTI>(c, w.x, o0);
+  gk_terminal_finish<float, G, ANTI>(c, w.y, o1);
+}
+
+// ---- Asian legs in packed pairs (FP32) -------------------------------------
+// Two Asian legs per FP32 instruction: two samples, or a sample and its
+// antithetic twin.  Each half is gk_asian's arithmetic bit for bit.
+struct AsianLeg2 {
+  float2 y, p0, p0c, p1, p2, q;
+};
+
+template <bool G, bool NEED_ARITH, bool NEED_GEO>
+__device__ __forceinline__ void gk_observe2(AsianLeg2& L, float w, float idx) {
+  if (NEED_ARITH) {
+    const float2 e = mul2(splat2(w), make_float2(__expf(L.y.x), __expf(L.y.y)));
+    const float2 yk = sub2(e, L.p0c);
+    const float2 t = add2(L.p0, yk);
+    L.p0c = sub2(sub2(t, L.p0), yk);
+    L.p0 = t;
+    if (G) {
+      L.p1 = fma2(e, L.y, L.p1);
+      L.p2 = fma2(e, splat2(idx), L.p2);
+    }
+  }
+  if (NEED_GEO) L.q = fma2(splat2(w), L.y, L.q);
+}
+
+__device__ __forceinline__ AsianLeg<float> asian_half(const AsianLeg2& L, int e) {
+  AsianLeg<float> o;
+  o.y = e ? L.y.y : L.y.x;
+  o.p0 = e ? L.p0.y : L.p0.x;
+  o.p0c = e ? L.p0c.y : L.p0c.x;
+  o.p1 = e ? L.p1.y : L.p1.x;
+  o.p2 = e ? L.p2.y : L.p2.x;
+  o.q = e ? L.q.y : L.q.x;
+  return o;
+}
+
+// The step loop of gk_asian<float, G, ...> for two legs.  TWIN: sample i0 and
+// its antithetic twin (one stream, normals z and -z); otherwise samples i0
+// and i1.
+template <bool G, bool TWIN, bool DAILY, bool NEED_ARITH, bool NEED_GEO>
+__device__ __forceinline__ void gk_asian_legs2(const GreekConsts<float>& c, uint64_t i0, uint64_t i1,
+                                               const PhiloxKeys& K, const float* __restrict__ obs_w, AsianLeg2& L) {
+  const uint32_t lo0 = (uint32_t)i0, hi0 = (uint32_t)(i0 >> 32), lo1 = (uint32_t)i1, hi1 = (uint32_t)(i1 >> 32);
+  L = AsianLeg2{};
+  if (!DAILY) {
+    const float w0 = __ldg(obs_w + c.obs_offset);
+    if (NEED_ARITH) L.p0 = splat2(w0);
+  }
+  const float2 beta = TWIN ? make_float2(c.beta, -c.beta) : splat2(c.beta);
+  float idx = 0.0f;
+  auto step = [&](float2 z, int32_t j) {
+    idx += 1.0f;
+    L.y = fma2(beta, z, add2(L.y, splat2(c.alpha)));
+    const float w = DAILY ? 1.0f : __ldg(obs_w + c.obs_offset + j + 1);
+    if (DAILY || w != 0.0f) gk_observe2<G, NEED_ARITH, NEED_GEO>(L, w, idx);
+  };
+  for (int32_t j = 0; j < c.steps; j += 4) {
+    const uint4 r0 = philox4x32_10(make_uint4((uint32_t)(j >> 2), lo0, hi0, c.stream), K);
+    float2 w1, w2, w3, w4;
+    if (TWIN) {  // w1 = (z_j, z_j+2), w2 = (z_j+1, z_j+3)
+      normal_pairs_scaled2_from_u32(r0.x, r0.y, r0.z, r0.w, kBoxMullerK2, w1, w2);
+      w3 = splat2(w1.y);
+      w4 = splat2(w2.y);
+      w1 = splat2(w1.x);
+      w2 = splat2(w2.x);
+    } else {
+      const uint4 r1 = philox4x32_10(make_uint4((uint32_t)(j >> 2), lo1, hi1, c.stream), K);
+      normal_pairs_scaled2_from_u32(r0.x, r0.y, r1.x, r1.y, kBoxMullerK2, w1, w2);
+      normal_pairs_scaled2_from_u32(r0.z, r0.w, r1.z, r1.w, kBoxMullerK2, w3, w4);
+    }
+    step(w1, j);
+    if (j + 1 < c.steps) step(w2, j + 1);
+    if (j + 2 < c.steps) step(w3, j + 2);
+    if (j + 3 < c.steps) step(w4, j + 3);
+  }
+}
+
+template <bool G, bool DAILY, bool NEED_ARITH, bool NEED_GEO>
+__device__ __forceinline__ void gk_asian_twin(const GreekConsts<float>& c, uint64_t i, const PhiloxKeys& K,
+                                              const float* __restrict__ obs_w, GreekSample<float>& out) {
+  AsianLeg2 L;
+  gk_asian_legs2<G, true, DAILY, NEED_ARITH, NEED_GEO>(c, i, i, K, obs_w, L);
+  gk_asian_finish<float, G, true, NEED_GEO>(c, asian_half(L, 0), asian_half(L, 1), out);
+}
+
+template <bool G, bool DAILY, bool NEED_ARITH, bool NEED_GEO>
+__device__ __forceinline__ void gk_asian_pair(const GreekConsts<float>& c, uint64_t i0, uint64_t i1,
+                                              const PhiloxKeys& K, const float* __restrict__ obs_w,
+                                              GreekSample<float>& o0, GreekSample<float>& o1) {
+  AsianLeg2 L;
+  gk_asian_legs2<G, false, DAILY, NEED_ARITH, NEED_GEO>(c, i0, i1, K, obs_w, L);
+  const AsianLeg<float> a = asian_half(L, 0), b = asian_half(L, 1);
+  gk_asian_finish<float, G, false, NEED_GEO>(c, a, a, o0);
+  gk_asian_finish<float, G, false, NEED_GEO>(c, b, b, o1);
 }
 
 // ---- barrier: one-step survival -------------------------------------------
@@ -664,6 +801,18 @@ __device__ __forceinline__ void gk_sample_group_anti(const GreekConsts<R>& c, ui
   if (KG == KG_TERMINAL) {
     gk_terminal<R, G, ANTI>(c, i, K, out);
   } else if (KG == KG_ASIAN) {
+    if constexpr (std::is_same<R, float>::value && ANTI) {  // the twin legs in packed pairs
+      if (c.kind == GK_ASIAN_DAILY) {
+        if (c.flags & GF_GEOMETRIC) gk_asian_twin<G, true, false, true>(c, i, K, obs_w, out);
+        else if (c.cv_kind == GCV_GEOMETRIC_ASIAN) gk_asian_twin<G, true, true, true>(c, i, K, obs_w, out);
+        else gk_asian_twin<G, true, true, false>(c, i, K, obs_w, out);
+      } else {
+        if (c.flags & GF_GEOMETRIC) gk_asian_twin<G, false, false, true>(c, i, K, obs_w, out);
+        else if (c.cv_kind == GCV_GEOMETRIC_ASIAN) gk_asian_twin<G, false, true, true>(c, i, K, obs_w, out);
+        else gk_asian_twin<G, false, true, false>(c, i, K, obs_w, out);
+      }
+      return;
+    }
     if (c.kind == GK_ASIAN_DAILY) {
       if (c.flags & GF_GEOMETRIC) gk_asian<R, G, ANTI, true, false, true>(c, i, K, obs_w, out);
       else if (c.cv_kind == GCV_GEOMETRIC_ASIAN) gk_asian<R, G, ANTI, true, true, true>(c, i, K, obs_w, out);
@@ -681,6 +830,32 @@ __device__ __forceinline__ void gk_sample_group_anti(const GreekConsts<R>& c, ui
       if (c.kind == GK_BARRIER_OUT) gk_barrier<R, G, ANTI, false>(c, i, K, out);
       else gk_barrier<R, G, ANTI, true>(c, i, K, out);
     }
+  }
+}
+
+// Two samples of a terminal-only option (FP32 modes; antithetic twins are
+// the negated sum of the same normals).
+template <bool G>
+__device__ __forceinline__ void gk_terminal_pair_group(const GreekConsts<float>& c, uint64_t i0, uint64_t i1,
+                                                       const PhiloxKeys& K, GreekSample<float>& o0,
+                                                       GreekSample<float>& o1) {
+  if (c.flags & GF_ANTI) gk_terminal_pair<G, true>(c, i0, i1, K, o0, o1);
+  else gk_terminal_pair<G, false>(c, i0, i1, K, o0, o1);
+}
+
+// Two samples of an Asian option without antithetic twins (FP32 modes).
+template <bool G>
+__device__ __forceinline__ void gk_asian_pair_group(const GreekConsts<float>& c, uint64_t i0, uint64_t i1,
+                                                    const PhiloxKeys& K, const float* __restrict__ obs_w,
+                                                    GreekSample<float>& o0, GreekSample<float>& o1) {
+  if (c.kind == GK_ASIAN_DAILY) {
+    if (c.flags & GF_GEOMETRIC) gk_asian_pair<G, true, false, true>(c, i0, i1, K, obs_w, o0, o1);
+    else if (c.cv_kind == GCV_GEOMETRIC_ASIAN) gk_asian_pair<G, true, true, true>(c, i0, i1, K, obs_w, o0, o1);
+    else gk_asian_pair<G, true, true, false>(c, i0, i1, K, obs_w, o0, o1);
+  } else {
+    if (c.flags & GF_GEOMETRIC) gk_asian_pair<G, false, false, true>(c, i0, i1, K, obs_w, o0, o1);
+    else if (c.cv_kind == GCV_GEOMETRIC_ASIAN) gk_asian_pair<G, false, true, true>(c, i0, i1, K, obs_w, o0, o1);
+    else gk_asian_pair<G, false, true, false>(c, i0, i1, K, obs_w, o0, o1);
   }
 }
 

@@ -1240,17 +1240,21 @@ __global__ void __launch_bounds__(256, (KG == of::KG_BARRIER || !G) ? 2 : 3)
     const BookTile tile = P.tiles[t];
     const of::GreekConsts<R>& c = gc[tile.opt];
     GreekAcc<R, G> acc;
-    // FP32 barrier options without antithetic twins: two samples at a time in
-    // packed pairs (the sums take them in the same order)
-    const bool pairs = KG == of::KG_BARRIER && std::is_same<R, float>::value && !(c.flags & of::GF_ANTI);
+    // FP32: two samples at a time in packed pairs (terminal-only options, and
+    // Asian and barrier options without antithetic twins, whose twins pair
+    // inside one sample); the sums take them in the same order
+    constexpr bool kPairs = std::is_same<R, float>::value;
+    const bool pairs = kPairs && (KG == of::KG_TERMINAL || !(c.flags & of::GF_ANTI));
     for (int k = 0; k < P.ppt; ++k) {
       const int local = k * blockDim.x + threadIdx.x;
       if (local >= tile.count) break;
-      if constexpr (KG == of::KG_BARRIER && std::is_same<R, float>::value) {
+      if constexpr (kPairs) {
         if (pairs && k + 1 < P.ppt && local + (int)blockDim.x < tile.count) {
           of::GreekSample<float> v0, v1;
-          of::gk_barrier_pair_group<G>(c, (uint64_t)(tile.first + local), (uint64_t)(tile.first + local) + blockDim.x,
-                                       P.keys, v0, v1);
+          const uint64_t i0 = (uint64_t)(tile.first + local), i1 = i0 + blockDim.x;
+          if constexpr (KG == of::KG_BARRIER) of::gk_barrier_pair_group<G>(c, i0, i1, P.keys, v0, v1);
+          else if constexpr (KG == of::KG_ASIAN) of::gk_asian_pair_group<G>(c, i0, i1, P.keys, P.obs_w, v0, v1);
+          else of::gk_terminal_pair_group<G>(c, i0, i1, P.keys, v0, v1);
           acc.add(v0);
           acc.add(v1);
           ++k;
