@@ -785,7 +785,9 @@ struct BookOpt {
 // payoff reads: nothing per step (vanilla, terminal-only Asian), the barrier
 // test, or the daily-fixing arithmetic sum.  Everything else takes the
 // general loop.
-enum : int32_t { BK_GENERIC = 0, BK_TERMINAL = 1, BK_BARRIER = 2, BK_ASIAN_DAILY = 3 };
+// BK_ASIAN_DAILY_GEO: a daily-fixing arithmetic Asian that also carries the
+// geometric sum of its control variate.
+enum : int32_t { BK_GENERIC = 0, BK_TERMINAL = 1, BK_BARRIER = 2, BK_ASIAN_DAILY = 3, BK_ASIAN_DAILY_GEO = 4 };
 
 // A dividend trigger in log-spot form: after step `step`, a cash dividend
 // sets y = log(max(e^y - a, 0)) with a = D/S0; a proportional one adds
@@ -982,9 +984,13 @@ __device__ __forceinline__ void book_sample_gbm(const BookOpt& o, uint64_t i, co
     if (KIND == BK_BARRIER) {
       oa.hit |= sg * ya >= sgb;
       if (ANTI) ob.hit |= sg * yb >= sgb;
-    } else if (KIND == BK_ASIAN_DAILY) {
+    } else if (KIND == BK_ASIAN_DAILY || KIND == BK_ASIAN_DAILY_GEO) {
       add_fixing(oa, ya);
       if (ANTI) add_fixing(ob, yb);
+      if (KIND == BK_ASIAN_DAILY_GEO) {  // the general loop's fmaf(1, y, sum): one rounding
+        oa.geo_sum += ya;
+        if (ANTI) ob.geo_sum += yb;
+      }
     }
   };
   const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
@@ -1031,6 +1037,7 @@ __device__ __forceinline__ void book_gbm_legs2(const BookOpt& o, uint64_t i0, ui
   const float sg = (o.flags & BF_UP) ? 1.0f : -1.0f, sgb = sg * o.barrier_y;
   y = make_float2(0.0f, 0.0f);
   float2 as = make_float2(0.0f, 0.0f), ac = make_float2(0.0f, 0.0f);  // Kahan sums of the daily fixings
+  float2 ag = make_float2(0.0f, 0.0f);                                 // geometric sums
   bool ha = false, hb = false;
   if (KIND == BK_BARRIER) ha = hb = 0.0f >= sgb;  // the scan includes path[0]
   auto step = [&](float2 z) {
@@ -1039,11 +1046,12 @@ __device__ __forceinline__ void book_gbm_legs2(const BookOpt& o, uint64_t i0, ui
       const float2 t = mul2(splat2(sg), y);
       ha |= t.x >= sgb;
       hb |= t.y >= sgb;
-    } else if (KIND == BK_ASIAN_DAILY) {
+    } else if (KIND == BK_ASIAN_DAILY || KIND == BK_ASIAN_DAILY_GEO) {
       const float2 yk = sub2(make_float2(__expf(y.x), __expf(y.y)), ac);
       const float2 t = add2(as, yk);
       ac = sub2(sub2(t, as), yk);
       as = t;
+      if (KIND == BK_ASIAN_DAILY_GEO) ag = add2(ag, y);
     }
   };
   const uint32_t lo0 = (uint32_t)i0, hi0 = (uint32_t)(i0 >> 32), lo1 = (uint32_t)i1, hi1 = (uint32_t)(i1 >> 32);
@@ -1072,8 +1080,8 @@ __device__ __forceinline__ void book_gbm_legs2(const BookOpt& o, uint64_t i0, ui
       if (j + 2 < o.steps) step(w3);
     }
   }
-  oa = PathObs{as.x, ac.x, 0.0f, ha};
-  ob = PathObs{as.y, ac.y, 0.0f, hb};
+  oa = PathObs{as.x, ac.x, ag.x, ha};
+  ob = PathObs{as.y, ac.y, ag.y, hb};
 }
 
 // book_sample_gbm<KIND, false> of two samples in one packed loop.
@@ -1104,6 +1112,10 @@ __device__ __forceinline__ void book_dispatch(const BookOpt& o, uint64_t i, cons
     case BK_ASIAN_DAILY:
       if (anti) book_sample_gbm<BK_ASIAN_DAILY, true>(o, i, P.keys, x, y);
       else book_sample_gbm<BK_ASIAN_DAILY, false>(o, i, P.keys, x, y);
+      return;
+    case BK_ASIAN_DAILY_GEO:
+      if (anti) book_sample_gbm<BK_ASIAN_DAILY_GEO, true>(o, i, P.keys, x, y);
+      else book_sample_gbm<BK_ASIAN_DAILY_GEO, false>(o, i, P.keys, x, y);
       return;
     default:
       break;
@@ -1151,6 +1163,7 @@ __global__ void __launch_bounds__(256, 3) book_kernel(const __grid_constant__ Bo
         float x1, y1;
         if (o.kind == BK_TERMINAL) book_sample_gbm_pair<BK_TERMINAL>(o, i, i1, P.keys, x, y, x1, y1);
         else if (o.kind == BK_BARRIER) book_sample_gbm_pair<BK_BARRIER>(o, i, i1, P.keys, x, y, x1, y1);
+        else if (o.kind == BK_ASIAN_DAILY_GEO) book_sample_gbm_pair<BK_ASIAN_DAILY_GEO>(o, i, i1, P.keys, x, y, x1, y1);
         else book_sample_gbm_pair<BK_ASIAN_DAILY>(o, i, i1, P.keys, x, y, x1, y1);
         add(x, y);
         add(x1, y1);
@@ -1622,10 +1635,14 @@ static of_status book_plan_create(of_ctx* ctx, const of_book_entry* e, int64_t n
     if (asian && !need_arith && !need_geo) f |= BF_TERMINAL_ONLY;
     d.flags = f;
     d.kind = BK_GENERIC;
-    if (d.model == OF_MODEL_GBM && d.n_div == 0 && !need_geo) {
-      if (b.payoff.kind == OF_PAYOFF_VANILLA || (f & BF_TERMINAL_ONLY)) d.kind = BK_TERMINAL;
-      else if (b.payoff.kind == OF_PAYOFF_BARRIER) d.kind = BK_BARRIER;
-      else if (need_arith && (f & BF_DAILY)) d.kind = BK_ASIAN_DAILY;
+    if (d.model == OF_MODEL_GBM && d.n_div == 0) {
+      if (!need_geo) {
+        if (b.payoff.kind == OF_PAYOFF_VANILLA || (f & BF_TERMINAL_ONLY)) d.kind = BK_TERMINAL;
+        else if (b.payoff.kind == OF_PAYOFF_BARRIER) d.kind = BK_BARRIER;
+        else if (need_arith && (f & BF_DAILY)) d.kind = BK_ASIAN_DAILY;
+      } else if (need_arith && (f & BF_DAILY)) {  // with the geometric control variate
+        d.kind = BK_ASIAN_DAILY_GEO;
+      }
     }
     if (pl->mode != OF_BOOK_PRICE) {
       st = book_greek_consts(ctx, b, o, d, w, daily_obs, gcs[(size_t)o]);

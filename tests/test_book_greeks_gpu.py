@@ -205,3 +205,25 @@ def test_book_greeks_mode_matches_the_oracle_on_the_same_draws(anti):
         gg = g32[k].result.greeks
         for name, value, ref in zip(("delta", "vega", "rho", "theta"), (gg.delta, gg.vega, gg.rho, gg.theta), g):
             assert abs(value - ref) <= 1e-4 * abs(ref) + 2e-5, (kind, name, value, ref)
+
+
+@pytest.mark.parametrize("anti", [False, True])
+def test_price_mode_geometric_control_variate_matches_fp64_same_draws(anti):
+    """Daily-fixing arithmetic Asians priced with the geometric-Asian control
+    variate take a step loop specialised for them in the price mode (the
+    fixings' compensated sum and the log-spots' sum); the FP64 mode prices the
+    same draws with the same estimator, so the two agree to FP32 rounding, the
+    control-variate adjustment included."""
+    from dataclasses import replace
+    from openferric_b200.engines import VarianceReduction
+    from openferric_b200.instruments import AsianOption
+    book = [e for e in synthetic_book(n=30, seed=12, min_log2_paths=13, max_log2_paths=14)
+            if isinstance(e.instrument, AsianOption)]
+    book = [replace(e, variance_reduction=VarianceReduction.ControlVariate) for e in book]
+    if anti:  # the reference's ArithmeticAsianMC: antithetic pairs and the control variate
+        book = [replace(e, variance_reduction=VarianceReduction.Antithetic) for e in book[:3]] + book[3:]
+    p32 = price_book(book, seed=5)
+    p64 = price_book_fp64(book, seed=5)
+    for e, a, b in zip(book, p32, p64):
+        assert abs(a.price - b.price) <= 1e-4 * abs(b.price) + 1e-6, (e.instrument.strike, a.price, b.price)
+        assert abs(a.stderr - b.stderr) <= 1e-3 * b.stderr + 1e-8, (a.stderr, b.stderr)
