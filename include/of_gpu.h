@@ -313,24 +313,28 @@ typedef struct of_stderr_round {
 } of_stderr_round;
 
 /* A pilot launch prices every entry with target->pilot_paths paths
- * (entries[i].num_paths is ignored).  Every option above its target is then
- * priced again, all in one launch.  Its paths are scaled by
- * (stderr / target)^2 x 1.1 and rounded up to 256.  This repeats until all
- * meet the target or max_rounds launches have run.
- * Round r draws with seed cfg->seed + r.  cfg->block and
+ * (entries[i].num_paths is ignored).  Every option above its target then gets
+ * more paths, all in one launch: its total is scaled by (stderr / target)^2 x
+ * 1.1 and the launch runs the difference, rounded up to 256.  This repeats
+ * until all meet the target or max_rounds launches have run.
+ * Round r draws with seed cfg->seed + r (independent streams), and an option's
+ * estimate pools the samples of all its rounds: its running sums are added
+ * over the rounds, so the result is that of one run over all those samples
+ * (the control-variate coefficient estimated on all of them).  cfg->block and
  * cfg->paths_per_thread of 0 choose a tile shape with at most ~2^18 tiles per
  * launch; cfg->use_graph is ignored.
  * Outputs:
- *   results[i]   = option i's result from its last launch;
- *   paths_out[i] = that launch's path count (optional);
+ *   results[i]   = option i's pooled result (sums and samples over its rounds;
+ *                  kernel_ms of its last launch);
+ *   paths_out[i] = its total paths over its rounds (optional);
  *   rounds[r]    = round r's statistics (optional, capacity max_rounds);
  *   *n_rounds    = the launches run. */
 of_status of_book_price_to_stderr(of_ctx* ctx, const of_book_entry* entries, int64_t n, const of_book_config* cfg,
                                   const of_stderr_target* target, of_mc_result* results, int64_t* paths_out,
                                   of_stderr_round* rounds, int32_t* n_rounds);
 /* The same in mode OF_BOOK_GREEKS (cfg->mode is ignored): every option priced
- * to its standard-error target with its pathwise Greeks from the same launch
- * (greeks[i] from option i's last launch). */
+ * to its standard-error target with its pathwise Greeks from the same
+ * launches (greeks[i] pooled over option i's rounds like its price). */
 of_status of_book_price_to_stderr_greeks(of_ctx* ctx, const of_book_entry* entries, int64_t n,
                                          const of_book_config* cfg, const of_stderr_target* target,
                                          of_mc_result* results, of_book_greeks* greeks, int64_t* paths_out,

@@ -222,16 +222,16 @@ def price_book_to_stderr(entries: Sequence[BookEntry], seed: int, se_rel: float 
     (of_book_price_to_stderr).
 
     A pilot launch of the whole book with `pilot_paths` per option estimates
-    each option's standard error; every option above its target is priced
-    again, in one book launch, with the paths `paths_for_stderr` derives from
-    that estimate, and so on until all meet the target or `max_rounds`
-    launches have run.  Each round draws from its own seed (seed + round), and
-    an option's result is the one of its last round (its diagnostics carry
-    that round's path count).  Returns the results and the rounds.
+    each option's standard error; every option above its target gets more
+    paths, in one book launch (its total scaled by (SE/target)^2 x 1.1), and so
+    on until all meet the target or `max_rounds` launches have run.  Each round
+    draws from its own seed (seed + round), and an option's result pools the
+    samples of all its rounds (its diagnostics carry their total path count).
+    Returns the results and the rounds.
 
     greeks=True prices every launch with the pathwise Greeks
     (of_book_price_to_stderr_greeks): the results are then BookGreeksResult,
-    each option's Greeks from the launch of its price."""
+    each option's Greeks pooled over the same launches as its price."""
     ctx = context(device)
     n = len(entries)
     arr, keep, vols = book_entries_abi(entries)

@@ -141,3 +141,50 @@ def test_price_book_to_stderr_meets_the_target(mixed_vr):
     from openferric_b200 import PricingError
     with pytest.raises(PricingError, match="max_rounds"):
         price_book_to_stderr(book, seed=3, max_rounds=0)
+
+
+def test_price_book_to_stderr_pools_its_rounds():
+    """Each round draws from its own seed and an option's result pools the
+    running sums of all its rounds: replaying the rounds with plain book
+    launches (the same sub-books, seeds and path counts) and adding their sums
+    gives the driver's results."""
+    import math
+    from dataclasses import replace
+    from openferric_b200.book import BookPlan, price_book_to_stderr
+    book = synthetic_book(n=8, seed=8, min_log2_paths=10, max_log2_paths=11)
+    se_rel, pilot, seed = 2e-3, 2048, 3
+    res, rounds = price_book_to_stderr(book, seed=seed, se_rel=se_rel, pilot_paths=pilot)
+    assert len(rounds) >= 2  # the test needs at least one follow-up round
+    sums = [[0.0] * 5 for _ in book]
+    samples, paths = [0] * len(book), [0] * len(book)
+    pending, nxt = list(range(len(book))), {i: pilot for i in range(len(book))}
+    for r in range(len(rounds)):
+        sub = [replace(book[i], num_paths=nxt[i]) for i in pending]
+        plan = BookPlan(sub, seed + r, block=256, paths_per_thread=4, use_graph=False)  # the driver's tile shape here
+        try:
+            plan.launch()
+            raw = plan.raw_results()
+        finally:
+            plan.close()
+        still = []
+        for i, o in zip(pending, raw):
+            for k, f in enumerate(("sum_x", "sum_x2", "sum_y", "sum_xy", "sum_y2")):
+                sums[i][k] += getattr(o, f)
+            samples[i] += o.samples
+            paths[i] += nxt[i]
+            n = samples[i]
+            df = math.exp(-book[i].market.rate * book[i].instrument.expiry)
+            var = (sums[i][1] - sums[i][0] ** 2 / n) / (n - 1)
+            se = df * math.sqrt(var / n)
+            tgt = se_rel * book[i].market.spot
+            if se > tgt:
+                need = paths[i] * (se / tgt) ** 2 * 1.1
+                nxt[i] = max(256, math.ceil((need - paths[i]) / 256.0) * 256)
+                still.append(i)
+        pending = still
+    for i, (e, got) in enumerate(zip(book, res)):
+        n = samples[i]
+        df = math.exp(-e.market.rate * e.instrument.expiry)
+        price = df * sums[i][0] / n
+        assert abs(got.price - price) <= 1e-9 * abs(price) + 1e-12, (i, got.price, price)
+        assert int(got.diagnostics.get("num_paths")) == paths[i]
