@@ -175,6 +175,61 @@ __global__ void __launch_bounds__(128) mc_ref_kernel(RefParams P, double* __rest
     for (int k = 0; k < 5; ++k) partials[(int64_t)blockIdx.x * 5 + k] = acc[k];
 }
 
+// GBM European without dividends: the path matters only through S_T, a
+// product of per-step factors, so two adjacent lanes share a sample.  Both
+// step the sample's stream; lane p computes the normal and the factor
+// exp(fma(sigma sqrt(dt), z, drift)) of the steps j = p (mod 2), and the pair
+// multiplies its two partial products.  The draws and each step's factor are
+// mc_ref_kernel's; only the order of the product's roundings differs (S_T to
+// about 1e-15 relative).  Half the FP64 work per lane and twice the lanes
+// for the same samples: this workload has too few samples per SM to hide the
+// FP64 exp and divide latencies with one lane per sample.
+template <typename RNG>
+__global__ void __launch_bounds__(128) mc_ref_gbm_terminal(RefParams P, double* __restrict__ partials) {
+  __shared__ double sh[5 * 4];
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  const int lane = (int)(threadIdx.x & 31u), par = lane & 1;
+  const int64_t pair0 = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u)) >> 1;  // the warp's first sample
+  const int64_t stride = ((int64_t)gridDim.x * blockDim.x) >> 1;
+  for (int64_t base = pair0; base < P.samples; base += stride) {  // warp-uniform trip count
+    const int64_t i = base + (lane >> 1);
+    const bool valid = i < P.samples;
+    RNG rng;
+    rng.seed(P.seed + (uint64_t)i * 7919ULL);  // stream_seed, fast_rng.rs:203-205
+    double fa = 1.0, fb = 1.0;
+    // both lanes draw steps j and j+1 of the stream; each takes its own (no
+    // divergence: every lane runs the inverse normal and exp each iteration)
+    for (int64_t j = 0; j < P.steps; j += 2) {
+      const double u0 = rng.next_f64();
+      const double u1 = j + 1 < P.steps ? rng.next_f64() : 0.5;
+      if (j + par < P.steps) {
+        const double z = of::acklam_inv_cdf(par ? u1 : u0);
+        fa *= exp(fma(P.diffusion, z, P.drift));  // simulation.rs:67-71
+        if (P.antithetic) fb *= exp(fma(P.diffusion, -z, P.drift));
+      }
+    }
+    const double oa = __shfl_xor_sync(of::kFullMask, fa, 1);
+    const double ob = __shfl_xor_sync(of::kFullMask, fb, 1);
+    if (par == 0 && valid) {
+      Leg a{P.s0 * fa * oa, 0.0, 0.0, 0.0, false}, b{P.s0 * fb * ob, 0.0, 0.0, 0.0, false};
+      double x = vanilla(P.option_type, a.s, P.strike);
+      double y = leg_cv(a, P);
+      if (P.antithetic) {  // simulation.rs:235-252
+        x = 0.5 * (x + vanilla(P.option_type, b.s, P.strike));
+        y = 0.5 * (y + leg_cv(b, P));
+      }
+      acc[0] += x;
+      acc[1] += x * x;
+      acc[2] += y;
+      acc[3] += x * y;
+      acc[4] += y * y;
+    }
+  }
+  of::block_sum<5>(acc, sh);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 5; ++k) partials[(int64_t)blockIdx.x * 5 + k] = acc[k];
+}
+
 }  // namespace
 
 // Observation index of average_for_observations (mc_engine.rs:100-104):
@@ -360,9 +415,16 @@ extern "C" of_status of_mc_run(of_ctx* ctx, const of_model* m, const of_payoff* 
   }
 
   const int block = 128;
-  const void* kern = c->rng_kind == OF_RNG_PCG64 ? (const void*)mc_ref_kernel<of::Pcg64>
-                                                 : (const void*)mc_ref_kernel<of::Xoshiro256pp>;
-  const int64_t want = (P.samples + block - 1) / block;
+  // a GBM European without dividends (its control variate, if any, reads S_T
+  // only): two lanes per sample
+  const bool terminal = P.model == OF_MODEL_GBM && P.payoff == OF_PAYOFF_VANILLA && P.n_div == 0 && !P.inj &&
+                        P.cv_kind != OF_CV_GEOMETRIC_ASIAN;
+  const bool pcg = c->rng_kind == OF_RNG_PCG64;
+  const void* kern = terminal ? (pcg ? (const void*)mc_ref_gbm_terminal<of::Pcg64>
+                                     : (const void*)mc_ref_gbm_terminal<of::Xoshiro256pp>)
+                              : (pcg ? (const void*)mc_ref_kernel<of::Pcg64> : (const void*)mc_ref_kernel<of::Xoshiro256pp>);
+  const int64_t lanes = terminal ? 2 * P.samples : P.samples;
+  const int64_t want = (lanes + block - 1) / block;
   const int64_t cap = (int64_t)ctx->sm_count * of_blocks_per_sm(kern, block, 0);
   const int grid = (int)(want < cap ? want : cap);
   void *d_part = nullptr, *d_sums = nullptr, *h = nullptr;
@@ -371,7 +433,9 @@ extern "C" of_status of_mc_run(of_ctx* ctx, const of_model* m, const of_payoff* 
   OF_TRY(of_pinned(ctx, 5 * sizeof(double), &h));
 
   OF_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
-  if (c->rng_kind == OF_RNG_PCG64) mc_ref_kernel<of::Pcg64><<<grid, block, 0, ctx->stream>>>(P, (double*)d_part);
+  if (terminal && pcg) mc_ref_gbm_terminal<of::Pcg64><<<grid, block, 0, ctx->stream>>>(P, (double*)d_part);
+  else if (terminal) mc_ref_gbm_terminal<of::Xoshiro256pp><<<grid, block, 0, ctx->stream>>>(P, (double*)d_part);
+  else if (pcg) mc_ref_kernel<of::Pcg64><<<grid, block, 0, ctx->stream>>>(P, (double*)d_part);
   else mc_ref_kernel<of::Xoshiro256pp><<<grid, block, 0, ctx->stream>>>(P, (double*)d_part);
   OF_CUDA_TRY(ctx, cudaGetLastError());
   OF_TRY(of_reduce_rows(ctx, (const double*)d_part, grid, 5, (double*)d_sums));
