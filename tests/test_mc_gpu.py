@@ -154,7 +154,8 @@ def test_odd_path_count_and_single_sample(orc):
 
 @pytest.mark.parametrize("model", ["gbm", "heston"])
 @pytest.mark.parametrize("anti", [False, True])
-def test_fp64_pcg64_streams_match_oracle(orc, model, anti):
+@pytest.mark.parametrize("name", ["asian_arith_call", "put"])
+def test_fp64_pcg64_streams_match_oracle(orc, model, anti, name):
     """with_rng_kind(FastRngKind::Pcg64): every sample draws from
     Pcg64::seed_from_u64(stream_seed(seed, i)) (fast_rng.rs:86-128,
     simulation.rs:215-216); the FP64 engine equals the oracle's restatement,
@@ -162,7 +163,7 @@ def test_fp64_pcg64_streams_match_oracle(orc, model, anti):
     from openferric_b200.engines import FastRngKind
     T, steps, paths, seed = 1.0, 24, 3001, 1234
     gen = GENS[model](T, steps)
-    inst = _instruments(T)["asian_arith_call"]
+    inst = _instruments(T)[name]  # a GBM put takes the two-lanes-per-sample kernel
     gpu = MonteCarloEngine(paths, seed).with_antithetic(anti).with_rng_kind(FastRngKind.Pcg64).run_full(gen, inst, 0.97)
     ref = _oracle_run(orc, gen, inst, anti, None, 0.97, paths, seed, rng_kind=A.OF_RNG_PCG64)
     xo = MonteCarloEngine(paths, seed).with_antithetic(anti).run_full(gen, inst, 0.97)
