@@ -887,16 +887,11 @@ __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, floa
   const uint8_t* can = B.can_ex + (size_t)c * (B.steps + 1);
   F32Pass P;
   P.ex_now = can[t];
-  const int nb = (t + 1) & 1;  // betas of date t+1 were written by the previous pass
-  P.have_beta = (t + 1 < B.steps) && can[t + 1] && B.beta_ok[(size_t)nb * B.nc + c];
+  // S(t+1) is loaded whenever date t+1 may exercise; whether it does (betas
+  // fitted there) is known only once the previous pass has completed
+  const bool load1 = (t + 1 < B.steps) && can[t + 1];
+  P.have_beta = false;
   P.b0 = P.b1 = P.b2 = P.b3 = 0.0f;
-  if (P.have_beta) {
-    const double* bp = B.betas + ((size_t)nb * B.nc + c) * 4;
-    P.b0 = (float)bp[0];
-    P.b1 = (float)bp[1];
-    P.b2 = (float)bp[2];
-    P.b3 = (float)bp[3];
-  }
   const LsmStep* st = B.st + (size_t)c * (B.steps + 1);
   P.k1 = st[t + 1].fstrike;
   P.ik1 = st[t + 1].finv_strike;
@@ -907,25 +902,51 @@ __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, floa
   P.dl = (float)(disc - (double)P.dh);
   P.want_delta = B.want_delta != 0;
   const int n_chunks = (B.blocks - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
-  const uint32_t bytes = kChunkBytes * (1u + (P.have_beta ? 1u : 0u) + (P.ex_now ? 1u : 0u));
-  // stage layout: [S(t+1) | S(t) | V], kPathsPerBlock floats each
-  auto issue = [&](int j) {
+  const uint32_t bytes = kChunkBytes * (1u + (load1 ? 1u : 0u) + (P.ex_now ? 1u : 0u));
+  // stage layout: [S(t+1) | S(t) | V], kPathsPerBlock floats each.  The path
+  // columns (written by the generator, long complete) and the cash flows
+  // (written by the previous pass) are issued separately: see below.
+  auto issue_s = [&](int j) {
     const int s = j % kStages;
     const int64_t off = ((int64_t)blockIdx.x + (int64_t)j * gridDim.x) * kPathsPerBlock;
     float* dst = ring + (size_t)s * 3 * kPathsPerBlock;
     const uint32_t bar = of::smem_u32(full + s);
     of::mbar_arrive_expect_tx(bar, bytes);
-    if (P.have_beta) of::bulk_load(of::smem_u32(dst), gS1 + off, kChunkBytes, bar);
+    if (load1) of::bulk_load(of::smem_u32(dst), gS1 + off, kChunkBytes, bar);
     if (P.ex_now) of::bulk_load(of::smem_u32(dst + kPathsPerBlock), gS0 + off, kChunkBytes, bar);
-    of::bulk_load(of::smem_u32(dst + 2 * kPathsPerBlock), gV + off, kChunkBytes, bar);
+  };
+  auto issue_v = [&](int j) {
+    const int s = j % kStages;
+    const int64_t off = ((int64_t)blockIdx.x + (int64_t)j * gridDim.x) * kPathsPerBlock;
+    float* dst = ring + (size_t)s * 3 * kPathsPerBlock;
+    of::bulk_load(of::smem_u32(dst + 2 * kPathsPerBlock), gV + off, kChunkBytes, of::smem_u32(full + s));
+  };
+  auto issue = [&](int j) {
+    issue_s(j);
+    issue_v(j);
   };
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) of::mbar_init(of::smem_u32(full + s), 1);
     of::mbar_fence_init();
   }
   __syncthreads();
+  // The first chunks' path columns stream in while the previous date's pass
+  // finishes (it was launched with programmatic stream serialisation); its
+  // outputs (cash flows, betas) are read only after griddepcontrol.wait.
   if (threadIdx.x == 0)
-    for (int j = 0; j < kStages && j < n_chunks; ++j) issue(j);
+    for (int j = 0; j < kStages && j < n_chunks; ++j) issue_s(j);
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const int nb = (t + 1) & 1;  // betas of date t+1 were written by the previous pass
+  P.have_beta = load1 && B.beta_ok[(size_t)nb * B.nc + c];
+  if (P.have_beta) {
+    const double* bp = B.betas + ((size_t)nb * B.nc + c) * 4;
+    P.b0 = (float)bp[0];
+    P.b1 = (float)bp[1];
+    P.b2 = (float)bp[2];
+    P.b3 = (float)bp[3];
+  }
+  if (threadIdx.x == 0)
+    for (int j = 0; j < kStages && j < n_chunks; ++j) issue_v(j);
   unsigned n_ex = 0, n_itm = 0;
   float ext = PUT ? 0.0f : __int_as_float(0x7F800000);
   double mom[nm];
@@ -1011,15 +1032,17 @@ __device__ __forceinline__ void lsm_pass_f32_body(const LsmBatch& B, int t, floa
 template <int DEG>
 // Launched with programmatic stream serialisation: the next date's pass may
 // be scheduled while this one finishes (its last blocks reduce the moments
-// and solve for the betas); it waits here for this grid to complete and its
-// writes (betas, cash flows, flag rows) to be visible before it reads any.
+// and solve for the betas).  It issues its first path-column copies at once
+// and waits (griddepcontrol.wait, in the body) for this grid to complete and
+// its writes (betas, cash flows, flag rows) to be visible before it reads any.
 __global__ void __launch_bounds__(kPassThreads, 4) lsm_pass_f32(const __grid_constant__ LsmBatch B, int t) {
   __shared__ __align__(128) float ring[kStages * 3 * kPathsPerBlock];
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ double red_sh[kPassThreads];
   __shared__ double mom_sh[kMaxMoments];
   __shared__ double warp_mom[kPassThreads / 32 * 10];
-  asm volatile("griddepcontrol.wait;" ::: "memory");
+  // griddepcontrol.wait is in the body, after the loads that do not depend on
+  // the previous pass
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const bool put = B.c[blockIdx.y].put;
   if (B.track) {
