@@ -244,7 +244,10 @@ typedef struct of_book_entry {
  * OF_BOOK_PRICE_FP64: the prices of OF_BOOK_GREEKS in FP64 path arithmetic on
  *                     the same draws, for bump-and-revalue checks of the Greeks
  *                     with common random numbers. */
-enum { OF_BOOK_PRICE = 0, OF_BOOK_GREEKS = 1, OF_BOOK_PRICE_FP64 = 2 };
+/* OF_BOOK_GREEKS_FP64: the prices and pathwise Greeks of OF_BOOK_GREEKS in
+ *                     FP64 path arithmetic on the same draws: the FP32 mode's
+ *                     rounding apart, the same estimator. */
+enum { OF_BOOK_PRICE = 0, OF_BOOK_GREEKS = 1, OF_BOOK_PRICE_FP64 = 2, OF_BOOK_GREEKS_FP64 = 3 };
 
 typedef struct of_book_config {
   uint64_t seed;

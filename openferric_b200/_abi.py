@@ -108,6 +108,7 @@ class OfBookEntry(C.Structure):
 OF_BOOK_PRICE = 0
 OF_BOOK_GREEKS = 1
 OF_BOOK_PRICE_FP64 = 2
+OF_BOOK_GREEKS_FP64 = 3
 
 
 class OfBookConfig(C.Structure):

@@ -93,8 +93,9 @@ class BookPlan:
     """Device tables + CUDA graph for a book; launch() replays without a host sync.
 
     mode: A.OF_BOOK_PRICE (prices), A.OF_BOOK_GREEKS (prices and pathwise
-    Greeks; `greeks()` reads them) or A.OF_BOOK_PRICE_FP64 (the Greeks mode's
-    prices in FP64 on the same draws, for bump-and-revalue checks)."""
+    Greeks; `greeks_results()` reads them), A.OF_BOOK_PRICE_FP64 (the Greeks
+    mode's prices in FP64 on the same draws, for bump-and-revalue checks) or
+    A.OF_BOOK_GREEKS_FP64 (its prices and Greeks in FP64 on the same draws)."""
 
     def __init__(self, entries: Sequence[BookEntry], seed: int, block: int = 0, paths_per_thread: int = 0,
                  use_graph: bool = True, device: int = 0, mode: int = A.OF_BOOK_PRICE):
@@ -133,7 +134,7 @@ class BookPlan:
         return list(out)
 
     def greeks_results(self) -> List[BookGreeksResult]:
-        """Prices and Greeks of the last launch (mode OF_BOOK_GREEKS)."""
+        """Prices and Greeks of the last launch (mode OF_BOOK_GREEKS or OF_BOOK_GREEKS_FP64)."""
         out = []
         for r, g in zip(self.results(), self.raw_greeks()):
             r.greeks, se = _greeks_of(g)
@@ -169,6 +170,20 @@ def price_book_greeks(entries: Sequence[BookEntry], seed: int, block: int = 0, p
     discrete dividends; barrier options are priced by one-step survival (no
     control variate), the other payoffs by the book's own estimator."""
     plan = BookPlan(entries, seed, block, paths_per_thread, use_graph=False, device=device, mode=A.OF_BOOK_GREEKS)
+    try:
+        plan.launch()
+        return plan.greeks_results()
+    finally:
+        plan.close()
+
+
+def price_book_greeks_fp64(entries: Sequence[BookEntry], seed: int, block: int = 0, paths_per_thread: int = 0,
+                           device: int = 0) -> List[BookGreeksResult]:
+    """The prices and pathwise Greeks of `price_book_greeks` in FP64 path
+    arithmetic on the same draws (mode OF_BOOK_GREEKS_FP64): the same
+    estimator without the FP32 rounding."""
+    plan = BookPlan(entries, seed, block, paths_per_thread, use_graph=False, device=device,
+                    mode=A.OF_BOOK_GREEKS_FP64)
     try:
         plan.launch()
         return plan.greeks_results()

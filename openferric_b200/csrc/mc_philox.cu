@@ -1218,6 +1218,32 @@ struct GreekAcc<float, true> {
 };
 
 template <>
+struct GreekAcc<double, true> {
+  double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, g[4] = {0.0, 0.0, 0.0, 0.0}, g2[4] = {0.0, 0.0, 0.0, 0.0};
+  __device__ __forceinline__ void add(const of::GreekSample<double>& v) {
+    s[0] += v.x;
+    s[1] += v.x * v.x;
+    s[2] += v.y;
+    s[3] += v.x * v.y;
+    s[4] += v.y * v.y;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      g[t] += v.g[t];
+      g2[t] = fma(v.g[t], v.g[t], g2[t]);
+    }
+  }
+  __device__ __forceinline__ void values(double (&out)[13]) const {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = s[k];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      out[5 + t] = g[t];
+      out[9 + t] = g2[t];
+    }
+  }
+};
+
+template <>
 struct GreekAcc<double, false> {
   double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   __device__ __forceinline__ void add(const of::GreekSample<double>& v) {
@@ -1240,7 +1266,7 @@ struct GreekAcc<double, false> {
 // step of the barrier group needs the most registers: two blocks per SM;
 // the vanilla and Asian groups fit three.
 template <typename R, bool G, int KG>
-__global__ void __launch_bounds__(256, (KG == of::KG_BARRIER || !G) ? 2 : 3)
+__global__ void __launch_bounds__(256, (KG == of::KG_BARRIER || !G || sizeof(R) == 8) ? 2 : 3)
     book_greeks_kernel(const __grid_constant__ BookParams P, const of::GreekConsts<R>* __restrict__ gc) {
   constexpr int NC = G ? 13 : 5;
   __shared__ int tile_sh;
@@ -1459,6 +1485,7 @@ static const void* book_greeks_kernel_for(int kg) {
 static const void* book_kernel_for(int mode, int kg) {
   if (mode == OF_BOOK_GREEKS) return book_greeks_kernel_for<float, true>(kg);
   if (mode == OF_BOOK_PRICE_FP64) return book_greeks_kernel_for<double, false>(kg);
+  if (mode == OF_BOOK_GREEKS_FP64) return book_greeks_kernel_for<double, true>(kg);
   return (const void*)book_kernel;
 }
 
@@ -1483,6 +1510,9 @@ static void book_enqueue(of_book_plan* pl, cudaStream_t s) {
   } else if (pl->mode == OF_BOOK_PRICE_FP64) {
     book_greeks_enqueue<double, false>(pl, s);
     book_reduce_kernel<5><<<rgrid, 256, 0, s>>>(pl->d_partials, pl->d_begin, (int)pl->n, pl->d_sums);
+  } else if (pl->mode == OF_BOOK_GREEKS_FP64) {
+    book_greeks_enqueue<double, true>(pl, s);
+    book_reduce_kernel<13><<<rgrid, 256, 0, s>>>(pl->d_partials, pl->d_begin, (int)pl->n, pl->d_sums);
   } else {
     book_kernel<<<pl->grid, pl->block, 0, s>>>(pl->P);
     book_reduce_kernel<5><<<rgrid, 256, 0, s>>>(pl->d_partials, pl->d_begin, (int)pl->n, pl->d_sums);
@@ -1530,12 +1560,13 @@ static of_status book_plan_create(of_ctx* ctx, const of_book_entry* e, int64_t n
   pl->ppt = cfg->paths_per_thread > 0 ? cfg->paths_per_thread : 4;
   pl->use_graph = cfg->use_graph != 0;
   pl->mode = cfg->mode;
-  if (pl->mode != OF_BOOK_PRICE && pl->mode != OF_BOOK_GREEKS && pl->mode != OF_BOOK_PRICE_FP64) {
+  if (pl->mode != OF_BOOK_PRICE && pl->mode != OF_BOOK_GREEKS && pl->mode != OF_BOOK_PRICE_FP64 &&
+      pl->mode != OF_BOOK_GREEKS_FP64) {
     const int m = pl->mode;
     of_book_plan_destroy(pl);
     return of_fail(ctx, OF_ERR_INVALID_INPUT, "unknown book mode %d", m);
   }
-  pl->nc = pl->mode == OF_BOOK_GREEKS ? 13 : 5;
+  pl->nc = (pl->mode == OF_BOOK_GREEKS || pl->mode == OF_BOOK_GREEKS_FP64) ? 13 : 5;
   if (pl->block % 32 != 0 || pl->block > 256) {
     of_book_plan_destroy(pl);
     return of_fail(ctx, OF_ERR_INVALID_INPUT, "block must be a multiple of 32 and <= 256");
@@ -1707,7 +1738,7 @@ static of_status book_plan_create(of_ctx* ctx, const of_book_entry* e, int64_t n
       return fail(of_fail(ctx, OF_ERR_ALLOC, "book plan allocation failed"));
     if (cudaMemcpy(pl->d_gc, gf.data(), gf.size() * sizeof(gf[0]), cudaMemcpyHostToDevice) != cudaSuccess)
       return fail(of_fail(ctx, OF_ERR_CUDA, "book upload failed"));
-  } else if (pl->mode == OF_BOOK_PRICE_FP64) {
+  } else if (pl->mode == OF_BOOK_PRICE_FP64 || pl->mode == OF_BOOK_GREEKS_FP64) {
     if (!dalloc(&pl->d_gc, gcs.size() * sizeof(gcs[0]), SLOT_BOOK_GC))
       return fail(of_fail(ctx, OF_ERR_ALLOC, "book plan allocation failed"));
     if (cudaMemcpy(pl->d_gc, gcs.data(), gcs.size() * sizeof(gcs[0]), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -1790,8 +1821,8 @@ extern "C" of_status of_book_plan_results(of_book_plan* pl, of_mc_result* res) {
 
 extern "C" of_status of_book_plan_greeks(of_book_plan* pl, of_book_greeks* out) {
   if (!pl || !out) return OF_ERR_INVALID_INPUT;
-  if (pl->mode != OF_BOOK_GREEKS)
-    return of_fail(pl->ctx, OF_ERR_INVALID_INPUT, "the plan was not created in mode OF_BOOK_GREEKS");
+  if (pl->mode != OF_BOOK_GREEKS && pl->mode != OF_BOOK_GREEKS_FP64)
+    return of_fail(pl->ctx, OF_ERR_INVALID_INPUT, "the plan was not created in mode OF_BOOK_GREEKS(_FP64)");
   OF_CUDA_TRY(pl->ctx, cudaStreamSynchronize(pl->ctx->stream));
   for (int64_t o = 0; o < pl->n; ++o) {
     const double* s = pl->h_sums + o * pl->nc;

@@ -227,3 +227,33 @@ def test_price_mode_geometric_control_variate_matches_fp64_same_draws(anti):
     for e, a, b in zip(book, p32, p64):
         assert abs(a.price - b.price) <= 1e-4 * abs(b.price) + 1e-6, (e.instrument.strike, a.price, b.price)
         assert abs(a.stderr - b.stderr) <= 1e-3 * b.stderr + 1e-8, (a.stderr, b.stderr)
+
+
+@pytest.mark.parametrize("anti", [False, True])
+def test_fp64_greeks_mode_is_the_derivative_of_the_fp64_prices(anti):
+    """Mode OF_BOOK_GREEKS_FP64 runs the Greeks mode's estimator in FP64 on the
+    same draws: its pathwise Greeks are the derivatives of the FP64 prices
+    (central differences with common random numbers), to the differences'
+    own truncation and rounding, for every payoff kind; and the FP32 Greeks
+    are those numbers up to FP32 rounding."""
+    from openferric_b200.book import price_book_greeks_fp64
+    base = (BASE["spot"], BASE["vol"], BASE["rate"], 1.25)
+    seed = 20261205
+    g64 = price_book_greeks_fp64(_book(base, anti), seed)
+    g32 = price_book_greeks(_book(base, anti), seed)
+    h = 1e-5
+    for t, name in enumerate(("delta", "vega", "rho", "theta")):
+        up, dn = list(base), list(base)
+        up[t] *= 1.0 + h
+        dn[t] *= 1.0 - h
+        pu = price_book_fp64(_book(tuple(up), anti), seed)
+        pd = price_book_fp64(_book(tuple(dn), anti), seed)
+        for k, kind in enumerate(KINDS):
+            fd = (pu[k].price - pd[k].price) / (2.0 * h * base[t])
+            fd = -fd if name == "theta" else fd
+            v64, v32 = getattr(g64[k].result.greeks, name), getattr(g32[k].result.greeks, name)
+            # the payoff's kink crossed within the bump: O(h) in the difference
+            assert abs(v64 - fd) <= 1e-4 * abs(fd) + 1e-5, (kind, name, v64, fd)
+            assert abs(v32 - v64) <= 1e-3 * abs(v64) + 2e-4, (kind, name, v32, v64)
+    for k in range(len(KINDS)):
+        assert abs(g32[k].result.price - g64[k].result.price) <= 2e-5 * abs(g64[k].result.price) + 1e-6
