@@ -303,6 +303,8 @@ typedef struct of_stderr_target {
   int64_t pilot_paths;  /* paths per option in the first launch */
   int32_t max_rounds;   /* launches at most (1..64) */
   int32_t reserved0;
+  double margin;        /* a follow-up launch aims at (stderr / target)^2 x margin x the paths so far;
+                           0 = 1.05 */
 } of_stderr_target;
 
 /* One launch of of_book_price_to_stderr. */
@@ -318,7 +320,8 @@ typedef struct of_stderr_round {
 /* A pilot launch prices every entry with target->pilot_paths paths
  * (entries[i].num_paths is ignored).  Every option above its target then gets
  * more paths, all in one launch: its total is scaled by (stderr / target)^2 x
- * 1.1 and the launch runs the difference, rounded up to 256.  This repeats
+ * target->margin (1.05 by default) and the launch runs the difference, rounded
+ * up to 256.  This repeats
  * until all meet the target or max_rounds launches have run.
  * Round r draws with seed cfg->seed + r (independent streams), and an option's
  * estimate pools the samples of all its rounds: its running sums are added

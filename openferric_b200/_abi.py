@@ -132,6 +132,7 @@ class OfStderrTarget(C.Structure):
         ("pilot_paths", C.c_int64),
         ("max_rounds", C.c_int32),
         ("reserved0", C.c_int32),
+        ("margin", C.c_double),
     ]
 
 

@@ -222,9 +222,10 @@ class StderrRound:
 def paths_for_stderr(paths: int, stderr: float, target: float, margin: float = 1.1, granule: int = 256) -> int:
     """Paths that bring a standard error measured with `paths` down to
     `target` (stderr scales as paths^-1/2), with a safety margin, rounded up to
-    a multiple of `granule`; never fewer than `paths`.  The rule
-    of_book_price_to_stderr applies between rounds (margin 1.1, granule 256),
-    for planning a book's cost on the host."""
+    a multiple of `granule`; never fewer than `paths`: the total that
+    of_book_price_to_stderr aims at for an option after a round (where the
+    follow-up launch runs the difference), for planning a book's cost on the
+    host."""
     if not (stderr > target):
         return paths
     need = paths * (stderr / target) ** 2 * margin
@@ -232,13 +233,14 @@ def paths_for_stderr(paths: int, stderr: float, target: float, margin: float = 1
 
 
 def price_book_to_stderr(entries: Sequence[BookEntry], seed: int, se_rel: float = 1e-4, pilot_paths: int = 8192,
-                         max_rounds: int = 4, device: int = 0, greeks: bool = False):
+                         max_rounds: int = 4, device: int = 0, greeks: bool = False, margin: float = 0.0):
     """Prices every entry to a standard error of at most `se_rel` x its spot
     (of_book_price_to_stderr).
 
     A pilot launch of the whole book with `pilot_paths` per option estimates
     each option's standard error; every option above its target gets more
-    paths, in one book launch (its total scaled by (SE/target)^2 x 1.1), and so
+    paths, in one book launch (its total scaled by (SE/target)^2 x `margin`,
+    0 = the default 1.05), and so
     on until all meet the target or `max_rounds` launches have run.  Each round
     draws from its own seed (seed + round), and an option's result pools the
     samples of all its rounds (its diagnostics carry their total path count).
@@ -251,7 +253,8 @@ def price_book_to_stderr(entries: Sequence[BookEntry], seed: int, se_rel: float 
     n = len(entries)
     arr, keep, vols = book_entries_abi(entries)
     cfg = A.OfBookConfig(seed=int(seed) & 0xFFFFFFFFFFFFFFFF)
-    tgt = A.OfStderrTarget(se_rel=float(se_rel), pilot_paths=int(pilot_paths), max_rounds=int(max_rounds))
+    tgt = A.OfStderrTarget(se_rel=float(se_rel), pilot_paths=int(pilot_paths), max_rounds=int(max_rounds),
+                           margin=float(margin))
     out = (A.OfMcResult * n)()
     paths = (C.c_int64 * n)()
     rounds = (A.OfStderrRound * max(1, int(max_rounds)))()

@@ -13,10 +13,10 @@
 namespace {
 
 // Total paths that bring a standard error measured over `paths` down to
-// `target` (stderr ~ paths^-1/2), with a 10 % margin; the next round runs the
+// `target` (stderr ~ paths^-1/2), times `margin`; the next round runs the
 // difference, rounded up to a multiple of 256 (at least 256).
-int64_t more_paths_for_stderr(int64_t paths, double se, double target) {
-  const double need = (double)paths * (se / target) * (se / target) * 1.1;
+int64_t more_paths_for_stderr(int64_t paths, double se, double target, double margin) {
+  const double need = (double)paths * (se / target) * (se / target) * margin;
   const int64_t more = (int64_t)std::ceil((need - (double)paths) / 256.0) * 256;
   return more > 256 ? more : 256;
 }
@@ -49,6 +49,9 @@ static of_status price_to_stderr(of_ctx* ctx, const of_book_entry* entries, int6
   if (target->pilot_paths <= 0) return of_fail(ctx, OF_ERR_INVALID_INPUT, "pilot_paths must be > 0");
   if (target->max_rounds <= 0 || target->max_rounds > 64)
     return of_fail(ctx, OF_ERR_INVALID_INPUT, "max_rounds must be in 1..64");
+  if (!(target->margin >= 0.0) || !std::isfinite(target->margin) || (target->margin > 0.0 && target->margin < 1.0))
+    return of_fail(ctx, OF_ERR_INVALID_INPUT, "margin must be 0 (default) or finite and >= 1");
+  const double margin = target->margin > 0.0 ? target->margin : 1.05;
   std::vector<of_book_entry> cur(entries, entries + n);
   for (of_book_entry& e : cur) e.num_paths = target->pilot_paths;
   std::vector<Pool> pool((size_t)n);
@@ -129,7 +132,7 @@ static of_status price_to_stderr(of_ctx* ctx, const of_book_entry* entries, int6
       }
       const double tgt = target->se_rel * e.model.s0;
       if (results[i].stderr_ > tgt) {
-        cur[(size_t)i].num_paths = more_paths_for_stderr(p.paths, results[i].stderr_, tgt);
+        cur[(size_t)i].num_paths = more_paths_for_stderr(p.paths, results[i].stderr_, tgt, margin);
         still.push_back(i);
       }
     }

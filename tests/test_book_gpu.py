@@ -141,6 +141,13 @@ def test_price_book_to_stderr_meets_the_target(mixed_vr):
     from openferric_b200 import PricingError
     with pytest.raises(PricingError, match="max_rounds"):
         price_book_to_stderr(book, seed=3, max_rounds=0)
+    with pytest.raises(PricingError, match="margin"):
+        price_book_to_stderr(book, seed=3, margin=0.5)
+    # the same pilot (same seed) sends the same options to the first follow-up;
+    # a larger margin gives them more paths
+    _, wide = price_book_to_stderr(book, seed=3, se_rel=2e-3, pilot_paths=2048, margin=1.5)
+    assert wide[0].paths == rounds[0].paths and wide[1].options == rounds[1].options
+    assert wide[1].paths > rounds[1].paths
 
 
 def test_price_book_to_stderr_pools_its_rounds():
@@ -152,8 +159,8 @@ def test_price_book_to_stderr_pools_its_rounds():
     from dataclasses import replace
     from openferric_b200.book import BookPlan, price_book_to_stderr
     book = synthetic_book(n=8, seed=8, min_log2_paths=10, max_log2_paths=11)
-    se_rel, pilot, seed = 2e-3, 2048, 3
-    res, rounds = price_book_to_stderr(book, seed=seed, se_rel=se_rel, pilot_paths=pilot)
+    se_rel, pilot, seed, margin = 2e-3, 2048, 3, 1.1
+    res, rounds = price_book_to_stderr(book, seed=seed, se_rel=se_rel, pilot_paths=pilot, margin=margin)
     assert len(rounds) >= 2  # the test needs at least one follow-up round
     sums = [[0.0] * 5 for _ in book]
     samples, paths = [0] * len(book), [0] * len(book)
@@ -178,7 +185,7 @@ def test_price_book_to_stderr_pools_its_rounds():
             se = df * math.sqrt(var / n)
             tgt = se_rel * book[i].market.spot
             if se > tgt:
-                need = paths[i] * (se / tgt) ** 2 * 1.1
+                need = paths[i] * (se / tgt) ** 2 * margin
                 nxt[i] = max(256, math.ceil((need - paths[i]) / 256.0) * 256)
                 still.append(i)
         pending = still
