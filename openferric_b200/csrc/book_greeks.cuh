@@ -506,8 +506,8 @@ template <typename R, bool G>
 struct SurvLeg {
   R y, L;    // log-return of the conditioned path and its survival weight
   R ypl;     // knock-in: the unconditioned path of the same uniforms
-  R yd[4];   // tangents of y along (ln S0, sigma, r, T)
-  R ld[4];   // tangents of ln L
+  R e[3];    // tangent basis (u, y, z of surv_step, each times sib)
+  R le[3];   // the matching sums for ln L
 };
 
 template <typename R, bool G>
@@ -515,8 +515,10 @@ __device__ __forceinline__ void surv_init(SurvLeg<R, G>& s, const GreekConsts<R>
   s.y = (R)0;
   s.ypl = (R)0;
   s.L = c.sgn * c.bar > (R)0 ? (R)1 : (R)0;  // the scan includes path[0]: a spot already beyond the barrier is out
+  s.e[0] = s.e[1] = c.sib;
+  s.e[2] = (R)0;
 #pragma unroll
-  for (int t = 0; t < 4; ++t) s.yd[t] = s.ld[t] = (R)0;
+  for (int t = 0; t < 3; ++t) s.le[t] = (R)0;
 }
 
 // One step: h = sgn (bar - y - alpha) / beta is the standardised distance to
@@ -532,9 +534,22 @@ __device__ __forceinline__ void surv_init(SurvLeg<R, G>& s, const GreekConsts<R>
 // draw lands at the barrier (u -> 1, zeta -> h), the steps whose w ~ 1 carries
 // the barrier's sensitivity into y', so that w keeps its relative precision
 // there; the relative error of w adds up over the steps near the barrier.
+//
+// The four parameters share one linear recursion.  With sib = sgn / beta,
+// A = b' - alpha' and B = -beta' / beta, the parameter's e = A - y' obeys
+//   h' = sib e + B h,   e_next = (1 - w) e + B beta sgn (zeta - w h) - alpha',
+// and here alpha' = -A for sigma, r and T (the barrier does not move with
+// them), while ln S0 has A = -1 and alpha' = B = 0.  So every e is a fixed
+// combination of three sequences, kept scaled by sib:
+//   u_next = (1 - w) u,                 u_0 = sib   (ln S0: e = -u / sib)
+//   y_next = (1 - w) y + sib,           y_0 = sib   (e = A y / sib + B z / sib)
+//   z_next = (1 - w) z + zeta - w h,    z_0 = 0
+// with (ln L)' = -sum g u (ln S0) or A sum g y + B sum g (z + h): six running
+// values in place of eight, and no per-parameter arithmetic in the step.
+// surv_tangents turns them into y' and (ln L)' for the payoff.
 template <typename R, bool G, bool IN>
 __device__ __forceinline__ void surv_step(SurvLeg<R, G>& s, const GreekConsts<R>& c, R u) {
-  R h = c.sib * (c.bar - s.y - c.alpha);
+  R h = fma(-c.sib, s.y, c.sib * (c.bar - c.alpha));
   h = h > GMath<R>::kHMin ? h : GMath<R>::kHMin;
   R p, g;  // Phi(h) and phi(h) / Phi(h)
   GMath<R>::cdf_ratio(h, p, g);
@@ -543,30 +558,40 @@ __device__ __forceinline__ void surv_step(SurvLeg<R, G>& s, const GreekConsts<R>
   v = v > GMath<R>::kTiny ? v : GMath<R>::kTiny;
   q = q > GMath<R>::kTiny ? q : GMath<R>::kTiny;
   const R zeta = GMath<R>::icdf2(v, q);
-  const R z = c.sgn * zeta;
   if (G) {
-    const R w = u * GMath<R>::exp((R)0.5 * (zeta - h) * (zeta + h));
-    const R k = c.beta * c.sgn * w;  // d y_next / d h
-    // ln S0: b' = -1
-    const R h0 = c.sib * ((R)-1 - s.yd[0]);
-    s.ld[0] = fma(g, h0, s.ld[0]);
-    s.yd[0] = fma(k, h0, s.yd[0]);
-    // sigma: alpha' = -sigma dt, beta' / beta = 1 / sigma
-    const R h1 = fma(c.sib, c.sig_dt - s.yd[1], -h * c.inv_sig);
-    s.ld[1] = fma(g, h1, s.ld[1]);
-    s.yd[1] = fma(k, h1, s.yd[1] + fma(c.beta_over_sig, z, -c.sig_dt));
-    // r: alpha' = dt
-    const R h2 = c.sib * (-c.dt - s.yd[2]);
-    s.ld[2] = fma(g, h2, s.ld[2]);
-    s.yd[2] = fma(k, h2, s.yd[2] + c.dt);
-    // T (steps fixed): alpha' = alpha / T, beta' / beta = 1 / (2T)
-    const R h3 = fma(c.sib, -c.alpha_over_T - s.yd[3], -h * c.inv_2T);
-    s.ld[3] = fma(g, h3, s.ld[3]);
-    s.yd[3] = fma(k, h3, s.yd[3] + fma(c.beta_over_2T, z, c.alpha_over_T));
+    const R zmh = zeta - h;
+    const R w = u * GMath<R>::exp((R)0.5 * zmh * (zeta + h));
+    const R kap = (R)1 - w;
+    s.le[0] = fma(g, s.e[0], s.le[0]);
+    s.le[1] = fma(g, s.e[1], s.le[1]);
+    s.le[2] = fma(g, s.e[2] + h, s.le[2]);
+    s.e[0] = kap * s.e[0];
+    s.e[1] = fma(kap, s.e[1], c.sib);
+    s.e[2] = fma(kap, s.e[2], fma(kap, h, zmh));  // zeta - w h = (zeta - h) + (1 - w) h
   }
-  s.y = fma(c.beta, z, s.y + c.alpha);
+  s.y = fma(c.beta * c.sgn, zeta, s.y + c.alpha);
   s.L *= p;
   if (IN) s.ypl = fma(c.beta, GMath<R>::icdf2(u, (R)1 - u), s.ypl + c.alpha);
+}
+
+// y' and (ln L)' along (ln S0, sigma, r, T) from the tangent basis: with
+// A = (-1, sigma dt, -dt, -alpha / T), B = (0, -1 / sigma, 0, -1 / (2T)) and
+// the basis unscaled by beta sgn = 1 / sib,
+//   ln S0: y' = u - 1, (ln L)' = -lu;   others: y' = A (1 - y) - B z,
+//   (ln L)' = A ly + B lz.
+template <typename R, bool G>
+__device__ __forceinline__ void surv_tangents(const SurvLeg<R, G>& s, const GreekConsts<R>& c, R (&yd)[4],
+                                              R (&ld)[4]) {
+  const R bs = c.beta * c.sgn;
+  const R uu = bs * s.e[0], yy = (R)1 - bs * s.e[1], zz = bs * s.e[2];
+  yd[0] = uu - (R)1;
+  ld[0] = -s.le[0];
+  yd[1] = fma(c.sig_dt, yy, c.inv_sig * zz);
+  ld[1] = fma(c.sig_dt, s.le[1], -c.inv_sig * s.le[2]);
+  yd[2] = -c.dt * yy;
+  ld[2] = -c.dt * s.le[1];
+  yd[3] = fma(-c.alpha_over_T, yy, c.inv_2T * zz);
+  ld[3] = fma(-c.alpha_over_T, s.le[1], -c.inv_2T * s.le[2]);
 }
 
 template <typename R, bool G, bool IN>
@@ -574,17 +599,19 @@ __device__ __forceinline__ void surv_payoff(const SurvLeg<R, G>& s, const GreekC
   const bool call = c.flags & GF_CALL;
   R ds[4], dk[4] = {(R)0, (R)0, (R)0, (R)0}, dfo[4], dx[4];
   const R so = c.s0 * GMath<R>::exp(s.y);
+  R yd[4], ld[4];
   if (G) {  // S = s0 e^y with y depending on ln S0 through the barrier: dS/dlnS0 = S (1 + y')
-    ds[0] = so * ((R)1 + s.yd[0]);
+    surv_tangents(s, c, yd, ld);
+    ds[0] = so * ((R)1 + yd[0]);
 #pragma unroll
-    for (int t = 1; t < 4; ++t) ds[t] = so * s.yd[t];
+    for (int t = 1; t < 4; ++t) ds[t] = so * yd[t];
   }
   const R fo = gk_vanilla<R, G>(call, so, c.strike, ds, dk, dfo);
   if (!IN) {
     x = s.L * fo + ((R)1 - s.L) * c.rebate;  // L f + (1 - L) R
     if (G) {
 #pragma unroll
-      for (int t = 0; t < 4; ++t) dx[t] = s.L * fma(s.ld[t], fo - c.rebate, dfo[t]);
+      for (int t = 0; t < 4; ++t) dx[t] = s.L * fma(ld[t], fo - c.rebate, dfo[t]);
     }
   } else {
     R dp[4], dfp[4];
@@ -593,7 +620,7 @@ __device__ __forceinline__ void surv_payoff(const SurvLeg<R, G>& s, const GreekC
     x = fp - s.L * (fo - c.rebate);  // f(S') - L (f(S) - R)
     if (G) {
 #pragma unroll
-      for (int t = 0; t < 4; ++t) dx[t] = dfp[t] - s.L * fma(s.ld[t], fo - c.rebate, dfo[t]);
+      for (int t = 0; t < 4; ++t) dx[t] = dfp[t] - s.L * fma(ld[t], fo - c.rebate, dfo[t]);
     }
   }
   if (G) gk_discount(c, x, dx, g);
@@ -650,7 +677,7 @@ __host__ __device__ __forceinline__ int gk_group(int kind) {
 // stay scalar per half.
 struct SurvLeg2 {
   float2 y, L, ypl;
-  float2 yd[4], ld[4];
+  float2 e[3], le[3];
 };
 
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
@@ -679,14 +706,16 @@ __device__ __forceinline__ void surv_init2(SurvLeg2& s, const GreekConsts<float>
   s.y = s.ypl = make_float2(0.0f, 0.0f);
   s.L = splat2(c.sgn * c.bar > 0.0f ? 1.0f : 0.0f);
 #pragma unroll
-  for (int t = 0; t < 4; ++t) s.yd[t] = s.ld[t] = make_float2(0.0f, 0.0f);
+  for (int t = 0; t < 3; ++t) s.le[t] = make_float2(0.0f, 0.0f);
+  s.e[0] = s.e[1] = splat2(c.sib);
+  s.e[2] = make_float2(0.0f, 0.0f);
 }
 
 // surv_step<float, G, IN> of both halves
 template <bool G, bool IN>
 __device__ __forceinline__ void surv_step2(SurvLeg2& s, const GreekConsts<float>& c, float2 u) {
   using M = GMath<float>;
-  float2 h = mul2(splat2(c.sib), sub2(sub2(splat2(c.bar), s.y), splat2(c.alpha)));
+  float2 h = fma2(splat2(-c.sib), s.y, splat2(c.sib * (c.bar - c.alpha)));
   h.x = h.x > M::kHMin ? h.x : M::kHMin;
   h.y = h.y > M::kHMin ? h.y : M::kHMin;
   float2 p, g;
@@ -698,25 +727,19 @@ __device__ __forceinline__ void surv_step2(SurvLeg2& s, const GreekConsts<float>
   q.x = q.x > M::kTiny ? q.x : M::kTiny;
   q.y = q.y > M::kTiny ? q.y : M::kTiny;
   const float2 zeta = make_float2(M::icdf2(v.x, q.x), M::icdf2(v.y, q.y));
-  const float2 z = mul2(splat2(c.sgn), zeta);
   if (G) {
-    const float2 d = mul2(mul2(splat2(0.5f), sub2(zeta, h)), add2(zeta, h));
+    const float2 zmh = sub2(zeta, h);
+    const float2 d = mul2(mul2(splat2(0.5f), zmh), add2(zeta, h));
     const float2 w = mul2(u, make_float2(__expf(d.x), __expf(d.y)));
-    const float2 k = mul2(splat2(c.beta * c.sgn), w);
-    const float2 h0 = mul2(splat2(c.sib), sub2(splat2(-1.0f), s.yd[0]));
-    s.ld[0] = fma2(g, h0, s.ld[0]);
-    s.yd[0] = fma2(k, h0, s.yd[0]);
-    const float2 h1 = fma2(splat2(c.sib), sub2(splat2(c.sig_dt), s.yd[1]), mul2(neg2(h), splat2(c.inv_sig)));
-    s.ld[1] = fma2(g, h1, s.ld[1]);
-    s.yd[1] = fma2(k, h1, add2(s.yd[1], fma2(splat2(c.beta_over_sig), z, splat2(-c.sig_dt))));
-    const float2 h2 = mul2(splat2(c.sib), sub2(splat2(-c.dt), s.yd[2]));
-    s.ld[2] = fma2(g, h2, s.ld[2]);
-    s.yd[2] = fma2(k, h2, add2(s.yd[2], splat2(c.dt)));
-    const float2 h3 = fma2(splat2(c.sib), sub2(splat2(-c.alpha_over_T), s.yd[3]), mul2(neg2(h), splat2(c.inv_2T)));
-    s.ld[3] = fma2(g, h3, s.ld[3]);
-    s.yd[3] = fma2(k, h3, add2(s.yd[3], fma2(splat2(c.beta_over_2T), z, splat2(c.alpha_over_T))));
+    const float2 kap = sub2(splat2(1.0f), w);
+    s.le[0] = fma2(g, s.e[0], s.le[0]);
+    s.le[1] = fma2(g, s.e[1], s.le[1]);
+    s.le[2] = fma2(g, add2(s.e[2], h), s.le[2]);
+    s.e[0] = mul2(kap, s.e[0]);
+    s.e[1] = fma2(kap, s.e[1], splat2(c.sib));
+    s.e[2] = fma2(kap, s.e[2], fma2(kap, h, zmh));
   }
-  s.y = fma2(splat2(c.beta), z, add2(s.y, splat2(c.alpha)));
+  s.y = fma2(splat2(c.beta * c.sgn), zeta, add2(s.y, splat2(c.alpha)));
   s.L = mul2(s.L, p);
   if (IN) {
     const float2 zp = make_float2(M::icdf2(u.x, 1.0f - u.x), M::icdf2(u.y, 1.0f - u.y));
@@ -732,9 +755,9 @@ __device__ __forceinline__ SurvLeg<float, G> surv_half(const SurvLeg2& s, int e)
   o.L = e ? s.L.y : s.L.x;
   o.ypl = e ? s.ypl.y : s.ypl.x;
 #pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    o.yd[t] = e ? s.yd[t].y : s.yd[t].x;
-    o.ld[t] = e ? s.ld[t].y : s.ld[t].x;
+  for (int t = 0; t < 3; ++t) {
+    o.e[t] = e ? s.e[t].y : s.e[t].x;
+    o.le[t] = e ? s.le[t].y : s.le[t].x;
   }
   return o;
 }
