@@ -1262,11 +1262,13 @@ struct GreekAcc<double, false> {
 // The book's Greeks modes: the persistent tile loop of book_kernel over the
 // per-sample kernels of book_greeks.cuh, one launch per kind group (the
 // group's tiles only).  <float, true>: prices and pathwise Greeks (13 sums
-// per tile); <double, false>: FP64 prices on the same draws.  The survival
-// step of the barrier group needs the most registers: two blocks per SM;
-// the vanilla and Asian groups fit three.
+// per tile); <double, false>: FP64 prices on the same draws.  FP32 Greeks:
+// the terminal group at four blocks per SM (64 registers), the Asian and
+// survival-barrier groups at three (the survival step's 91 registers capped
+// at 80, with a 4-byte spill: 351 ms for the 4096-option book against
+// 368 ms at two blocks); the FP64 modes at two.
 template <typename R, bool G, int KG>
-__global__ void __launch_bounds__(256, (KG == of::KG_BARRIER || !G || sizeof(R) == 8) ? 2 : 3)
+__global__ void __launch_bounds__(256, (!G || sizeof(R) == 8) ? 2 : (KG == of::KG_TERMINAL ? 4 : 3))
     book_greeks_kernel(const __grid_constant__ BookParams P, const of::GreekConsts<R>* __restrict__ gc) {
   constexpr int NC = G ? 13 : 5;
   __shared__ int tile_sh;
