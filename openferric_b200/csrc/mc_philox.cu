@@ -1096,6 +1096,55 @@ __device__ __forceinline__ void book_sample_gbm_pair(const BookOpt& o, uint64_t 
   book_payoff(o, ob, y.y, x1, cv1);
 }
 
+// book_sample_gbm<BK_TERMINAL, true> of two samples in one packed loop.  The
+// halves are the samples i0 and i1: their Box-Muller pairs in packed pairs,
+// as book_gbm_legs2 without twins.  Their antithetic twins run as a second
+// pair of legs with the negated diffusion.  Each of the four legs is the
+// scalar loop's arithmetic bit for bit, and each sample's two legs are
+// averaged as book_sample_gbm averages them.  Two Philox streams per thread
+// instead of one.
+__device__ __forceinline__ void book_terminal_twin_pair(const BookOpt& o, uint64_t i0, uint64_t i1,
+                                                        const of::PhiloxKeys& K, float& x0, float& cv0, float& x1,
+                                                        float& cv1) {
+  using of::add2;
+  using of::fma2;
+  using of::splat2;
+  const float2 drift = splat2(o.c.drift), dp = splat2(o.c.diff), dm = splat2(-o.c.diff);
+  float2 ya = make_float2(0.0f, 0.0f), yb = make_float2(0.0f, 0.0f);  // (i0, i1) and their twins
+  auto step = [&](float2 z) {
+    ya = fma2(dp, z, add2(ya, drift));
+    yb = fma2(dm, z, add2(yb, drift));
+  };
+  const uint32_t lo0 = (uint32_t)i0, hi0 = (uint32_t)(i0 >> 32), lo1 = (uint32_t)i1, hi1 = (uint32_t)(i1 >> 32);
+  for (int32_t j = 0; j < o.steps; j += 4) {
+    const uint4 r0 = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo0, hi0, o.stream), K);
+    const uint4 r1 = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo1, hi1, o.stream), K);
+    float2 w1, w2, w3, w4;  // wk = step j+k-1 of (i0, i1)
+    of::normal_pairs_scaled2_from_u32(r0.x, r0.y, r1.x, r1.y, of::kBoxMullerK2, w1, w2);
+    of::normal_pairs_scaled2_from_u32(r0.z, r0.w, r1.z, r1.w, of::kBoxMullerK2, w3, w4);
+    if (j + 4 <= o.steps) {
+      step(w1);
+      step(w2);
+      step(w3);
+      step(w4);
+    } else {
+      step(w1);
+      if (j + 1 < o.steps) step(w2);
+      if (j + 2 < o.steps) step(w3);
+    }
+  }
+  const PathObs none{0.0f, 0.0f, 0.0f, false};
+  float xa, ca, xb, cb;
+  book_payoff(o, none, ya.x, xa, ca);
+  book_payoff(o, none, yb.x, xb, cb);
+  x0 = 0.5f * (xa + xb);
+  cv0 = 0.5f * (ca + cb);
+  book_payoff(o, none, ya.y, xa, ca);
+  book_payoff(o, none, yb.y, xb, cb);
+  x1 = 0.5f * (xa + xb);
+  cv1 = 0.5f * (ca + cb);
+}
+
 // One sample of option o: the specialised GBM loop when the option has one,
 // the general loop otherwise.
 __device__ __forceinline__ void book_dispatch(const BookOpt& o, uint64_t i, const BookParams& P, float& x, float& y) {
@@ -1150,9 +1199,10 @@ __global__ void __launch_bounds__(256, 3) book_kernel(const __grid_constant__ Bo
       acc[3].add(x * y);
       acc[4].add(y * y);
     };
-    // specialised GBM kinds without antithetic twins run two samples at a
-    // time in packed pairs; the sums take them in the same order
-    const bool pairs = o.kind != BK_GENERIC && !(o.flags & BF_ANTI);
+    // specialised GBM kinds without antithetic twins, and terminal-only
+    // options with them, run two samples at a time in packed pairs; the sums
+    // take them in the same order
+    const bool pairs = o.kind != BK_GENERIC && (!(o.flags & BF_ANTI) || o.kind == BK_TERMINAL);
     for (int k = 0; k < P.ppt; ++k) {
       const int local = k * blockDim.x + threadIdx.x;
       if (local >= tile.count) break;
@@ -1161,7 +1211,10 @@ __global__ void __launch_bounds__(256, 3) book_kernel(const __grid_constant__ Bo
       if (pairs && k + 1 < P.ppt && local + (int)blockDim.x < tile.count) {
         const uint64_t i1 = i + blockDim.x;
         float x1, y1;
-        if (o.kind == BK_TERMINAL) book_sample_gbm_pair<BK_TERMINAL>(o, i, i1, P.keys, x, y, x1, y1);
+        if (o.kind == BK_TERMINAL) {
+          if (o.flags & BF_ANTI) book_terminal_twin_pair(o, i, i1, P.keys, x, y, x1, y1);
+          else book_sample_gbm_pair<BK_TERMINAL>(o, i, i1, P.keys, x, y, x1, y1);
+        }
         else if (o.kind == BK_BARRIER) book_sample_gbm_pair<BK_BARRIER>(o, i, i1, P.keys, x, y, x1, y1);
         else if (o.kind == BK_ASIAN_DAILY_GEO) book_sample_gbm_pair<BK_ASIAN_DAILY_GEO>(o, i, i1, P.keys, x, y, x1, y1);
         else book_sample_gbm_pair<BK_ASIAN_DAILY>(o, i, i1, P.keys, x, y, x1, y1);
