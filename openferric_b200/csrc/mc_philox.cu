@@ -943,18 +943,87 @@ __device__ __forceinline__ void book_sample(const BookOpt& o, uint64_t i, const 
 }
 
 // The GBM step loop of one sample (and its antithetic twin) for the option
-// kinds BK_TERMINAL, BK_BARRIER and BK_ASIAN_DAILY: the same draws, steps and
-// observations as book_sample<OF_MODEL_GBM, false>, with the option's payoff
-// and flags resolved at compile time instead of tested every step.  Whole
-// Philox counter blocks (four steps) run without a bounds test; the last,
-// partial block follows.
+// kinds BK_BARRIER, BK_ASIAN_DAILY and BK_ASIAN_DAILY_GEO: the same draws,
+// steps and observations as book_sample<OF_MODEL_GBM, false>, bit for bit,
+// with the option's payoff and flags resolved at compile time instead of
+// tested every step.  Whole Philox counter blocks (four steps) run without a
+// bounds test; the last, partial block follows.  BK_TERMINAL options take the
+// sum of their normals instead (book_terminal_sum).
 template <int KIND, bool TWIN>
 __device__ __forceinline__ void book_gbm_legs2(const BookOpt& o, uint64_t i0, uint64_t i1, const of::PhiloxKeys& K,
                                                float2& y, PathObs& oa, PathObs& ob);
 
+// Terminal-only options (BK_TERMINAL) need y_T alone: y_T = steps drift +
+// diff sum z, with the sum of the path's normals taken four steps at a time,
+// ((z0 + z1) + (z2 + z3)), and the last partial block one by one.  The
+// antithetic twin has y_T = steps drift - diff sum z.  The drift is added
+// once instead of every step, so y_T differs from the stepwise sum of the
+// general loop by FP32 rounding only.  The packed-pair forms below sum in the
+// same order, so each of their halves is this scalar sum bit for bit.
+__device__ __forceinline__ float book_terminal_sum(const BookOpt& o, uint64_t i, const of::PhiloxKeys& K) {
+  const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
+  float w = 0.0f;
+  const int32_t full = o.steps & ~3;
+  for (int32_t j = 0; j < full; j += 4) {
+    const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo, hi, o.stream), K);
+    const float2 p01 = of::normal_pair_from_u32(r.x, r.y), p23 = of::normal_pair_from_u32(r.z, r.w);
+    w += (p01.x + p01.y) + (p23.x + p23.y);
+  }
+  if (full < o.steps) {
+    const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(full >> 2), lo, hi, o.stream), K);
+    const float2 p01 = of::normal_pair_from_u32(r.x, r.y), p23 = of::normal_pair_from_u32(r.z, r.w);
+    w += p01.x;
+    if (full + 1 < o.steps) w += p01.y;
+    if (full + 2 < o.steps) w += p23.x;
+  }
+  return w;
+}
+
+// book_terminal_sum of samples i0 and i1 in packed pairs
+__device__ __forceinline__ float2 book_terminal_sums2(const BookOpt& o, uint64_t i0, uint64_t i1,
+                                                      const of::PhiloxKeys& K) {
+  using of::add2;
+  const uint32_t lo0 = (uint32_t)i0, hi0 = (uint32_t)(i0 >> 32), lo1 = (uint32_t)i1, hi1 = (uint32_t)(i1 >> 32);
+  float2 w = make_float2(0.0f, 0.0f);
+  for (int32_t j = 0; j < o.steps; j += 4) {
+    const uint4 r0 = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo0, hi0, o.stream), K);
+    const uint4 r1 = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo1, hi1, o.stream), K);
+    float2 a1, a2, a3, a4;  // ak = step j+k-1 of (i0, i1)
+    of::normal_pairs_scaled2_from_u32(r0.x, r0.y, r1.x, r1.y, of::kBoxMullerK2, a1, a2);
+    of::normal_pairs_scaled2_from_u32(r0.z, r0.w, r1.z, r1.w, of::kBoxMullerK2, a3, a4);
+    if (j + 4 <= o.steps) {
+      w = add2(w, add2(add2(a1, a2), add2(a3, a4)));
+    } else {
+      w = add2(w, a1);
+      if (j + 1 < o.steps) w = add2(w, a2);
+      if (j + 2 < o.steps) w = add2(w, a3);
+    }
+  }
+  return w;
+}
+
+// The payoff of a terminal-only sample from its sum of normals w, averaged
+// with its antithetic twin's (-w) when ANTI.
+template <bool ANTI>
+__device__ __forceinline__ void book_terminal_payoff(const BookOpt& o, float w, float& x, float& cvy) {
+  const PathObs none{0.0f, 0.0f, 0.0f, false};
+  const float base = (float)o.steps * o.c.drift;
+  book_payoff(o, none, fmaf(o.c.diff, w, base), x, cvy);
+  if (ANTI) {
+    float xb, yb;
+    book_payoff(o, none, fmaf(-o.c.diff, w, base), xb, yb);
+    x = 0.5f * (x + xb);
+    cvy = 0.5f * (cvy + yb);
+  }
+}
+
 template <int KIND, bool ANTI>
 __device__ __forceinline__ void book_sample_gbm(const BookOpt& o, uint64_t i, const of::PhiloxKeys& K, float& x,
                                                 float& cvy) {
+  if (KIND == BK_TERMINAL) {
+    book_terminal_payoff<ANTI>(o, book_terminal_sum(o, i, K), x, cvy);
+    return;
+  }
   if (ANTI) {  // the sample and its antithetic twin as the two halves of packed pairs
     float2 y;
     PathObs oa, ob;
@@ -1096,53 +1165,15 @@ __device__ __forceinline__ void book_sample_gbm_pair(const BookOpt& o, uint64_t 
   book_payoff(o, ob, y.y, x1, cv1);
 }
 
-// book_sample_gbm<BK_TERMINAL, true> of two samples in one packed loop.  The
-// halves are the samples i0 and i1: their Box-Muller pairs in packed pairs,
-// as book_gbm_legs2 without twins.  Their antithetic twins run as a second
-// pair of legs with the negated diffusion.  Each of the four legs is the
-// scalar loop's arithmetic bit for bit, and each sample's two legs are
-// averaged as book_sample_gbm averages them.  Two Philox streams per thread
-// instead of one.
-__device__ __forceinline__ void book_terminal_twin_pair(const BookOpt& o, uint64_t i0, uint64_t i1,
-                                                        const of::PhiloxKeys& K, float& x0, float& cv0, float& x1,
-                                                        float& cv1) {
-  using of::add2;
-  using of::fma2;
-  using of::splat2;
-  const float2 drift = splat2(o.c.drift), dp = splat2(o.c.diff), dm = splat2(-o.c.diff);
-  float2 ya = make_float2(0.0f, 0.0f), yb = make_float2(0.0f, 0.0f);  // (i0, i1) and their twins
-  auto step = [&](float2 z) {
-    ya = fma2(dp, z, add2(ya, drift));
-    yb = fma2(dm, z, add2(yb, drift));
-  };
-  const uint32_t lo0 = (uint32_t)i0, hi0 = (uint32_t)(i0 >> 32), lo1 = (uint32_t)i1, hi1 = (uint32_t)(i1 >> 32);
-  for (int32_t j = 0; j < o.steps; j += 4) {
-    const uint4 r0 = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo0, hi0, o.stream), K);
-    const uint4 r1 = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo1, hi1, o.stream), K);
-    float2 w1, w2, w3, w4;  // wk = step j+k-1 of (i0, i1)
-    of::normal_pairs_scaled2_from_u32(r0.x, r0.y, r1.x, r1.y, of::kBoxMullerK2, w1, w2);
-    of::normal_pairs_scaled2_from_u32(r0.z, r0.w, r1.z, r1.w, of::kBoxMullerK2, w3, w4);
-    if (j + 4 <= o.steps) {
-      step(w1);
-      step(w2);
-      step(w3);
-      step(w4);
-    } else {
-      step(w1);
-      if (j + 1 < o.steps) step(w2);
-      if (j + 2 < o.steps) step(w3);
-    }
-  }
-  const PathObs none{0.0f, 0.0f, 0.0f, false};
-  float xa, ca, xb, cb;
-  book_payoff(o, none, ya.x, xa, ca);
-  book_payoff(o, none, yb.x, xb, cb);
-  x0 = 0.5f * (xa + xb);
-  cv0 = 0.5f * (ca + cb);
-  book_payoff(o, none, ya.y, xa, ca);
-  book_payoff(o, none, yb.y, xb, cb);
-  x1 = 0.5f * (xa + xb);
-  cv1 = 0.5f * (ca + cb);
+// book_sample_gbm<BK_TERMINAL, ANTI> of samples i0 and i1: their sums of
+// normals in packed pairs (two Philox streams per thread), then each sample's
+// payoff (and its twin's) as the scalar form takes it.
+template <bool ANTI>
+__device__ __forceinline__ void book_terminal_pair(const BookOpt& o, uint64_t i0, uint64_t i1, const of::PhiloxKeys& K,
+                                                   float& x0, float& cv0, float& x1, float& cv1) {
+  const float2 w = book_terminal_sums2(o, i0, i1, K);
+  book_terminal_payoff<ANTI>(o, w.x, x0, cv0);
+  book_terminal_payoff<ANTI>(o, w.y, x1, cv1);
 }
 
 // One sample of option o: the specialised GBM loop when the option has one,
@@ -1212,8 +1243,8 @@ __global__ void __launch_bounds__(256, 3) book_kernel(const __grid_constant__ Bo
         const uint64_t i1 = i + blockDim.x;
         float x1, y1;
         if (o.kind == BK_TERMINAL) {
-          if (o.flags & BF_ANTI) book_terminal_twin_pair(o, i, i1, P.keys, x, y, x1, y1);
-          else book_sample_gbm_pair<BK_TERMINAL>(o, i, i1, P.keys, x, y, x1, y1);
+          if (o.flags & BF_ANTI) book_terminal_pair<true>(o, i, i1, P.keys, x, y, x1, y1);
+          else book_terminal_pair<false>(o, i, i1, P.keys, x, y, x1, y1);
         }
         else if (o.kind == BK_BARRIER) book_sample_gbm_pair<BK_BARRIER>(o, i, i1, P.keys, x, y, x1, y1);
         else if (o.kind == BK_ASIAN_DAILY_GEO) book_sample_gbm_pair<BK_ASIAN_DAILY_GEO>(o, i, i1, P.keys, x, y, x1, y1);

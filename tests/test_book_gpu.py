@@ -9,6 +9,7 @@ import pytest
 from openferric_b200 import VarianceReduction
 from openferric_b200 import _abi as A
 from openferric_b200.book import BookEntry, BookPlan, price_book, synthetic_book
+from openferric_b200.instruments import VanillaOption
 from openferric_b200.engines import Gbm, GbmPathGenerator, _payoff_abi, instrument_control_variate
 
 pytestmark = pytest.mark.gpu
@@ -101,8 +102,10 @@ def test_specialised_step_loops_match_the_general_loop(vr):
     """Vanilla, daily-fixing Asian and barrier options take step loops
     specialised at compile time.  A 0 % proportional dividend (a jump that
     adds log(1) = 0 to the log-spot) sends the same options through the
-    general loop, which must give the same numbers bit for bit: same draws,
-    same arithmetic."""
+    general loop.  The Asian and barrier loops must give the same numbers
+    bit for bit: same draws, same arithmetic.  The vanilla loop sums the
+    same draws and adds the drift once (y_T = steps drift + diff sum z), so
+    its numbers differ from the stepwise sum by FP32 rounding only."""
     from dataclasses import replace
     from openferric_b200 import Market
     from openferric_b200.market import DividendEvent, DividendSchedule
@@ -117,7 +120,11 @@ def test_specialised_step_loops_match_the_general_loop(vr):
     a = price_book(book, seed=21)
     b = price_book(general, seed=21)
     for e, x, y in zip(book, a, b):
-        assert x.price == y.price and x.stderr == y.stderr, (e.instrument, x.price, y.price)
+        if isinstance(e.instrument, VanillaOption):
+            assert abs(x.price - y.price) <= 1e-5 * abs(y.price) + 1e-6, (e.instrument, x.price, y.price)
+            assert abs(x.stderr - y.stderr) <= 1e-4 * y.stderr + 1e-9, (e.instrument, x.stderr, y.stderr)
+        else:
+            assert x.price == y.price and x.stderr == y.stderr, (e.instrument, x.price, y.price)
 
 
 @pytest.mark.parametrize("mixed_vr", [False, True])
