@@ -205,17 +205,37 @@ __device__ __forceinline__ void gk_terminal(const GreekConsts<R>& c, uint64_t i,
   const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
   R w = (R)0;  // sum of the path's normals
   const int32_t full = c.steps & ~3;
-  for (int32_t j = 0; j < full; j += 4) {
-    R z[4];
-    gk_normals(c, (uint32_t)(j >> 2), lo, hi, K, z);
-    w += (z[0] + z[1]) + (z[2] + z[3]);
-  }
-  if (full < c.steps) {
-    R z[4];
-    gk_normals(c, (uint32_t)(full >> 2), lo, hi, K, z);
-    w += z[0];
-    if (full + 1 < c.steps) w += z[1];
-    if (full + 2 < c.steps) w += z[2];
+  if constexpr (std::is_same<R, float>::value) {
+    // each Box-Muller pair as its sum, sqrt(2) r sin(t + pi/4); a partial
+    // block of one or three steps adds its odd normal from the plain
+    // transform.  The FP64 modes add the pair's two normals: the same draws.
+    for (int32_t j = 0; j < full; j += 4) {
+      const uint4 r = philox4x32_10(make_uint4((uint32_t)(j >> 2), lo, hi, c.stream), K);
+      w += normal_pair_sum_from_u32(r.x, r.y) + normal_pair_sum_from_u32(r.z, r.w);
+    }
+    const int32_t rem = c.steps - full;
+    if (rem > 0) {
+      const uint4 r = philox4x32_10(make_uint4((uint32_t)(full >> 2), lo, hi, c.stream), K);
+      if (rem == 1) {
+        w += normal_pair_from_u32(r.x, r.y).x;
+      } else {
+        w += normal_pair_sum_from_u32(r.x, r.y);
+        if (rem == 3) w += normal_pair_from_u32(r.z, r.w).x;
+      }
+    }
+  } else {
+    for (int32_t j = 0; j < full; j += 4) {
+      R z[4];
+      gk_normals(c, (uint32_t)(j >> 2), lo, hi, K, z);
+      w += (z[0] + z[1]) + (z[2] + z[3]);
+    }
+    if (full < c.steps) {
+      R z[4];
+      gk_normals(c, (uint32_t)(full >> 2), lo, hi, K, z);
+      w += z[0];
+      if (full + 1 < c.steps) w += z[1];
+      if (full + 2 < c.steps) w += z[2];
+    }
   }
   gk_terminal_finish<R, G, ANTI>(c, w, out);
 }
@@ -383,24 +403,34 @@ __device__ __forceinline__ void gk_asian(const GreekConsts<R>& c, uint64_t i, co
 }
 
 // gk_terminal<float, G, ANTI> of samples i0 and i1: the normals' sums in
-// packed pairs (each half bit for bit the scalar sum).
+// packed pairs, in the scalar loop's order (each half bit for bit the scalar
+// sum).
 template <bool G, bool ANTI>
 __device__ __forceinline__ void gk_terminal_pair(const GreekConsts<float>& c, uint64_t i0, uint64_t i1,
                                                  const PhiloxKeys& K, GreekSample<float>& o0, GreekSample<float>& o1) {
   const uint32_t lo0 = (uint32_t)i0, hi0 = (uint32_t)(i0 >> 32), lo1 = (uint32_t)i1, hi1 = (uint32_t)(i1 >> 32);
   float2 w = make_float2(0.0f, 0.0f);
-  for (int32_t j = 0; j < c.steps; j += 4) {
+  const int32_t full = c.steps & ~3;
+  for (int32_t j = 0; j < full; j += 4) {
     const uint4 r0 = philox4x32_10(make_uint4((uint32_t)(j >> 2), lo0, hi0, c.stream), K);
     const uint4 r1 = philox4x32_10(make_uint4((uint32_t)(j >> 2), lo1, hi1, c.stream), K);
-    float2 a1, a2, a3, a4;  // the normals of steps j .. j+3 of (i0, i1)
-    normal_pairs_scaled2_from_u32(r0.x, r0.y, r1.x, r1.y, kBoxMullerK2, a1, a2);
-    normal_pairs_scaled2_from_u32(r0.z, r0.w, r1.z, r1.w, kBoxMullerK2, a3, a4);
-    if (j + 4 <= c.steps) {
-      w = add2(w, add2(add2(a1, a2), add2(a3, a4)));
-    } else {
+    w = add2(w, add2(normal_pair_sums2_from_u32(r0.x, r0.y, r1.x, r1.y),
+                     normal_pair_sums2_from_u32(r0.z, r0.w, r1.z, r1.w)));
+  }
+  const int32_t rem = c.steps - full;
+  if (rem > 0) {
+    const uint4 r0 = philox4x32_10(make_uint4((uint32_t)(full >> 2), lo0, hi0, c.stream), K);
+    const uint4 r1 = philox4x32_10(make_uint4((uint32_t)(full >> 2), lo1, hi1, c.stream), K);
+    float2 a1, a2;
+    if (rem == 1) {
+      normal_pairs_scaled2_from_u32(r0.x, r0.y, r1.x, r1.y, kBoxMullerK2, a1, a2);
       w = add2(w, a1);
-      if (j + 1 < c.steps) w = add2(w, a2);
-      if (j + 2 < c.steps) w = add2(w, a3);
+    } else {
+      w = add2(w, normal_pair_sums2_from_u32(r0.x, r0.y, r1.x, r1.y));
+      if (rem == 3) {
+        normal_pairs_scaled2_from_u32(r0.z, r0.w, r1.z, r1.w, kBoxMullerK2, a1, a2);
+        w = add2(w, a1);
+      }
     }
   }
   gk_terminal_finish<float, G, ANTI>(c, w.x, o0);

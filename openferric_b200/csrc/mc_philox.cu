@@ -954,27 +954,31 @@ __device__ __forceinline__ void book_gbm_legs2(const BookOpt& o, uint64_t i0, ui
                                                float2& y, PathObs& oa, PathObs& ob);
 
 // Terminal-only options (BK_TERMINAL) need y_T alone: y_T = steps drift +
-// diff sum z, with the sum of the path's normals taken four steps at a time,
-// ((z0 + z1) + (z2 + z3)), and the last partial block one by one.  The
-// antithetic twin has y_T = steps drift - diff sum z.  The drift is added
-// once instead of every step, so y_T differs from the stepwise sum of the
-// general loop by FP32 rounding only.  The packed-pair forms below sum in the
-// same order, so each of their halves is this scalar sum bit for bit.
+// diff sum z.  The sum of the path's normals takes each Box-Muller pair as
+// its sum (normal_pair_sum_from_u32), four steps at a time ((z0 + z1) +
+// (z2 + z3)); a last partial block of one or three steps adds its odd normal
+// from the plain transform.  The antithetic twin has y_T = steps drift -
+// diff sum z.  The drift is added once instead of every step, so y_T differs
+// from the stepwise sum of the general loop by FP32 rounding only.  The
+// packed-pair form below sums in the same order, so each of its halves is
+// this scalar sum bit for bit.
 __device__ __forceinline__ float book_terminal_sum(const BookOpt& o, uint64_t i, const of::PhiloxKeys& K) {
   const uint32_t lo = (uint32_t)i, hi = (uint32_t)(i >> 32);
   float w = 0.0f;
   const int32_t full = o.steps & ~3;
   for (int32_t j = 0; j < full; j += 4) {
     const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo, hi, o.stream), K);
-    const float2 p01 = of::normal_pair_from_u32(r.x, r.y), p23 = of::normal_pair_from_u32(r.z, r.w);
-    w += (p01.x + p01.y) + (p23.x + p23.y);
+    w += of::normal_pair_sum_from_u32(r.x, r.y) + of::normal_pair_sum_from_u32(r.z, r.w);
   }
-  if (full < o.steps) {
+  const int32_t rem = o.steps - full;
+  if (rem > 0) {
     const uint4 r = of::philox4x32_10(make_uint4((uint32_t)(full >> 2), lo, hi, o.stream), K);
-    const float2 p01 = of::normal_pair_from_u32(r.x, r.y), p23 = of::normal_pair_from_u32(r.z, r.w);
-    w += p01.x;
-    if (full + 1 < o.steps) w += p01.y;
-    if (full + 2 < o.steps) w += p23.x;
+    if (rem == 1) {
+      w += of::normal_pair_from_u32(r.x, r.y).x;
+    } else {
+      w += of::normal_pair_sum_from_u32(r.x, r.y);
+      if (rem == 3) w += of::normal_pair_from_u32(r.z, r.w).x;
+    }
   }
   return w;
 }
@@ -985,18 +989,27 @@ __device__ __forceinline__ float2 book_terminal_sums2(const BookOpt& o, uint64_t
   using of::add2;
   const uint32_t lo0 = (uint32_t)i0, hi0 = (uint32_t)(i0 >> 32), lo1 = (uint32_t)i1, hi1 = (uint32_t)(i1 >> 32);
   float2 w = make_float2(0.0f, 0.0f);
-  for (int32_t j = 0; j < o.steps; j += 4) {
+  const int32_t full = o.steps & ~3;
+  for (int32_t j = 0; j < full; j += 4) {
     const uint4 r0 = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo0, hi0, o.stream), K);
     const uint4 r1 = of::philox4x32_10(make_uint4((uint32_t)(j >> 2), lo1, hi1, o.stream), K);
-    float2 a1, a2, a3, a4;  // ak = step j+k-1 of (i0, i1)
-    of::normal_pairs_scaled2_from_u32(r0.x, r0.y, r1.x, r1.y, of::kBoxMullerK2, a1, a2);
-    of::normal_pairs_scaled2_from_u32(r0.z, r0.w, r1.z, r1.w, of::kBoxMullerK2, a3, a4);
-    if (j + 4 <= o.steps) {
-      w = add2(w, add2(add2(a1, a2), add2(a3, a4)));
-    } else {
+    w = add2(w, add2(of::normal_pair_sums2_from_u32(r0.x, r0.y, r1.x, r1.y),
+                     of::normal_pair_sums2_from_u32(r0.z, r0.w, r1.z, r1.w)));
+  }
+  const int32_t rem = o.steps - full;
+  if (rem > 0) {
+    const uint4 r0 = of::philox4x32_10(make_uint4((uint32_t)(full >> 2), lo0, hi0, o.stream), K);
+    const uint4 r1 = of::philox4x32_10(make_uint4((uint32_t)(full >> 2), lo1, hi1, o.stream), K);
+    float2 a1, a2;
+    if (rem == 1) {
+      of::normal_pairs_scaled2_from_u32(r0.x, r0.y, r1.x, r1.y, of::kBoxMullerK2, a1, a2);
       w = add2(w, a1);
-      if (j + 1 < o.steps) w = add2(w, a2);
-      if (j + 2 < o.steps) w = add2(w, a3);
+    } else {
+      w = add2(w, of::normal_pair_sums2_from_u32(r0.x, r0.y, r1.x, r1.y));
+      if (rem == 3) {
+        of::normal_pairs_scaled2_from_u32(r0.z, r0.w, r1.z, r1.w, of::kBoxMullerK2, a1, a2);
+        w = add2(w, a1);
+      }
     }
   }
   return w;

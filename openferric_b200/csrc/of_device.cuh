@@ -282,6 +282,34 @@ __device__ __forceinline__ void normal_pairs_scaled2_from_u32(uint32_t a0, uint3
   w2 = mul2(r, make_float2(s0, s1));
 }
 
+// The sum z1 + z2 of normal_pair_from_u32(a, b), r (cos t + sin t), as
+// sqrt(2) r sin(t + pi/4): one sine instead of a sine and a cosine, and one
+// multiply instead of two, for loops that read only the sum of a path's
+// normals.  The same draws as the pair, to FP32 rounding: sqrt(2) goes inside
+// the square root (k2 doubled, exactly) and pi/4 into the angle's constant
+// (-3 pi + pi/4 = -11 pi/4; the angle then spans [-3 pi/4, 5 pi/4)).
+constexpr float kBoxMullerAngSum = -8.63937979737193f;
+
+__device__ __forceinline__ float normal_pair_sum_from_u32(uint32_t a, uint32_t b) {
+  const float u1 = uniform_from_u32(a);
+  const float r = sqrtf((2.0f * kBoxMullerK2) * __log2f(u1));
+  const float ang = fmaf(6.28318530717959f, __uint_as_float(0x3F800000u | (b >> 9)), kBoxMullerAngSum);
+  return r * __sinf(ang);
+}
+
+// normal_pair_sum_from_u32 of two samples' draw pairs (a0, b0) and (a1, b1)
+// in packed pairs; each half is the scalar form bit for bit.
+__device__ __forceinline__ float2 normal_pair_sums2_from_u32(uint32_t a0, uint32_t b0, uint32_t a1, uint32_t b1) {
+  const float2 u1 = sub2(make_float2(__uint_as_float(0x3F800000u | (a0 >> 9)), __uint_as_float(0x3F800000u | (a1 >> 9))),
+                         splat2(0.999999940395355224609375f));
+  const float2 rr = mul2(splat2(2.0f * kBoxMullerK2), make_float2(__log2f(u1.x), __log2f(u1.y)));
+  const float2 r = make_float2(sqrtf(rr.x), sqrtf(rr.y));
+  const float2 ang = fma2(splat2(6.28318530717959f),
+                          make_float2(__uint_as_float(0x3F800000u | (b0 >> 9)), __uint_as_float(0x3F800000u | (b1 >> 9))),
+                          splat2(kBoxMullerAngSum));
+  return mul2(r, make_float2(__sinf(ang.x), __sinf(ang.y)));
+}
+
 // ---------------------------------------------------------------------------
 // Reductions
 // ---------------------------------------------------------------------------
