@@ -439,9 +439,12 @@ BOOK_SEED = 20261203
 def book_mufu_per_step(entry):
     """MUFU operations per path-step of the book's GBM step loops: half a
     Box-Muller pair (lg2, sqrt, sin, cos) per step, plus ex2 for an
-    arithmetic average's fixing."""
-    from openferric_b200.instruments import AsianOption
-    return 3.0 if isinstance(entry.instrument, AsianOption) else 2.0
+    arithmetic average's fixing; a European's loop takes each pair as its
+    sum (lg2, sqrt, sin: 1.5 per step)."""
+    from openferric_b200.instruments import AsianOption, VanillaOption
+    if isinstance(entry.instrument, AsianOption):
+        return 3.0
+    return 1.5 if isinstance(entry.instrument, VanillaOption) else 2.0
 
 
 def leg_book(stream, flush, steps, warmup, peaks, n=4096, greeks=False):

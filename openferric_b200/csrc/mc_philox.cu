@@ -1798,17 +1798,37 @@ static of_status book_plan_create(of_ctx* ctx, const of_book_entry* e, int64_t n
   std::vector<int32_t> begin((size_t)n + 1, 0);
   for (size_t k = 0; k < pend.size(); ++k) begin[(size_t)pend[k].opt + 1]++;
   for (int64_t o = 0; o < n; ++o) begin[(size_t)o + 1] += begin[(size_t)o];
-  std::vector<BookTile> tiles(pend.size());
-  for (size_t k = 0; k < pend.size(); ++k) tiles[k] = {pend[k].opt, pend[k].count, pend[k].first, (int32_t)k, 0};
-  std::vector<size_t> order(pend.size());
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return pend[a].cost > pend[b].cost; });
-  if (pl->mode != OF_BOOK_PRICE)  // Greeks modes: the tiles of each kind group together, longest first within
-    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
-      return of::gk_group(gcs[(size_t)pend[a].opt].kind) < of::gk_group(gcs[(size_t)pend[b].opt].kind);
-    });
-  std::vector<BookTile> sorted(pend.size());
-  for (size_t k = 0; k < order.size(); ++k) sorted[k] = tiles[order[k]];
+  // The schedule: the Greeks modes' kind groups in turn, longest tile first
+  // within a group, ties in slot order (a stable sort of the tiles by group,
+  // then cost descending).  An option's tiles are consecutive slots; all but
+  // its last share one cost, and the last may be shorter.  So the schedule is
+  // built from runs of equal-cost tiles, at most two per option, sorted
+  // stably: the same order as sorting the tiles, at O(n log n + tiles)
+  // instead of O(tiles log tiles) (a million tiles for a book of long-dated
+  // options at 2^25 paths each).
+  struct Run {
+    size_t begin, end;
+    int group;
+    double cost;
+  };
+  std::vector<Run> runs;
+  runs.reserve((size_t)n * 2);
+  for (size_t k = 0; k < pend.size();) {
+    const int32_t o = pend[k].opt;
+    const int group = pl->mode != OF_BOOK_PRICE ? of::gk_group(gcs[(size_t)o].kind) : 0;
+    size_t e = k;
+    while (e < pend.size() && pend[e].opt == o && pend[e].cost == pend[k].cost) ++e;
+    runs.push_back({k, e, group, pend[k].cost});
+    k = e;
+  }
+  std::stable_sort(runs.begin(), runs.end(), [](const Run& a, const Run& b) {
+    return a.group != b.group ? a.group < b.group : a.cost > b.cost;
+  });
+  std::vector<BookTile> sorted;
+  sorted.reserve(pend.size());
+  for (const Run& r : runs)
+    for (size_t k = r.begin; k < r.end; ++k)
+      sorted.push_back({pend[k].opt, pend[k].count, pend[k].first, (int32_t)k, 0});
   pl->n_tiles = (int64_t)sorted.size();
 
   const size_t nt = sorted.size();
