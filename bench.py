@@ -432,7 +432,7 @@ def leg_config1(steps, warmup, peaks, threads):
 # ---------------------------------------------------------------------------
 # Issued thread instructions per path-step of book_kernel on the synthetic
 # mixed book, from the ncu capture of 256 options (profiles/book_kernel_book256.md).
-BOOK_INSTR_PER_STEP = 19.7
+BOOK_INSTR_PER_STEP = 19.0
 BOOK_SEED = 20261203
 
 
