@@ -619,8 +619,10 @@ of_status of_heston_price_adjoint(of_ctx* ctx, const of_heston_adjoint_params* p
  * `cuda_stream` (NULL = the legacy default stream), and returns when the
  * results are on the host.  The first call in a context (per device, and
  * again after cudaDeviceReset) looks up the array's device address
- * (cudaGetSymbolAddress) with that device current: make that first call
- * before any stream capture.  The request is validated exactly as of_mc_strip
+ * (cudaGetSymbolAddress) with that device current.  Every call synchronises
+ * `cuda_stream` and copies through host stack buffers, so it cannot run on a
+ * capturing stream: it returns OF_ERR_UNSUPPORTED there, before issuing any
+ * work.  The request is validated exactly as of_mc_strip
  * validates it (same statuses and messages), then against the limits below.
  * All calls share the array: calls that overlap on the GPU (other streams,
  * other threads) race and must be serialised by the caller.  Every call

@@ -2154,6 +2154,17 @@ extern "C" of_status of_mc_strip_noalloc(void* cuda_stream, const of_model* m, i
     noalloc_msg(err, err_len, "cudaGetDevice failed: %s", cudaGetErrorString(e));
     return OF_ERR_CUDA;
   }
+  // The call synchronises its stream and copies through host stack buffers,
+  // neither of which a stream capture allows: refuse before touching it.
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if ((e = cudaStreamIsCapturing((cudaStream_t)cuda_stream, &capture)) != cudaSuccess) {
+    noalloc_msg(err, err_len, "cudaStreamIsCapturing failed: %s", cudaGetErrorString(e));
+    return OF_ERR_CUDA;
+  }
+  if (capture != cudaStreamCaptureStatusNone) {
+    noalloc_msg(err, err_len, "of_mc_strip_noalloc cannot run on a capturing stream");
+    return OF_ERR_UNSUPPORTED;
+  }
   void* base = nullptr;
   if ((e = noalloc_scratch_addr(&base)) != cudaSuccess) {
     noalloc_msg(err, err_len, "device address of the static scratch: %s", cudaGetErrorString(e));

@@ -23,14 +23,14 @@ pytestmark = pytest.mark.gpu
 STRIKES = [80.0 + 2.0 * k for k in range(21)]
 
 
-def noalloc_strip(model, option_type, strikes, num_paths, seed, df, antithetic=False, tile_ilp=0):
+def noalloc_strip(model, option_type, strikes, num_paths, seed, df, antithetic=False, tile_ilp=0, stream=None):
     L = _lib.load()
     ks = (C.c_double * len(strikes))(*strikes)
     cfg = A.OfMcConfig(num_paths=num_paths, seed=seed, precision=A.OF_PREC_FP32_PHILOX, discount_factor=df,
                        antithetic=int(antithetic), tile_ilp=tile_ilp)
     out = (A.OfMcResult * len(strikes))()
     err = C.create_string_buffer(256)
-    st = L.of_mc_strip_noalloc(None, C.byref(model), option_type, ks, len(strikes), C.byref(cfg), out, err,
+    st = L.of_mc_strip_noalloc(stream, C.byref(model), option_type, ks, len(strikes), C.byref(cfg), out, err,
                                len(err))
     return st, err.value.decode(), [(r.price, r.stderr_) for r in out]
 
@@ -84,3 +84,25 @@ def test_noalloc_strip_rejects_sizes_beyond_its_static_scratch():
     st, msg, _ = noalloc_strip(gen.to_abi(), A.OF_CALL, too_many, 1 << 10, 1, 1.0)
     assert st == A.OF_ERR_INVALID_INPUT
     assert "64" in msg
+
+
+def test_noalloc_strip_refuses_a_capturing_stream():
+    """The entry point synchronises its stream, which a capture forbids: on a
+    capturing stream it returns OF_ERR_UNSUPPORTED before issuing any work,
+    and the capture ends cleanly."""
+    import torch
+    gen = GbmPathGenerator(Gbm(0.03, 0.2), 100.0, 1.0, 16)
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        g.capture_begin()
+        try:
+            st, msg, _ = noalloc_strip(gen.to_abi(), A.OF_CALL, STRIKES, 4096, 3, 1.0,
+                                       stream=C.c_void_p(s.cuda_stream))
+        finally:
+            g.capture_end()
+    assert st == A.OF_ERR_UNSUPPORTED and "capturing" in msg, (st, msg)
+    st, msg, res = noalloc_strip(gen.to_abi(), A.OF_CALL, STRIKES, 4096, 3, 1.0,
+                                 stream=C.c_void_p(s.cuda_stream))
+    assert st == A.OF_OK, msg
+    assert all(math.isfinite(p) for p, _ in res)
