@@ -6,6 +6,8 @@ from __future__ import annotations
 from dataclasses import dataclass
 from typing import List, Sequence, Tuple
 
+import numpy as np
+
 from .core import (AsianSpec, Averaging, BarrierDirection, BarrierSpec, BarrierStyle, ExerciseStyle, OptionType,
                    PricingError, StrikeType)
 
@@ -73,7 +75,8 @@ class AsianOption:
             raise PricingError.InvalidInput("asian strike must be > 0")
         if not self.asian.observation_times:
             raise PricingError.InvalidInput("asian observation_times cannot be empty")
-        if any(t < 0.0 or t > self.expiry for t in self.asian.observation_times):
+        obs = np.asarray(self.asian.observation_times, dtype=np.float64)
+        if np.any((obs < 0.0) | (obs > self.expiry)):  # asian.rs:55-64; NaN compares false there too
             raise PricingError.InvalidInput("asian observation_times must lie in [0, expiry]")
 
 
