@@ -903,9 +903,9 @@ def main():
                                                           tile_ilp_ms={str(k): v for k, v in tune_ms.items()}),
         "roofline": dict(main_line, bound=bound, traffic=STRIP_DRAM_BYTES, traffic_source=STRIP_DRAM_SOURCE,
                          issue=issue_line, **{other_name: other_line},
-                         # the survey's declared count: a single-log inverse normal per draw
-                         # (2 lg2 per step) + sqrt + ex2; Box-Muller issues 5 (lg2, sqrt, sin, cos per
-                         # pair of normals, sqrt of the variance)
+                         # the workload's declared algorithmic count: a single-log inverse normal per
+                         # draw (2 lg2 per step) + sqrt + ex2 = 4 MUFU per path-step; Box-Muller issues
+                         # 5 (lg2, sqrt, sin, cos per pair of normals, sqrt of the variance)
                          frac_at_4_mufu_per_step=per_gpu * 4.0 / sfu_peak),
         "e2e": {"value": world * PATH_STEPS * args.steps / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": 41 * 4, "d2h_bytes_per_step": 41 * 2 * 8},
