@@ -25,3 +25,30 @@ def test_min_sum_in_order_is_bit_identical_to_the_double_loop():
     assert min_sum_in_order(daily) == _double_loop(daily)
     # the sorted O(n log n) form agrees up to summation order
     assert abs(geometric_asian_cov_sum_sorted(daily) - _double_loop(daily)) <= 1e-12 * _double_loop(daily)
+
+
+def test_exact_fma_is_correctly_rounded():
+    """_fma_exact (the reference's f64::mul_add on Pythons without math.fma)
+    against exact rational arithmetic: cancellations, signed zeros,
+    subnormal results and wide exponent ranges."""
+    import math
+    from fractions import Fraction
+
+    from openferric_b200.analytic import _fma_exact
+    rng = random.Random(3)
+
+    def rnd(e):
+        return rng.uniform(-1.0, 1.0) * 10.0 ** rng.randint(-e, e) if e else rng.uniform(-2.0, 2.0)
+
+    checked = 0
+    for _ in range(20000):
+        e = rng.choice([0, 1, 5, 30, 150])
+        a, b = rnd(e), rnd(e)
+        c = rng.choice([-a * b, a * b * (1.0 + 1e-15), rnd(e), 0.0, -0.0, 5e-324, math.ldexp(3.0, -1074)])
+        exact = float(Fraction(a) * Fraction(b) + Fraction(c))
+        got = _fma_exact(a, b, c)
+        assert got == exact and math.copysign(1.0, got) == math.copysign(1.0, exact), (a, b, c, got, exact)
+        checked += 1
+    assert checked == 20000
+    assert _fma_exact(0.1, 10.0, -1.0) == 5.551115123125783e-17  # the product's rounding error, kept
+    assert math.isnan(_fma_exact(math.inf, 0.0, 1.0))
