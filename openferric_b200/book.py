@@ -219,7 +219,7 @@ class StderrRound:
     wall_ms: float = 0.0
 
 
-def paths_for_stderr(paths: int, stderr: float, target: float, margin: float = 1.1, granule: int = 256) -> int:
+def paths_for_stderr(paths: int, stderr: float, target: float, margin: float = 1.05, granule: int = 256) -> int:
     """Paths that bring a standard error measured with `paths` down to
     `target` (stderr scales as paths^-1/2), with a safety margin, rounded up to
     a multiple of `granule`; never fewer than `paths`: the total that
