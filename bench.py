@@ -602,7 +602,10 @@ def fp64_plain_bump_greeks(entry, se_target, seed, bump=1e-4, pilot=8192, max_ro
         base = eng.price(entry.instrument, entry.market)
         if base.stderr <= se_target:
             break
-        paths = paths_for_stderr(paths, base.stderr, se_target)
+        # margin 1.1: this procedure reruns from scratch when it misses the
+        # target (no pooling), and 1.1 measured faster for it than the pooled
+        # driver's 1.05 (5.5 against 5.2 options/s on the 24 options)
+        paths = paths_for_stderr(paths, base.stderr, se_target, margin=1.1)
     greeks = {}
     for name in GREEK_NAMES:
         up, dn = _bumped(entry, name, bump), _bumped(entry, name, -bump)
